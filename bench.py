@@ -1,0 +1,361 @@
+#!/usr/bin/env python
+"""Benchmark of ysim's per-substep cloth hot path on B200.
+
+Workload: the plain TriangularCloth 512x512 self-colliding cloth (262,144
+vertices, 522,242 triangles) over a static displaced level-7 icosphere
+(327,680 triangles), subh = 1/1200, 20 substeps per frame.  A step is one
+substep: swept LBVH refit, broad phase (hash-semantics self rows + BVH rows
+against the obstacle), narrow phase, per-vertex contacts, spring forces and
+integration; every 10th frame also rebuilds the cloth's LBVH (Morton, radix
+sort, Karras), amortised into the timed steps as it comes.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Prints one JSON line (rank 0).  value = substeps/s over all ranks, timed on the
+device with CUDA events on the scene's stream, the L2 flushed (a 256 MiB
+write) between timed substeps and excluded from the timed intervals.  e2e =
+the same metric through the public API with host buffers: every frame uploads
+the external-force buffer from pinned host memory (applyEnvironmentForces'
+output) and reads the positions back into pinned host memory.
+Multi-GPU: replicas only (one independent cloth per rank, no collective on the
+data path); value sums the ranks' substeps over the slowest rank's time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+METRIC = "substeps/s at 262k-vert self-colliding cloth; batched vs plain; adjoint ms/step"
+UNIT = "substeps/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=400)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--preroll", type=int, default=240, help="untimed substeps before warm-up (reach contact)")
+    ap.add_argument("--e2e-frames", type=int, default=10)
+    ap.add_argument("--cpu-substeps", type=int, default=3, help="substeps of the CPU baseline sample")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--seed", type=int, default=2)
+    ap.add_argument("--P", type=int, default=512)
+    return ap.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def spec_for(args):
+    from ysim_b200 import generators as G
+    return G.config_c2(seed=args.seed, P=args.P)
+
+
+def workload_config(args, spec, extra=None):
+    cloth = spec.meshes[0]
+    ob = spec.meshes[1]
+    cfg = {
+        "workload": f"TriangularCloth {args.P}x{args.P} ({cloth.nV} v, {cloth.nF} tris) self-colliding + static "
+                    f"displaced icosphere L7 ({ob.nF} tris); subh 1/1200, 20 substeps/frame; rebuild every 10 frames",
+        "vertices": cloth.nV, "triangles": cloth.nF, "obstacle_triangles": ob.nF,
+        "self_collision": "cpu-spatial-hash semantics (reference default)",
+        "margin": spec.params.margin, "radius": spec.params.radius,
+        "l2": "flushed between timed substeps (256 MiB write), excluded from timing",
+        "seed": args.seed,
+    }
+    if extra:
+        cfg.update(extra)
+    return cfg
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            p = [q.strip() for q in ln.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                smax = float(p[2])
+            except ValueError:
+                continue
+            for nm, val in zip(names, p[5:9]):
+                if val.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ------------------------------------------------------------------ roofline
+def algorithmic_bytes(spec, rows_per_substep: float, contacts_per_substep: float):
+    """Compulsory bytes per substep of the reference dataflow (each buffer
+    element counted once per stage): refit kernel, and the stages the fused
+    kernel covers (query, narrow, bucket, forces, integrate, snapshot)."""
+    cloth, ob = spec.meshes[0], spec.meshes[1]
+    V, M = cloth.nV, cloth.nF
+    P = int(round(V ** 0.5))
+    E = 3 * (P - 1) ** 2 + 2 * (P - 1)
+    E_int = E - 4 * (P - 1)
+    C, K = rows_per_substep, contacts_per_substep
+    nodes = (2 * M - 1) + (2 * ob.nF - 1)
+    refit = M * (8 + 12 + 32) + V * 24 + (2 * M - 1) * 32 * 1.5 + (2 * M - 1) * 8
+    query = V * 12 + nodes * 32 + C * 8
+    narrow = C * 8 + K * 48 + V * 24
+    bucket = K * 48 * 2 + (V + 1) * 4 * 2
+    forces = V * 48 + 2 * E * 4 + E * 12 + 2 * E_int * 8
+    integ = V * (36 + 4 + 4 + 8 + 24) + K * 48
+    snap = V * 24
+    return {"refit": refit, "fused": query + narrow + bucket + forces + integ + snap}
+
+
+def measured_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+# ------------------------------------------------------------------ CPU baseline
+def cpu_baseline(spec, state, nsub, threads=None):
+    """Time the CPU oracle (all host threads) on `nsub` substeps of the same
+    workload, started from the GPU run's state."""
+    from oracle import oracle as O
+    if threads:
+        O.set_threads(threads)
+    cores = O.max_threads()
+    o = O.OracleScene(spec)
+    o.set("x", state["x"]); o.set("v", state["v"]); o.set("xprev", state["xprev"])
+    o.step(1)  # frame-0 preamble rebuild, untimed
+    t0 = time.perf_counter()
+    o.step(nsub)
+    dt = time.perf_counter() - t0
+    return nsub / dt, cores, dt
+
+
+def run_reference(args, rank, world):
+    """Reference arm: the CPU implementation of the path on the host cores."""
+    if rank != 0:
+        return
+    from ysim_b200 import generators as G  # noqa: F401
+    from oracle import oracle as O
+    spec = spec_for(args)
+    o = O.OracleScene(spec)
+    cores = O.max_threads()
+    # drop the cloth onto the obstacle exactly as the GPU arm does (pre-roll is
+    # untimed on both arms), but bounded: a scaled pre-roll keeps the run short
+    pre = min(args.preroll, 4)
+    o.step(max(pre, 1))
+    for _ in range(min(args.warmup, 1)):
+        o.step(1)
+    nsteps = max(1, min(args.steps, args.cpu_substeps))
+    t0 = time.perf_counter()
+    o.step(nsteps)
+    dt = time.perf_counter() - t0
+    v = nsteps / dt
+    kind = "port"
+    line = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world, "steps": nsteps,
+        "warmup": min(args.warmup, 1), "ms_per_step": 1000.0 * dt / nsteps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
+        "config": workload_config(args, spec, {"parallelism": "single process, OpenMP over host cores"}),
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": kind,
+                         "sample": f"{nsteps} substeps of the full workload after a {max(pre, 1)}-substep pre-roll "
+                                   "(bounded sample; the GPU arm times its substeps after a longer pre-roll)"},
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, rank, world, local):
+    import torch
+    import torch.distributed as dist
+    from ysim_b200.scene import Scene
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    spec = spec_for(args)
+    scene = Scene(spec, device=local)
+    lib = scene.lib
+    stream = torch.cuda.ExternalStream(scene.stream(), device=local)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{local}")
+
+    scene.step(args.preroll)
+    scene.step(max(args.warmup, 3))
+    scene.sync()
+    scene.clear_flags()
+    before = scene.totals()
+
+    # ---- device-timed substeps (value)
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    sampler = ClockSampler(local)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    sampler.start()
+    _lib_check = __import__("ysim_b200._lib", fromlist=["check"]).check
+    _lib_check(lib.ys_scene_set_timing(scene.h, 1), "set_timing")
+    for i in range(args.steps):
+        with torch.cuda.stream(stream):
+            flush.fill_(float(i))
+        starts[i].record(stream)
+        scene.step(1)
+        ends[i].record(stream)
+    torch.cuda.synchronize()
+    scene.sync()
+    clocks = sampler.stop()
+    ms = sum(s.elapsed_time(e) for s, e in zip(starts, ends))
+    import ctypes as C
+    kt = (C.c_double * 4)()
+    _lib_check(lib.ys_scene_kernel_times(scene.h, kt), "kernel_times")
+    _lib_check(lib.ys_scene_set_timing(scene.h, 0), "set_timing")
+    after = scene.totals()
+    st = scene.stats()
+    if world > 1:
+        t = torch.tensor([ms], device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = world * args.steps / (ms / 1000.0)
+    rows_ps = (after[0] - before[0]) / args.steps
+    cont_ps = (after[1] - before[1]) / args.steps
+
+    # ---- e2e through the public API with host buffers
+    nsub = spec.params.substeps
+    nV = scene.nV
+    ext = torch.empty((nV, 3), dtype=torch.float32).pin_memory()
+    mass = np.concatenate([m.mass if m.mass is not None else np.zeros(m.nV, np.float32) for m in spec.meshes])
+    cloth_mask = np.concatenate([np.full(m.nV, 1.0 if m.behavior in (0, 1) else 0.0, np.float32)
+                                 for m in spec.meshes])
+    g = np.asarray(spec.params.gravity, np.float32)
+    ext.numpy()[:] = (g[None, :] * (mass * cloth_mask)[:, None]).astype(np.float32)
+    xout = torch.empty((nV, 3), dtype=torch.float32).pin_memory()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(args.e2e_frames):
+        _lib_check(lib.ys_scene_set_external_forces(scene.h, C.c_void_p(ext.data_ptr())), "ext")
+        scene.step(nsub)
+        _lib_check(lib.ys_scene_read_positions_async(scene.h, C.c_void_p(xout.data_ptr())), "read")
+    e1.record(stream)
+    scene.sync()
+    torch.cuda.synchronize()
+    e2e_ms = e0.elapsed_time(e1)
+    if world > 1:
+        t = torch.tensor([e2e_ms], device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e_val = world * args.e2e_frames * nsub / (e2e_ms / 1000.0)
+    assert np.isfinite(xout.numpy()).all()
+
+    # ---- roofline of the dominant kernel
+    ab = algorithmic_bytes(spec, rows_ps, cont_ps)
+    fused_ms = kt[2] / max(kt[3], 1)
+    refit_ms = kt[0] / max(kt[1], 1)
+    peak, peak_kind = measured_peak()
+    ach = ab["fused"] / (fused_ms / 1000.0) / 1e9
+    roof = {"bound": "hbm", "kernel": "k_fused (query+narrow+contacts+forces+integrate)", "achieved": ach,
+            "peak": peak, "peak_source": peak_kind, "unit": "GB/s", "frac": ach / peak, "traffic": None,
+            "algorithmic_bytes": ab["fused"], "avg_launch_ms": fused_ms,
+            "refit_kernel": {"achieved": ab["refit"] / (refit_ms / 1000.0) / 1e9, "algorithmic_bytes": ab["refit"],
+                             "avg_launch_ms": refit_ms}}
+
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        state = {"x": scene.get("x"), "v": scene.get("v"), "xprev": scene.get("xprev")}
+        v_cpu, cores, dt = cpu_baseline(spec, state, args.cpu_substeps)
+        cpu = {"value": v_cpu, "unit": UNIT, "cores": cores, "kind": "port",
+               "sample": f"{args.cpu_substeps} substeps of the full workload from the GPU run's state "
+                         f"({dt:.1f} s, CPU oracle, OpenMP)"}
+
+    launches = int(kt[1] + kt[3])
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": max(args.warmup, 3), "ms_per_step": ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
+            "config": workload_config(args, spec, {"parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                                                   "candidate_rows_per_substep": rows_ps,
+                                                   "contacts_per_substep": cont_ps, "preroll_substeps": args.preroll,
+                                                   "flags": st["flags"]}),
+            "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": nV * 12 / nsub,
+                    "d2h_bytes_per_step": nV * 12 / nsub,
+                    "note": "per frame of 20 substeps: one external-force upload and one position read-back; "
+                            "bytes shown per substep"},
+            "gpu_launches": launches,
+            "roofline": roof,
+            "cpu_baseline": cpu,
+            "clocks": clocks,
+        }
+        print(json.dumps(line), flush=True)
+    scene.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    rank, world, local = dist_env()
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    run_ours(args, rank, world, local)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,206 @@
+/* ysim_b200.h -- C ABI of the B200 (sm_100a) implementation of ysim's
+ * per-substep cloth hot path.
+ *
+ * This is the drop-in boundary for the reference's empty `CUDA` backend slot
+ * (include/sim/core_types.hpp:9).  Plain pointers and sizes only; no CUDA or
+ * torch types appear in a signature (streams are passed as void*).  Every call
+ * returns ys_status (0 = ok, negative = error, see ys_last_error()).  Device
+ * conditions (overflow, non-finite output, iteration caps) are latched in a
+ * per-scene flag word read with ys_scene_stats().
+ *
+ * Threading: one scene = one CUDA stream; a scene is not thread-safe, distinct
+ * scenes may be driven from distinct threads.
+ */
+#ifndef YSIM_B200_H
+#define YSIM_B200_H
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int ys_status;
+#define YS_OK 0
+#define YS_ERR_BAD_ARG (-1)
+#define YS_ERR_CUDA (-2)
+#define YS_ERR_STATE (-3)
+#define YS_ERR_CAPACITY (-4)
+
+/* Device flag bits (ys_scene_stats out[5]); the reference's QueryFlag
+ * (bvh.hpp:396-400) and anomalyFlag (symplectic_system.hpp:184) folded into
+ * one word. */
+#define YS_FLAG_NONFINITE 1u
+#define YS_FLAG_STACK_OVF 2u
+#define YS_FLAG_PAIR_OVF 4u
+#define YS_FLAG_ITER_CAP 8u
+#define YS_FLAG_CONTACT_OVF 16u
+
+/* BehaviorType values (mesh_state.hpp:108-124). */
+#define YS_TRIANGULAR_CLOTH 0u
+#define YS_FAST_GRID_CLOTH 1u
+#define YS_RIGID 3u
+#define YS_FLOAT 4u
+#define YS_KINEMATIC 7u
+
+/* Mesh flags (GeneralMesh::isStatic / collidable / selfCollide, scene.hpp:58). */
+#define YS_MESH_STATIC 1u
+#define YS_MESH_COLLIDABLE 2u
+#define YS_MESH_SELF_COLLIDE 4u
+
+/* Self-collision row source: off, the reference default CPU-spatial-hash
+ * semantics (Simulator::useCpuShSelf, simulator.hpp:93; CpuSpatialHash
+ * spatial_hash.hpp:1946-1989) or BVH self queries (checkSelfCollisions,
+ * bvh.hpp:1842-1848). */
+#define YS_SELF_OFF 0u
+#define YS_SELF_HASH 1u
+#define YS_SELF_BVH 2u
+
+/* Simulator / SymplecticSystem parameters: subh, kair, kd
+ * (symplectic_system.hpp:191-198), gravity (Scene::environment), margin and
+ * radius (simulator.hpp:180-181), substeps per frame, BVH rebuild period in
+ * frames (simulator.hpp:3253), self-collision mode, collision budget per
+ * vertex (approxColsPerPoints, scene.hpp:1139). */
+typedef struct ys_sim_params {
+    float subh, kair, kd;
+    float gravity[3];
+    float margin, radius;
+    uint32_t substeps, rebuild_frames, self_mode, cols_per_point;
+} ys_sim_params;
+
+/* One mesh (GeneralMesh: MeshState + MeshAdjacency + behavior params,
+ * scene.hpp / mesh_state.hpp / collision_pod.hpp:349-396).  Arrays are host
+ * pointers in the reference layout: x, v = 3 floats per vertex; facets = 3
+ * local vertex ids per triangle; mass, mask = one float per vertex.
+ * k* / thickness: ClothBehaviorParams (stretch, shear, bend, thickness) or
+ * FastGridClothBehaviorParams (kstretch, kshear, kbend, thickness) with
+ * grid_n = particleNum1D and grid_rest = stretchRestX/Y, shearRestA/B,
+ * bendRestX/Y.  group: meshes only collide with meshes of the same group
+ * (independent scene instances in one batched scene). */
+typedef struct ys_mesh_desc {
+    uint32_t behavior, flags, num_vertices, num_facets;
+    const float* x;
+    const float* v;
+    const float* mass;
+    const float* mask;
+    const uint32_t* facets;
+    float kstretch, kshear, kbend, thickness;
+    uint32_t grid_n;
+    float grid_rest[6];
+    uint32_t group;
+} ys_mesh_desc;
+
+typedef struct ys_scene ys_scene;
+typedef struct ys_lbvh ys_lbvh;
+
+/* Last error message of the calling thread. */
+const char* ys_last_error(void);
+/* Library version string. */
+const char* ys_version(void);
+
+/* ---- Scene (Scene<CUDA,PR>::pack, scene.hpp:783-1180) ---------------- */
+ys_status ys_scene_create(ys_scene** out, const ys_sim_params* params, int device);
+ys_status ys_scene_destroy(ys_scene* s);
+ys_status ys_scene_add_mesh(ys_scene* s, const ys_mesh_desc* mesh, int* index_out);
+/* Upload, build adjacency (MeshAdjacencyInitializer, mesh_state.hpp:236-411),
+ * build every tree (BroadPhase::build, bvh.hpp:2537-2590). */
+ys_status ys_scene_pack(ys_scene* s);
+
+/* ---- Reference stage surfaces (one call per Simulator::update stage) --- */
+/* Frame preamble: periodic rebuild (simulator.hpp:3253-3261) + environment
+ * forces (applyEnvironmentForces, simulator.hpp:3123-3166); no-op mid-frame. */
+ys_status ys_frame_preamble(ys_scene* s);
+/* BroadPhase::refitSwept (bvh.hpp:2752-2806): swept leaves + bottom-up. */
+ys_status ys_broad_refit(ys_scene* s);
+/* BroadPhase::detectCollisions (bvh.hpp:2853-2949) with the hybrid self pass
+ * (simulator.hpp:3678-3701): writes broad rows. */
+ys_status ys_broad_detect(ys_scene* s);
+/* BruteForce::narrowAndSortByVertices (bruteforce.hpp:311-383). */
+ys_status ys_narrow_and_sort(ys_scene* s);
+/* SymplecticSystem::snapshotXPrev (symplectic_system.hpp:230-250). */
+ys_status ys_snapshot_xprev(ys_scene* s);
+/* SymplecticSystem::update (symplectic_system.hpp:341-409). */
+ys_status ys_system_update(ys_scene* s);
+
+/* ---- Whole substeps ---------------------------------------------------- */
+/* n substeps through the staged kernels above (one launch group per stage). */
+ys_status ys_scene_step_staged(ys_scene* s, uint32_t n);
+/* n substeps through the fused path: refit + one kernel doing detect,
+ * narrow, per-vertex contacts, spring forces and integration (same results
+ * as the staged path). */
+ys_status ys_scene_step(ys_scene* s, uint32_t n);
+/* Record the fused path's per-vertex contacts for inspection (slower). */
+ys_status ys_scene_set_record(ys_scene* s, int record);
+ys_status ys_scene_sync(ys_scene* s);
+/* CUDA stream of the scene (cudaStream_t) as void*. */
+ys_status ys_scene_stream(ys_scene* s, void** stream_out);
+
+/* ---- Inspection --------------------------------------------------------- */
+/* which: 0 x, 1 v, 2 xPrev, 3 f (staged path only); packed 3 floats/vertex. */
+ys_status ys_scene_get_state(ys_scene* s, int which, float* host_out);
+ys_status ys_scene_set_state(ys_scene* s, int which, const float* host_in);
+/* out[0] frame, out[1] substep cursor, out[2] broad rows of the last detect,
+ * out[3] narrow contacts of the last narrow, out[4] anomaly (0/1),
+ * out[5] flag word, out[6] total vertices, out[7] substeps run. */
+ys_status ys_scene_stats(ys_scene* s, uint64_t out[8]);
+ys_status ys_scene_clear_flags(ys_scene* s);
+/* Running totals since pack: out[0] candidate rows, out[1] contacts (fused
+ * path). */
+ys_status ys_scene_totals(ys_scene* s, uint64_t out[2]);
+/* Upload the per-vertex external force buffer (3 floats per vertex) that
+ * Simulator::applyEnvironmentForces fills each frame (simulator.hpp:3123-3166).
+ * Until the first call (or after a call with NULL) the kernels use g * m. */
+ys_status ys_scene_set_external_forces(ys_scene* s, const float* host_ext);
+/* Enqueue a device-to-host copy of the current positions (3 floats per
+ * vertex) on the scene stream; complete after ys_scene_sync.  host_out
+ * should be pinned for an asynchronous copy. */
+ys_status ys_scene_read_positions_async(ys_scene* s, float* host_out);
+/* CUDA-event timing of the fused path's kernels (refit, fused substep). */
+ys_status ys_scene_set_timing(ys_scene* s, int on);
+/* out[0] refit ms total, out[1] refit launches, out[2] fused ms total,
+ * out[3] fused launches, since ys_scene_set_timing(s, 1). */
+ys_status ys_scene_kernel_times(ys_scene* s, double out[4]);
+/* Broad rows of the last staged detect (BroadCollision, 32 B each). */
+ys_status ys_scene_rows(ys_scene* s, void* host_rows, uint64_t cap, uint64_t* n_out);
+/* Per-vertex contacts of the last narrow (staged) or fused step (record on):
+ * offsets (num_vertices + 1) and 24-byte records {tobj, tri, nx, ny, nz, d},
+ * canonical (tobj, tri) order within each vertex. */
+ys_status ys_scene_contacts(ys_scene* s, uint32_t* host_offsets, void* host_contacts, uint64_t cap, uint64_t* n_out);
+/* Tree of one mesh: nodes (2N-1, 32 B BVHNode), parents, sorted codes and
+ * primitive indices (any pointer may be NULL). */
+ys_status ys_scene_tree(ys_scene* s, int mesh, void* nodes, int32_t* parent, uint32_t* codes, uint32_t* idx,
+                        uint32_t* num_prims_out);
+
+/* ---- Standalone LBVH over one triangle soup (BVH<CUDA,PR,LINEAR,TRIANGLE>,
+ * bvh.hpp:141-2308).  Device pointers; x / v packed xyz floats. ---------- */
+ys_status ys_lbvh_create(ys_lbvh** out, uint32_t max_prims, int device, void* stream);
+ys_status ys_lbvh_destroy(ys_lbvh* t);
+/* build(): scene box, Morton, radix sort, Karras, leaves, bottom-up
+ * (bvh.hpp:1194-1301). */
+ys_status ys_lbvh_build(ys_lbvh* t, const float* d_x, uint32_t num_vertices, const uint32_t* d_facets,
+                        uint32_t num_facets);
+/* refit() / refitSwept(dt) (bvh.hpp:1555-1606, 1100-1115). */
+ys_status ys_lbvh_refit(ys_lbvh* t, const float* d_x, const float* d_v, float dt, int swept);
+/* queryPoints (bvh.hpp:1803-1841): (point, triangle) pairs for every query
+ * point whose box [p - margin, p + margin] overlaps a leaf; self = skip
+ * triangles containing the point.  *d_count receives the candidate count
+ * (pairs beyond cap are counted, not written). */
+ys_status ys_lbvh_query(ys_lbvh* t, const float* d_qx, uint32_t num_queries, float margin, int self,
+                        uint32_t* d_pairs, uint64_t cap, unsigned long long* d_count);
+/* Device pointers of the tree arrays (nodes, parents, codes, indices). */
+ys_status ys_lbvh_arrays(ys_lbvh* t, void** nodes, int32_t** parent, uint32_t** codes, uint32_t** idx,
+                         uint32_t* num_prims);
+
+/* Standalone primitives used by the build. */
+ys_status ys_morton_codes(const float* d_x, uint32_t num_vertices, const uint32_t* d_facets, uint32_t num_facets,
+                          uint32_t* d_codes, uint32_t* d_idx, void* stream);
+/* Stable LSD radix sort of (key, value) pairs, 8-bit digits, bits
+ * [0, 32) (RadixSorter<METAL>::sort, spatial_hash.hpp:48-70). d_scratch of
+ * ys_radix_sort_scratch_bytes(n) bytes. */
+size_t ys_radix_sort_scratch_bytes(uint32_t n);
+ys_status ys_radix_sort_pairs(uint32_t* d_keys, uint32_t* d_vals, uint32_t n, void* d_scratch, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* YSIM_B200_H */

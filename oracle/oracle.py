@@ -1,0 +1,255 @@
+"""ctypes wrapper of the CPU oracle (oracle/ys_oracle.cpp).
+
+TEST INFRASTRUCTURE ONLY: loaded by tests/, __graft_entry__.smoke() and the
+CPU-baseline legs of bench.py, never by the product package.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from .build_oracle import OUT, build
+
+NODE_DTYPE = np.dtype([("mn", "<f4", 3), ("a", "<i4"), ("mx", "<f4", 3), ("b", "<i4")])
+ROW_DTYPE = np.dtype([("point", "<u4"), ("tri", "<u4"), ("qobj", "<u4"), ("tobj", "<u4"), ("qbeh", "<u4"),
+                      ("tbeh", "<u4"), ("qshape", "<u4"), ("tshape", "<u4")])
+CONTACT_DTYPE = np.dtype([("point", "<u4"), ("tri", "<u4"), ("qobj", "<u4"), ("tobj", "<u4"), ("n", "<f4", 3),
+                          ("d", "<f4"), ("qbeh", "<u4"), ("tbeh", "<u4"), ("qshape", "<u4"), ("tshape", "<u4")])
+
+_lib = None
+vp = C.c_void_p
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        path = OUT if os.path.exists(OUT) else build()
+        L = C.CDLL(path)
+        sig = {
+            "yso_set_threads": (None, [C.c_int]),
+            "yso_max_threads": (C.c_int, []),
+            "yso_scene_box": (None, [vp, C.c_uint32, vp]),
+            "yso_fill_mortons": (None, [vp, vp, C.c_uint32, vp, vp, vp]),
+            "yso_radix_sort": (None, [vp, vp, C.c_uint32]),
+            "yso_karras": (None, [vp, vp, C.c_uint32, vp, vp]),
+            "yso_leaves": (None, [vp, vp, C.c_float, C.c_int, vp, C.c_uint32, vp]),
+            "yso_bottom_up": (None, [vp, C.c_uint32]),
+            "yso_build_tree": (None, [vp, C.c_uint32, vp, C.c_uint32, vp, vp, vp, vp]),
+            "yso_query_points": (C.c_uint64, [vp, C.c_uint32, vp, vp, C.c_uint32, C.c_float, C.c_int, vp,
+                                              C.c_uint64]),
+            "yso_self_hash": (C.c_uint64, [vp, vp, C.c_uint32, vp, C.c_uint32, C.c_float, vp, C.c_uint64]),
+            "yso_brute_q1": (C.c_uint64, [vp, vp, C.c_uint32, vp, C.c_uint32, C.c_float, C.c_int, vp, C.c_uint64]),
+            "yso_brute_h1": (C.c_uint64, [vp, vp, C.c_uint32, vp, C.c_uint32, C.c_float, vp, C.c_uint64]),
+            "yso_point_tri_sq": (C.c_float, [vp, vp, vp, vp]),
+            "yso_narrow_one": (C.c_int, [vp, vp, vp, vp, vp, C.c_float, vp, vp]),
+            "yso_adj_new": (vp, [vp, C.c_uint32, vp, C.c_uint32]),
+            "yso_adj_size": (C.c_uint64, [vp, C.c_int]),
+            "yso_adj_get": (None, [vp, C.c_int, vp]),
+            "yso_adj_free": (None, [vp]),
+            "yso_scene_new": (vp, [vp, vp]),
+            "yso_scene_free": (None, [vp]),
+            "yso_scene_add_mesh": (C.c_int, [vp, C.c_uint32, C.c_uint32, C.c_uint32, vp, vp, vp, vp, C.c_uint32, vp,
+                                             vp, C.c_uint32, vp]),
+            "yso_scene_pack": (None, [vp]),
+            "yso_scene_step": (None, [vp, C.c_uint32]),
+            "yso_scene_stage": (None, [vp, C.c_int]),
+            "yso_scene_get": (None, [vp, C.c_int, vp]),
+            "yso_scene_set": (None, [vp, C.c_int, vp]),
+            "yso_scene_stats": (None, [vp, vp]),
+            "yso_scene_nrows": (C.c_uint64, [vp]),
+            "yso_scene_rows": (None, [vp, vp]),
+            "yso_scene_ncontacts": (C.c_uint64, [vp]),
+            "yso_scene_contacts": (None, [vp, vp, vp]),
+            "yso_scene_tree_nodes": (C.c_uint64, [vp, C.c_int]),
+            "yso_scene_tree": (None, [vp, C.c_int, vp, vp, vp, vp]),
+        }
+        for k, (r, a) in sig.items():
+            f = getattr(L, k)
+            f.restype = r
+            f.argtypes = a
+        _lib = L
+    return _lib
+
+
+def P(a):
+    return None if a is None else a.ctypes.data_as(vp)
+
+
+def set_threads(n: int):
+    lib().yso_set_threads(n)
+
+
+def max_threads() -> int:
+    return lib().yso_max_threads()
+
+
+def build_tree(x: np.ndarray, F: np.ndarray):
+    x = np.ascontiguousarray(x, np.float32)
+    F = np.ascontiguousarray(F, np.uint32)
+    n = len(F)
+    nodes = np.zeros(2 * n - 1, NODE_DTYPE)
+    parent = np.zeros(2 * n - 1, np.int32)
+    codes = np.zeros(n, np.uint32)
+    idx = np.zeros(n, np.uint32)
+    lib().yso_build_tree(P(x), len(x), P(F), n, P(nodes), P(parent), P(codes), P(idx))
+    return nodes, parent, codes, idx
+
+
+def morton(x, F):
+    x = np.ascontiguousarray(x, np.float32)
+    F = np.ascontiguousarray(F, np.uint32)
+    box = np.zeros(6, np.float32)
+    lib().yso_scene_box(P(x), len(x), P(box))
+    codes = np.zeros(len(F), np.uint32)
+    idx = np.zeros(len(F), np.uint32)
+    lib().yso_fill_mortons(P(x), P(F), len(F), P(box), P(codes), P(idx))
+    return codes, idx
+
+
+def radix_sort(keys, vals):
+    k = np.ascontiguousarray(keys, np.uint32).copy()
+    v = np.ascontiguousarray(vals, np.uint32).copy()
+    lib().yso_radix_sort(P(k), P(v), len(k))
+    return k, v
+
+
+def refit(nodes, x, v, F, dt, swept):
+    nodes = nodes.copy()
+    n = (len(nodes) + 1) // 2
+    x = np.ascontiguousarray(x, np.float32)
+    v = None if v is None else np.ascontiguousarray(v, np.float32)
+    F = np.ascontiguousarray(F, np.uint32)
+    lib().yso_leaves(P(x), P(v), dt, 1 if swept else 0, P(F), n, P(nodes))
+    lib().yso_bottom_up(P(nodes), len(nodes))
+    return nodes
+
+
+def query_points(nodes, F, q, margin, self_query=False, cap=None):
+    q = np.ascontiguousarray(q, np.float32)
+    F = np.ascontiguousarray(F, np.uint32)
+    n = lib().yso_query_points(P(nodes), len(nodes), P(F), P(q), len(q), margin, int(self_query), None, 0)
+    out = np.zeros((n, 2), np.uint32)
+    lib().yso_query_points(P(nodes), len(nodes), P(F), P(q), len(q), margin, int(self_query), P(out), n)
+    return out
+
+
+def brute_q1(x, F, q, margin, self_query=False):
+    x = np.ascontiguousarray(x, np.float32)
+    F = np.ascontiguousarray(F, np.uint32)
+    q = np.ascontiguousarray(q, np.float32)
+    n = lib().yso_brute_q1(P(x), P(F), len(F), P(q), len(q), margin, int(self_query), None, 0)
+    out = np.zeros((n, 2), np.uint32)
+    lib().yso_brute_q1(P(x), P(F), len(F), P(q), len(q), margin, int(self_query), P(out), n)
+    return out
+
+
+def self_hash(x, xp, F, m):
+    x = np.ascontiguousarray(x, np.float32)
+    xp = np.ascontiguousarray(xp, np.float32)
+    F = np.ascontiguousarray(F, np.uint32)
+    n = lib().yso_self_hash(P(x), P(xp), len(x), P(F), len(F), m, None, 0)
+    out = np.zeros((n, 2), np.uint32)
+    lib().yso_self_hash(P(x), P(xp), len(x), P(F), len(F), m, P(out), n)
+    return out
+
+
+def brute_h1(x, xp, F, m):
+    x = np.ascontiguousarray(x, np.float32)
+    xp = np.ascontiguousarray(xp, np.float32)
+    F = np.ascontiguousarray(F, np.uint32)
+    n = lib().yso_brute_h1(P(x), P(xp), len(x), P(F), len(F), m, None, 0)
+    out = np.zeros((n, 2), np.uint32)
+    lib().yso_brute_h1(P(x), P(xp), len(x), P(F), len(F), m, P(out), n)
+    return out
+
+
+def adjacency(x, F):
+    x = np.ascontiguousarray(x, np.float32)
+    F = np.ascontiguousarray(F, np.uint32)
+    h = lib().yso_adj_new(P(x), len(x), P(F), len(F))
+    names = ["vaf_off", "vaf", "edges", "rest_edge", "vae_off", "vae", "opp_off", "opp", "rest_opp"]
+    out = {}
+    for i, nm in enumerate(names):
+        n = lib().yso_adj_size(h, i)
+        a = np.zeros(n, np.float32 if nm.startswith("rest") else np.uint32)
+        lib().yso_adj_get(h, i, P(a))
+        out[nm] = a
+    lib().yso_adj_free(h)
+    return out
+
+
+class OracleScene:
+    """CPU restatement of the packed scene + Simulator::update substeps."""
+
+    def __init__(self, spec):
+        p = spec.params
+        fp = np.array([p.subh, p.kair, p.kd, *p.gravity, p.margin, p.radius], np.float32)
+        ip = np.array([p.substeps, p.rebuild_frames, p.self_mode, p.cols_per_point], np.uint32)
+        self.h = lib().yso_scene_new(P(fp), P(ip))
+        self.spec = spec
+        self._keep = []
+        for m in spec.meshes:
+            x = np.ascontiguousarray(m.x, np.float32)
+            v = np.ascontiguousarray(m.v if m.v is not None else np.zeros_like(x), np.float32)
+            mass = np.ascontiguousarray(m.mass if m.mass is not None else np.ones(m.nV, np.float32), np.float32)
+            mask = np.ascontiguousarray(m.mask if m.mask is not None else np.ones(m.nV, np.float32), np.float32)
+            F = np.ascontiguousarray(m.facets, np.uint32)
+            kp = np.array([m.kstretch, m.kshear, m.kbend, m.thickness], np.float32)
+            rest = np.array(m.grid_rest, np.float32)
+            lib().yso_scene_add_mesh(self.h, m.behavior, m.flags, m.nV, P(x), P(v), P(mass), P(mask), m.nF, P(F),
+                                     P(kp), m.grid_n, P(rest))
+        lib().yso_scene_pack(self.h)
+        self.nV = spec.nV
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().yso_scene_free(self.h)
+            self.h = None
+
+    def step(self, n=1):
+        lib().yso_scene_step(self.h, n)
+
+    def stage(self, which: int):
+        lib().yso_scene_stage(self.h, which)
+
+    def get(self, which: str):
+        code = {"x": 0, "v": 1, "xprev": 2, "f": 3, "ext": 4}[which]
+        out = np.zeros((self.nV, 3), np.float32)
+        lib().yso_scene_get(self.h, code, P(out))
+        return out
+
+    def set(self, which: str, arr):
+        code = {"x": 0, "v": 1, "xprev": 2}[which]
+        a = np.ascontiguousarray(arr, np.float32)
+        lib().yso_scene_set(self.h, code, P(a))
+
+    def stats(self):
+        out = np.zeros(7, np.uint64)
+        lib().yso_scene_stats(self.h, P(out))
+        keys = ("frame", "cursor", "broad_rows", "contacts_kept", "anomaly", "flags", "contacts")
+        return dict(zip(keys, (int(v) for v in out)))
+
+    def rows(self):
+        n = lib().yso_scene_nrows(self.h)
+        out = np.zeros(n, ROW_DTYPE)
+        lib().yso_scene_rows(self.h, P(out))
+        return out
+
+    def contacts(self):
+        n = lib().yso_scene_ncontacts(self.h)
+        off = np.zeros(self.nV + 1, np.uint32)
+        out = np.zeros(n, CONTACT_DTYPE)
+        lib().yso_scene_contacts(self.h, P(off), P(out))
+        return off, out
+
+    def tree(self, mesh: int):
+        nn = lib().yso_scene_tree_nodes(self.h, mesh)
+        nodes = np.zeros(nn, NODE_DTYPE)
+        parent = np.zeros(nn, np.int32)
+        n = (nn + 1) // 2
+        codes = np.zeros(n, np.uint32)
+        idx = np.zeros(n, np.uint32)
+        lib().yso_scene_tree(self.h, mesh, P(nodes), P(parent), P(codes), P(idx))
+        return nodes, parent, codes, idx

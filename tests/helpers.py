@@ -1,0 +1,27 @@
+"""Shared helpers for the parity tests."""
+import numpy as np
+
+
+def canon_pairs(pairs: np.ndarray) -> np.ndarray:
+    """(point, tri) pairs sorted lexicographically."""
+    p = np.asarray(pairs, np.uint32).reshape(-1, 2)
+    if len(p) == 0:
+        return p
+    o = np.lexsort((p[:, 1], p[:, 0]))
+    return p[o]
+
+
+def canon_rows(rows) -> np.ndarray:
+    """Broad rows as a sorted (qobj, point, tobj, tri) uint32 table."""
+    t = np.stack([rows["qobj"], rows["point"], rows["tobj"], rows["tri"]], 1).astype(np.uint32)
+    if len(t) == 0:
+        return t
+    o = np.lexsort((t[:, 3], t[:, 2], t[:, 1], t[:, 0]))
+    return t[o]
+
+
+def rel_err(a, b) -> float:
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    scale = max(np.abs(b).max(), 1e-30)
+    return float(np.abs(a - b).max() / scale) if a.size else 0.0

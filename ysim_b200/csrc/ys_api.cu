@@ -1,0 +1,172 @@
+// ys_api.cu -- C ABI of the standalone LBVH (one triangle soup) and of the
+// build primitives (Morton codes, radix sort).  BVH<CUDA,PR,LINEAR,TRIANGLE>
+// surface: build (bvh.hpp:1194-1301), refit / refitSwept (bvh.hpp:1555-1606,
+// 1100-1115), queryPoints (bvh.hpp:1803-1841).
+#include <string>
+
+#include "ys_collide.cuh"
+#include "ys_common.cuh"
+#include "ys_lbvh.cuh"
+#include "ys_sort.cuh"
+#include "ysim_b200.h"
+
+namespace ys {
+ys_status fail(ys_status code, const std::string& msg);
+
+// queryPoints (bvh.metal:1394-1412): one thread per query point; pairs are
+// (point, triangle), appended with one atomic per lane-batch.
+__global__ void __launch_bounds__(128) k_query_points(const Node* __restrict__ nodes, u32 numNodes,
+                                                      const u32* __restrict__ F, const float* __restrict__ qx, u32 nQ,
+                                                      float m, int self, u32* __restrict__ pairs, u64 cap,
+                                                      unsigned long long* count, u32* status) {
+    const u32 p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= nQ) return;
+    const f3 q = ldp(qx, p);
+    const f3 qmn = q - mk(m, m, m), qmx = q + mk(m, m, m);
+    u32 st = traverse(nodes, numNodes, qmn, qmx, [&](u32 f) {
+        if (self && (F[3 * f] == p || F[3 * f + 1] == p || F[3 * f + 2] == p)) return;
+        unsigned long long i = atomicAdd(count, 1ull);
+        if (i < cap) { pairs[2 * i] = p; pairs[2 * i + 1] = f; }
+    });
+    if (st) atomicOr(status, st);
+}
+
+}  // namespace ys
+
+using namespace ys;
+
+struct ys_lbvh {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    u32 maxPrims = 0, n = 0;
+    Node* nodes = nullptr;
+    i32* parent = nullptr;
+    u32 *codes = nullptr, *idx = nullptr, *visits = nullptr, *box = nullptr, *status = nullptr;
+    void* scratch = nullptr;
+    RefitJob* job = nullptr;
+    const u32* facets = nullptr;
+};
+
+#define YS_CK2(call)                                                                                   \
+    do {                                                                                               \
+        cudaError_t e_ = (call);                                                                       \
+        if (e_ != cudaSuccess) return fail(YS_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+extern "C" {
+
+ys_status ys_lbvh_create(ys_lbvh** out, uint32_t maxPrims, int device, void* stream) {
+    if (!out || maxPrims == 0) return fail(YS_ERR_BAD_ARG, "bad argument");
+    YS_CK2(cudaSetDevice(device));
+    ys_lbvh* t = new ys_lbvh();
+    t->device = device;
+    t->stream = (cudaStream_t)stream;
+    t->maxPrims = maxPrims;
+    size_t nn = 2 * (size_t)maxPrims - 1;
+    cudaError_t e = cudaSuccess;
+    if (e == cudaSuccess) e = cudaMalloc((void**)&t->nodes, nn * sizeof(Node));
+    if (e == cudaSuccess) e = cudaMalloc((void**)&t->parent, nn * 4);
+    if (e == cudaSuccess) e = cudaMalloc((void**)&t->codes, (size_t)maxPrims * 4);
+    if (e == cudaSuccess) e = cudaMalloc((void**)&t->idx, (size_t)maxPrims * 4);
+    if (e == cudaSuccess) e = cudaMalloc((void**)&t->visits, (size_t)maxPrims * 4);
+    if (e == cudaSuccess) e = cudaMalloc((void**)&t->box, 32);
+    if (e == cudaSuccess) e = cudaMalloc((void**)&t->status, 4);
+    if (e == cudaSuccess) e = cudaMalloc(&t->scratch, sort_scratch_bytes(maxPrims));
+    if (e == cudaSuccess) e = cudaMalloc((void**)&t->job, sizeof(RefitJob));
+    if (e == cudaSuccess) e = cudaMemset(t->status, 0, 4);
+    if (e != cudaSuccess) {
+        ys_lbvh_destroy(t);
+        return fail(YS_ERR_CUDA, cudaGetErrorString(e));
+    }
+    *out = t;
+    return YS_OK;
+}
+
+ys_status ys_lbvh_destroy(ys_lbvh* t) {
+    if (!t) return YS_OK;
+    cudaSetDevice(t->device);
+    cudaStreamSynchronize(t->stream);
+    cudaFree(t->nodes); cudaFree(t->parent); cudaFree(t->codes); cudaFree(t->idx); cudaFree(t->visits);
+    cudaFree(t->box); cudaFree(t->status); cudaFree(t->scratch); cudaFree(t->job);
+    delete t;
+    return YS_OK;
+}
+
+static ys_status run_refit(ys_lbvh* t, const float* x, const float* v, float dt, int swept) {
+    RefitJob J;
+    memset(&J, 0, sizeof(J));
+    J.nodes = t->nodes; J.parent = t->parent; J.visits = t->visits; J.facets = t->facets;
+    J.x3 = x; J.v3 = v; J.voff = 0; J.n = t->n; J.leafBase = 0; J.dt = dt; J.swept = swept ? 1u : 0u;
+    J.selfMargin = 0.f; J.maxExt = t->box;
+    YS_CK2(cudaMemcpyAsync(t->job, &J, sizeof(J), cudaMemcpyHostToDevice, t->stream));
+    launch_refit(t->job, 1, t->n, t->status, t->stream);
+    YS_CK2(cudaGetLastError());
+    YS_CK2(cudaStreamSynchronize(t->stream));
+    return YS_OK;
+}
+
+ys_status ys_lbvh_build(ys_lbvh* t, const float* x, uint32_t nV, const uint32_t* F, uint32_t nF) {
+    if (!t || !x || !F || nF == 0 || nV == 0) return fail(YS_ERR_BAD_ARG, "bad argument");
+    if (nF > t->maxPrims) return fail(YS_ERR_CAPACITY, "more primitives than the tree was created for");
+    t->n = nF;
+    t->facets = F;
+    launch_box_init(t->box, t->stream);
+    launch_box(nullptr, x, 0, nV, t->box, t->stream);
+    launch_morton(nullptr, x, 0, F, nF, t->box, t->codes, t->idx, t->stream);
+    YS_CK2(radix_sort_pairs(t->codes, t->idx, nF, t->scratch, 0, 32, t->stream));
+    launch_karras(t->codes, t->idx, nF, t->nodes, t->parent, t->visits, t->stream);
+    YS_CK2(cudaGetLastError());
+    return run_refit(t, x, nullptr, 0.f, 0);
+}
+
+ys_status ys_lbvh_refit(ys_lbvh* t, const float* x, const float* v, float dt, int swept) {
+    if (!t || !x || t->n == 0) return fail(YS_ERR_BAD_ARG, "bad argument / tree not built");
+    if (swept && !v) return fail(YS_ERR_BAD_ARG, "swept refit needs velocities");
+    return run_refit(t, x, v, dt, swept);
+}
+
+ys_status ys_lbvh_query(ys_lbvh* t, const float* qx, uint32_t nQ, float margin, int self, uint32_t* pairs, uint64_t cap,
+                        unsigned long long* count) {
+    if (!t || !qx || !count || t->n == 0) return fail(YS_ERR_BAD_ARG, "bad argument / tree not built");
+    YS_CK2(cudaMemsetAsync(count, 0, 8, t->stream));
+    if (nQ) k_query_points<<<ceil_div(nQ, 128), 128, 0, t->stream>>>(t->nodes, 2 * t->n - 1, t->facets, qx, nQ, margin,
+                                                                      self, pairs, cap, count, t->status);
+    YS_CK2(cudaGetLastError());
+    YS_CK2(cudaStreamSynchronize(t->stream));
+    return YS_OK;
+}
+
+ys_status ys_lbvh_arrays(ys_lbvh* t, void** nodes, int32_t** parent, uint32_t** codes, uint32_t** idx, uint32_t* n) {
+    if (!t) return fail(YS_ERR_BAD_ARG, "null tree");
+    if (nodes) *nodes = t->nodes;
+    if (parent) *parent = t->parent;
+    if (codes) *codes = t->codes;
+    if (idx) *idx = t->idx;
+    if (n) *n = t->n;
+    return YS_OK;
+}
+
+ys_status ys_morton_codes(const float* x, uint32_t nV, const uint32_t* F, uint32_t nF, uint32_t* codes, uint32_t* idx,
+                          void* stream) {
+    if (!x || !F || !codes || !idx || nV == 0) return fail(YS_ERR_BAD_ARG, "bad argument");
+    cudaStream_t s = (cudaStream_t)stream;
+    u32* box = nullptr;
+    YS_CK2(cudaMallocAsync((void**)&box, 32, s));
+    launch_box_init(box, s);
+    launch_box(nullptr, x, 0, nV, box, s);
+    launch_morton(nullptr, x, 0, F, nF, box, codes, idx, s);
+    YS_CK2(cudaFreeAsync(box, s));
+    YS_CK2(cudaStreamSynchronize(s));
+    return YS_OK;
+}
+
+size_t ys_radix_sort_scratch_bytes(uint32_t n) { return sort_scratch_bytes(n); }
+
+ys_status ys_radix_sort_pairs(uint32_t* keys, uint32_t* vals, uint32_t n, void* scratch, void* stream) {
+    if ((!keys || !vals || !scratch) && n > 1) return fail(YS_ERR_BAD_ARG, "bad argument");
+    YS_CK2(radix_sort_pairs(keys, vals, n, scratch, 0, 32, (cudaStream_t)stream));
+    YS_CK2(cudaStreamSynchronize((cudaStream_t)stream));
+    return YS_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,44 @@
+// ys_lbvh.cuh -- linear BVH over triangles: Morton codes, Karras topology,
+// swept refit.  Node layout and slot numbering follow the reference
+// (bvh.hpp:148-177, bvh.metal:260-393): internal nodes [0, N-2] with the root
+// at slot 0, leaves at [N-1, 2N-2].
+#pragma once
+#include "ys_common.cuh"
+
+namespace ys {
+
+// One tree to refit: leaves are recomputed from positions (optionally swept by
+// v*dt) and combined bottom-up.  Positions/velocities are float4 (padded) or
+// packed float3 (reference layout) depending on which pointer is set.
+struct RefitJob {
+    Node* nodes;            // 2N-1 nodes
+    const i32* parent;      // 2N-1 parents (root -1)
+    u32* visits;            // N-1 per-internal-node arrival counters
+    const u32* facets;      // 3 local vertex ids per face (packed)
+    const float4* x4;       // positions (float4) or nullptr
+    const float4* v4;
+    const float* x3;        // positions (packed xyz) or nullptr
+    const float* v3;
+    u32 voff;               // vertex offset of this mesh in x4/v4
+    u32 n;                  // leaves
+    u32 leafBase;           // prefix of leaves over jobs
+    float dt;
+    u32 swept;
+    float selfMargin;       // > 0: also reduce the H1 grid extent into *maxExt
+    u32* maxExt;            // float bits, atomicMax (positive floats order as ints)
+};
+
+// Scene box of a mesh (min/max over all its vertices) into box[6] (float
+// bits stored via ordered-int atomics; call box_init first).
+void launch_box_init(u32* box, cudaStream_t s);
+void launch_box(const float4* x4, const float* x3, u32 voff, u32 nV, u32* box, cudaStream_t s);
+// Morton code per face from the scene box (fillMortons_Tri, bvh.metal:42-63).
+void launch_morton(const float4* x4, const float* x3, u32 voff, const u32* facets, u32 nF, const u32* box, u32* codes,
+                   u32* idx, cudaStream_t s);
+// Karras topology (buildTree_Tri, bvh.metal:352-393); zeroes visit counters.
+void launch_karras(const u32* codes, const u32* idx, u32 n, Node* nodes, i32* parent, u32* visits, cudaStream_t s);
+// Leaves + bottom-up for every job (jobs in device memory, jobsHost mirrors
+// them for the launch size).
+void launch_refit(const RefitJob* jobsDev, u32 numJobs, u32 totalLeaves, u32* status, cudaStream_t s);
+
+}  // namespace ys

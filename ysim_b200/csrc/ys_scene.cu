@@ -1,0 +1,1231 @@
+// ys_scene.cu -- the packed scene, the per-substep kernels and the C ABI.
+//
+// Host side restates Scene<BE,PR>::pack (scene.hpp:783-1180),
+// MeshAdjacencyInitializer (mesh_state.hpp:236-411) and the substep order of
+// Simulator::update (simulator.hpp:3512-3815).  Device side has two paths
+// with identical results:
+//   staged -- one kernel group per reference stage: swept refit, broad rows,
+//             narrow contacts, per-vertex CSR, forces, integrate;
+//   fused  -- swept refit, then ONE kernel per substep in which the thread of
+//             a vertex traverses the trees, runs the narrow test on every
+//             candidate, keeps its contacts in canonical order in local
+//             memory, gathers its spring forces and integrates.  Broad rows,
+//             contacts and forces never touch HBM.
+// xPrev is not copied: positions live in three rotating buffers (current,
+// previous, next), so SymplecticSystem::snapshotXPrev becomes a pointer
+// rotation.
+#include <algorithm>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "ys_collide.cuh"
+#include "ys_common.cuh"
+#include "ys_lbvh.cuh"
+#include "ys_scan.cuh"
+#include "ys_sort.cuh"
+#include "ysim_b200.h"
+
+namespace ys {
+
+thread_local std::string g_err;
+ys_status fail(ys_status code, const std::string& msg) {
+    g_err = msg;
+    return code;
+}
+#define YS_CK(call)                                                                                   \
+    do {                                                                                              \
+        cudaError_t e_ = (call);                                                                      \
+        if (e_ != cudaSuccess) return fail(YS_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+enum : u32 { MF_STATIC = 1, MF_COLLIDABLE = 2, MF_SELF = 4, MF_QUERY = 8, MF_CLOTH = 16, MF_TREE = 32, MF_GRID = 64 };
+static constexpr int MAXC = 32;  // per-vertex contact buffer of the fused kernel
+
+struct MeshDev {
+    u32 voff, nV, foff, nF;
+    u32 node_off, behavior, flags, grid_n;
+    float kstretch, kshear, kbend, thickness;
+    float rest[6];
+    u32 tgt_begin, tgt_end;
+};
+
+struct StepArgs {
+    const float4* x;
+    const float4* xp;
+    const float4* v;
+    float4* xn;
+    float4* vn;
+    const float* mass;
+    const float* mask;
+    const u32* vobj;
+    const MeshDev* meshes;
+    const u32* targets;
+    const uint4* F;
+    const Node* nodes;
+    const u32* spr_off;
+    const u32* spr_split;
+    const u32* spr_nbr;
+    const float* spr_rest;
+    const u32* vaf_off;
+    const u32* vaf;
+    const u32* maxext;
+    const float4* ext;  // external forces (applyEnvironmentForces) or null: g * m
+    float subh, kair, kd, gx, gy, gz, margin, band;
+    u32 nV, self_mode, record, cap;
+    u32* status;
+    unsigned long long* counters;  // [0] broad rows, [1] contacts, [2] pool fill, [3] [4] running totals of 0, 1
+    // fused record pool
+    VContact* pool;
+    u32* vstart;
+    u32* vcount;
+    // staged path
+    Row* rows;
+    Contact* contacts;
+    float4* f;
+    u32* bucket;    // per-vertex counts / fill (V + 1)
+    u32* csr_off;   // V + 1
+    VContact* csr;
+};
+
+// ------------------------------------------------------------------ query
+// BroadPhase::detectCollisions for one query vertex (bvh.hpp:2853-2949 and
+// the hybrid self pass, simulator.hpp:3678-3701): self rows first, then every
+// target mesh whose root box overlaps this mesh's root box.
+template <class Sink>
+__device__ __forceinline__ u32 query_vertex(const StepArgs& A, u32 g, u32 m, const MeshDev& M, f3 xc, f3 xpv,
+                                            Sink&& sink) {
+    u32 st = 0;
+    if (!(M.flags & MF_QUERY) || !(M.flags & MF_TREE)) return 0;
+    const u32 lid = g - M.voff;
+    const float mg = A.margin;
+    if (A.self_mode == YS_SELF_HASH && (M.flags & MF_CLOTH) && (M.flags & MF_SELF)) {
+        float mx = __uint_as_float(A.maxext[m]);
+        float cs = (mx > 1e-5f) ? mx : 1e-5f;
+        float inv = 1.f / cs;
+        H1Vertex h;
+        if (h1_vertex(xc, xpv, inv, h)) {
+            f3 qmn, qmx;
+            h1_query_box(h, mg, qmn, qmx);
+            st |= traverse(A.nodes + M.node_off, 2 * M.nF - 1, qmn, qmx, [&](u32 f) {
+                uint4 tri = A.F[M.foff + f];
+                if (h1_face(A.x, M.voff, tri, lid, mg, inv, h)) sink(m, f, tri, M.voff);
+            });
+        }
+    } else if (A.self_mode == YS_SELF_BVH) {
+        f3 qmn = xc - mk(mg, mg, mg), qmx = xc + mk(mg, mg, mg);
+        st |= traverse(A.nodes + M.node_off, 2 * M.nF - 1, qmn, qmx, [&](u32 f) {
+            uint4 tri = A.F[M.foff + f];
+            if (tri.x == lid || tri.y == lid || tri.z == lid) return;
+            sink(m, f, tri, M.voff);
+        });
+    }
+    for (u32 k = M.tgt_begin; k < M.tgt_end; ++k) {
+        const u32 t = A.targets[k];
+        const u32 tno = A.meshes[t].node_off, tnf = A.meshes[t].nF, tfo = A.meshes[t].foff, tvo = A.meshes[t].voff;
+        if (!root_overlap(A.nodes + M.node_off, A.nodes + tno)) continue;
+        f3 qmn = xc - mk(mg, mg, mg), qmx = xc + mk(mg, mg, mg);
+        st |= traverse(A.nodes + tno, 2 * tnf - 1, qmn, qmx, [&](u32 f) {
+            uint4 tri = A.F[tfo + f];
+            sink(t, f, tri, tvo);
+        });
+    }
+    return st;
+}
+
+__device__ __forceinline__ bool key_less(u32 t1, u32 f1, u32 t2, u32 f2) { return t1 < t2 || (t1 == t2 && f1 < f2); }
+
+// Spring forces of one cloth vertex from the old state:
+// compute_cloth_grid_forces_fast (physics.metal:171-224) or
+// compute_tri_spring_forces (physics.metal:319-378).
+__device__ __forceinline__ f3 vertex_force(const StepArgs& A, const MeshDev& M, u32 g, f3 pos, f3 vel, float mass) {
+    f3 force = (A.ext ? ld(A.ext, g) : mk(A.gx * mass, A.gy * mass, A.gz * mass)) + vel * A.kair;
+    const float kd = A.kd;
+    if (M.flags & MF_GRID) {
+        const int N = (int)M.grid_n;
+        const u32 lid = g - M.voff;
+        const int row = (int)(lid / (u32)N), col = (int)(lid % (u32)N);
+        auto G = [&](int r, int c, float rest, float k) {
+            u32 j = M.voff + (u32)(r * N + c);
+            force = force + spring(pos, vel, ld(A.x, j), ld(A.v, j), rest, k, kd);
+        };
+        if (col > 0) G(row, col - 1, M.rest[0], M.kstretch);
+        if (col < N - 1) G(row, col + 1, M.rest[0], M.kstretch);
+        if (row > 0) G(row - 1, col, M.rest[1], M.kstretch);
+        if (row < N - 1) G(row + 1, col, M.rest[1], M.kstretch);
+        if (col > 0 && row > 0) G(row - 1, col - 1, M.rest[2], M.kshear);
+        if (col < N - 1 && row > 0) G(row - 1, col + 1, M.rest[3], M.kshear);
+        if (col > 0 && row < N - 1) G(row + 1, col - 1, M.rest[3], M.kshear);
+        if (col < N - 1 && row < N - 1) G(row + 1, col + 1, M.rest[2], M.kshear);
+        if (col > 1) G(row, col - 2, M.rest[4], M.kbend);
+        if (col < N - 2) G(row, col + 2, M.rest[4], M.kbend);
+        if (row > 1) G(row - 2, col, M.rest[5], M.kbend);
+        if (row < N - 2) G(row + 2, col, M.rest[5], M.kbend);
+    } else {
+        const u32 b = A.spr_off[g], s = A.spr_split[g], e = A.spr_off[g + 1];
+        for (u32 i = b; i < s; ++i) {
+            u32 j = A.spr_nbr[i];
+            force = force + spring(pos, vel, ld(A.x, j), ld(A.v, j), A.spr_rest[i], M.kstretch, kd);
+        }
+        for (u32 i = s; i < e; ++i) {
+            u32 j = A.spr_nbr[i];
+            force = force + spring(pos, vel, ld(A.x, j), ld(A.v, j), A.spr_rest[i], M.kbend, kd);
+        }
+    }
+    return force;
+}
+
+// Warp-aggregated add of v into ctr[0] and the running total ctr[3].
+__device__ __forceinline__ void warp_count(unsigned long long* ctr, u32 v) {
+    const unsigned act = __activemask();
+    u32 s = __reduce_add_sync(act, v);
+    if ((threadIdx.x & 31) == (unsigned)(__ffs(act) - 1) && s) {
+        atomicAdd(ctr, (unsigned long long)s);
+        atomicAdd(ctr + 3, (unsigned long long)s);
+    }
+}
+
+// ------------------------------------------------------------------ fused
+__global__ void __launch_bounds__(128) k_fused(StepArgs A) {
+    const u32 g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= A.nV) return;
+    const u32 m = A.vobj[g];
+    const MeshDev M = A.meshes[m];
+    const f3 xc = ld(A.x, g);
+    VContact buf[MAXC];
+    int nc = 0;
+    u32 nrows = 0, st = 0;
+    if (M.flags & MF_QUERY) {
+        const f3 xpv = ld(A.xp, g);
+        st |= query_vertex(A, g, m, M, xc, xpv, [&](u32 t, u32 f, uint4 tri, u32 tvoff) {
+            ++nrows;
+            f3 n;
+            float d;
+            if (!narrow_one(xc, xpv, ld(A.x, tvoff + tri.x), ld(A.x, tvoff + tri.y), ld(A.x, tvoff + tri.z), A.band, n,
+                            d))
+                return;
+            if (nc == MAXC) {
+                st |= ST_CONTACT_OVF;
+                if (!key_less(t, f, buf[MAXC - 1].tobj, buf[MAXC - 1].tri)) return;
+                --nc;
+            }
+            int i = nc;
+            while (i > 0 && key_less(t, f, buf[i - 1].tobj, buf[i - 1].tri)) { buf[i] = buf[i - 1]; --i; }
+            buf[i] = VContact{t, f, n.x, n.y, n.z, d};
+            ++nc;
+        });
+    }
+    if (M.flags & MF_CLOTH) {
+        f3 vel = ld(A.v, g);
+        const float mass = A.mass[g], mask = A.mask[g];
+        const f3 force = vertex_force(A, M, g, xc, vel, mass);
+        f3 pos = xc;
+        vel = vel + ((force * A.subh) / mass) * mask;
+        contact_response(pos, vel, nc, M.thickness, [&](int i) { return buf[i]; });
+        pos = pos + (vel * A.subh) * mask;
+        if (sanitize(pos, vel, xc)) st |= ST_NONFINITE;
+        A.xn[g] = make_float4(pos.x, pos.y, pos.z, 0.f);
+        A.vn[g] = make_float4(vel.x, vel.y, vel.z, 0.f);
+    } else if (!(M.flags & MF_STATIC)) {
+        // not integrated (Rigid / Float / Kinematic): carry the state over
+        A.xn[g] = A.x[g];
+        A.vn[g] = A.v[g];
+    }
+    if (A.record) {
+        u32 base = (u32)atomicAdd(&A.counters[2], (unsigned long long)nc);
+        if (base + (u32)nc > A.cap) {
+            st |= ST_PAIR_OVF;
+            A.vstart[g] = 0;
+            A.vcount[g] = 0;
+        } else {
+            for (int i = 0; i < nc; ++i) A.pool[base + i] = buf[i];
+            A.vstart[g] = base;
+            A.vcount[g] = (u32)nc;
+        }
+    }
+    warp_count(&A.counters[0], nrows);
+    warp_count(&A.counters[1], (u32)nc);
+    if (st) atomicOr(A.status, st);
+}
+
+// ------------------------------------------------------------------ staged
+// queryPoints append (bvh.metal:1372-1381) / CPU-hash row append.
+__global__ void __launch_bounds__(128) k_detect_rows(StepArgs A) {
+    const u32 g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= A.nV) return;
+    const u32 m = A.vobj[g];
+    const MeshDev M = A.meshes[m];
+    if (!(M.flags & MF_QUERY)) return;
+    const f3 xc = ld(A.x, g), xpv = ld(A.xp, g);
+    const u32 lid = g - M.voff;
+    u32 st = query_vertex(A, g, m, M, xc, xpv, [&](u32 t, u32 f, uint4, u32) {
+        unsigned long long idx = atomicAdd(&A.counters[0], 1ull);
+        if (idx >= A.cap) { atomicOr(A.status, ST_PAIR_OVF); return; }
+        A.rows[idx] = Row{lid, f, m, t, M.behavior, A.meshes[t].behavior, 0u, 0u};
+    });
+    if (st) atomicOr(A.status, st);
+}
+
+// narrow_pt_tri over the broad rows (bruteforce.metal:41-178).
+__global__ void __launch_bounds__(128) k_narrow_rows(StepArgs A, u32 nrows) {
+    const u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nrows) return;
+    const Row r = A.rows[i];
+    const MeshDev& T = A.meshes[r.tobj];
+    const uint4 tri = A.F[T.foff + r.tri];
+    if (r.qobj == r.tobj) {
+        u32 gp = r.point + T.voff;
+        for (u32 k = A.vaf_off[gp]; k < A.vaf_off[gp + 1]; ++k)
+            if (A.vaf[k] == r.tri) return;
+    }
+    const u32 qo = A.meshes[r.qobj].voff, to = T.voff;
+    f3 n;
+    float d;
+    if (!narrow_one(ld(A.x, r.point + qo), ld(A.xp, r.point + qo), ld(A.x, to + tri.x), ld(A.x, to + tri.y),
+                    ld(A.x, to + tri.z), A.band, n, d))
+        return;
+    unsigned long long o = atomicAdd(&A.counters[1], 1ull);
+    if (o >= A.cap) { atomicOr(A.status, ST_PAIR_OVF); return; }
+    Contact c;
+    c.point = r.point; c.tri = r.tri; c.qobj = r.qobj; c.tobj = r.tobj;
+    c.nx = n.x; c.ny = n.y; c.nz = n.z; c.d = d;
+    c.qbeh = r.qbeh; c.tbeh = r.tbeh; c.qshape = r.qshape; c.tshape = r.tshape;
+    A.contacts[o] = c;
+}
+
+// Per-vertex CSR of the contacts (narrow_bucket_count/scan/scatter,
+// physics.metal:566-616), then canonical (tobj, tri) order per vertex.
+__global__ void k_bucket_count(StepArgs A, u32 nc) {
+    const u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nc) return;
+    const Contact& c = A.contacts[i];
+    atomicAdd(&A.bucket[A.meshes[c.qobj].voff + c.point], 1u);
+}
+__global__ void k_bucket_scatter(StepArgs A, u32 nc) {
+    const u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nc) return;
+    const Contact c = A.contacts[i];
+    const u32 g = A.meshes[c.qobj].voff + c.point;
+    const u32 slot = A.csr_off[g] + atomicAdd(&A.bucket[g], 1u);
+    A.csr[slot] = VContact{c.tobj, c.tri, c.nx, c.ny, c.nz, c.d};
+}
+__global__ void k_bucket_sort(StepArgs A) {
+    const u32 g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= A.nV) return;
+    const u32 b = A.csr_off[g], e = A.csr_off[g + 1];
+    for (u32 i = b + 1; i < e; ++i) {
+        VContact c = A.csr[i];
+        u32 j = i;
+        while (j > b && key_less(c.tobj, c.tri, A.csr[j - 1].tobj, A.csr[j - 1].tri)) { A.csr[j] = A.csr[j - 1]; --j; }
+        A.csr[j] = c;
+    }
+}
+// Pass 1 of SymplecticSystem::update: forces of every cloth vertex.
+__global__ void __launch_bounds__(128) k_forces(StepArgs A) {
+    const u32 g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= A.nV) return;
+    const MeshDev M = A.meshes[A.vobj[g]];
+    if (!(M.flags & MF_CLOTH)) return;
+    f3 f = vertex_force(A, M, g, ld(A.x, g), ld(A.v, g), A.mass[g]);
+    A.f[g] = make_float4(f.x, f.y, f.z, 0.f);
+}
+// Pass 2: integrate_cloth / integrate_cloth_grid (physics.metal:226-312, 380-466).
+__global__ void __launch_bounds__(128) k_integrate(StepArgs A) {
+    const u32 g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= A.nV) return;
+    const MeshDev M = A.meshes[A.vobj[g]];
+    if (!(M.flags & MF_CLOTH)) {
+        if (!(M.flags & MF_STATIC)) { A.xn[g] = A.x[g]; A.vn[g] = A.v[g]; }
+        return;
+    }
+    const f3 xc = ld(A.x, g);
+    f3 vel = ld(A.v, g), pos = xc;
+    const f3 force = ld(A.f, g);
+    const float mass = A.mass[g], mask = A.mask[g];
+    vel = vel + ((force * A.subh) / mass) * mask;
+    const u32 b = A.csr_off[g];
+    contact_response(pos, vel, (int)(A.csr_off[g + 1] - b), M.thickness, [&](int i) { return A.csr[b + i]; });
+    pos = pos + (vel * A.subh) * mask;
+    if (sanitize(pos, vel, xc)) atomicOr(A.status, ST_NONFINITE);
+    A.xn[g] = make_float4(pos.x, pos.y, pos.z, 0.f);
+    A.vn[g] = make_float4(vel.x, vel.y, vel.z, 0.f);
+}
+
+__global__ void k_pack4(const float* __restrict__ in, float4* __restrict__ out, u32 n) {
+    u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = make_float4(in[3 * i], in[3 * i + 1], in[3 * i + 2], 0.f);
+}
+__global__ void k_unpack4(const float4* __restrict__ in, float* __restrict__ out, u32 n) {
+    u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) { float4 q = in[i]; out[3 * i] = q.x; out[3 * i + 1] = q.y; out[3 * i + 2] = q.z; }
+}
+
+// ------------------------------------------------------------------ host
+struct HostMesh {
+    ys_mesh_desc d;
+    std::vector<float> x, v, mass, mask;
+    std::vector<u32> F;
+    u32 voff = 0, foff = 0, node_off = 0, flags = 0;
+    bool built = false;
+    // TriangularCloth springs (mesh-local ids)
+    std::vector<u32> spr_off, spr_split, spr_nbr, vaf_off, vaf;
+    std::vector<float> spr_rest;
+};
+
+template <class T>
+struct DBuf {
+    T* p = nullptr;
+    size_t n = 0;
+    cudaError_t alloc(size_t count) {
+        if (p) { cudaFree(p); p = nullptr; }
+        n = count;
+        if (count == 0) return cudaSuccess;
+        return cudaMalloc((void**)&p, count * sizeof(T));
+    }
+    void free() { if (p) cudaFree(p); p = nullptr; n = 0; }
+};
+
+// MeshAdjacencyInitializer::initialize (mesh_state.hpp:236-411) restricted to
+// what the path consumes: vertexAdjFacets CSR, unique edges with rest
+// lengths, vertexAdjEdges and vertexOppVertices with rest lengths; merged
+// into one per-vertex spring list (stretch entries, then bend entries).
+static void build_adjacency(HostMesh& H) {
+    const u32 nV = H.d.num_vertices, nF = H.d.num_facets;
+    const u32* F = H.F.data();
+    const float* x = H.x.data();
+    H.vaf_off.assign(nV + 1, 0);
+    for (u32 f = 0; f < nF; ++f) for (int k = 0; k < 3; ++k) H.vaf_off[F[3 * f + k] + 1]++;
+    for (u32 v = 0; v < nV; ++v) H.vaf_off[v + 1] += H.vaf_off[v];
+    H.vaf.assign(H.vaf_off[nV], 0);
+    {
+        std::vector<u32> o(nV, 0);
+        for (u32 f = 0; f < nF; ++f)
+            for (int k = 0; k < 3; ++k) { u32 v = F[3 * f + k]; H.vaf[H.vaf_off[v] + o[v]++] = f; }
+    }
+    struct E { u32 v0, v1; i32 o0, o1; };
+    std::vector<E> tmp;
+    tmp.reserve(3 * (size_t)nF);
+    for (u32 f = 0; f < nF; ++f) {
+        u32 a = F[3 * f], b = F[3 * f + 1], c = F[3 * f + 2];
+        u32 tri[3][3] = {{a, b, c}, {b, c, a}, {c, a, b}};
+        for (auto& t : tri) {
+            u32 p = t[0], q = t[1];
+            if (p > q) std::swap(p, q);
+            tmp.push_back(E{p, q, (i32)t[2], -1});
+        }
+    }
+    std::stable_sort(tmp.begin(), tmp.end(), [](const E& p, const E& q) { return p.v0 < q.v0 || (p.v0 == q.v0 && p.v1 < q.v1); });
+    std::vector<E> edges;
+    for (const E& e : tmp) {
+        if (edges.empty() || edges.back().v0 != e.v0 || edges.back().v1 != e.v1) edges.push_back(e);
+        else edges.back().o1 = e.o0;
+    }
+    auto len = [&](u32 a, u32 b) {
+        float dx = x[3 * b] - x[3 * a], dy = x[3 * b + 1] - x[3 * a + 1], dz = x[3 * b + 2] - x[3 * a + 2];
+        return sqrtf(dx * dx + dy * dy + dz * dz);
+    };
+    std::vector<u32> ne(nV, 0), no(nV, 0);
+    for (const E& e : edges) {
+        ne[e.v0]++; ne[e.v1]++;
+        if (e.o1 != -1) { no[(u32)e.o0]++; no[(u32)e.o1]++; }
+    }
+    H.spr_off.assign(nV + 1, 0);
+    H.spr_split.assign(nV, 0);
+    for (u32 v = 0; v < nV; ++v) H.spr_off[v + 1] = H.spr_off[v] + ne[v] + no[v];
+    for (u32 v = 0; v < nV; ++v) H.spr_split[v] = H.spr_off[v] + ne[v];
+    H.spr_nbr.assign(H.spr_off[nV], 0);
+    H.spr_rest.assign(H.spr_off[nV], 0.f);
+    std::vector<u32> fe(nV, 0), fo(nV, 0);
+    for (const E& e : edges) {
+        // vertexOppVertices entries (bend), in edge order
+        if (e.o1 != -1) {
+            u32 o0 = (u32)e.o0, o1 = (u32)e.o1;
+            float r = len(o0, o1);
+            u32 s0 = H.spr_split[o0] + fo[o0]++, s1 = H.spr_split[o1] + fo[o1]++;
+            H.spr_nbr[s0] = o1; H.spr_rest[s0] = r;
+            H.spr_nbr[s1] = o0; H.spr_rest[s1] = r;
+        }
+        // vertexAdjEdges entries (stretch), in edge order
+        float r = len(e.v0, e.v1);
+        u32 a = H.spr_off[e.v0] + fe[e.v0]++, b = H.spr_off[e.v1] + fe[e.v1]++;
+        H.spr_nbr[a] = e.v1; H.spr_rest[a] = r;
+        H.spr_nbr[b] = e.v0; H.spr_rest[b] = r;
+    }
+}
+
+}  // namespace ys
+
+using namespace ys;
+
+struct ys_scene {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    ys_sim_params P{};
+    std::vector<HostMesh> meshes;
+    bool packed = false;
+    u32 nV = 0, nF = 0, nNodes = 0;
+    // device state
+    DBuf<float4> X[3], V[2], Fbuf;
+    int cur = 0, prev = 1, cv = 0;
+    bool snapshot_pending = false;
+    DBuf<float> mass, mask;
+    DBuf<u32> vobj, targets, spr_off, spr_split, spr_nbr, vaf_off, vaf, maxext, status, codes, idx, visits, box;
+    DBuf<float> spr_rest, scratch3;
+    DBuf<uint4> F4;
+    DBuf<u32> F3;  // packed facets (3 per face) for the refit kernel
+    DBuf<Node> nodes;
+    DBuf<i32> parent;
+    DBuf<MeshDev> dmeshes;
+    DBuf<RefitJob> jobs;            // 6 tables (cur x cv) of njobs, then one build slot
+    std::vector<RefitJob> hjobs;
+    u32 njobs = 0;
+    u32 refitLeaves = 0;
+    DBuf<unsigned long long> counters;
+    DBuf<float4> ext;
+    bool use_ext = false;
+    // per-kernel CUDA-event timing of the fused path
+    bool timing = false;
+    std::vector<cudaEvent_t> evPool;
+    size_t evUsed = 0;
+    std::vector<size_t> evRefit, evFused;  // indices of (begin, end) event pairs
+    DBuf<char> sortScratch, scanScratch;
+    // staged / record buffers
+    u32 cap = 0;
+    DBuf<Row> rows;
+    DBuf<Contact> contacts;
+    DBuf<VContact> csr, pool;
+    DBuf<u32> bucket, csr_off, vstart, vcount;
+    bool staged_ready = false, record = false, record_ready = false;
+    int last_contacts = 0;  // 0 none, 1 staged csr, 2 fused pool
+    // progress
+    uint64_t frame = 0, substeps_run = 0;
+    u32 cursor = 0;
+    uint64_t last_rows = 0, last_contacts_n = 0;
+};
+
+namespace {
+
+ys_status check_scene(ys_scene* s) {
+    if (!s) return fail(YS_ERR_BAD_ARG, "null scene");
+    if (!s->packed) return fail(YS_ERR_STATE, "scene not packed");
+    return YS_OK;
+}
+
+StepArgs make_args(ys_scene* s) {
+    StepArgs A;
+    memset(&A, 0, sizeof(A));
+    const int nxt = 3 - s->cur - s->prev;
+    A.x = s->X[s->cur].p;
+    A.xp = s->X[s->prev].p;
+    A.xn = s->X[nxt].p;
+    A.v = s->V[s->cv].p;
+    A.vn = s->V[1 - s->cv].p;
+    A.mass = s->mass.p;
+    A.mask = s->mask.p;
+    A.vobj = s->vobj.p;
+    A.meshes = s->dmeshes.p;
+    A.targets = s->targets.p;
+    A.F = s->F4.p;
+    A.nodes = s->nodes.p;
+    A.spr_off = s->spr_off.p;
+    A.spr_split = s->spr_split.p;
+    A.spr_nbr = s->spr_nbr.p;
+    A.spr_rest = s->spr_rest.p;
+    A.vaf_off = s->vaf_off.p;
+    A.vaf = s->vaf.p;
+    A.maxext = s->maxext.p;
+    A.ext = s->use_ext ? s->ext.p : nullptr;
+    A.subh = s->P.subh; A.kair = s->P.kair; A.kd = s->P.kd;
+    A.gx = s->P.gravity[0]; A.gy = s->P.gravity[1]; A.gz = s->P.gravity[2];
+    A.margin = s->P.margin;
+    A.band = s->P.radius + s->P.margin;
+    A.nV = s->nV;
+    A.self_mode = s->P.self_mode;
+    A.record = s->record ? 1u : 0u;
+    A.cap = s->cap;
+    A.status = s->status.p;
+    A.counters = s->counters.p;
+    A.pool = s->pool.p; A.vstart = s->vstart.p; A.vcount = s->vcount.p;
+    A.rows = s->rows.p; A.contacts = s->contacts.p; A.f = s->Fbuf.p;
+    A.bucket = s->bucket.p; A.csr_off = s->csr_off.p; A.csr = s->csr.p;
+    return A;
+}
+
+// Rotate the position / velocity buffers after an integrate:
+// prev <- cur when xPrev was snapshotted, cur <- next.
+void rotate(ys_scene* s) {
+    const int nxt = 3 - s->cur - s->prev;
+    if (s->snapshot_pending) s->prev = s->cur;
+    s->cur = nxt;
+    if (s->prev == s->cur) s->prev = 3 - s->cur - nxt;  // unreachable guard
+    s->cv = 1 - s->cv;
+    s->snapshot_pending = false;
+    s->substeps_run++;
+    if (++s->cursor >= s->P.substeps) { s->cursor = 0; s->frame++; }
+}
+
+// BVH<..,LINEAR,TRIANGLE>::build for one mesh on the current positions.
+ys_status build_tree(ys_scene* s, HostMesh& H) {
+    const u32 n = H.d.num_facets;
+    if (n == 0) return YS_OK;
+    cudaStream_t st = s->stream;
+    u32* codes = s->codes.p + H.foff;
+    u32* idx = s->idx.p + H.foff;
+    launch_box_init(s->box.p, st);
+    launch_box(s->X[s->cur].p, nullptr, H.voff, H.d.num_vertices, s->box.p, st);
+    launch_morton(s->X[s->cur].p, nullptr, H.voff, s->F3.p + 3 * (size_t)H.foff, n, s->box.p, codes, idx, st);
+    YS_CK(radix_sort_pairs(codes, idx, n, s->sortScratch.p, 0, 32, st));
+    launch_karras(codes, idx, n, s->nodes.p + H.node_off, s->parent.p + H.node_off, s->visits.p + H.foff, st);
+    RefitJob J;
+    memset(&J, 0, sizeof(J));
+    J.nodes = s->nodes.p + H.node_off;
+    J.parent = s->parent.p + H.node_off;
+    J.visits = s->visits.p + H.foff;
+    J.facets = s->F3.p + 3 * (size_t)H.foff;
+    J.x4 = s->X[s->cur].p;
+    J.voff = H.voff;
+    J.n = n;
+    J.leafBase = 0;
+    J.swept = 0;
+    J.selfMargin = 0.f;
+    J.maxExt = s->maxext.p;  // unused (selfMargin == 0)
+    RefitJob* slot = s->jobs.p + 6 * (size_t)s->njobs;
+    YS_CK(cudaMemcpyAsync(slot, &J, sizeof(J), cudaMemcpyHostToDevice, st));
+    launch_refit(slot, 1, n, s->status.p, st);
+    YS_CK(cudaStreamSynchronize(st));  // J lives on the host stack
+    H.built = true;
+    return YS_OK;
+}
+
+ys_status preamble(ys_scene* s) {
+    if (s->cursor != 0) return YS_OK;
+    if (s->P.rebuild_frames && s->frame % s->P.rebuild_frames == 0) {
+        for (auto& H : s->meshes) {
+            if (H.built && H.d.behavior == YS_FLOAT) continue;
+            ys_status r = build_tree(s, H);
+            if (r) return r;
+        }
+    }
+    // environment forces (ext = g * m) are evaluated inside the force kernels
+    return YS_OK;
+}
+
+ys_status refit(ys_scene* s) {
+    if (s->njobs == 0) return YS_OK;
+    // the job table for the current (position, velocity) buffer pair
+    const RefitJob* table = s->jobs.p + (size_t)(s->cur * 2 + s->cv) * s->njobs;
+    YS_CK(cudaMemsetAsync(s->maxext.p, 0, s->maxext.n * 4, s->stream));
+    launch_refit(table, s->njobs, s->refitLeaves, s->status.p, s->stream);
+    return YS_OK;
+}
+
+ys_status ensure_staged(ys_scene* s) {
+    if (s->staged_ready) return YS_OK;
+    YS_CK(s->rows.alloc(s->cap));
+    YS_CK(s->contacts.alloc(s->cap));
+    YS_CK(s->csr.alloc(s->cap));
+    YS_CK(s->bucket.alloc(s->nV + 1));
+    YS_CK(s->csr_off.alloc(s->nV + 1));
+    YS_CK(s->Fbuf.alloc(s->nV));
+    YS_CK(cudaMemset(s->Fbuf.p, 0, s->nV * sizeof(float4)));
+    YS_CK(s->scanScratch.alloc(scan_scratch_bytes(s->nV + 1)));
+    s->staged_ready = true;
+    return YS_OK;
+}
+
+ys_status ensure_record(ys_scene* s) {
+    if (s->record_ready) return YS_OK;
+    YS_CK(s->pool.alloc(s->cap));
+    YS_CK(s->vstart.alloc(s->nV));
+    YS_CK(s->vcount.alloc(s->nV));
+    YS_CK(cudaMemset(s->vcount.p, 0, s->nV * 4));
+    YS_CK(cudaMemset(s->vstart.p, 0, s->nV * 4));
+    s->record_ready = true;
+    return YS_OK;
+}
+
+ys_status detect(ys_scene* s) {
+    ys_status r = ensure_staged(s);
+    if (r) return r;
+    YS_CK(cudaMemsetAsync(s->counters.p, 0, 8, s->stream));
+    StepArgs A = make_args(s);
+    k_detect_rows<<<ceil_div(s->nV, 128), 128, 0, s->stream>>>(A);
+    YS_CK(cudaGetLastError());
+    return YS_OK;
+}
+
+ys_status narrow_and_sort(ys_scene* s) {
+    ys_status r = ensure_staged(s);
+    if (r) return r;
+    unsigned long long cnt[2];
+    YS_CK(cudaMemcpyAsync(cnt, s->counters.p, 16, cudaMemcpyDeviceToHost, s->stream));
+    YS_CK(cudaStreamSynchronize(s->stream));
+    u32 nrows = (u32)std::min<unsigned long long>(cnt[0], s->cap);
+    s->last_rows = cnt[0];
+    YS_CK(cudaMemsetAsync(s->counters.p + 1, 0, 8, s->stream));
+    StepArgs A = make_args(s);
+    if (nrows) k_narrow_rows<<<ceil_div(nrows, 128), 128, 0, s->stream>>>(A, nrows);
+    YS_CK(cudaMemcpyAsync(cnt, s->counters.p, 16, cudaMemcpyDeviceToHost, s->stream));
+    YS_CK(cudaStreamSynchronize(s->stream));
+    u32 nc = (u32)std::min<unsigned long long>(cnt[1], s->cap);
+    s->last_contacts_n = cnt[1];
+    YS_CK(cudaMemsetAsync(s->bucket.p, 0, (s->nV + 1) * 4, s->stream));
+    if (nc) k_bucket_count<<<ceil_div(nc, 256), 256, 0, s->stream>>>(A, nc);
+    YS_CK(cudaMemcpyAsync(s->csr_off.p, s->bucket.p, (s->nV + 1) * 4, cudaMemcpyDeviceToDevice, s->stream));
+    YS_CK(exclusive_scan(s->csr_off.p, s->nV + 1, s->scanScratch.p, s->stream));
+    YS_CK(cudaMemsetAsync(s->bucket.p, 0, (s->nV + 1) * 4, s->stream));
+    if (nc) k_bucket_scatter<<<ceil_div(nc, 256), 256, 0, s->stream>>>(A, nc);
+    k_bucket_sort<<<ceil_div(s->nV, 256), 256, 0, s->stream>>>(A);
+    YS_CK(cudaGetLastError());
+    s->last_contacts = 1;
+    return YS_OK;
+}
+
+ys_status system_update(ys_scene* s) {
+    ys_status r = ensure_staged(s);
+    if (r) return r;
+    StepArgs A = make_args(s);
+    k_forces<<<ceil_div(s->nV, 128), 128, 0, s->stream>>>(A);
+    k_integrate<<<ceil_div(s->nV, 128), 128, 0, s->stream>>>(A);
+    YS_CK(cudaGetLastError());
+    // non-cloth vertices are never written: keep every buffer equal for them
+    rotate(s);
+    return YS_OK;
+}
+
+cudaEvent_t next_event(ys_scene* s) {
+    if (s->evUsed == s->evPool.size()) {
+        cudaEvent_t e;
+        if (cudaEventCreate(&e) != cudaSuccess) return nullptr;
+        s->evPool.push_back(e);
+    }
+    return s->evPool[s->evUsed++];
+}
+
+ys_status fused_substep(ys_scene* s) {
+    ys_status r = preamble(s);
+    if (r) return r;
+    if (s->timing) {
+        s->evRefit.push_back(s->evUsed);
+        YS_CK(cudaEventRecord(next_event(s), s->stream));
+    }
+    r = refit(s);
+    if (r) return r;
+    if (s->timing) {
+        YS_CK(cudaEventRecord(next_event(s), s->stream));
+    }
+    if (s->record) {
+        r = ensure_record(s);
+        if (r) return r;
+        YS_CK(cudaMemsetAsync(s->counters.p, 0, 24, s->stream));
+    } else {
+        // counters [0] [1] only; [3] [4] keep running totals
+        YS_CK(cudaMemsetAsync(s->counters.p, 0, 16, s->stream));
+    }
+    StepArgs A = make_args(s);
+    if (s->timing) {
+        s->evFused.push_back(s->evUsed);
+        YS_CK(cudaEventRecord(next_event(s), s->stream));
+    }
+    k_fused<<<ceil_div(s->nV, 128), 128, 0, s->stream>>>(A);
+    YS_CK(cudaGetLastError());
+    if (s->timing) YS_CK(cudaEventRecord(next_event(s), s->stream));
+    s->snapshot_pending = true;
+    rotate(s);
+    if (s->record) s->last_contacts = 2;
+    return YS_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* ys_last_error(void) { return g_err.c_str(); }
+const char* ys_version(void) { return "ysim_b200 0.1 (sm_100a)"; }
+
+ys_status ys_scene_create(ys_scene** out, const ys_sim_params* p, int device) {
+    if (!out || !p) return fail(YS_ERR_BAD_ARG, "null argument");
+    if (p->substeps == 0) return fail(YS_ERR_BAD_ARG, "substeps must be > 0");
+    if (p->self_mode > YS_SELF_BVH) return fail(YS_ERR_BAD_ARG, "bad self_mode");
+    YS_CK(cudaSetDevice(device));
+    ys_scene* s = new ys_scene();
+    s->device = device;
+    s->P = *p;
+    if (s->P.cols_per_point == 0) s->P.cols_per_point = 15;
+    cudaError_t e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) { delete s; return fail(YS_ERR_CUDA, cudaGetErrorString(e)); }
+    *out = s;
+    return YS_OK;
+}
+
+ys_status ys_scene_destroy(ys_scene* s) {
+    if (!s) return YS_OK;
+    cudaSetDevice(s->device);
+    cudaStreamSynchronize(s->stream);
+    for (auto& b : s->X) b.free();
+    for (auto& b : s->V) b.free();
+    s->Fbuf.free(); s->mass.free(); s->mask.free(); s->vobj.free(); s->targets.free(); s->spr_off.free();
+    s->spr_split.free(); s->spr_nbr.free(); s->vaf_off.free(); s->vaf.free(); s->maxext.free(); s->status.free();
+    s->codes.free(); s->idx.free(); s->visits.free(); s->box.free(); s->spr_rest.free(); s->scratch3.free(); s->F4.free(); s->F3.free();
+    s->nodes.free(); s->parent.free(); s->dmeshes.free(); s->jobs.free(); s->counters.free(); s->sortScratch.free();
+    s->scanScratch.free(); s->rows.free(); s->contacts.free(); s->csr.free(); s->pool.free(); s->bucket.free();
+    s->csr_off.free(); s->vstart.free(); s->vcount.free(); s->ext.free();
+    for (auto e : s->evPool) cudaEventDestroy(e);
+    cudaStreamDestroy(s->stream);
+    delete s;
+    return YS_OK;
+}
+
+ys_status ys_scene_add_mesh(ys_scene* s, const ys_mesh_desc* d, int* index_out) {
+    if (!s || !d) return fail(YS_ERR_BAD_ARG, "null argument");
+    if (s->packed) return fail(YS_ERR_STATE, "scene already packed");
+    if (d->num_vertices == 0 || !d->x) return fail(YS_ERR_BAD_ARG, "mesh needs vertices");
+    if (d->num_facets && !d->facets) return fail(YS_ERR_BAD_ARG, "facets missing");
+    const bool cloth = d->behavior == YS_TRIANGULAR_CLOTH || d->behavior == YS_FAST_GRID_CLOTH;
+    if (cloth && (!d->mass || !d->mask)) return fail(YS_ERR_BAD_ARG, "cloth needs mass and mask");
+    if (d->behavior == YS_FAST_GRID_CLOTH && (d->grid_n < 3 || d->grid_n * d->grid_n != d->num_vertices))
+        return fail(YS_ERR_BAD_ARG, "FastGridCloth needs grid_n^2 vertices, grid_n >= 3");
+    for (u32 i = 0; i < 3 * d->num_facets; ++i)
+        if (d->facets[i] >= d->num_vertices) return fail(YS_ERR_BAD_ARG, "facet index out of range");
+    HostMesh H;
+    H.d = *d;
+    const u32 nV = d->num_vertices;
+    H.x.assign(d->x, d->x + 3 * (size_t)nV);
+    if (d->v) H.v.assign(d->v, d->v + 3 * (size_t)nV); else H.v.assign(3 * (size_t)nV, 0.f);
+    if (d->mass) H.mass.assign(d->mass, d->mass + nV); else H.mass.assign(nV, 1.f);
+    if (d->mask) H.mask.assign(d->mask, d->mask + nV); else H.mask.assign(nV, 1.f);
+    H.F.assign(d->facets, d->facets + 3 * (size_t)d->num_facets);
+    H.d.x = H.d.v = H.d.mass = H.d.mask = nullptr;
+    H.d.facets = nullptr;
+    s->meshes.push_back(std::move(H));
+    if (index_out) *index_out = (int)s->meshes.size() - 1;
+    return YS_OK;
+}
+
+ys_status ys_scene_pack(ys_scene* s) {
+    if (!s) return fail(YS_ERR_BAD_ARG, "null scene");
+    if (s->packed) return fail(YS_ERR_STATE, "already packed");
+    if (s->meshes.empty()) return fail(YS_ERR_BAD_ARG, "empty scene");
+    YS_CK(cudaSetDevice(s->device));
+    u32 nV = 0, nF = 0, nNodes = 0, maxF = 1;
+    for (auto& H : s->meshes) {
+        H.voff = nV; H.foff = nF; H.node_off = nNodes;
+        nV += H.d.num_vertices;
+        nF += H.d.num_facets;
+        nNodes += H.d.num_facets ? 2 * H.d.num_facets - 1 : 0;
+        maxF = std::max(maxF, H.d.num_facets);
+        const bool cloth = H.d.behavior == YS_TRIANGULAR_CLOTH || H.d.behavior == YS_FAST_GRID_CLOTH;
+        u32 f = 0;
+        if (H.d.flags & YS_MESH_STATIC) f |= MF_STATIC;
+        if (H.d.flags & YS_MESH_COLLIDABLE) f |= MF_COLLIDABLE;
+        if (H.d.flags & YS_MESH_SELF_COLLIDE) f |= MF_SELF;
+        if ((H.d.flags & YS_MESH_COLLIDABLE) && H.d.behavior != YS_FLOAT && H.d.behavior != YS_KINEMATIC) f |= MF_QUERY;
+        if (cloth) f |= MF_CLOTH;
+        if (H.d.num_facets) f |= MF_TREE;
+        if (H.d.behavior == YS_FAST_GRID_CLOTH) f |= MF_GRID;
+        H.flags = f;
+        build_adjacency(H);
+    }
+    s->nV = nV; s->nF = nF; s->nNodes = nNodes;
+    s->cap = s->P.cols_per_point * nV;
+    // host staging of packed arrays
+    std::vector<float> x3(3 * (size_t)nV), v3(3 * (size_t)nV), mass(nV), mask(nV);
+    std::vector<u32> vobj(nV), F3(3 * (size_t)nF), spr_off(nV + 1, 0), spr_split(nV, 0), vaf_off(nV + 1, 0);
+    std::vector<uint4> F4(nF);
+    std::vector<u32> spr_nbr, vaf;
+    std::vector<float> spr_rest;
+    std::vector<MeshDev> md(s->meshes.size());
+    std::vector<u32> targets;
+    for (size_t m = 0; m < s->meshes.size(); ++m) {
+        HostMesh& H = s->meshes[m];
+        const u32 n = H.d.num_vertices;
+        std::copy(H.x.begin(), H.x.end(), x3.begin() + 3 * (size_t)H.voff);
+        std::copy(H.v.begin(), H.v.end(), v3.begin() + 3 * (size_t)H.voff);
+        std::copy(H.mass.begin(), H.mass.end(), mass.begin() + H.voff);
+        std::copy(H.mask.begin(), H.mask.end(), mask.begin() + H.voff);
+        for (u32 i = 0; i < n; ++i) vobj[H.voff + i] = (u32)m;
+        for (u32 f = 0; f < H.d.num_facets; ++f) {
+            F4[H.foff + f] = make_uint4(H.F[3 * f], H.F[3 * f + 1], H.F[3 * f + 2], 0u);
+            for (int k = 0; k < 3; ++k) F3[3 * ((size_t)H.foff + f) + k] = H.F[3 * f + k];
+        }
+        // springs: global neighbour ids
+        const u32 sbase = (u32)spr_nbr.size();
+        for (u32 i = 0; i < n; ++i) {
+            spr_off[H.voff + i] = sbase + H.spr_off[i];
+            spr_split[H.voff + i] = sbase + H.spr_split[i];
+        }
+        for (u32 j : H.spr_nbr) spr_nbr.push_back(H.voff + j);
+        spr_rest.insert(spr_rest.end(), H.spr_rest.begin(), H.spr_rest.end());
+        const u32 abase = (u32)vaf.size();
+        for (u32 i = 0; i < n; ++i) vaf_off[H.voff + i] = abase + H.vaf_off[i];
+        vaf.insert(vaf.end(), H.vaf.begin(), H.vaf.end());
+        MeshDev D;
+        memset(&D, 0, sizeof(D));
+        D.voff = H.voff; D.nV = n; D.foff = H.foff; D.nF = H.d.num_facets; D.node_off = H.node_off;
+        D.behavior = H.d.behavior; D.flags = H.flags; D.grid_n = H.d.grid_n;
+        D.kstretch = H.d.kstretch; D.kshear = H.d.kshear; D.kbend = H.d.kbend; D.thickness = H.d.thickness;
+        for (int k = 0; k < 6; ++k) D.rest[k] = H.d.grid_rest[k];
+        // inter-object targets, in mesh order (bvh.hpp:2884-2941)
+        D.tgt_begin = (u32)targets.size();
+        if (H.flags & MF_QUERY)
+            for (size_t t = 0; t < s->meshes.size(); ++t) {
+                if (t == m) continue;
+                const HostMesh& T = s->meshes[t];
+                if (!(T.d.flags & YS_MESH_COLLIDABLE) || T.d.num_facets == 0) continue;
+                if (T.d.group != H.d.group) continue;
+                targets.push_back((u32)t);
+            }
+        D.tgt_end = (u32)targets.size();
+        md[m] = D;
+    }
+    spr_off[nV] = (u32)spr_nbr.size();
+    vaf_off[nV] = (u32)vaf.size();
+    cudaStream_t st = s->stream;
+    // device allocations
+    for (auto& b : s->X) YS_CK(b.alloc(nV));
+    for (auto& b : s->V) YS_CK(b.alloc(nV));
+    YS_CK(s->mass.alloc(nV)); YS_CK(s->mask.alloc(nV)); YS_CK(s->vobj.alloc(nV));
+    YS_CK(s->targets.alloc(std::max<size_t>(targets.size(), 1)));
+    YS_CK(s->spr_off.alloc(nV + 1)); YS_CK(s->spr_split.alloc(nV));
+    YS_CK(s->spr_nbr.alloc(std::max<size_t>(spr_nbr.size(), 1))); YS_CK(s->spr_rest.alloc(std::max<size_t>(spr_rest.size(), 1)));
+    YS_CK(s->vaf_off.alloc(nV + 1)); YS_CK(s->vaf.alloc(std::max<size_t>(vaf.size(), 1)));
+    YS_CK(s->maxext.alloc(s->meshes.size())); YS_CK(s->status.alloc(1)); YS_CK(s->box.alloc(8));
+    YS_CK(s->codes.alloc(std::max(nF, 1u))); YS_CK(s->idx.alloc(std::max(nF, 1u))); YS_CK(s->visits.alloc(std::max(nF, 1u)));
+    YS_CK(s->F4.alloc(std::max(nF, 1u))); YS_CK(s->F3.alloc(3 * (size_t)std::max(nF, 1u)));
+    YS_CK(s->nodes.alloc(std::max(nNodes, 1u))); YS_CK(s->parent.alloc(std::max(nNodes, 1u)));
+    YS_CK(s->dmeshes.alloc(md.size())); YS_CK(s->jobs.alloc(6 * s->meshes.size() + 1));
+    YS_CK(s->counters.alloc(8));
+    YS_CK(s->sortScratch.alloc(sort_scratch_bytes(maxF)));
+    // uploads
+    DBuf<float> tmp3;
+    YS_CK(tmp3.alloc(3 * (size_t)nV));
+    YS_CK(cudaMemcpy(tmp3.p, x3.data(), 12 * (size_t)nV, cudaMemcpyHostToDevice));
+    for (auto& b : s->X) k_pack4<<<ceil_div(nV, 256), 256, 0, st>>>(tmp3.p, b.p, nV);
+    YS_CK(cudaStreamSynchronize(st));
+    YS_CK(cudaMemcpy(tmp3.p, v3.data(), 12 * (size_t)nV, cudaMemcpyHostToDevice));
+    for (auto& b : s->V) k_pack4<<<ceil_div(nV, 256), 256, 0, st>>>(tmp3.p, b.p, nV);
+    YS_CK(cudaStreamSynchronize(st));
+    tmp3.free();
+    YS_CK(cudaMemcpy(s->mass.p, mass.data(), 4 * (size_t)nV, cudaMemcpyHostToDevice));
+    YS_CK(cudaMemcpy(s->mask.p, mask.data(), 4 * (size_t)nV, cudaMemcpyHostToDevice));
+    YS_CK(cudaMemcpy(s->vobj.p, vobj.data(), 4 * (size_t)nV, cudaMemcpyHostToDevice));
+    if (!targets.empty()) YS_CK(cudaMemcpy(s->targets.p, targets.data(), 4 * targets.size(), cudaMemcpyHostToDevice));
+    YS_CK(cudaMemcpy(s->spr_off.p, spr_off.data(), 4 * (size_t)(nV + 1), cudaMemcpyHostToDevice));
+    YS_CK(cudaMemcpy(s->spr_split.p, spr_split.data(), 4 * (size_t)nV, cudaMemcpyHostToDevice));
+    if (!spr_nbr.empty()) {
+        YS_CK(cudaMemcpy(s->spr_nbr.p, spr_nbr.data(), 4 * spr_nbr.size(), cudaMemcpyHostToDevice));
+        YS_CK(cudaMemcpy(s->spr_rest.p, spr_rest.data(), 4 * spr_rest.size(), cudaMemcpyHostToDevice));
+    }
+    YS_CK(cudaMemcpy(s->vaf_off.p, vaf_off.data(), 4 * (size_t)(nV + 1), cudaMemcpyHostToDevice));
+    if (!vaf.empty()) YS_CK(cudaMemcpy(s->vaf.p, vaf.data(), 4 * vaf.size(), cudaMemcpyHostToDevice));
+    if (nF) {
+        YS_CK(cudaMemcpy(s->F4.p, F4.data(), 16 * (size_t)nF, cudaMemcpyHostToDevice));
+        YS_CK(cudaMemcpy(s->F3.p, F3.data(), 12 * (size_t)nF, cudaMemcpyHostToDevice));
+    }
+    YS_CK(cudaMemcpy(s->dmeshes.p, md.data(), sizeof(MeshDev) * md.size(), cudaMemcpyHostToDevice));
+    YS_CK(cudaMemset(s->status.p, 0, 4));
+    YS_CK(cudaMemset(s->maxext.p, 0, 4 * s->meshes.size()));
+    YS_CK(cudaMemset(s->counters.p, 0, 8 * s->counters.n));
+    // refit jobs: every non-static mesh with a tree, plus static cloth that
+    // needs the self-hash grid extent
+    s->hjobs.clear();
+    u32 leaves = 0;
+    for (size_t m = 0; m < s->meshes.size(); ++m) {
+        HostMesh& H = s->meshes[m];
+        if (!H.d.num_facets) continue;
+        const bool selfHash = s->P.self_mode == YS_SELF_HASH && (H.flags & MF_CLOTH) && (H.flags & MF_SELF) &&
+                              (H.flags & MF_QUERY);
+        if ((H.flags & MF_STATIC) && !selfHash) continue;
+        RefitJob J;
+        memset(&J, 0, sizeof(J));
+        J.nodes = s->nodes.p + H.node_off;
+        J.parent = s->parent.p + H.node_off;
+        J.visits = s->visits.p + H.foff;
+        J.facets = s->F3.p + 3 * (size_t)H.foff;
+        J.voff = H.voff;
+        J.n = H.d.num_facets;
+        J.leafBase = leaves;
+        J.dt = s->P.subh;
+        J.swept = (H.flags & MF_STATIC) ? 0u : 1u;
+        J.selfMargin = selfHash ? s->P.margin : 0.f;
+        J.maxExt = s->maxext.p + m;
+        s->hjobs.push_back(J);
+        leaves += J.n;
+    }
+    s->refitLeaves = leaves;
+    s->njobs = (u32)s->hjobs.size();
+    for (int c = 0; c < 3; ++c)
+        for (int w = 0; w < 2; ++w) {
+            std::vector<RefitJob> t = s->hjobs;
+            for (auto& J : t) { J.x4 = s->X[c].p; J.v4 = s->V[w].p; }
+            if (!t.empty())
+                YS_CK(cudaMemcpy(s->jobs.p + (size_t)(c * 2 + w) * s->njobs, t.data(), t.size() * sizeof(RefitJob),
+                                 cudaMemcpyHostToDevice));
+        }
+    s->packed = true;
+    s->cur = 0; s->prev = 1; s->cv = 0;
+    // BroadPhase::build at initialize (Simulator::initialize -> build)
+    for (auto& H : s->meshes) {
+        ys_status r = build_tree(s, H);
+        if (r) return r;
+    }
+    YS_CK(cudaStreamSynchronize(st));
+    return YS_OK;
+}
+
+ys_status ys_frame_preamble(ys_scene* s) { ys_status r = check_scene(s); return r ? r : preamble(s); }
+ys_status ys_broad_refit(ys_scene* s) { ys_status r = check_scene(s); return r ? r : refit(s); }
+ys_status ys_broad_detect(ys_scene* s) { ys_status r = check_scene(s); return r ? r : detect(s); }
+ys_status ys_narrow_and_sort(ys_scene* s) { ys_status r = check_scene(s); return r ? r : narrow_and_sort(s); }
+ys_status ys_snapshot_xprev(ys_scene* s) {
+    ys_status r = check_scene(s);
+    if (r) return r;
+    s->snapshot_pending = true;
+    return YS_OK;
+}
+ys_status ys_system_update(ys_scene* s) { ys_status r = check_scene(s); return r ? r : system_update(s); }
+
+ys_status ys_scene_step_staged(ys_scene* s, uint32_t n) {
+    ys_status r = check_scene(s);
+    if (r) return r;
+    for (u32 i = 0; i < n; ++i) {
+        if ((r = preamble(s)) || (r = refit(s)) || (r = detect(s)) || (r = narrow_and_sort(s))) return r;
+        s->snapshot_pending = true;
+        if ((r = system_update(s))) return r;
+    }
+    return YS_OK;
+}
+
+ys_status ys_scene_step(ys_scene* s, uint32_t n) {
+    ys_status r = check_scene(s);
+    if (r) return r;
+    for (u32 i = 0; i < n; ++i)
+        if ((r = fused_substep(s))) return r;
+    return YS_OK;
+}
+
+ys_status ys_scene_set_record(ys_scene* s, int record) {
+    if (!s) return fail(YS_ERR_BAD_ARG, "null scene");
+    s->record = record != 0;
+    return YS_OK;
+}
+
+ys_status ys_scene_sync(ys_scene* s) {
+    if (!s) return fail(YS_ERR_BAD_ARG, "null scene");
+    YS_CK(cudaStreamSynchronize(s->stream));
+    return YS_OK;
+}
+
+ys_status ys_scene_stream(ys_scene* s, void** out) {
+    if (!s || !out) return fail(YS_ERR_BAD_ARG, "null argument");
+    *out = (void*)s->stream;
+    return YS_OK;
+}
+
+ys_status ys_scene_get_state(ys_scene* s, int which, float* out) {
+    ys_status r = check_scene(s);
+    if (r) return r;
+    if (!out) return fail(YS_ERR_BAD_ARG, "null output");
+    const float4* src = nullptr;
+    if (which == 0) src = s->X[s->cur].p;
+    else if (which == 1) src = s->V[s->cv].p;
+    else if (which == 2) src = s->snapshot_pending ? s->X[s->cur].p : s->X[s->prev].p;
+    else if (which == 3) { r = ensure_staged(s); if (r) return r; src = s->Fbuf.p; }
+    else return fail(YS_ERR_BAD_ARG, "bad state id");
+    DBuf<float> tmp;
+    YS_CK(tmp.alloc(3 * (size_t)s->nV));
+    k_unpack4<<<ceil_div(s->nV, 256), 256, 0, s->stream>>>(src, tmp.p, s->nV);
+    YS_CK(cudaMemcpyAsync(out, tmp.p, 12 * (size_t)s->nV, cudaMemcpyDeviceToHost, s->stream));
+    YS_CK(cudaStreamSynchronize(s->stream));
+    tmp.free();
+    return YS_OK;
+}
+
+ys_status ys_scene_set_state(ys_scene* s, int which, const float* in) {
+    ys_status r = check_scene(s);
+    if (r) return r;
+    if (!in) return fail(YS_ERR_BAD_ARG, "null input");
+    DBuf<float> tmp;
+    YS_CK(tmp.alloc(3 * (size_t)s->nV));
+    YS_CK(cudaMemcpyAsync(tmp.p, in, 12 * (size_t)s->nV, cudaMemcpyHostToDevice, s->stream));
+    if (which == 0) k_pack4<<<ceil_div(s->nV, 256), 256, 0, s->stream>>>(tmp.p, s->X[s->cur].p, s->nV);
+    else if (which == 1) k_pack4<<<ceil_div(s->nV, 256), 256, 0, s->stream>>>(tmp.p, s->V[s->cv].p, s->nV);
+    else if (which == 2) k_pack4<<<ceil_div(s->nV, 256), 256, 0, s->stream>>>(tmp.p, s->X[s->prev].p, s->nV);
+    else { tmp.free(); return fail(YS_ERR_BAD_ARG, "bad state id"); }
+    // vertices of static meshes are never rewritten by a substep, so every
+    // rotating buffer must hold the same values for them
+    if (which == 0 || which == 1)
+        for (auto& H : s->meshes) {
+            if (!(H.flags & MF_STATIC)) continue;
+            const size_t bytes = sizeof(float4) * H.d.num_vertices;
+            if (which == 0) {
+                for (int b = 0; b < 3; ++b)
+                    if (b != s->cur)
+                        YS_CK(cudaMemcpyAsync(s->X[b].p + H.voff, s->X[s->cur].p + H.voff, bytes,
+                                              cudaMemcpyDeviceToDevice, s->stream));
+            } else {
+                YS_CK(cudaMemcpyAsync(s->V[1 - s->cv].p + H.voff, s->V[s->cv].p + H.voff, bytes,
+                                      cudaMemcpyDeviceToDevice, s->stream));
+            }
+        }
+    YS_CK(cudaStreamSynchronize(s->stream));
+    tmp.free();
+    return YS_OK;
+}
+
+ys_status ys_scene_stats(ys_scene* s, uint64_t out[8]) {
+    ys_status r = check_scene(s);
+    if (r) return r;
+    unsigned long long cnt[3];
+    u32 st;
+    YS_CK(cudaMemcpyAsync(cnt, s->counters.p, 24, cudaMemcpyDeviceToHost, s->stream));
+    YS_CK(cudaMemcpyAsync(&st, s->status.p, 4, cudaMemcpyDeviceToHost, s->stream));
+    YS_CK(cudaStreamSynchronize(s->stream));
+    out[0] = s->frame;
+    out[1] = s->cursor;
+    out[2] = cnt[0];
+    out[3] = cnt[1];
+    out[4] = (st & ST_NONFINITE) ? 1 : 0;
+    if (cnt[0] > s->cap || cnt[1] > s->cap) st |= ST_PAIR_OVF;
+    out[5] = st;
+    out[6] = s->nV;
+    out[7] = s->substeps_run;
+    return YS_OK;
+}
+
+ys_status ys_scene_set_external_forces(ys_scene* s, const float* host_ext) {
+    ys_status r = check_scene(s);
+    if (r) return r;
+    if (!host_ext) { s->use_ext = false; return YS_OK; }
+    if (!s->ext.p) {
+        YS_CK(s->ext.alloc(s->nV));
+        YS_CK(s->scratch3.alloc(3 * (size_t)s->nV));
+    }
+    YS_CK(cudaMemcpyAsync(s->scratch3.p, host_ext, 12 * (size_t)s->nV, cudaMemcpyHostToDevice, s->stream));
+    k_pack4<<<ceil_div(s->nV, 256), 256, 0, s->stream>>>(s->scratch3.p, s->ext.p, s->nV);
+    YS_CK(cudaGetLastError());
+    s->use_ext = true;
+    return YS_OK;
+}
+
+ys_status ys_scene_read_positions_async(ys_scene* s, float* host_out) {
+    ys_status r = check_scene(s);
+    if (r) return r;
+    if (!host_out) return fail(YS_ERR_BAD_ARG, "null output");
+    if (!s->scratch3.p) YS_CK(s->scratch3.alloc(3 * (size_t)s->nV));
+    k_unpack4<<<ceil_div(s->nV, 256), 256, 0, s->stream>>>(s->X[s->cur].p, s->scratch3.p, s->nV);
+    YS_CK(cudaMemcpyAsync(host_out, s->scratch3.p, 12 * (size_t)s->nV, cudaMemcpyDeviceToHost, s->stream));
+    return YS_OK;
+}
+
+ys_status ys_scene_set_timing(ys_scene* s, int on) {
+    ys_status r = check_scene(s);
+    if (r) return r;
+    YS_CK(cudaStreamSynchronize(s->stream));
+    s->timing = on != 0;
+    s->evUsed = 0;
+    s->evRefit.clear();
+    s->evFused.clear();
+    return YS_OK;
+}
+
+ys_status ys_scene_kernel_times(ys_scene* s, double out[4]) {
+    ys_status r = check_scene(s);
+    if (r) return r;
+    YS_CK(cudaStreamSynchronize(s->stream));
+    double tr = 0, tf = 0;
+    for (size_t i : s->evRefit) { float ms; YS_CK(cudaEventElapsedTime(&ms, s->evPool[i], s->evPool[i + 1])); tr += ms; }
+    for (size_t i : s->evFused) { float ms; YS_CK(cudaEventElapsedTime(&ms, s->evPool[i], s->evPool[i + 1])); tf += ms; }
+    out[0] = tr; out[1] = (double)s->evRefit.size(); out[2] = tf; out[3] = (double)s->evFused.size();
+    return YS_OK;
+}
+
+ys_status ys_scene_totals(ys_scene* s, uint64_t out[2]) {
+    ys_status r = check_scene(s);
+    if (r) return r;
+    unsigned long long c[2];
+    YS_CK(cudaMemcpyAsync(c, s->counters.p + 3, 16, cudaMemcpyDeviceToHost, s->stream));
+    YS_CK(cudaStreamSynchronize(s->stream));
+    out[0] = c[0]; out[1] = c[1];
+    return YS_OK;
+}
+
+ys_status ys_scene_clear_flags(ys_scene* s) {
+    ys_status r = check_scene(s);
+    if (r) return r;
+    YS_CK(cudaMemsetAsync(s->status.p, 0, 4, s->stream));
+    YS_CK(cudaStreamSynchronize(s->stream));
+    return YS_OK;
+}
+
+ys_status ys_scene_rows(ys_scene* s, void* out, uint64_t cap, uint64_t* n_out) {
+    ys_status r = check_scene(s);
+    if (r) return r;
+    if (!s->staged_ready) { if (n_out) *n_out = 0; return YS_OK; }
+    unsigned long long cnt;
+    YS_CK(cudaMemcpyAsync(&cnt, s->counters.p, 8, cudaMemcpyDeviceToHost, s->stream));
+    YS_CK(cudaStreamSynchronize(s->stream));
+    uint64_t n = std::min<uint64_t>(cnt, s->cap);
+    if (n_out) *n_out = n;
+    if (out && n) YS_CK(cudaMemcpy(out, s->rows.p, sizeof(Row) * std::min(n, cap), cudaMemcpyDeviceToHost));
+    return YS_OK;
+}
+
+ys_status ys_scene_contacts(ys_scene* s, uint32_t* off, void* out, uint64_t cap, uint64_t* n_out) {
+    ys_status r = check_scene(s);
+    if (r) return r;
+    YS_CK(cudaStreamSynchronize(s->stream));
+    if (s->last_contacts == 1) {
+        std::vector<u32> o(s->nV + 1);
+        YS_CK(cudaMemcpy(o.data(), s->csr_off.p, 4 * (size_t)(s->nV + 1), cudaMemcpyDeviceToHost));
+        uint64_t n = o[s->nV];
+        if (n_out) *n_out = n;
+        if (off) memcpy(off, o.data(), 4 * (size_t)(s->nV + 1));
+        if (out && n) YS_CK(cudaMemcpy(out, s->csr.p, sizeof(VContact) * std::min(n, cap), cudaMemcpyDeviceToHost));
+        return YS_OK;
+    }
+    if (s->last_contacts == 2) {
+        std::vector<u32> vs(s->nV), vc(s->nV);
+        YS_CK(cudaMemcpy(vs.data(), s->vstart.p, 4 * (size_t)s->nV, cudaMemcpyDeviceToHost));
+        YS_CK(cudaMemcpy(vc.data(), s->vcount.p, 4 * (size_t)s->nV, cudaMemcpyDeviceToHost));
+        unsigned long long fill;
+        YS_CK(cudaMemcpy(&fill, s->counters.p + 2, 8, cudaMemcpyDeviceToHost));
+        std::vector<VContact> pool(std::min<unsigned long long>(fill, s->cap));
+        if (!pool.empty()) YS_CK(cudaMemcpy(pool.data(), s->pool.p, sizeof(VContact) * pool.size(), cudaMemcpyDeviceToHost));
+        std::vector<u32> o(s->nV + 1, 0);
+        for (u32 g = 0; g < s->nV; ++g) o[g + 1] = o[g] + vc[g];
+        uint64_t n = o[s->nV];
+        if (n_out) *n_out = n;
+        if (off) memcpy(off, o.data(), 4 * (size_t)(s->nV + 1));
+        if (out) {
+            VContact* dst = (VContact*)out;
+            for (u32 g = 0; g < s->nV; ++g)
+                for (u32 k = 0; k < vc[g]; ++k)
+                    if (o[g] + k < cap) dst[o[g] + k] = pool[vs[g] + k];
+        }
+        return YS_OK;
+    }
+    if (n_out) *n_out = 0;
+    if (off) memset(off, 0, 4 * (size_t)(s->nV + 1));
+    return YS_OK;
+}
+
+ys_status ys_scene_tree(ys_scene* s, int mesh, void* nodes, int32_t* parent, uint32_t* codes, uint32_t* idx,
+                        uint32_t* nprims) {
+    ys_status r = check_scene(s);
+    if (r) return r;
+    if (mesh < 0 || (size_t)mesh >= s->meshes.size()) return fail(YS_ERR_BAD_ARG, "bad mesh index");
+    HostMesh& H = s->meshes[mesh];
+    const u32 n = H.d.num_facets;
+    if (nprims) *nprims = n;
+    YS_CK(cudaStreamSynchronize(s->stream));
+    if (n == 0) return YS_OK;
+    const size_t nn = 2 * (size_t)n - 1;
+    if (nodes) YS_CK(cudaMemcpy(nodes, s->nodes.p + H.node_off, 32 * nn, cudaMemcpyDeviceToHost));
+    if (parent) YS_CK(cudaMemcpy(parent, s->parent.p + H.node_off, 4 * nn, cudaMemcpyDeviceToHost));
+    if (codes) YS_CK(cudaMemcpy(codes, s->codes.p + H.foff, 4 * (size_t)n, cudaMemcpyDeviceToHost));
+    if (idx) YS_CK(cudaMemcpy(idx, s->idx.p + H.foff, 4 * (size_t)n, cudaMemcpyDeviceToHost));
+    return YS_OK;
+}
+
+}  // extern "C"

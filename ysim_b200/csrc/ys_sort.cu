@@ -1,0 +1,170 @@
+// ys_sort.cu -- stable LSD radix sort of (uint32 key, uint32 value) pairs.
+//
+// Restates the reference RadixSorter (spatial_hash.hpp:48-70,
+// radixsort.metal:21-111): 8-bit digits, least significant first, stable, the
+// value carried with its key.  Because the sort is stable and the values enter
+// in index order, the output is the unique (key, original index) order, so it
+// is bit-identical to the CPU twin radixSortCPU (bvh.hpp:723-765).
+//
+// B200 design, per pass (3 launches):
+//   upsweep  -- each 256-thread CTA owns a tile of TILE keys and builds a
+//               256-bin digit histogram with warp-aggregated shared atomics
+//               (__match_any_sync: one atomic per distinct digit per warp);
+//   scan     -- one CTA per digit scans that digit's column of tile counts;
+//               digit bases come from a 256-entry scan done redundantly by
+//               every scatter CTA (256 loads, no extra launch);
+//   scatter  -- the tile is walked in 256-key rounds in index order; a key's
+//               stable rank = running count of its digit in this tile + keys
+//               with the same digit in earlier warps of the round (shared
+//               table) + lower lanes of its own warp with the same digit
+//               (match mask popcount).
+#include "ys_common.cuh"
+#include "ys_sort.cuh"
+
+namespace ys {
+
+static constexpr int SORT_THREADS = 256;
+static constexpr int SORT_ITEMS = 16;
+static constexpr int TILE = SORT_THREADS * SORT_ITEMS;  // 4096 keys per CTA
+
+// hist layout: digit-major, hist[d * numTiles + tile].
+__global__ void __launch_bounds__(SORT_THREADS) k_sort_upsweep(const u32* __restrict__ keys, u32 n, int shift,
+                                                               u32* __restrict__ hist, u32 numTiles) {
+    __shared__ u32 h[256];
+    const int tid = threadIdx.x;
+    h[tid] = 0;
+    __syncthreads();
+    const u32 base = blockIdx.x * (u32)TILE;
+    const int lane = tid & 31;
+#pragma unroll 4
+    for (int r = 0; r < SORT_ITEMS; ++r) {
+        u32 i = base + (u32)r * SORT_THREADS + tid;
+        bool valid = i < n;
+        u32 d = valid ? (keys[i] >> shift) & 255u : 256u + lane;  // invalid lanes get unique digits
+        u32 peers = __match_any_sync(0xffffffffu, d);
+        int leader = __ffs(peers) - 1;
+        if (valid && lane == leader) atomicAdd(&h[d], (u32)__popc(peers));
+    }
+    __syncthreads();
+    hist[(u32)tid * numTiles + blockIdx.x] = h[tid];
+}
+
+// One CTA per digit: exclusive scan of hist[d, 0..numTiles) in place; total
+// of digit d to totals[d].
+__global__ void __launch_bounds__(1024) k_sort_scan(u32* __restrict__ hist, u32 numTiles, u32* __restrict__ totals) {
+    __shared__ u32 warpSums[32];
+    __shared__ u32 carry;
+    const int d = blockIdx.x, tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+    u32* row = hist + (u64)d * numTiles;
+    if (tid == 0) carry = 0;
+    __syncthreads();
+    for (u32 base = 0; base < numTiles; base += 1024) {
+        u32 i = base + tid;
+        u32 v = (i < numTiles) ? row[i] : 0u;
+        u32 x = v;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) { u32 y = __shfl_up_sync(0xffffffffu, x, o); if (lane >= o) x += y; }
+        if (lane == 31) warpSums[w] = x;
+        __syncthreads();
+        if (w == 0) {
+            u32 s = warpSums[lane];
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) { u32 y = __shfl_up_sync(0xffffffffu, s, o); if (lane >= o) s += y; }
+            warpSums[lane] = s;
+        }
+        __syncthreads();
+        u32 incl = x + (w > 0 ? warpSums[w - 1] : 0u) + carry;
+        if (i < numTiles) row[i] = incl - v;
+        __syncthreads();
+        if (tid == 1023) carry = incl;
+        __syncthreads();
+    }
+    if (tid == 0) totals[d] = carry;
+}
+
+__global__ void __launch_bounds__(SORT_THREADS) k_sort_scatter(const u32* __restrict__ kin, const u32* __restrict__ vin,
+                                                               u32* __restrict__ kout, u32* __restrict__ vout, u32 n,
+                                                               int shift, const u32* __restrict__ hist, u32 numTiles,
+                                                               const u32* __restrict__ totals) {
+    constexpr int W = SORT_THREADS / 32;
+    __shared__ u32 base[256];         // global start of each digit for this tile
+    __shared__ u32 running[256];      // keys of each digit already placed by this tile
+    __shared__ u32 wcnt[W][256];      // per-warp digit counts of the current round
+    __shared__ u32 scanTmp[256];
+    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+
+    // digit bases: exclusive scan of totals (every CTA does it; 256 entries)
+    u32 t = totals[tid];
+    scanTmp[tid] = t;
+    __syncthreads();
+    for (int o = 1; o < 256; o <<= 1) {
+        u32 add = (tid >= o) ? scanTmp[tid - o] : 0u;
+        __syncthreads();
+        scanTmp[tid] += add;
+        __syncthreads();
+    }
+    base[tid] = scanTmp[tid] - t + hist[(u32)tid * numTiles + blockIdx.x];
+    running[tid] = 0;
+    __syncthreads();
+
+    const u32 tileBase = blockIdx.x * (u32)TILE;
+    for (int r = 0; r < SORT_ITEMS; ++r) {
+        for (int k = tid; k < W * 256; k += SORT_THREADS) (&wcnt[0][0])[k] = 0;
+        __syncthreads();
+        u32 i = tileBase + (u32)r * SORT_THREADS + tid;
+        bool valid = i < n;
+        u32 key = 0, val = 0, d = 256u + lane;
+        if (valid) { key = kin[i]; val = vin[i]; d = (key >> shift) & 255u; }
+        u32 peers = __match_any_sync(0xffffffffu, d);
+        u32 lower = __popc(peers & ((1u << lane) - 1u));
+        int leader = __ffs(peers) - 1;
+        if (valid && lane == leader) wcnt[w][d] = (u32)__popc(peers);
+        __syncthreads();
+        if (valid) {
+            u32 before = 0;
+            for (int ww = 0; ww < w; ++ww) before += wcnt[ww][d];
+            u32 dst = base[d] + running[d] + before + lower;
+            kout[dst] = key;
+            vout[dst] = val;
+        }
+        __syncthreads();
+        // advance running counts by this round's totals
+        {
+            u32 s = 0;
+#pragma unroll
+            for (int ww = 0; ww < W; ++ww) s += wcnt[ww][tid];
+            running[tid] += s;
+        }
+        __syncthreads();
+    }
+}
+
+size_t sort_scratch_bytes(u32 n) {
+    u32 tiles = (u32)ceil_div(n > 0 ? n : 1, TILE);
+    return (size_t)256 * tiles * 4 + 256 * 4 + (size_t)2 * n * 4;
+}
+
+// Sort keys/vals in place.  scratch must hold sort_scratch_bytes(n) bytes.
+cudaError_t radix_sort_pairs(u32* keys, u32* vals, u32 n, void* scratch, int beginBit, int endBit, cudaStream_t s) {
+    if (n <= 1) return cudaSuccess;
+    u32 tiles = (u32)ceil_div(n, TILE);
+    u32* hist = (u32*)scratch;
+    u32* totals = hist + (size_t)256 * tiles;
+    u32* k2 = totals + 256;
+    u32* v2 = k2 + n;
+    u32 *ki = keys, *vi = vals, *ko = k2, *vo = v2;
+    for (int shift = beginBit; shift < endBit; shift += 8) {
+        k_sort_upsweep<<<tiles, SORT_THREADS, 0, s>>>(ki, n, shift, hist, tiles);
+        k_sort_scan<<<256, 1024, 0, s>>>(hist, tiles, totals);
+        k_sort_scatter<<<tiles, SORT_THREADS, 0, s>>>(ki, vi, ko, vo, n, shift, hist, tiles, totals);
+        u32* tk = ki; ki = ko; ko = tk;
+        u32* tv = vi; vi = vo; vo = tv;
+    }
+    if (ki != keys) {
+        cudaMemcpyAsync(keys, ki, (size_t)n * 4, cudaMemcpyDeviceToDevice, s);
+        cudaMemcpyAsync(vals, vi, (size_t)n * 4, cudaMemcpyDeviceToDevice, s);
+    }
+    return cudaGetLastError();
+}
+
+}  // namespace ys

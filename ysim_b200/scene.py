@@ -1,0 +1,200 @@
+"""Host mirror of the reference's stage surfaces over the C ABI.
+
+Names follow the reference so a caller of ysim finds the same stages:
+  Scene.pack()                          Scene<BE,PR>::pack            (scene.hpp:783)
+  Scene.broad_phase.build/refit_swept/detect_collisions
+                                        BVH<SCENE,OBJECT>             (bvh.hpp:2537-2949)
+  Scene.narrow_phase.narrow_and_sort_by_vertices
+                                        BruteForce::narrowAndSortByVertices (bruteforce.hpp:311)
+  Scene.system.snapshot_xprev / update  SymplecticSystem              (symplectic_system.hpp:230, 341)
+  Simulator.update()                    one frame of substeps         (simulator.hpp:3169-3870)
+Every call goes through the CUDA library; there is no CPU path.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import Optional
+
+import numpy as np
+
+from . import _lib
+from .generators import SceneSpec
+
+ROW_DTYPE = np.dtype([("point", "<u4"), ("tri", "<u4"), ("qobj", "<u4"), ("tobj", "<u4"), ("qbeh", "<u4"),
+                      ("tbeh", "<u4"), ("qshape", "<u4"), ("tshape", "<u4")])
+VCONTACT_DTYPE = np.dtype([("tobj", "<u4"), ("tri", "<u4"), ("nx", "<f4"), ("ny", "<f4"), ("nz", "<f4"),
+                           ("d", "<f4")])
+NODE_DTYPE = np.dtype([("mn", "<f4", 3), ("a", "<i4"), ("mx", "<f4", 3), ("b", "<i4")])
+
+
+def _ptr(a: Optional[np.ndarray]):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+class _BroadPhase:
+    def __init__(self, scene: "Scene"):
+        self._s = scene
+
+    def build(self):
+        """Frame preamble: rebuild due trees (frame % rebuild_frames == 0)."""
+        _lib.check(self._s.lib.ys_frame_preamble(self._s.h), "ys_frame_preamble")
+
+    def refit_swept(self):
+        _lib.check(self._s.lib.ys_broad_refit(self._s.h), "ys_broad_refit")
+
+    def detect_collisions(self):
+        _lib.check(self._s.lib.ys_broad_detect(self._s.h), "ys_broad_detect")
+
+
+class _NarrowPhase:
+    def __init__(self, scene: "Scene"):
+        self._s = scene
+
+    def narrow_and_sort_by_vertices(self):
+        _lib.check(self._s.lib.ys_narrow_and_sort(self._s.h), "ys_narrow_and_sort")
+
+
+class _System:
+    def __init__(self, scene: "Scene"):
+        self._s = scene
+
+    def snapshot_xprev(self):
+        _lib.check(self._s.lib.ys_snapshot_xprev(self._s.h), "ys_snapshot_xprev")
+
+    def update(self):
+        _lib.check(self._s.lib.ys_system_update(self._s.h), "ys_system_update")
+
+
+class Scene:
+    """A packed scene on one GPU (one CUDA stream)."""
+
+    def __init__(self, spec: SceneSpec, device: int = 0, pack: bool = True):
+        self.lib = _lib.load()
+        self.spec = spec
+        p = spec.params
+        sp = _lib.SimParams(p.subh, p.kair, p.kd, (C.c_float * 3)(*p.gravity), p.margin, p.radius, p.substeps,
+                            p.rebuild_frames, p.self_mode, p.cols_per_point)
+        h = C.c_void_p()
+        _lib.check(self.lib.ys_scene_create(C.byref(h), C.byref(sp), device), "ys_scene_create")
+        self.h = h
+        self._keep = []
+        for m in spec.meshes:
+            x = np.ascontiguousarray(m.x, np.float32)
+            v = np.ascontiguousarray(m.v if m.v is not None else np.zeros_like(x), np.float32)
+            mass = np.ascontiguousarray(m.mass if m.mass is not None else np.ones(m.nV, np.float32), np.float32)
+            mask = np.ascontiguousarray(m.mask if m.mask is not None else np.ones(m.nV, np.float32), np.float32)
+            fac = np.ascontiguousarray(m.facets, np.uint32)
+            d = _lib.MeshDesc(m.behavior, m.flags, m.nV, m.nF, _ptr(x), _ptr(v), _ptr(mass), _ptr(mask), _ptr(fac),
+                              m.kstretch, m.kshear, m.kbend, m.thickness, m.grid_n,
+                              (C.c_float * 6)(*m.grid_rest), m.group)
+            idx = C.c_int()
+            _lib.check(self.lib.ys_scene_add_mesh(self.h, C.byref(d), C.byref(idx)), "ys_scene_add_mesh")
+        self.nV = spec.nV
+        self.broad_phase = _BroadPhase(self)
+        self.narrow_phase = _NarrowPhase(self)
+        self.system = _System(self)
+        if pack:
+            self.pack()
+
+    def pack(self):
+        _lib.check(self.lib.ys_scene_pack(self.h), "ys_scene_pack")
+
+    def close(self):
+        if self.h:
+            self.lib.ys_scene_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # ---- stepping
+    def step(self, n: int = 1):
+        """n substeps on the fused path."""
+        _lib.check(self.lib.ys_scene_step(self.h, n), "ys_scene_step")
+
+    def step_staged(self, n: int = 1):
+        """n substeps, one kernel group per reference stage."""
+        _lib.check(self.lib.ys_scene_step_staged(self.h, n), "ys_scene_step_staged")
+
+    def set_record(self, on: bool):
+        _lib.check(self.lib.ys_scene_set_record(self.h, 1 if on else 0), "ys_scene_set_record")
+
+    def sync(self):
+        _lib.check(self.lib.ys_scene_sync(self.h), "ys_scene_sync")
+
+    def stream(self) -> int:
+        s = C.c_void_p()
+        _lib.check(self.lib.ys_scene_stream(self.h, C.byref(s)), "ys_scene_stream")
+        return s.value or 0
+
+    # ---- state
+    def get(self, which: str) -> np.ndarray:
+        code = {"x": 0, "v": 1, "xprev": 2, "f": 3}[which]
+        out = np.empty((self.nV, 3), np.float32)
+        _lib.check(self.lib.ys_scene_get_state(self.h, code, _ptr(out)), "ys_scene_get_state")
+        return out
+
+    def set(self, which: str, arr: np.ndarray):
+        code = {"x": 0, "v": 1, "xprev": 2}[which]
+        a = np.ascontiguousarray(arr, np.float32)
+        _lib.check(self.lib.ys_scene_set_state(self.h, code, _ptr(a)), "ys_scene_set_state")
+
+    def stats(self) -> dict:
+        out = (C.c_uint64 * 8)()
+        _lib.check(self.lib.ys_scene_stats(self.h, out), "ys_scene_stats")
+        keys = ("frame", "cursor", "broad_rows", "contacts", "anomaly", "flags", "num_vertices", "substeps")
+        return dict(zip(keys, (int(v) for v in out)))
+
+    def totals(self):
+        out = (C.c_uint64 * 2)()
+        _lib.check(self.lib.ys_scene_totals(self.h, out), "ys_scene_totals")
+        return int(out[0]), int(out[1])
+
+    def clear_flags(self):
+        _lib.check(self.lib.ys_scene_clear_flags(self.h), "ys_scene_clear_flags")
+
+    def rows(self) -> np.ndarray:
+        n = C.c_uint64()
+        _lib.check(self.lib.ys_scene_rows(self.h, None, 0, C.byref(n)), "ys_scene_rows")
+        out = np.empty(n.value, ROW_DTYPE)
+        _lib.check(self.lib.ys_scene_rows(self.h, _ptr(out), n.value, C.byref(n)), "ys_scene_rows")
+        return out
+
+    def contacts(self):
+        n = C.c_uint64()
+        off = np.empty(self.nV + 1, np.uint32)
+        _lib.check(self.lib.ys_scene_contacts(self.h, _ptr(off), None, 0, C.byref(n)), "ys_scene_contacts")
+        out = np.empty(n.value, VCONTACT_DTYPE)
+        _lib.check(self.lib.ys_scene_contacts(self.h, _ptr(off), _ptr(out), n.value, C.byref(n)),
+                   "ys_scene_contacts")
+        return off, out
+
+    def tree(self, mesh: int):
+        n = C.c_uint32()
+        _lib.check(self.lib.ys_scene_tree(self.h, mesh, None, None, None, None, C.byref(n)), "ys_scene_tree")
+        N = n.value
+        nodes = np.empty(max(2 * N - 1, 0), NODE_DTYPE)
+        parent = np.empty(max(2 * N - 1, 0), np.int32)
+        codes = np.empty(N, np.uint32)
+        idx = np.empty(N, np.uint32)
+        _lib.check(self.lib.ys_scene_tree(self.h, mesh, _ptr(nodes), _ptr(parent), _ptr(codes), _ptr(idx),
+                                          C.byref(n)), "ys_scene_tree")
+        return nodes, parent, codes, idx
+
+
+class Simulator:
+    """Frame driver: Simulator::update (simulator.hpp:3169-3870) over a Scene."""
+
+    def __init__(self, scene: Scene, fused: bool = True):
+        self.scene = scene
+        self.fused = fused
+
+    def update(self):
+        n = self.scene.spec.params.substeps
+        if self.fused:
+            self.scene.step(n)
+        else:
+            self.scene.step_staged(n)
