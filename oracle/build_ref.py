@@ -1,5 +1,57 @@
-"""Placeholder replaced below."""
+"""Host build of the reference's own Metal compute kernels: oracle/_ref/libysref.so.
+
+TEST INFRASTRUCTURE ONLY.  Compiles oracle/ref_harness.cpp three times, each
+time including one shader of the reference checkout in place
+(src/metal/bvh.metal, bruteforce.metal, physics.metal) with oracle/ref_shim
+standing in for <metal_stdlib>; nothing of the reference is copied into this
+repository.  Skipped (returns None) when the reference checkout is absent;
+the built library is git-ignored but travels with the working tree.
+
+    python -m oracle.build_ref
+"""
+from __future__ import annotations
+
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF = os.environ.get("YSIM_REFERENCE", "/root/reference")
+OUT_DIR = os.path.join(HERE, "_ref")
+OUT = os.path.join(OUT_DIR, "libysref.so")
+SHADERS = {"BVH": "bvh.metal", "NARROW": "bruteforce.metal", "PHYSICS": "physics.metal"}
 
 
-def build():
-    return None
+def available() -> bool:
+    return all(os.path.exists(os.path.join(REF, "src", "metal", f)) for f in SHADERS.values())
+
+
+def build(force: bool = False):
+    if not available():
+        return OUT if os.path.exists(OUT) else None
+    deps = [os.path.join(HERE, "ref_harness.cpp"), os.path.join(HERE, "ref_shim", "metal_shim.h")]
+    if not force and os.path.exists(OUT) and all(os.path.getmtime(OUT) >= os.path.getmtime(d) for d in deps):
+        return OUT
+    os.makedirs(OUT_DIR, exist_ok=True)
+    objs = []
+    for key, shader in SHADERS.items():
+        obj = os.path.join(OUT_DIR, f"{key.lower()}.o")
+        cmd = ["g++", "-std=c++17", "-O3", "-ffp-contract=off", "-fno-fast-math", "-fopenmp", "-fPIC", "-w",
+               "-I", os.path.join(HERE, "ref_shim"), f"-DYS_REF_{key}",
+               f"-DYS_REF_SRC={os.path.join(REF, 'src', 'metal', shader)}", "-c",
+               os.path.join(HERE, "ref_harness.cpp"), "-o", obj]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"reference build failed for {shader}:\n{r.stdout}{r.stderr}")
+        objs.append(obj)
+    r = subprocess.run(["g++", "-shared", "-fopenmp", "-o", OUT + ".tmp", *objs], capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError("reference link failed:\n" + r.stdout + r.stderr)
+    os.replace(OUT + ".tmp", OUT)
+    for o in objs:
+        os.remove(o)
+    return OUT
+
+
+if __name__ == "__main__":
+    print(build(force="--force" in sys.argv))

@@ -1,0 +1,148 @@
+"""ctypes wrapper of oracle/_ref/libysref.so: the reference's own Metal kernels
+compiled for the host (see oracle/build_ref.py).  TEST INFRASTRUCTURE ONLY."""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import build_ref
+from .oracle import CONTACT_DTYPE, NODE_DTYPE, ROW_DTYPE
+
+vp = C.c_void_p
+u32 = C.c_uint32
+f32 = C.c_float
+_lib = None
+
+
+def available() -> bool:
+    return os.path.exists(build_ref.OUT) or build_ref.available()
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        path = build_ref.build()
+        if not path:
+            raise FileNotFoundError("reference kernels not built (reference checkout absent)")
+        L = C.CDLL(path)
+        sig = {
+            "yref_fill_mortons": (None, [vp, vp, u32, vp, vp]),
+            "yref_build_tree": (None, [vp, vp, u32, vp, vp, vp]),
+            "yref_leaves": (None, [vp, vp, u32, vp, vp]),
+            "yref_swept_leaves": (None, [vp, vp, vp, u32, f32, vp, vp]),
+            "yref_bottom_up": (None, [vp, vp, u32, vp]),
+            "yref_query_points": (u32, [vp, u32, vp, vp, u32, f32, u32, u32, vp, u32, vp]),
+            "yref_narrow": (u32, [vp, u32, vp, vp, vp, vp, vp, vp, f32, f32, vp, vp, u32]),
+            "yref_tri_forces": (None, [vp, vp, vp, vp, vp, vp, f32, f32, f32, vp, vp, vp, vp, vp, vp, vp, vp, vp,
+                                       u32]),
+            "yref_integrate_tri": (None, [vp, vp, vp, vp, vp, vp, vp, vp, u32, f32, vp, u32, vp]),
+            "yref_grid_forces": (None, [vp, vp, vp, vp, vp, f32, f32, f32, vp, u32]),
+            "yref_integrate_grid": (None, [vp, vp, vp, vp, vp, vp, vp, vp, u32, f32, vp, u32, vp]),
+            "yref_bucket": (None, [vp, u32, vp, u32, vp, vp, vp]),
+        }
+        for k, (r, a) in sig.items():
+            fn = getattr(L, k)
+            fn.restype = r
+            fn.argtypes = a
+        _lib = L
+    return _lib
+
+
+def P(a):
+    return None if a is None else a.ctypes.data_as(vp)
+
+
+def c32(a, dt=np.float32):
+    return np.ascontiguousarray(a, dt)
+
+
+def fill_mortons(x, F, box6):
+    x, F, box6 = c32(x), c32(F, np.uint32), c32(box6)
+    m = np.zeros((len(F), 2), np.uint32)
+    lib().yref_fill_mortons(P(x), P(F), len(F), P(box6), P(m))
+    return m[:, 0].copy(), m[:, 1].copy()
+
+
+def build_tree(x, F, codes, idx):
+    """buildTree_Tri + zeroVisitCounts + bottomUpBoxes on sorted (code, index)."""
+    x, F = c32(x), c32(F, np.uint32)
+    n = len(F)
+    m = np.ascontiguousarray(np.stack([codes, idx], 1), np.uint32)
+    nodes = np.zeros(2 * n - 1, NODE_DTYPE)
+    parent = np.full(2 * n - 1, -1, np.int32)
+    lib().yref_build_tree(P(x), P(F), n, P(m), P(nodes), P(parent))
+    visits = np.zeros(2 * n - 1, np.uint32)
+    lib().yref_bottom_up(P(nodes), P(parent), n, P(visits))
+    return nodes, parent
+
+
+def refit(nodes, parent, x, v, F, codes, idx, dt, swept):
+    nodes = nodes.copy()
+    x, F = c32(x), c32(F, np.uint32)
+    n = len(F)
+    m = np.ascontiguousarray(np.stack([codes, idx], 1), np.uint32)
+    if swept:
+        lib().yref_swept_leaves(P(x), P(c32(v)), P(F), n, dt, P(m), P(nodes))
+    else:
+        lib().yref_leaves(P(x), P(F), n, P(m), P(nodes))
+    visits = np.zeros(2 * n - 1, np.uint32)
+    lib().yref_bottom_up(P(nodes), P(c32(parent, np.int32)), n, P(visits))
+    return nodes
+
+
+def query_points(qx, F, nodes, margin, qobj, tobj, cap=None):
+    qx, F = c32(qx), c32(F, np.uint32)
+    cap = cap or max(64, len(qx) * 64)
+    rows = np.zeros(cap, ROW_DTYPE)
+    flags = np.zeros(2, np.uint32)
+    n = lib().yref_query_points(P(qx), len(qx), P(F), P(nodes), len(nodes), margin, qobj, tobj, P(rows), cap,
+                                P(flags))
+    return rows[: min(n, cap)], n, flags
+
+
+def narrow(rows, x, voff, F, foff, vaf, vaf_off, radius, thickness, xprev, cap=None):
+    cap = cap or max(64, len(rows))
+    out = np.zeros(cap, CONTACT_DTYPE)
+    n = lib().yref_narrow(P(np.ascontiguousarray(rows)), len(rows), P(c32(x)), P(c32(voff, np.uint32)),
+                          P(c32(F, np.uint32)), P(c32(foff, np.uint32)), P(c32(vaf, np.uint32)),
+                          P(c32(vaf_off, np.uint32)), radius, thickness, P(c32(xprev)), P(out), cap)
+    return out[: min(n, cap)]
+
+
+def tri_forces(x, v, ext, mass3, mask, subh, kair, kd, cp4, adj, F):
+    x, v = c32(x), c32(v)
+    f = np.zeros_like(x)
+    lib().yref_tri_forces(P(x), P(v), P(f), P(c32(mass3)), P(c32(mask)), P(c32(ext)), subh, kair, kd,
+                          P(c32(cp4)), P(c32(adj["edges"], np.uint32)), P(c32(F, np.uint32)),
+                          P(c32(adj["vae"], np.uint32)), P(c32(adj["vae_off"], np.uint32)), P(c32(adj["rest_edge"])),
+                          P(c32(adj["opp"], np.uint32)), P(c32(adj["opp_off"], np.uint32)), P(c32(adj["rest_opp"])),
+                          len(x))
+    return f
+
+
+def grid_params(P1, rest6, k3, thickness):
+    a = np.zeros(11, np.uint32)
+    a[0] = P1
+    a[1:7] = np.asarray(rest6, np.float32).view(np.uint32)
+    a[7:10] = np.asarray(k3, np.float32).view(np.uint32)
+    a[10] = np.asarray([thickness], np.float32).view(np.uint32)[0]
+    return a
+
+
+def grid_forces(x, v, ext, mass3, subh, kair, kd, gp11):
+    x, v = c32(x), c32(v)
+    f = np.zeros_like(x)
+    lib().yref_grid_forces(P(x), P(v), P(f), P(c32(mass3)), P(c32(ext)), subh, kair, kd, P(c32(gp11, np.uint32)),
+                           len(x))
+    return f
+
+
+def integrate(kind, x, v, f, mass3, mask, csr, csr_off, voff, oid, subh, params):
+    x, v = c32(x).copy(), c32(v).copy()
+    an = np.zeros(1, np.uint32)
+    fn = lib().yref_integrate_tri if kind == "tri" else lib().yref_integrate_grid
+    fn(P(x), P(v), P(c32(f)), P(c32(mass3)), P(c32(mask)), P(np.ascontiguousarray(csr)), P(c32(csr_off, np.uint32)),
+       P(c32(voff, np.uint32)), oid, subh, P(c32(params, np.float32 if kind == "tri" else np.uint32)), len(x), P(an))
+    return x, v, int(an[0])

@@ -1,0 +1,129 @@
+"""Generate the golden vectors in tests/golden/ from the reference's own kernels.
+
+    python tests/golden/make_golden.py
+
+Needs the reference checkout (oracle/_ref is built from it by
+oracle/build_ref.py); the fixtures it writes are committed so that the tests
+can check the CUDA path and the oracle against reference outputs on machines
+without the reference.  Inputs are seeded synthetic data of this repository's
+generators; outputs are the reference kernels' results:
+  morton_tree.npz -- fillMortons_Tri codes, stable sort, buildTree_Tri topology,
+                     bottomUpBoxes boxes, buildSweptLeaf_Tri refit, queryPoints
+                     pairs (inclusive AABB test, h = 1e-3 and a self query);
+  substep_*.npz   -- one mid-drape substep of a small scene: broad rows (the
+                     oracle's), narrow_pt_tri contacts, the cloth's spring
+                     forces and integrate_cloth(_grid) positions / velocities.
+"""
+from __future__ import annotations
+
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+from oracle import oracle as O  # noqa: E402
+from oracle import refkernels as R  # noqa: E402
+from ysim_b200 import generators as G  # noqa: E402
+
+
+def canon(p):
+    p = np.asarray(p, np.uint32).reshape(-1, 2)
+    return p[np.lexsort((p[:, 1], p[:, 0]))] if len(p) else p
+
+
+def morton_tree():
+    out = {}
+    for name, (x, f, q) in {"soup": G.soup(2000, seed=41),
+                            "grid": G.grid_cloth(24, 1.0, (0.0, 0.2, 0.0)) + (None,)}.items():
+        if q is None:
+            rng = np.random.default_rng(42)
+            x = (x + rng.uniform(-1e-3, 1e-3, x.shape)).astype(np.float32)
+            q = x.copy()
+        box = np.zeros(6, np.float32)
+        O.lib().yso_scene_box(O.P(x), len(x), O.P(box))
+        codes, idx = R.fill_mortons(x, f, box)
+        o = np.argsort(codes, kind="stable")
+        codes, idx = codes[o], idx[o]
+        nodes, parent = R.build_tree(x, f, codes, idx)
+        v = np.random.default_rng(43).normal(0, 0.5, x.shape).astype(np.float32)
+        swept = R.refit(nodes, parent, x, v, f, codes, idx, np.float32(1.0 / 1200.0), True)
+        self_q = name == "grid"
+        margin = np.float32(0.03 if self_q else 0.02)
+        rows, n, _ = R.query_points(q, f, swept, margin, 0, 0 if self_q else 1)
+        out.update({f"{name}_x": x, f"{name}_f": f, f"{name}_q": q, f"{name}_v": v, f"{name}_box": box,
+                    f"{name}_codes": codes, f"{name}_idx": idx, f"{name}_a": nodes["a"], f"{name}_b": nodes["b"],
+                    f"{name}_mn": nodes["mn"], f"{name}_mx": nodes["mx"], f"{name}_parent": parent,
+                    f"{name}_swept_mn": swept["mn"], f"{name}_swept_mx": swept["mx"], f"{name}_margin": margin,
+                    f"{name}_self": np.int32(self_q),
+                    f"{name}_pairs": canon(np.stack([rows["point"], rows["tri"]], 1))})
+    np.savez_compressed(os.path.join(HERE, "morton_tree.npz"), **out)
+
+
+SPECS = {
+    "c1": lambda: G.config_c1(P=24, level=2, height=0.2999),
+    "c2hash": lambda: G.config_c2(P=32, level=3, height=0.315),
+}
+
+
+def substep(name):
+    spec = SPECS[name]()
+    o = O.OracleScene(spec)
+    o.step(3 * spec.params.substeps + 1)
+    o.stage(0); o.stage(1); o.stage(2)
+    x, xp, v = o.get("x"), o.get("xprev"), o.get("v")
+    rows = o.rows()
+    p = spec.params
+    voff, foff, F, vaf, vaf_off = [0], [0], [], [], [0]
+    for m in spec.meshes:
+        a = O.adjacency(m.x, m.facets)
+        vaf_off += list(vaf_off[-1] + a["vaf_off"][1:])
+        vaf.append(a["vaf"])
+        F.append(m.facets.reshape(-1))
+        voff.append(voff[-1] + m.nV)
+        foff.append(foff[-1] + m.nF)
+    voff = np.array(voff, np.uint32)
+    rc = R.narrow(rows, x, voff, np.concatenate(F).astype(np.uint32), np.array(foff, np.uint32),
+                  np.concatenate(vaf).astype(np.uint32), np.array(vaf_off, np.uint32), np.float32(p.radius),
+                  np.float32(p.margin), xp)
+    rc = rc[np.lexsort((rc["tri"], rc["tobj"], rc["point"], rc["qobj"]))]
+    # canonical per-vertex CSR of the reference contacts
+    nV = spec.nV
+    g = voff[rc["qobj"]] + rc["point"]
+    off = np.zeros(nV + 1, np.uint32)
+    np.add.at(off, g + 1, 1)
+    off = np.cumsum(off).astype(np.uint32)
+    m = spec.meshes[0]
+    n0 = m.nV
+    mass3 = np.repeat(m.mass, 3).astype(np.float32)
+    ext = (np.asarray(p.gravity, np.float32)[None, :] * m.mass[:, None]).astype(np.float32)
+    if m.behavior == 0:
+        adj = O.adjacency(m.x, m.facets)
+        prm = np.array([m.kstretch, m.kshear, m.kbend, m.thickness], np.float32)
+        f = R.tri_forces(x[:n0], v[:n0], ext, mass3, m.mask, np.float32(p.subh), np.float32(p.kair),
+                         np.float32(p.kd), prm, adj, m.facets.reshape(-1))
+        kind = "tri"
+    else:
+        prm = R.grid_params(m.grid_n, m.grid_rest, (m.kstretch, m.kshear, m.kbend), m.thickness)
+        f = R.grid_forces(x[:n0], v[:n0], ext, mass3, np.float32(p.subh), np.float32(p.kair), np.float32(p.kd), prm)
+        kind = "grid"
+    xn, vn, anomaly = R.integrate(kind, x[:n0], v[:n0], f, mass3, m.mask, rc, off, voff, 0, np.float32(p.subh), prm)
+    rws = np.stack([rows["qobj"], rows["point"], rows["tobj"], rows["tri"]], 1).astype(np.uint32)
+    rws = rws[np.lexsort((rws[:, 3], rws[:, 2], rws[:, 1], rws[:, 0]))]
+    np.savez_compressed(os.path.join(HERE, f"substep_{name}.npz"), x=x, xprev=xp, v=v, rows=rws,
+                        c_point=rc["point"], c_tri=rc["tri"], c_qobj=rc["qobj"], c_tobj=rc["tobj"], c_n=rc["n"],
+                        c_d=rc["d"], csr_off=off, f=f, x_next=xn, v_next=vn, anomaly=np.int32(anomaly))
+
+
+if __name__ == "__main__":
+    if not R.available():
+        sys.exit("reference checkout absent: cannot regenerate golden vectors")
+    morton_tree()
+    for k in SPECS:
+        substep(k)
+    for fn in sorted(os.listdir(HERE)):
+        if fn.endswith(".npz"):
+            print(fn, os.path.getsize(os.path.join(HERE, fn)))
