@@ -84,6 +84,25 @@ def workload_config(args, spec, extra=None):
     return cfg
 
 
+# ------------------------------------------------------------------ ranks
+def max_over_ranks(ms: float, world: int, device=None) -> float:
+    """Slowest rank's time (the timed region is bracketed by barriers on every
+    rank; replicas do no data-path collective)."""
+    if world <= 1:
+        return ms
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([ms], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def aggregate(ms: float, steps: int, world: int, device=None):
+    """Whole-job substeps/s: every rank ran `steps` substeps of its own replica."""
+    slow = max_over_ranks(ms, world, device)
+    return world * steps / (slow / 1000.0), slow
+
+
 # ------------------------------------------------------------------ clocks
 class ClockSampler:
     QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
@@ -174,44 +193,61 @@ def cpu_baseline(spec, state, nsub, threads=None):
     if threads:
         O.set_threads(threads)
     cores = O.max_threads()
-    o = O.OracleScene(spec)
-    o.set("x", state["x"]); o.set("v", state["v"]); o.set("xprev", state["xprev"])
+    o, kind = reference_scene(spec)
+    if kind == "reference":
+        o.x, o.v, o.xp = state["x"].copy(), state["v"].copy(), state["xprev"].copy()
+    else:
+        o.set("x", state["x"]); o.set("v", state["v"]); o.set("xprev", state["xprev"])
     o.step(1)  # frame-0 preamble rebuild, untimed
     t0 = time.perf_counter()
     o.step(nsub)
     dt = time.perf_counter() - t0
-    return nsub / dt, cores, dt
+    return nsub / dt, cores, dt, kind
+
+
+def reference_scene(spec):
+    """The reference's own kernels on the host (oracle/_ref) when they were
+    built from the reference checkout, else the pinned CPU restatement."""
+    from oracle import oracle as O
+    try:
+        from oracle import refkernels
+        if refkernels.available():
+            refkernels.lib()
+            from oracle.refdriver import RefScene
+            return RefScene(spec), "reference"
+    except (OSError, FileNotFoundError, RuntimeError):
+        pass
+    return O.OracleScene(spec), "port"
 
 
 def run_reference(args, rank, world):
-    """Reference arm: the CPU implementation of the path on the host cores."""
+    """Reference arm: the path's CPU implementation on the host cores, all
+    threads (OpenMP), on this arm's config.  Rank 0 alone works."""
     if rank != 0:
         return
-    from ysim_b200 import generators as G  # noqa: F401
     from oracle import oracle as O
     spec = spec_for(args)
-    o = O.OracleScene(spec)
+    scene, kind = reference_scene(spec)
     cores = O.max_threads()
-    # drop the cloth onto the obstacle exactly as the GPU arm does (pre-roll is
-    # untimed on both arms), but bounded: a scaled pre-roll keeps the run short
-    pre = min(args.preroll, 4)
-    o.step(max(pre, 1))
-    for _ in range(min(args.warmup, 1)):
-        o.step(1)
+    scene.step(1)  # frame-0 preamble (tree build), untimed
+    warm = min(max(args.warmup, 0), 1)
+    scene.step(warm)
     nsteps = max(1, min(args.steps, args.cpu_substeps))
     t0 = time.perf_counter()
-    o.step(nsteps)
+    scene.step(nsteps)
     dt = time.perf_counter() - t0
     v = nsteps / dt
-    kind = "port"
     line = {
         "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world, "steps": nsteps,
-        "warmup": min(args.warmup, 1), "ms_per_step": 1000.0 * dt / nsteps, "higher_is_better": True,
+        "warmup": warm, "ms_per_step": 1000.0 * dt / nsteps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
-        "config": workload_config(args, spec, {"parallelism": "single process, OpenMP over host cores"}),
+        "config": workload_config(args, spec, {"parallelism": "host cores, OpenMP over kernel thread ids"}),
         "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": kind,
-                         "sample": f"{nsteps} substeps of the full workload after a {max(pre, 1)}-substep pre-roll "
-                                   "(bounded sample; the GPU arm times its substeps after a longer pre-roll)"},
+                         "sample": f"{nsteps} substeps of the full workload after the frame-0 build and {warm} "
+                                   "warm-up substep(s); the reference's Metal kernels compiled for the host "
+                                   "(oracle/_ref) with the pinned CPU-hash restatement for self rows"
+                                   if kind == "reference" else
+                                   f"{nsteps} substeps of the full workload (CPU restatement, OpenMP)"},
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -263,11 +299,7 @@ def run_ours(args, rank, world, local):
     _lib_check(lib.ys_scene_set_timing(scene.h, 0), "set_timing")
     after = scene.totals()
     st = scene.stats()
-    if world > 1:
-        t = torch.tensor([ms], device=f"cuda:{local}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-    value = world * args.steps / (ms / 1000.0)
+    value, ms = aggregate(ms, args.steps, world, device=f"cuda:{local}")
     rows_ps = (after[0] - before[0]) / args.steps
     cont_ps = (after[1] - before[1]) / args.steps
 
@@ -295,11 +327,7 @@ def run_ours(args, rank, world, local):
     scene.sync()
     torch.cuda.synchronize()
     e2e_ms = e0.elapsed_time(e1)
-    if world > 1:
-        t = torch.tensor([e2e_ms], device=f"cuda:{local}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
-    e2e_val = world * args.e2e_frames * nsub / (e2e_ms / 1000.0)
+    e2e_val, e2e_ms = aggregate(e2e_ms, args.e2e_frames * nsub, world, device=f"cuda:{local}")
     assert np.isfinite(xout.numpy()).all()
 
     # ---- roofline of the dominant kernel
@@ -317,10 +345,12 @@ def run_ours(args, rank, world, local):
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
         state = {"x": scene.get("x"), "v": scene.get("v"), "xprev": scene.get("xprev")}
-        v_cpu, cores, dt = cpu_baseline(spec, state, args.cpu_substeps)
-        cpu = {"value": v_cpu, "unit": UNIT, "cores": cores, "kind": "port",
+        v_cpu, cores, dt, kind = cpu_baseline(spec, state, args.cpu_substeps)
+        cpu = {"value": v_cpu, "unit": UNIT, "cores": cores, "kind": kind,
                "sample": f"{args.cpu_substeps} substeps of the full workload from the GPU run's state "
-                         f"({dt:.1f} s, CPU oracle, OpenMP)"}
+                         f"({dt:.1f} s on {cores} threads; "
+                         + ("reference Metal kernels compiled for the host + pinned CPU-hash restatement)"
+                            if kind == "reference" else "CPU restatement)")}
 
     launches = int(kt[1] + kt[3])
     if rank == 0:

@@ -25,3 +25,20 @@ def rel_err(a, b) -> float:
     b = np.asarray(b, np.float64)
     scale = max(np.abs(b).max(), 1e-30)
     return float(np.abs(a - b).max() / scale) if a.size else 0.0
+
+
+def reachable(nodes) -> np.ndarray:
+    """Mask of the nodes a traversal from the root can reach (runs of three or
+    more equal Morton codes leave unclaimed subtrees in the reference's
+    topology; their boxes are never read)."""
+    n = (len(nodes) + 1) // 2
+    seen = np.zeros(len(nodes), bool)
+    stack = [0]
+    while stack:
+        i = stack.pop()
+        if seen[i]:
+            continue
+        seen[i] = True
+        if nodes["a"][i] >= 0 and i < n - 1:
+            stack += [int(nodes["a"][i]), int(nodes["b"][i])]
+    return seen

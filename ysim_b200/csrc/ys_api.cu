@@ -41,6 +41,7 @@ struct ys_lbvh {
     u32 maxPrims = 0, n = 0;
     Node* nodes = nullptr;
     i32* parent = nullptr;
+    i32* parent2 = nullptr;
     u32 *codes = nullptr, *idx = nullptr, *visits = nullptr, *box = nullptr, *status = nullptr;
     void* scratch = nullptr;
     RefitJob* job = nullptr;
@@ -66,6 +67,7 @@ ys_status ys_lbvh_create(ys_lbvh** out, uint32_t maxPrims, int device, void* str
     cudaError_t e = cudaSuccess;
     if (e == cudaSuccess) e = cudaMalloc((void**)&t->nodes, nn * sizeof(Node));
     if (e == cudaSuccess) e = cudaMalloc((void**)&t->parent, nn * 4);
+    if (e == cudaSuccess) e = cudaMalloc((void**)&t->parent2, nn * 4);
     if (e == cudaSuccess) e = cudaMalloc((void**)&t->codes, (size_t)maxPrims * 4);
     if (e == cudaSuccess) e = cudaMalloc((void**)&t->idx, (size_t)maxPrims * 4);
     if (e == cudaSuccess) e = cudaMalloc((void**)&t->visits, (size_t)maxPrims * 4);
@@ -86,7 +88,7 @@ ys_status ys_lbvh_destroy(ys_lbvh* t) {
     if (!t) return YS_OK;
     cudaSetDevice(t->device);
     cudaStreamSynchronize(t->stream);
-    cudaFree(t->nodes); cudaFree(t->parent); cudaFree(t->codes); cudaFree(t->idx); cudaFree(t->visits);
+    cudaFree(t->nodes); cudaFree(t->parent); cudaFree(t->parent2); cudaFree(t->codes); cudaFree(t->idx); cudaFree(t->visits);
     cudaFree(t->box); cudaFree(t->status); cudaFree(t->scratch); cudaFree(t->job);
     delete t;
     return YS_OK;
@@ -95,7 +97,7 @@ ys_status ys_lbvh_destroy(ys_lbvh* t) {
 static ys_status run_refit(ys_lbvh* t, const float* x, const float* v, float dt, int swept) {
     RefitJob J;
     memset(&J, 0, sizeof(J));
-    J.nodes = t->nodes; J.parent = t->parent; J.visits = t->visits; J.facets = t->facets;
+    J.nodes = t->nodes; J.parent = t->parent; J.parent2 = t->parent2; J.visits = t->visits; J.facets = t->facets;
     J.x3 = x; J.v3 = v; J.voff = 0; J.n = t->n; J.leafBase = 0; J.dt = dt; J.swept = swept ? 1u : 0u;
     J.selfMargin = 0.f; J.maxExt = t->box;
     YS_CK2(cudaMemcpyAsync(t->job, &J, sizeof(J), cudaMemcpyHostToDevice, t->stream));
@@ -114,7 +116,7 @@ ys_status ys_lbvh_build(ys_lbvh* t, const float* x, uint32_t nV, const uint32_t*
     launch_box(nullptr, x, 0, nV, t->box, t->stream);
     launch_morton(nullptr, x, 0, F, nF, t->box, t->codes, t->idx, t->stream);
     YS_CK2(radix_sort_pairs(t->codes, t->idx, nF, t->scratch, 0, 32, t->stream));
-    launch_karras(t->codes, t->idx, nF, t->nodes, t->parent, t->visits, t->stream);
+    launch_karras(t->codes, t->idx, nF, t->nodes, t->parent, t->parent2, t->visits, t->stream);
     YS_CK2(cudaGetLastError());
     return run_refit(t, x, nullptr, 0.f, 0);
 }

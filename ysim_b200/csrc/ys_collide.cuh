@@ -7,7 +7,11 @@
 namespace ys {
 
 static constexpr int STACK_DEPTH = 64;          // queryAABB stack (bvh.metal:1333)
-static constexpr u32 VISIT_CAP = 1u << 22;      // queryAABB visit cap (bvh.metal:1352)
+// Visit cap of one descent.  The reference's wedge guard allows 2^22
+// (bvh.metal:1352); a healthy query here visits a few hundred nodes, and a
+// descent that reaches 2^16 is reported (YS_FLAG_STACK_OVF) and stopped so a
+// degenerate tree cannot keep a kernel busy for minutes.
+static constexpr u32 VISIT_CAP = 1u << 16;
 
 // intersectAABB (bvh.metal:1285-1290): inclusive box overlap.
 __device__ __forceinline__ bool overlap(f3 qmn, f3 qmx, float4 n0, float4 n1) {

@@ -107,16 +107,20 @@ struct KarrasView {
     }
 };
 
+__global__ void k_parent_init(i32* __restrict__ parent, i32* __restrict__ parent2, u32 numNodes) {
+    u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < numNodes) { parent[i] = -1; parent2[i] = 0x7FFFFFFF; }
+}
+
 __global__ void __launch_bounds__(256) k_karras(const u32* __restrict__ codes, const u32* __restrict__ idx, u32 n,
                                                 Node* __restrict__ nodes, i32* __restrict__ parent,
-                                                u32* __restrict__ visits) {
+                                                i32* __restrict__ parent2, u32* __restrict__ visits) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= (int)n) return;
     KarrasView K{codes, idx, (int)n};
     Node* L = nodes + (n - 1 + i);
     L->a = -1;
     L->b = (i32)idx[i];
-    if (i == 0) parent[0] = -1;
     if (i + 1 >= (int)n) return;
     visits[i] = 0;
     int d = (K.delta(i, i + 1) - K.delta(i, i - 1) >= 0) ? 1 : -1;
@@ -148,13 +152,17 @@ __global__ void __launch_bounds__(256) k_karras(const u32* __restrict__ codes, c
     int cb = (s + 1 == last) ? s + (int)n : s + 1;
     nodes[i].a = ca;
     nodes[i].b = cb;
-    parent[ca] = i;
-    parent[cb] = i;
+    atomicMax(&parent[ca], i);
+    atomicMin(&parent2[ca], i);
+    atomicMax(&parent[cb], i);
+    atomicMin(&parent2[cb], i);
 }
 
-void launch_karras(const u32* codes, const u32* idx, u32 n, Node* nodes, i32* parent, u32* visits, cudaStream_t s) {
+void launch_karras(const u32* codes, const u32* idx, u32 n, Node* nodes, i32* parent, i32* parent2, u32* visits,
+                   cudaStream_t s) {
     if (n == 0) return;
-    k_karras<<<ceil_div(n, 256), 256, 0, s>>>(codes, idx, n, nodes, parent, visits);
+    k_parent_init<<<ceil_div(2 * n - 1, 256), 256, 0, s>>>(parent, parent2, 2 * n - 1);
+    k_karras<<<ceil_div(n, 256), 256, 0, s>>>(codes, idx, n, nodes, parent, parent2, visits);
 }
 
 // ------------------------------------------------------------------ refit
@@ -162,8 +170,9 @@ void launch_karras(const u32* codes, const u32* idx, u32 n, Node* nodes, i32* pa
 // (bvh.metal:510-586).  One thread per leaf writes its box, then climbs: the
 // first thread to arrive at a parent stops, the second combines both children
 // and continues.  Arrival counters are never reset between refits: every
-// internal node receives exactly two arrivals per refit, so an even old value
-// means "first", odd means "second".  Karras zeroes them at build.
+// internal node receives exactly two arrivals per refit (one per child it
+// lists), so an even old value means "first", odd means "second".  Karras
+// zeroes them at build.
 // Memory order: box store -> __threadfence -> atomicAdd (release); atomicAdd
 // -> __threadfence -> L1-bypassing loads of the children (acquire).
 __device__ __forceinline__ void store_box(Node* nd, f3 lo, f3 hi) {
@@ -245,35 +254,51 @@ __global__ void __launch_bounds__(256) k_refit(const RefitJob* __restrict__ jobs
     }
     store_box(&nodes[leaf], lo, hi);
     if (n == 1) return;
-    const u32 numNodes = 2 * n - 1;
+    const u32 numInner = n - 1;
+    // Climb: deliver this node's arrival to every internal node that claims
+    // it as a child (one claimant in a consistent tree); the second arrival
+    // at a claimant combines it and climbs on from there.  Extra climbs (a
+    // node with two claimants) wait in a small pending list.
+    u32 pending[4];
+    int np = 0;
     u32 child = leaf;
     __threadfence();
     for (u32 step = 0; step < 2 * n; ++step) {
-        i32 par = __ldcg(&J.parent[child]);
-        if (par < 0 || (u32)par >= numNodes || (u32)par >= n - 1) {
-            if (par != -1 || child != 0) atomicOr(status, ST_ITER_CAP);
-            return;
+        const i32 p1 = __ldcg(&J.parent[child]);
+        const i32 p2 = __ldcg(&J.parent2[child]);
+        i32 claim[2] = {p1, (p2 != p1 && p2 != 0x7FFFFFFF) ? p2 : -1};
+        i32 next = -1;
+#pragma unroll
+        for (int c = 0; c < 2; ++c) {
+            const i32 par = claim[c];
+            if (par < 0) continue;
+            if ((u32)par >= numInner) { atomicOr(status, ST_ITER_CAP); continue; }
+            u32 old = atomicAdd(&J.visits[par], 1u);
+            if ((old & 1u) == 0u) continue;  // first arrival: the sibling's thread combines
+            __threadfence();
+            const float4* pn = reinterpret_cast<const float4*>(&nodes[par]);
+            const float4 h0 = __ldcg(pn), h1 = __ldcg(pn + 1);
+            const i32 ca = __float_as_int(h0.w), cb = __float_as_int(h1.w);
+            if (ca < 0 || (u32)ca >= 2 * n - 1 || cb < 0 || (u32)cb >= 2 * n - 1) {
+                atomicOr(status, ST_ITER_CAP);
+                continue;
+            }
+            const float4* A = reinterpret_cast<const float4*>(&nodes[ca]);
+            const float4* B = reinterpret_cast<const float4*>(&nodes[cb]);
+            float4 a0 = __ldcg(A), a1 = __ldcg(A + 1), b0 = __ldcg(B), b1 = __ldcg(B + 1);
+            f3 plo = vmin(mk(a0.x, a0.y, a0.z), mk(b0.x, b0.y, b0.z));
+            f3 phi = vmax(mk(a1.x, a1.y, a1.z), mk(b1.x, b1.y, b1.z));
+            store_box(&nodes[par], plo, phi);
+            __threadfence();
+            if (next < 0) next = par;
+            else if (np < 4) pending[np++] = (u32)par;
+            else atomicOr(status, ST_ITER_CAP);
         }
-        u32 old = atomicAdd(&J.visits[par], 1u);
-        if ((old & 1u) == 0u) return;  // first arrival
-        __threadfence();
-        const float4* pn = reinterpret_cast<const float4*>(&nodes[par]);
-        float4 hdr = __ldcg(pn + 1);
-        i32 ca = __ldcg(&nodes[par].a);
-        i32 cb = __float_as_int(hdr.w);
-        if (ca < 0 || (u32)ca >= numNodes || cb < 0 || (u32)cb >= numNodes) {
-            atomicOr(status, ST_ITER_CAP);
-            return;
+        if (next < 0) {
+            if (np == 0) return;  // root reached, first arrival, or an unclaimed node
+            next = (i32)pending[--np];
         }
-        const float4* A = reinterpret_cast<const float4*>(&nodes[ca]);
-        const float4* B = reinterpret_cast<const float4*>(&nodes[cb]);
-        float4 a0 = __ldcg(A), a1 = __ldcg(A + 1), b0 = __ldcg(B), b1 = __ldcg(B + 1);
-        f3 plo = vmin(mk(a0.x, a0.y, a0.z), mk(b0.x, b0.y, b0.z));
-        f3 phi = vmax(mk(a1.x, a1.y, a1.z), mk(b1.x, b1.y, b1.z));
-        store_box(&nodes[par], plo, phi);
-        __threadfence();
-        child = (u32)par;
-        if (child == 0) return;
+        child = (u32)next;
     }
     atomicOr(status, ST_ITER_CAP);
 }

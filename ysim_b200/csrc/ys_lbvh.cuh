@@ -12,7 +12,8 @@ namespace ys {
 // packed float3 (reference layout) depending on which pointer is set.
 struct RefitJob {
     Node* nodes;            // 2N-1 nodes
-    const i32* parent;      // 2N-1 parents (root -1)
+    const i32* parent;      // 2N-1: largest internal node claiming the node as a child (-1: none)
+    const i32* parent2;     // 2N-1: smallest claimant (== parent when one claimant, INT_MAX when none)
     u32* visits;            // N-1 per-internal-node arrival counters
     const u32* facets;      // 3 local vertex ids per face (packed)
     const float4* x4;       // positions (float4) or nullptr
@@ -36,7 +37,14 @@ void launch_box(const float4* x4, const float* x3, u32 voff, u32 nV, u32* box, c
 void launch_morton(const float4* x4, const float* x3, u32 voff, const u32* facets, u32 nF, const u32* box, u32* codes,
                    u32* idx, cudaStream_t s);
 // Karras topology (buildTree_Tri, bvh.metal:352-393); zeroes visit counters.
-void launch_karras(const u32* codes, const u32* idx, u32 n, Node* nodes, i32* parent, u32* visits, cudaStream_t s);
+// Runs of three or more equal Morton codes make the reference's topology
+// inconsistent (findSplit splits them at the midpoint, bvh.metal:204, while
+// determineRange orders them by index): a node can then be claimed as a child
+// by two internal nodes, or by none.  Child arrays stay exactly the
+// reference's; parent keeps the largest claimant (what a serial build loop
+// leaves behind) and parent2 the smallest, so the refit reaches every claimant.
+void launch_karras(const u32* codes, const u32* idx, u32 n, Node* nodes, i32* parent, i32* parent2, u32* visits,
+                   cudaStream_t s);
 // Leaves + bottom-up for every job (jobs in device memory, jobsHost mirrors
 // them for the launch size).
 void launch_refit(const RefitJob* jobsDev, u32 numJobs, u32 totalLeaves, u32* status, cudaStream_t s);

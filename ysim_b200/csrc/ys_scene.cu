@@ -474,7 +474,7 @@ struct ys_scene {
     DBuf<uint4> F4;
     DBuf<u32> F3;  // packed facets (3 per face) for the refit kernel
     DBuf<Node> nodes;
-    DBuf<i32> parent;
+    DBuf<i32> parent, parent2;
     DBuf<MeshDev> dmeshes;
     DBuf<RefitJob> jobs;            // 6 tables (cur x cv) of njobs, then one build slot
     std::vector<RefitJob> hjobs;
@@ -575,11 +575,13 @@ ys_status build_tree(ys_scene* s, HostMesh& H) {
     launch_box(s->X[s->cur].p, nullptr, H.voff, H.d.num_vertices, s->box.p, st);
     launch_morton(s->X[s->cur].p, nullptr, H.voff, s->F3.p + 3 * (size_t)H.foff, n, s->box.p, codes, idx, st);
     YS_CK(radix_sort_pairs(codes, idx, n, s->sortScratch.p, 0, 32, st));
-    launch_karras(codes, idx, n, s->nodes.p + H.node_off, s->parent.p + H.node_off, s->visits.p + H.foff, st);
+    launch_karras(codes, idx, n, s->nodes.p + H.node_off, s->parent.p + H.node_off, s->parent2.p + H.node_off,
+                  s->visits.p + H.foff, st);
     RefitJob J;
     memset(&J, 0, sizeof(J));
     J.nodes = s->nodes.p + H.node_off;
     J.parent = s->parent.p + H.node_off;
+    J.parent2 = s->parent2.p + H.node_off;
     J.visits = s->visits.p + H.foff;
     J.facets = s->F3.p + 3 * (size_t)H.foff;
     J.x4 = s->X[s->cur].p;
@@ -767,7 +769,7 @@ ys_status ys_scene_destroy(ys_scene* s) {
     s->Fbuf.free(); s->mass.free(); s->mask.free(); s->vobj.free(); s->targets.free(); s->spr_off.free();
     s->spr_split.free(); s->spr_nbr.free(); s->vaf_off.free(); s->vaf.free(); s->maxext.free(); s->status.free();
     s->codes.free(); s->idx.free(); s->visits.free(); s->box.free(); s->spr_rest.free(); s->scratch3.free(); s->F4.free(); s->F3.free();
-    s->nodes.free(); s->parent.free(); s->dmeshes.free(); s->jobs.free(); s->counters.free(); s->sortScratch.free();
+    s->nodes.free(); s->parent.free(); s->parent2.free(); s->dmeshes.free(); s->jobs.free(); s->counters.free(); s->sortScratch.free();
     s->scanScratch.free(); s->rows.free(); s->contacts.free(); s->csr.free(); s->pool.free(); s->bucket.free();
     s->csr_off.free(); s->vstart.free(); s->vcount.free(); s->ext.free();
     for (auto e : s->evPool) cudaEventDestroy(e);
@@ -893,6 +895,7 @@ ys_status ys_scene_pack(ys_scene* s) {
     YS_CK(s->codes.alloc(std::max(nF, 1u))); YS_CK(s->idx.alloc(std::max(nF, 1u))); YS_CK(s->visits.alloc(std::max(nF, 1u)));
     YS_CK(s->F4.alloc(std::max(nF, 1u))); YS_CK(s->F3.alloc(3 * (size_t)std::max(nF, 1u)));
     YS_CK(s->nodes.alloc(std::max(nNodes, 1u))); YS_CK(s->parent.alloc(std::max(nNodes, 1u)));
+    YS_CK(s->parent2.alloc(std::max(nNodes, 1u)));
     YS_CK(s->dmeshes.alloc(md.size())); YS_CK(s->jobs.alloc(6 * s->meshes.size() + 1));
     YS_CK(s->counters.alloc(8));
     YS_CK(s->sortScratch.alloc(sort_scratch_bytes(maxF)));
@@ -940,6 +943,7 @@ ys_status ys_scene_pack(ys_scene* s) {
         memset(&J, 0, sizeof(J));
         J.nodes = s->nodes.p + H.node_off;
         J.parent = s->parent.p + H.node_off;
+        J.parent2 = s->parent2.p + H.node_off;
         J.visits = s->visits.p + H.foff;
         J.facets = s->F3.p + 3 * (size_t)H.foff;
         J.voff = H.voff;
