@@ -52,6 +52,9 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--seed", type=int, default=2)
     ap.add_argument("--P", type=int, default=512)
+    ap.add_argument("--workload", choices=["cloth", "collide"], default="cloth",
+                    help="cloth: the headline substep benchmark; collide: the LBVH / spatial-hash microbenchmark")
+    ap.add_argument("--sizes", default="1000000,4000000,16000000")
     return ap.parse_args()
 
 
@@ -267,7 +270,18 @@ def run_ours(args, rank, world, local):
     stream = torch.cuda.ExternalStream(scene.stream(), device=local)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{local}")
 
-    scene.step(args.preroll)
+    # pre-roll frame by frame so a scene that goes unstable stops the run early
+    done = 0
+    while done < args.preroll:
+        n = min(spec.params.substeps, args.preroll - done)
+        scene.step(n)
+        done += n
+        st0 = scene.stats()
+        if st0["flags"] & 1:
+            if rank == 0:
+                print(json.dumps({"metric": METRIC, "error": f"scene went non-finite during pre-roll at substep {done}",
+                                  "stats": st0}), flush=True)
+            sys.exit(3)
     scene.step(max(args.warmup, 3))
     scene.sync()
     scene.clear_flags()
@@ -378,9 +392,83 @@ def run_ours(args, rank, world, local):
         dist.destroy_process_group()
 
 
+# ------------------------------------------------------------------ collide
+def run_collide(args):
+    """Collision microbenchmark: N triangles (centroids U[0,1]^3, vertex
+    offsets N(0, sigma^2), sigma log-normal around 1e-3) and N query points;
+    LBVH build + refit + point query within h = 1e-3 against the spatial-hash
+    broad phase (cell 2h).  Device-timed with CUDA events; the two candidate
+    sets are checked for equality on the device.  One JSON line per N."""
+    import ctypes as C
+    import torch
+    from ysim_b200 import _lib, generators as G
+    lib = _lib.load()
+    torch.cuda.set_device(0)
+    h = np.float32(1e-3)
+
+    def dev(a):
+        return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+
+    def P(t):
+        return C.c_void_p(t.data_ptr())
+
+    def timed(fn, reps):
+        ts = []
+        for _ in range(reps):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            a.record()
+            fn()
+            b.record()
+            torch.cuda.synchronize()
+            ts.append(a.elapsed_time(b))
+        return statistics.median(ts)
+
+    for n in [int(v) for v in args.sizes.split(",")]:
+        x, f, q = G.soup(n, seed=3)
+        dx, df, dq = dev(x.reshape(-1)), dev(f.reshape(-1).astype(np.int32)), dev(q.reshape(-1))
+        v = dev(np.random.default_rng(4).normal(0, 0.1, x.shape).astype(np.float32).reshape(-1))
+        cap = 8 * n
+        pairs = torch.empty(2 * cap, dtype=torch.int32, device="cuda")
+        cnt = torch.zeros(1, dtype=torch.int64, device="cuda")
+        t = C.c_void_p()
+        _lib.check(lib.ys_lbvh_create(C.byref(t), n, 0, None), "lbvh_create")
+        reps = max(3, min(args.steps, 10))
+        build_ms = timed(lambda: _lib.check(lib.ys_lbvh_build(t, P(dx), len(x), P(df), n)), reps)
+        refit_ms = timed(lambda: _lib.check(lib.ys_lbvh_refit(t, P(dx), P(v), np.float32(1e-3), 1)), reps)
+        _lib.check(lib.ys_lbvh_build(t, P(dx), len(x), P(df), n))
+        query_ms = timed(lambda: _lib.check(lib.ys_lbvh_query(t, P(dq), len(q), h, 0, P(pairs), cap, P(cnt))), reps)
+        nb = int(cnt.item())
+        key_b = (pairs[0:2 * min(nb, cap):2].long() << 32) | pairs[1:2 * min(nb, cap):2].long()
+        key_b = torch.sort(key_b).values
+        _lib.check(lib.ys_lbvh_destroy(t), "lbvh_destroy")
+        sh = C.c_void_p()
+        _lib.check(lib.ys_shash_create(C.byref(sh), n, 40 * n, 0, None), "shash_create")
+        sh_build_ms = timed(lambda: _lib.check(lib.ys_shash_build(sh, P(dx), P(df), n, np.float32(2 * h))), reps)
+        sh_query_ms = timed(lambda: _lib.check(lib.ys_shash_query(sh, P(dq), len(q), h, P(pairs), cap, P(cnt))), reps)
+        ns = int(cnt.item())
+        ent, big = C.c_uint32(), C.c_uint32()
+        _lib.check(lib.ys_shash_entries(sh, C.byref(ent), C.byref(big)))
+        key_s = (pairs[0:2 * min(ns, cap):2].long() << 32) | pairs[1:2 * min(ns, cap):2].long()
+        key_s = torch.sort(key_s).values
+        same = bool(nb == ns and torch.equal(key_b, key_s))
+        _lib.check(lib.ys_shash_destroy(sh))
+        line = {"workload": "collision microbenchmark", "triangles": n, "queries": n, "h": float(h),
+                "lbvh_build_ms": build_ms, "lbvh_refit_swept_ms": refit_ms, "lbvh_query_ms": query_ms,
+                "shash_build_ms": sh_build_ms, "shash_query_ms": sh_query_ms, "candidates": nb,
+                "shash_entries": ent.value, "shash_oversized": big.value, "candidate_sets_equal": same,
+                "timing": f"CUDA events, median of {reps}; calls include their host-side synchronisation"}
+        print(json.dumps(line), flush=True)
+        del dx, df, dq, v, pairs
+
+
 def main():
     args = parse()
     rank, world, local = dist_env()
+    if args.workload == "collide":
+        if rank == 0:
+            run_collide(args)
+        return
     if args.impl == "reference":
         run_reference(args, rank, world)
         return

@@ -92,6 +92,7 @@ typedef struct ys_mesh_desc {
 
 typedef struct ys_scene ys_scene;
 typedef struct ys_lbvh ys_lbvh;
+typedef struct ys_shash ys_shash;
 
 /* Last error message of the calling thread. */
 const char* ys_last_error(void);
@@ -131,6 +132,9 @@ ys_status ys_scene_step_staged(ys_scene* s, uint32_t n);
 ys_status ys_scene_step(ys_scene* s, uint32_t n);
 /* Record the fused path's per-vertex contacts for inspection (slower). */
 ys_status ys_scene_set_record(ys_scene* s, int record);
+/* Replay each fused substep as a captured CUDA graph (default on; substeps
+ * that rebuild trees, record contacts or time kernels run eagerly). */
+ys_status ys_scene_set_graphs(ys_scene* s, int on);
 ys_status ys_scene_sync(ys_scene* s);
 /* CUDA stream of the scene (cudaStream_t) as void*. */
 ys_status ys_scene_stream(ys_scene* s, void** stream_out);
@@ -190,6 +194,22 @@ ys_status ys_lbvh_query(ys_lbvh* t, const float* d_qx, uint32_t num_queries, flo
 /* Device pointers of the tree arrays (nodes, parents, codes, indices). */
 ys_status ys_lbvh_arrays(ys_lbvh* t, void** nodes, int32_t** parent, uint32_t** codes, uint32_t** idx,
                          uint32_t* num_prims);
+
+/* ---- Uniform-grid spatial-hash broad phase, point vs triangle (the
+ * spatial-hash family of the reference: SpatialHashing<METAL>::detectCollisions,
+ * spatial_hash.hpp:880-960, and CpuSpatialHash, spatial_hash.hpp:1547-2016).
+ * Its candidate set equals ys_lbvh_query's under the same inclusive AABB test.
+ * Device pointers; x packed xyz floats. ------------------------------------ */
+ys_status ys_shash_create(ys_shash** out, uint32_t max_tris, uint32_t max_entries, int device, void* stream);
+ys_status ys_shash_destroy(ys_shash* h);
+/* Bin every triangle's AABB into the grid cells (edge `cell`) it overlaps. */
+ys_status ys_shash_build(ys_shash* h, const float* d_x, const uint32_t* d_facets, uint32_t num_facets, float cell);
+/* (point, triangle) pairs whose boxes [p - margin, p + margin] and triangle
+ * AABB overlap; requires cell >= 2 * margin. */
+ys_status ys_shash_query(ys_shash* h, const float* d_qx, uint32_t num_queries, float margin, uint32_t* d_pairs,
+                         uint64_t cap, unsigned long long* d_count);
+/* Cell entries of the last build and triangles too large for the grid. */
+ys_status ys_shash_entries(ys_shash* h, uint32_t* n_entries, uint32_t* n_oversized);
 
 /* Standalone primitives used by the build. */
 ys_status ys_morton_codes(const float* d_x, uint32_t num_vertices, const uint32_t* d_facets, uint32_t num_facets,

@@ -13,15 +13,15 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 OUT = os.path.join(HERE, "_build", "libysoracle.so")
-SRC = os.path.join(HERE, "ys_oracle.cpp")
+SRCS = [os.path.join(HERE, "ys_oracle.cpp"), os.path.join(HERE, "ys_adjoint_oracle.cpp")]
 
 
 def build(force: bool = False) -> str:
-    if not force and os.path.exists(OUT) and os.path.getmtime(OUT) >= os.path.getmtime(SRC):
+    if not force and os.path.exists(OUT) and all(os.path.getmtime(OUT) >= os.path.getmtime(s) for s in SRCS):
         return OUT
     os.makedirs(os.path.dirname(OUT), exist_ok=True)
     cmd = ["g++", "-O3", "-std=c++17", "-ffp-contract=off", "-fno-fast-math", "-fopenmp", "-fPIC", "-shared",
-           "-o", OUT + ".tmp", SRC]
+           "-o", OUT + ".tmp", *SRCS]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError("oracle build failed:\n" + r.stdout + r.stderr)

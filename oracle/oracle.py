@@ -253,3 +253,55 @@ class OracleScene:
         idx = np.zeros(n, np.uint32)
         lib().yso_scene_tree(self.h, mesh, P(nodes), P(parent), P(codes), P(idx))
         return nodes, parent, codes, idx
+
+
+# ---------------------------------------------------------------- adjoint (FP64)
+class Rollout:
+    """FP64 CPU reference of the differentiable FastGridCloth rollout
+    (ys_adjoint_oracle.cpp): forward substeps and the hand-derived adjoint."""
+
+    def __init__(self, spec, k, L, v0=None):
+        d = ctypes_double = C.c_double
+        L_ = lib()
+        for name, res, args in [("yso_roll_new", vp, [vp, vp, vp, vp, vp, vp, vp, vp]),
+                                ("yso_roll_free", None, [vp]), ("yso_roll_num_springs", C.c_uint64, [vp]),
+                                ("yso_roll_set", None, [vp, vp, vp, vp]),
+                                ("yso_roll_forward", C.c_uint64, [vp, C.c_int, C.c_int, vp]),
+                                ("yso_roll_backward", None, [vp, C.c_int, vp, vp, vp, vp])]:
+            fn = getattr(L_, name)
+            fn.restype = res
+            fn.argtypes = args
+        del d, ctypes_double
+        cloth, ob = spec.meshes[0], spec.meshes[1]
+        p = spec.params
+        self.N = cloth.grid_n
+        self.V = cloth.nV
+        ip = np.array([cloth.grid_n, ob.nV, ob.nF], np.int32)
+        dp = np.array([p.kd, p.kair, p.subh, cloth.thickness, p.margin, p.radius, *p.gravity], np.float64)
+        self._arrs = [np.ascontiguousarray(a, np.float64) for a in
+                      (cloth.x, cloth.v if v0 is None else v0, cloth.mass, cloth.mask, ob.x)]
+        oF = np.ascontiguousarray(ob.facets, np.uint32)
+        self.h = L_.yso_roll_new(P(ip), P(dp), *[P(a) for a in self._arrs], P(oF))
+        self.S = int(L_.yso_roll_num_springs(self.h))
+        self.set(k, L)
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().yso_roll_free(self.h)
+            self.h = None
+
+    def set(self, k=None, L=None, v0=None):
+        a = [None if t is None else np.ascontiguousarray(t, np.float64) for t in (k, L, v0)]
+        lib().yso_roll_set(self.h, *[P(t) for t in a])
+
+    def forward(self, T, keep=False):
+        x = np.zeros((self.V, 3), np.float64)
+        n = lib().yso_roll_forward(self.h, T, 1 if keep else 0, P(x))
+        return x, int(n)
+
+    def backward(self, T, dLdx):
+        gk = np.zeros(self.S, np.float64)
+        gL = np.zeros(self.S, np.float64)
+        gv = np.zeros((self.V, 3), np.float64)
+        lib().yso_roll_backward(self.h, T, P(np.ascontiguousarray(dLdx, np.float64)), P(gk), P(gL), P(gv))
+        return gk, gL, gv

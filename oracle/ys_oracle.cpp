@@ -179,7 +179,9 @@ struct Karras {
 void karras_topology(const u32* codes, const u32* idx, u32 n, Node* tree, i32* parent) {
     Karras K{codes, idx, (int)n};
     for (u32 i = 0; i < n; ++i) { Node& L = tree[n - 1 + i]; L.a = -1; L.b = (i32)idx[i]; }
-    parent[0] = -1;
+    // unclaimed nodes keep -1; a node claimed twice (runs of >= 3 equal codes)
+    // keeps the last writer of this ascending loop, the largest claimant
+    for (u32 i = 0; i + 1 < 2 * n; ++i) parent[i] = -1;
     for (int i = 0; i + 1 < (int)n; ++i) {
         int f, l; K.range(i, f, l);
         int s = (int)K.split(f, l);

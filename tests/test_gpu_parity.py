@@ -265,3 +265,41 @@ def test_full_size_c2_runs_clean(cuda_lib):
         assert st["flags"] & ~0 == 0, st
     finally:
         s.close()
+
+
+@pytest.mark.parametrize("case", ["soup", "sparse", "huge_tri"])
+def test_spatial_hash_equals_lbvh_query(cuda_lib, oracle, case):
+    """Spatial-hash broad phase == LBVH point query (== brute force) as sets."""
+    import torch
+    from ysim_b200 import _lib, generators as G
+    x, f, q = G.soup(60_000 if case != "sparse" else 20_000, seed=31, nq=40_000)
+    if case == "huge_tri":  # a few triangles spanning far more cells than the grid allows
+        x = x.copy()
+        x[0:9] = np.array([[0, 0, 0], [1, 0, 0], [0, 1, 1]] * 3, np.float32)
+    h_margin = np.float32(1e-3 if case != "sparse" else 4e-3)
+    cell = np.float32(2 * h_margin)
+    dx, df, dq = _dev(x.reshape(-1)), _dev(f.reshape(-1).astype(np.int32)), _dev(q.reshape(-1))
+    cap = 1 << 22
+    sh = C.c_void_p()
+    _lib.check(cuda_lib.ys_shash_create(C.byref(sh), len(f), 64 * len(f), 0, None))
+    try:
+        _lib.check(cuda_lib.ys_shash_build(sh, _p(dx), _p(df), len(f), cell))
+        pairs = torch.empty(2 * cap, dtype=torch.int32, device="cuda")
+        cnt = torch.zeros(1, dtype=torch.int64, device="cuda")
+        _lib.check(cuda_lib.ys_shash_query(sh, _p(dq), len(q), h_margin, _p(pairs), cap, _p(cnt)))
+        n = int(cnt.item())
+        got = canon_pairs(pairs[: 2 * n].cpu().numpy().view(np.uint32))
+    finally:
+        _lib.check(cuda_lib.ys_shash_destroy(sh))
+    h, _, _ = _lbvh(cuda_lib, x, f)
+    try:
+        pairs = torch.empty(2 * cap, dtype=torch.int32, device="cuda")
+        cnt = torch.zeros(1, dtype=torch.int64, device="cuda")
+        _lib.check(cuda_lib.ys_lbvh_query(h, _p(dq), len(q), h_margin, 0, _p(pairs), cap, _p(cnt)))
+        n = int(cnt.item())
+        bvh = canon_pairs(pairs[: 2 * n].cpu().numpy().view(np.uint32))
+    finally:
+        _lib.check(cuda_lib.ys_lbvh_destroy(h))
+    assert len(got) > 0
+    assert np.array_equal(got, bvh)
+    assert np.array_equal(got, canon_pairs(oracle.brute_q1(x, f, q, float(h_margin), False)))

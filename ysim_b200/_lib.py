@@ -78,6 +78,7 @@ _PROTOS = {
     "ys_scene_step_staged": (C.c_int, [C.c_void_p, C.c_uint32]),
     "ys_scene_step": (C.c_int, [C.c_void_p, C.c_uint32]),
     "ys_scene_set_record": (C.c_int, [C.c_void_p, C.c_int]),
+    "ys_scene_set_graphs": (C.c_int, [C.c_void_p, C.c_int]),
     "ys_scene_sync": (C.c_int, [C.c_void_p]),
     "ys_scene_stream": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
     "ys_scene_get_state": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
@@ -101,6 +102,12 @@ _PROTOS = {
                                 C.c_void_p]),
     "ys_lbvh_arrays": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p), C.POINTER(C.c_void_p),
                                  C.POINTER(C.c_void_p), C.POINTER(C.c_uint32)]),
+    "ys_shash_create": (C.c_int, [C.POINTER(C.c_void_p), C.c_uint32, C.c_uint32, C.c_int, C.c_void_p]),
+    "ys_shash_destroy": (C.c_int, [C.c_void_p]),
+    "ys_shash_build": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_float]),
+    "ys_shash_query": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_float, C.c_void_p, C.c_uint64,
+                                 C.c_void_p]),
+    "ys_shash_entries": (C.c_int, [C.c_void_p, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]),
     "ys_morton_codes": (C.c_int, [C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p,
                                   C.c_void_p]),
     "ys_radix_sort_scratch_bytes": (C.c_size_t, [C.c_uint32]),

@@ -488,6 +488,10 @@ struct ys_scene {
     std::vector<cudaEvent_t> evPool;
     size_t evUsed = 0;
     std::vector<size_t> evRefit, evFused;  // indices of (begin, end) event pairs
+    // one executable graph per buffer-rotation state (cur, prev, cv): the
+    // refit + fused substep replayed without host launch overhead
+    bool use_graphs = true;
+    cudaGraphExec_t graphs[18] = {};
     DBuf<char> sortScratch, scanScratch;
     // staged / record buffers
     u32 cap = 0;
@@ -695,6 +699,22 @@ ys_status system_update(ys_scene* s) {
     return YS_OK;
 }
 
+void drop_graphs(ys_scene* s) {
+    for (auto& g : s->graphs)
+        if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+}
+
+// Enqueue the device work of one fused substep (no preamble, no rotation).
+ys_status enqueue_fused(ys_scene* s) {
+    ys_status r = refit(s);
+    if (r) return r;
+    YS_CK(cudaMemsetAsync(s->counters.p, 0, s->record ? 24 : 16, s->stream));
+    StepArgs A = make_args(s);
+    k_fused<<<ceil_div(s->nV, 128), 128, 0, s->stream>>>(A);
+    YS_CK(cudaGetLastError());
+    return YS_OK;
+}
+
 cudaEvent_t next_event(ys_scene* s) {
     if (s->evUsed == s->evPool.size()) {
         cudaEvent_t e;
@@ -707,6 +727,24 @@ cudaEvent_t next_event(ys_scene* s) {
 ys_status fused_substep(ys_scene* s) {
     ys_status r = preamble(s);
     if (r) return r;
+    if (s->use_graphs && !s->timing && !s->record) {
+        const int key = (s->cur * 3 + s->prev) * 2 + s->cv;
+        if (!s->graphs[key]) {
+            cudaGraph_t g = nullptr;
+            YS_CK(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
+            ys_status er = enqueue_fused(s);
+            cudaError_t ce = cudaStreamEndCapture(s->stream, &g);
+            if (er) { if (g) cudaGraphDestroy(g); return er; }
+            if (ce != cudaSuccess) return fail(YS_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(ce));
+            ce = cudaGraphInstantiate(&s->graphs[key], g, 0);
+            cudaGraphDestroy(g);
+            if (ce != cudaSuccess) return fail(YS_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ce));
+        }
+        YS_CK(cudaGraphLaunch(s->graphs[key], s->stream));
+        s->snapshot_pending = true;
+        rotate(s);
+        return YS_OK;
+    }
     if (s->timing) {
         s->evRefit.push_back(s->evUsed);
         YS_CK(cudaEventRecord(next_event(s), s->stream));
@@ -771,6 +809,7 @@ ys_status ys_scene_destroy(ys_scene* s) {
     s->codes.free(); s->idx.free(); s->visits.free(); s->box.free(); s->spr_rest.free(); s->scratch3.free(); s->F4.free(); s->F3.free();
     s->nodes.free(); s->parent.free(); s->parent2.free(); s->dmeshes.free(); s->jobs.free(); s->counters.free(); s->sortScratch.free();
     s->scanScratch.free(); s->rows.free(); s->contacts.free(); s->csr.free(); s->pool.free(); s->bucket.free();
+    drop_graphs(s);
     s->csr_off.free(); s->vstart.free(); s->vcount.free(); s->ext.free();
     for (auto e : s->evPool) cudaEventDestroy(e);
     cudaStreamDestroy(s->stream);
@@ -1014,6 +1053,13 @@ ys_status ys_scene_set_record(ys_scene* s, int record) {
     return YS_OK;
 }
 
+ys_status ys_scene_set_graphs(ys_scene* s, int on) {
+    if (!s) return fail(YS_ERR_BAD_ARG, "null scene");
+    s->use_graphs = on != 0;
+    if (!s->use_graphs) drop_graphs(s);
+    return YS_OK;
+}
+
 ys_status ys_scene_sync(ys_scene* s) {
     if (!s) return fail(YS_ERR_BAD_ARG, "null scene");
     YS_CK(cudaStreamSynchronize(s->stream));
@@ -1100,7 +1146,12 @@ ys_status ys_scene_stats(ys_scene* s, uint64_t out[8]) {
 ys_status ys_scene_set_external_forces(ys_scene* s, const float* host_ext) {
     ys_status r = check_scene(s);
     if (r) return r;
-    if (!host_ext) { s->use_ext = false; return YS_OK; }
+    if (!host_ext) {
+        if (s->use_ext) drop_graphs(s);
+        s->use_ext = false;
+        return YS_OK;
+    }
+    if (!s->use_ext) drop_graphs(s);  // captured graphs read g * m, not the buffer
     if (!s->ext.p) {
         YS_CK(s->ext.alloc(s->nV));
         YS_CK(s->scratch3.alloc(3 * (size_t)s->nV));

@@ -212,7 +212,8 @@ def config_c2(seed: int = 2, P: int = 512, level: int = 7, height: float = 0.40,
     level-7 icosphere (r 0.3, radial noise amplitude 0.05); subh 1/1200,
     20 substeps/frame.  Margin and radius are the reference defaults scaled by
     the grid-spacing ratio (1/511)/(1/63) so the contact band stays about one
-    edge length, as in the reference's 64-grid scenes."""
+    edge length, as in the reference's 64-grid scenes; the contact thickness
+    is C1's 1e-3 scaled the same way (about 6% of an edge)."""
     from ._lib import MESH_COLLIDABLE, MESH_SELF_COLLIDE, TRIANGULAR_CLOTH
     rng = np.random.Generator(np.random.PCG64(seed))
     s = 1.0 / (P - 1)
@@ -220,7 +221,7 @@ def config_c2(seed: int = 2, P: int = 512, level: int = 7, height: float = 0.40,
     x = (x + rng.uniform(-0.1 * s, 0.1 * s, x.shape).astype(F32)).astype(F32)
     cloth = Mesh(behavior=TRIANGULAR_CLOTH, flags=MESH_COLLIDABLE | MESH_SELF_COLLIDE, x=x, facets=f,
                  v=np.zeros_like(x), mass=np.full(P * P, 1e-2, F32), mask=np.ones(P * P, F32), kstretch=1e3,
-                 kshear=5e2, kbend=1e1, thickness=1e-3)
+                 kshear=5e2, kbend=1e1, thickness=1e-3 * (63.0 / (P - 1)))
     scale = (1.0 / (P - 1)) / (1.0 / 63.0)
     prm = Params(subh=1.0 / 1200.0, substeps=20, margin=0.015 * scale, radius=0.012 * scale, self_mode=self_mode)
     meshes = [cloth]
@@ -264,3 +265,32 @@ def config_c4(seed: int = 4, instances: int = 256, lo: int = 16, hi: int = 256, 
         ob.group = i
         meshes += [cloth, ob]
     return SceneSpec(f"c4_batched{instances}", Params(subh=1.0 / 600.0, substeps=10), meshes, seed)
+
+
+# ---------------------------------------------------------------- adjoint
+def grid_spring_params(N: int, rest6, k3):
+    """Per-spring stiffness and rest length of a FastGridCloth in the canonical
+    spring order: stretch-x (r,c)-(r,c+1), stretch-y (r,c)-(r+1,c), shear "\\\\"
+    (r,c)-(r+1,c+1), shear "/" (r,c+1)-(r+1,c), bend-x (r,c)-(r,c+2), bend-y
+    (r,c)-(r+2,c), each row-major.  Uniform values reproduce
+    FastGridClothBehaviorParams exactly."""
+    fam = [(N * (N - 1), rest6[0], k3[0]), ((N - 1) * N, rest6[1], k3[0]), ((N - 1) ** 2, rest6[2], k3[1]),
+           ((N - 1) ** 2, rest6[3], k3[1]), (N * (N - 2), rest6[4], k3[2]), ((N - 2) * N, rest6[5], k3[2])]
+    k = np.concatenate([np.full(n, kk, F32) for n, _, kk in fam])
+    L = np.concatenate([np.full(n, rr, F32) for n, rr, _ in fam])
+    return k, L
+
+
+def config_c5(seed: int = 5, N: int = 128, level: int = 4, height: float = 0.33) -> SceneSpec:
+    """Differentiable rollout: FastGridCloth N x N (size 1) above a static
+    level-4 icosphere (r 0.3); subh 1/600, one substep per step; m 1e-2,
+    k 1e3/5e2/1e1 (stable at this step), thickness 1e-3."""
+    from ._lib import FAST_GRID_CLOTH, MESH_COLLIDABLE
+    rng = np.random.Generator(np.random.PCG64(seed))
+    x, f = grid_cloth(N, 1.0, (0.0, height, 0.0))
+    x[:, 1] = (x[:, 1] + rng.uniform(0.0, 1e-4, N * N).astype(F32)).astype(F32)
+    cloth = Mesh(behavior=FAST_GRID_CLOTH, flags=MESH_COLLIDABLE, x=x, facets=f, v=np.zeros_like(x),
+                 mass=np.full(N * N, 1e-2, F32), mask=np.ones(N * N, F32), kstretch=1e3, kshear=5e2, kbend=1e1,
+                 thickness=1e-3, grid_n=N, grid_rest=fast_grid_rest(x, N))
+    obst = obstacle_sphere(level, 0.3)
+    return SceneSpec(f"c5_adjoint{N}", Params(subh=1.0 / 600.0, substeps=1, rebuild_frames=10), [cloth, obst], seed)

@@ -122,6 +122,9 @@ class Scene:
     def set_record(self, on: bool):
         _lib.check(self.lib.ys_scene_set_record(self.h, 1 if on else 0), "ys_scene_set_record")
 
+    def set_graphs(self, on: bool):
+        _lib.check(self.lib.ys_scene_set_graphs(self.h, 1 if on else 0), "ys_scene_set_graphs")
+
     def sync(self):
         _lib.check(self.lib.ys_scene_sync(self.h), "ys_scene_sync")
 
