@@ -93,6 +93,7 @@ typedef struct ys_mesh_desc {
 typedef struct ys_scene ys_scene;
 typedef struct ys_lbvh ys_lbvh;
 typedef struct ys_shash ys_shash;
+typedef struct ys_adjoint ys_adjoint;
 
 /* Last error message of the calling thread. */
 const char* ys_last_error(void);
@@ -174,6 +175,29 @@ ys_status ys_scene_contacts(ys_scene* s, uint32_t* host_offsets, void* host_cont
  * primitive indices (any pointer may be NULL). */
 ys_status ys_scene_tree(ys_scene* s, int mesh, void* nodes, int32_t* parent, uint32_t* codes, uint32_t* idx,
                         uint32_t* num_prims_out);
+
+/* ---- Differentiable rollouts (adjoint of the substep) --------------------
+ * Per-spring parameters of a FastGridCloth (FastGridClothBehaviorParams has
+ * three stiffnesses and six rest lengths, collision_pod.hpp:388-396; uniform
+ * arrays reproduce it exactly).  Canonical spring order: stretch x
+ * (r,c)-(r,c+1), stretch y (r,c)-(r+1,c), shear (r,c)-(r+1,c+1), shear
+ * (r,c+1)-(r+1,c), bend x (r,c)-(r,c+2), bend y (r,c)-(r+2,c), each family
+ * row-major.  Device pointers. */
+ys_status ys_scene_set_grid_springs(ys_scene* s, int mesh, const float* d_k, const float* d_L);
+/* Adjoint of `steps` substeps of one FastGridCloth mesh against static
+ * obstacles (self-collision off), checkpointing the scene state every
+ * `checkpoint_every` substeps and replaying one segment at a time in the
+ * reverse pass.  The rollout starts from the scene's state at creation. */
+ys_status ys_adjoint_create(ys_adjoint** out, ys_scene* s, int mesh, uint32_t steps, uint32_t checkpoint_every);
+ys_status ys_adjoint_destroy(ys_adjoint* a);
+uint32_t ys_adjoint_num_springs(ys_adjoint* a);
+/* Per-spring stiffness, rest length and the cloth's initial velocity (device
+ * pointers; NULL keeps the current value). */
+ys_status ys_adjoint_set_params(ys_adjoint* a, const float* d_k, const float* d_L, const float* d_v0);
+/* Forward rollout; the cloth's final positions (3 floats per vertex) into d_xT. */
+ys_status ys_adjoint_forward(ys_adjoint* a, float* d_xT);
+/* dL/dx_T in; dL/dk, dL/dL (per spring) and dL/dv0 (3 floats per vertex) out. */
+ys_status ys_adjoint_backward(ys_adjoint* a, const float* d_dLdx, float* d_gk, float* d_gL, float* d_gv0);
 
 /* ---- Standalone LBVH over one triangle soup (BVH<CUDA,PR,LINEAR,TRIANGLE>,
  * bvh.hpp:141-2308).  Device pointers; x / v packed xyz floats. ---------- */

@@ -21,9 +21,11 @@
 // Grid springs: 6 families with canonical ids (the enumeration the CUDA path
 // uses), gathered per vertex in the stencil order of
 // compute_cloth_grid_forces_fast (physics.metal:197-218).
+#include <algorithm>
 #include <cmath>
 #include <cstdint>
 #include <cstring>
+#include <unordered_map>
 #include <vector>
 
 namespace {
@@ -53,6 +55,30 @@ struct Roll {
     std::vector<uint32_t> oF;         // obstacle faces
     std::vector<double> obmin, obmax; // per-face AABB
     D3 orootmin, orootmax;
+    // static uniform grid over the obstacle's face boxes (candidate search)
+    double cell = 1.0;
+    std::unordered_map<uint64_t, std::vector<uint32_t>> grid;
+    static uint64_t key(long long x, long long y, long long z) {
+        return ((uint64_t)(x + (1 << 20)) & 0x1FFFFF) | (((uint64_t)(y + (1 << 20)) & 0x1FFFFF) << 21) |
+               (((uint64_t)(z + (1 << 20)) & 0x1FFFFF) << 42);
+    }
+    void build_grid() {
+        const size_t nf = oF.size() / 3;
+        double ext = 1e-6;
+        for (size_t f = 0; f < nf; ++f)
+            for (int a = 0; a < 3; ++a) ext = std::max(ext, obmax[3 * f + a] - obmin[3 * f + a]);
+        cell = ext;
+        for (size_t f = 0; f < nf; ++f) {
+            long long lo[3], hi[3];
+            for (int a = 0; a < 3; ++a) {
+                lo[a] = (long long)std::floor(obmin[3 * f + a] / cell);
+                hi[a] = (long long)std::floor(obmax[3 * f + a] / cell);
+            }
+            for (long long z = lo[2]; z <= hi[2]; ++z)
+                for (long long y = lo[1]; y <= hi[1]; ++y)
+                    for (long long x = lo[0]; x <= hi[0]; ++x) grid[key(x, y, z)].push_back((uint32_t)f);
+        }
+    }
     // per-vertex springs in stencil order
     std::vector<std::vector<Nb>> nbs;
     // trajectory (for the backward pass)
@@ -122,13 +148,24 @@ struct Roll {
         if (hi.x < orootmin.x || lo.x > orootmax.x || hi.y < orootmin.y || lo.y > orootmax.y || hi.z < orootmin.z ||
             lo.z > orootmax.z)
             return;
-        const size_t nf = oF.size() / 3;
 #pragma omp parallel for schedule(dynamic, 64)
         for (long long il = 0; il < (long long)V; ++il) {
             size_t i = (size_t)il;
             D3 p = ld(x, i), pp = ld(xp, i);
             D3 qmn = p - d3(margin, margin, margin), qmx = p + d3(margin, margin, margin);
-            for (size_t f = 0; f < nf; ++f) {
+            std::vector<uint32_t> cand;
+            const double qa[3] = {qmn.x, qmn.y, qmn.z}, qb[3] = {qmx.x, qmx.y, qmx.z};
+            long long lo[3], hi[3];
+            for (int a = 0; a < 3; ++a) { lo[a] = (long long)std::floor(qa[a] / cell); hi[a] = (long long)std::floor(qb[a] / cell); }
+            for (long long z = lo[2]; z <= hi[2]; ++z)
+                for (long long y = lo[1]; y <= hi[1]; ++y)
+                    for (long long xx = lo[0]; xx <= hi[0]; ++xx) {
+                        auto it = grid.find(key(xx, y, z));
+                        if (it != grid.end()) cand.insert(cand.end(), it->second.begin(), it->second.end());
+                    }
+            std::sort(cand.begin(), cand.end());
+            cand.erase(std::unique(cand.begin(), cand.end()), cand.end());
+            for (uint32_t f : cand) {
                 if (qmx.x < obmin[3 * f] || qmn.x > obmax[3 * f] || qmx.y < obmin[3 * f + 1] || qmn.y > obmax[3 * f + 1] ||
                     qmx.z < obmin[3 * f + 2] || qmn.z > obmax[3 * f + 2])
                     continue;
@@ -284,6 +321,7 @@ void* yso_roll_new(const int* ip, const double* dp, const double* x0, const doub
         R->orootmin = d3(std::fmin(R->orootmin.x, R->obmin[3 * f]), std::fmin(R->orootmin.y, R->obmin[3 * f + 1]), std::fmin(R->orootmin.z, R->obmin[3 * f + 2]));
         R->orootmax = d3(std::fmax(R->orootmax.x, R->obmax[3 * f]), std::fmax(R->orootmax.y, R->obmax[3 * f + 1]), std::fmax(R->orootmax.z, R->obmax[3 * f + 2]));
     }
+    R->build_grid();
     R->springs();
     R->k.assign(R->S, 0.0);
     R->L.assign(R->S, 0.0);

@@ -65,7 +65,7 @@ def morton_tree():
 
 SPECS = {
     "c1": lambda: G.config_c1(P=24, level=2, height=0.2999),
-    "c2hash": lambda: G.config_c2(P=32, level=3, height=0.315),
+    "c2hash": lambda: G.config_c2(P=32, level=3, height=0.315, gravity=-9.81),
 }
 
 

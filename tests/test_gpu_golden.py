@@ -63,7 +63,7 @@ def test_gpu_substep_matches_golden(cuda_lib, name, fused):
     from ysim_b200 import generators as G
     from ysim_b200.scene import Scene
     spec = {"c1": lambda: G.config_c1(P=24, level=2, height=0.2999),
-            "c2hash": lambda: G.config_c2(P=32, level=3, height=0.315)}[name]()
+            "c2hash": lambda: G.config_c2(P=32, level=3, height=0.315, gravity=-9.81)}[name]()
     g = np.load(os.path.join(GOLD, f"substep_{name}.npz"))
     s = Scene(spec)
     try:

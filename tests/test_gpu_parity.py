@@ -156,8 +156,8 @@ def _small_specs():
     from ysim_b200 import generators as G
     return {
         "c1": G.config_c1(P=24, level=2, height=0.2999),
-        "c2hash": G.config_c2(P=40, level=3, height=0.33),
-        "c2bvh": G.config_c2(P=40, level=3, height=0.33, self_mode=2),
+        "c2hash": G.config_c2(P=40, level=3, height=0.33, gravity=-9.81),
+        "c2bvh": G.config_c2(P=40, level=3, height=0.33, self_mode=2, gravity=-9.81),
     }
 
 

@@ -96,8 +96,8 @@ def _packed(spec):
 def test_substep_stages_match_reference_kernels(oracle, name):
     from ysim_b200 import generators as G
     spec = {"c1": G.config_c1(P=24, level=2, height=0.2999),
-            "c2hash": G.config_c2(P=40, level=3, height=0.33),
-            "c2bvh": G.config_c2(P=40, level=3, height=0.33, self_mode=2)}[name]
+            "c2hash": G.config_c2(P=40, level=3, height=0.33, gravity=-9.81),
+            "c2bvh": G.config_c2(P=40, level=3, height=0.33, self_mode=2, gravity=-9.81)}[name]
     o = oracle.OracleScene(spec)
     o.step(3 * spec.params.substeps + 1)  # mid-drape, contacts present
     voff, foff, F, vaf, vaf_off = _packed(spec)
@@ -151,7 +151,7 @@ def test_bucket_kernels_partition_like_oracle(oracle):
     """narrow_bucket_* (GPU CSR, order nondeterministic) == oracle CSR as
     per-vertex multisets."""
     from ysim_b200 import generators as G
-    spec = G.config_c2(P=40, level=3, height=0.33)
+    spec = G.config_c2(P=40, level=3, height=0.33, gravity=-9.81)
     o = oracle.OracleScene(spec)
     o.step(3 * spec.params.substeps + 1)
     for k in range(4):

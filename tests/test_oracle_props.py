@@ -192,7 +192,7 @@ def test_oracle_matches_golden_morton_tree(oracle):
 def test_oracle_matches_golden_substep(oracle, name):
     from ysim_b200 import generators as G
     spec = {"c1": lambda: G.config_c1(P=24, level=2, height=0.2999),
-            "c2hash": lambda: G.config_c2(P=32, level=3, height=0.315)}[name]()
+            "c2hash": lambda: G.config_c2(P=32, level=3, height=0.315, gravity=-9.81)}[name]()
     g = np.load(os.path.join(GOLD, f"substep_{name}.npz"))
     o = oracle.OracleScene(spec)
     o.set("x", g["x"]); o.set("v", g["v"]); o.set("xprev", g["xprev"])

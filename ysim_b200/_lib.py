@@ -108,6 +108,13 @@ _PROTOS = {
     "ys_shash_query": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_float, C.c_void_p, C.c_uint64,
                                  C.c_void_p]),
     "ys_shash_entries": (C.c_int, [C.c_void_p, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]),
+    "ys_scene_set_grid_springs": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]),
+    "ys_adjoint_create": (C.c_int, [C.POINTER(C.c_void_p), C.c_void_p, C.c_int, C.c_uint32, C.c_uint32]),
+    "ys_adjoint_destroy": (C.c_int, [C.c_void_p]),
+    "ys_adjoint_num_springs": (C.c_uint32, [C.c_void_p]),
+    "ys_adjoint_set_params": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "ys_adjoint_forward": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "ys_adjoint_backward": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "ys_morton_codes": (C.c_int, [C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p,
                                   C.c_void_p]),
     "ys_radix_sort_scratch_bytes": (C.c_size_t, [C.c_uint32]),

@@ -48,7 +48,9 @@ struct MeshDev {
     float kstretch, kshear, kbend, thickness;
     float rest[6];
     u32 tgt_begin, tgt_end;
+    u32 gspr;  // FastGridCloth: offset of this mesh's per-spring k / L arrays, or NO_SPRINGS
 };
+static constexpr u32 NO_SPRINGS = 0xFFFFFFFFu;
 
 struct StepArgs {
     const float4* x;
@@ -71,6 +73,8 @@ struct StepArgs {
     const u32* vaf;
     const u32* maxext;
     const float4* ext;  // external forces (applyEnvironmentForces) or null: g * m
+    const float* gk;    // per-spring stiffness / rest length of grid cloths (MeshDev::gspr)
+    const float* gL;
     float subh, kair, kd, gx, gy, gz, margin, band;
     u32 nV, self_mode, record, cap;
     u32* status;
@@ -135,6 +139,43 @@ __device__ __forceinline__ u32 query_vertex(const StepArgs& A, u32 g, u32 m, con
 
 __device__ __forceinline__ bool key_less(u32 t1, u32 f1, u32 t2, u32 f2) { return t1 < t2 || (t1 == t2 && f1 < f2); }
 
+// The 12 stencil springs of grid vertex (row, col) in the order of
+// compute_cloth_grid_forces_fast (physics.metal:197-218): fn(r, c, family,
+// spring id).  Families 0..5 = stretch x, stretch y, shear "\\", shear "/",
+// bend x, bend y (rest[family]; k = kstretch, kstretch, kshear, kshear,
+// kbend, kbend); spring ids number each family row-major, families
+// concatenated in that order.
+template <class Fn>
+__device__ __forceinline__ void grid_stencil(int N, int row, int col, Fn&& fn) {
+    const u32 n = (u32)N;
+    const u32 bSY = n * (n - 1), bHA = bSY + (n - 1) * n, bHB = bHA + (n - 1) * (n - 1), bBX = bHB + (n - 1) * (n - 1),
+              bBY = bBX + n * (n - 2);
+    const u32 r = (u32)row, c = (u32)col;
+    if (col > 0) fn(row, col - 1, 0, r * (n - 1) + c - 1);
+    if (col < N - 1) fn(row, col + 1, 0, r * (n - 1) + c);
+    if (row > 0) fn(row - 1, col, 1, bSY + (r - 1) * n + c);
+    if (row < N - 1) fn(row + 1, col, 1, bSY + r * n + c);
+    if (col > 0 && row > 0) fn(row - 1, col - 1, 2, bHA + (r - 1) * (n - 1) + c - 1);
+    if (col < N - 1 && row > 0) fn(row - 1, col + 1, 3, bHB + (r - 1) * (n - 1) + c);
+    if (col > 0 && row < N - 1) fn(row + 1, col - 1, 3, bHB + r * (n - 1) + c - 1);
+    if (col < N - 1 && row < N - 1) fn(row + 1, col + 1, 2, bHA + r * (n - 1) + c);
+    if (col > 1) fn(row, col - 2, 4, bBX + r * (n - 2) + c - 2);
+    if (col < N - 2) fn(row, col + 2, 4, bBX + r * (n - 2) + c);
+    if (row > 1) fn(row - 2, col, 5, bBY + (r - 2) * n + c);
+    if (row < N - 2) fn(row + 2, col, 5, bBY + r * n + c);
+}
+
+__device__ __forceinline__ void grid_spring_kL(const StepArgs& A, const MeshDev& M, int fam, u32 sid, float& k,
+                                               float& rest) {
+    if (M.gspr != NO_SPRINGS) {
+        k = A.gk[M.gspr + sid];
+        rest = A.gL[M.gspr + sid];
+    } else {
+        k = fam < 2 ? M.kstretch : (fam < 4 ? M.kshear : M.kbend);
+        rest = M.rest[fam];
+    }
+}
+
 // Spring forces of one cloth vertex from the old state:
 // compute_cloth_grid_forces_fast (physics.metal:171-224) or
 // compute_tri_spring_forces (physics.metal:319-378).
@@ -145,22 +186,12 @@ __device__ __forceinline__ f3 vertex_force(const StepArgs& A, const MeshDev& M, 
         const int N = (int)M.grid_n;
         const u32 lid = g - M.voff;
         const int row = (int)(lid / (u32)N), col = (int)(lid % (u32)N);
-        auto G = [&](int r, int c, float rest, float k) {
+        grid_stencil(N, row, col, [&](int r, int c, int fam, u32 sid) {
+            float k, rest;
+            grid_spring_kL(A, M, fam, sid, k, rest);
             u32 j = M.voff + (u32)(r * N + c);
             force = force + spring(pos, vel, ld(A.x, j), ld(A.v, j), rest, k, kd);
-        };
-        if (col > 0) G(row, col - 1, M.rest[0], M.kstretch);
-        if (col < N - 1) G(row, col + 1, M.rest[0], M.kstretch);
-        if (row > 0) G(row - 1, col, M.rest[1], M.kstretch);
-        if (row < N - 1) G(row + 1, col, M.rest[1], M.kstretch);
-        if (col > 0 && row > 0) G(row - 1, col - 1, M.rest[2], M.kshear);
-        if (col < N - 1 && row > 0) G(row - 1, col + 1, M.rest[3], M.kshear);
-        if (col > 0 && row < N - 1) G(row + 1, col - 1, M.rest[3], M.kshear);
-        if (col < N - 1 && row < N - 1) G(row + 1, col + 1, M.rest[2], M.kshear);
-        if (col > 1) G(row, col - 2, M.rest[4], M.kbend);
-        if (col < N - 2) G(row, col + 2, M.rest[4], M.kbend);
-        if (row > 1) G(row - 2, col, M.rest[5], M.kbend);
-        if (row < N - 2) G(row + 2, col, M.rest[5], M.kbend);
+        });
     } else {
         const u32 b = A.spr_off[g], s = A.spr_split[g], e = A.spr_off[g + 1];
         for (u32 i = b; i < s; ++i) {
@@ -370,6 +401,7 @@ struct HostMesh {
     // TriangularCloth springs (mesh-local ids)
     std::vector<u32> spr_off, spr_split, spr_nbr, vaf_off, vaf;
     std::vector<float> spr_rest;
+    bool grid_springs_on = false;  // per-spring parameters set (ys_scene_set_grid_springs)
 };
 
 template <class T>
@@ -483,6 +515,8 @@ struct ys_scene {
     DBuf<unsigned long long> counters;
     DBuf<float4> ext;
     bool use_ext = false;
+    DBuf<float> gk, gL;              // per-spring grid-cloth parameters
+    std::vector<MeshDev> hmeshes;    // host copy of the device mesh table
     // per-kernel CUDA-event timing of the fused path
     bool timing = false;
     std::vector<cudaEvent_t> evPool;
@@ -539,6 +573,8 @@ StepArgs make_args(ys_scene* s) {
     A.vaf = s->vaf.p;
     A.maxext = s->maxext.p;
     A.ext = s->use_ext ? s->ext.p : nullptr;
+    A.gk = s->gk.p;
+    A.gL = s->gL.p;
     A.subh = s->P.subh; A.kair = s->P.kair; A.kd = s->P.kd;
     A.gx = s->P.gravity[0]; A.gy = s->P.gravity[1]; A.gz = s->P.gravity[2];
     A.margin = s->P.margin;
@@ -806,7 +842,7 @@ ys_status ys_scene_destroy(ys_scene* s) {
     for (auto& b : s->V) b.free();
     s->Fbuf.free(); s->mass.free(); s->mask.free(); s->vobj.free(); s->targets.free(); s->spr_off.free();
     s->spr_split.free(); s->spr_nbr.free(); s->vaf_off.free(); s->vaf.free(); s->maxext.free(); s->status.free();
-    s->codes.free(); s->idx.free(); s->visits.free(); s->box.free(); s->spr_rest.free(); s->scratch3.free(); s->F4.free(); s->F3.free();
+    s->codes.free(); s->idx.free(); s->visits.free(); s->box.free(); s->spr_rest.free(); s->scratch3.free(); s->gk.free(); s->gL.free(); s->F4.free(); s->F3.free();
     s->nodes.free(); s->parent.free(); s->parent2.free(); s->dmeshes.free(); s->jobs.free(); s->counters.free(); s->sortScratch.free();
     s->scanScratch.free(); s->rows.free(); s->contacts.free(); s->csr.free(); s->pool.free(); s->bucket.free();
     drop_graphs(s);
@@ -917,6 +953,7 @@ ys_status ys_scene_pack(ys_scene* s) {
                 targets.push_back((u32)t);
             }
         D.tgt_end = (u32)targets.size();
+        D.gspr = NO_SPRINGS;
         md[m] = D;
     }
     spr_off[nV] = (u32)spr_nbr.size();
@@ -965,6 +1002,7 @@ ys_status ys_scene_pack(ys_scene* s) {
         YS_CK(cudaMemcpy(s->F3.p, F3.data(), 12 * (size_t)nF, cudaMemcpyHostToDevice));
     }
     YS_CK(cudaMemcpy(s->dmeshes.p, md.data(), sizeof(MeshDev) * md.size(), cudaMemcpyHostToDevice));
+    s->hmeshes = md;
     YS_CK(cudaMemset(s->status.p, 0, 4));
     YS_CK(cudaMemset(s->maxext.p, 0, 4 * s->meshes.size()));
     YS_CK(cudaMemset(s->counters.p, 0, 8 * s->counters.n));
@@ -1280,6 +1318,380 @@ ys_status ys_scene_tree(ys_scene* s, int mesh, void* nodes, int32_t* parent, uin
     if (parent) YS_CK(cudaMemcpy(parent, s->parent.p + H.node_off, 4 * nn, cudaMemcpyDeviceToHost));
     if (codes) YS_CK(cudaMemcpy(codes, s->codes.p + H.foff, 4 * (size_t)n, cudaMemcpyDeviceToHost));
     if (idx) YS_CK(cudaMemcpy(idx, s->idx.p + H.foff, 4 * (size_t)n, cudaMemcpyDeviceToHost));
+    return YS_OK;
+}
+
+}  // extern "C"
+
+// =====================================================================
+// Adjoint of the substep for one FastGridCloth (differentiable rollouts).
+//
+// Forward step of the cloth (the fused substep's arithmetic):
+//   f_i = ext_i + kair v_i + sum_s (k_s (l - L_s) + kd (dv . n)) n
+//   v'  = v + (subh f / m) mask;  for each contact (n_c, d_c) with d_c < thickness:
+//         { if v'.n_c < 0: v' -= (v'.n_c) n_c;  x += (thickness - d_c) n_c }
+//   x'  = x + subh v' mask
+// Reverse step with the forward's active set frozen (which contacts exist,
+// push and project): the contact push is x -> x + (t - n.(x - t0)) n, so its
+// transpose removes the normal component; the projections are symmetric and
+// are undone in reverse order; the spring force's Jacobian is
+//   dF/d(dx)^T g = (k n + kd (I - nn^T) dv / l)(n.g) + a/l (I - nn^T) g,
+//   dF/d(dv)^T g = kd n (n.g),  dF/dk = (l - L) n,  dF/dL = -k n.
+// Checkpoints of the whole scene state every K steps; the backward pass
+// replays one segment at a time (recording its contacts and states) and
+// reverses it.
+namespace ys {
+
+struct AdjArgs {
+    const float4* x;   // scene positions at step t (all vertices)
+    const float4* v;   // velocities at step t
+    const u32* vstart; const u32* vcount; const VContact* pool;  // contacts recorded at step t
+    const float4* ax;  // dL/dx_{t+1} (all vertices; only the mesh's are used)
+    const float4* av;  // dL/dv_{t+1}
+    float4* xbar; float4* vbar; float4* fbar;
+    float4* ax_out; float4* av_out;
+    float* gk; float* gL;  // per-spring accumulators (this mesh's arrays)
+    u32 voff, nV, N;
+};
+
+__global__ void __launch_bounds__(128) k_adj_vertex(StepArgs A, AdjArgs J, u32 m) {
+    const u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= J.nV) return;
+    const u32 g = J.voff + i;
+    const MeshDev M = A.meshes[m];
+    const f3 x = ld(J.x, g);
+    f3 vel = ld(J.v, g);
+    const float mass = A.mass[g], mask = A.mask[g];
+    const f3 force = vertex_force(A, M, g, x, vel, mass);
+    vel = vel + ((force * A.subh) / mass) * mask;
+    // replay the contact loop of contact_response to freeze its active set
+    const u32 b = J.vstart[g], nc = J.vcount[g];
+    u32 proj = 0, push = 0;  // bit c: contact c projected the velocity / pushed the position
+    for (u32 c = 0; c < nc && c < 32; ++c) {
+        const VContact ci = J.pool[b + c];
+        bool dup = false;
+        for (u32 d = 0; d < c; ++d) {
+            const VContact cd = J.pool[b + d];
+            if (cd.tobj == ci.tobj && cd.tri == ci.tri) { dup = true; break; }
+        }
+        if (dup) continue;
+        f3 n = mk(ci.nx, ci.ny, ci.nz);
+        float nl2 = dot(n, n);
+        if (nl2 < 1e-12f) continue;
+        n = n * (1.0f / sqrtf(nl2));
+        float vn = dot(vel, n);
+        if (ci.d < M.thickness) {
+            if (vn < 0.0f) { vel = vel - n * vn; proj |= 1u << c; }
+            push |= 1u << c;
+        }
+    }
+    const f3 axi = ld(J.ax, g);
+    f3 vb = ld(J.av, g) + axi * (A.subh * mask);
+    for (int c = (int)(nc < 32 ? nc : 32) - 1; c >= 0; --c) {
+        if (!(proj >> c & 1u)) continue;
+        const VContact ci = J.pool[b + c];
+        f3 n = mk(ci.nx, ci.ny, ci.nz);
+        n = n * (1.0f / sqrtf(dot(n, n)));
+        vb = vb - n * dot(n, vb);
+    }
+    f3 xb = axi;
+    for (u32 c = 0; c < nc && c < 32; ++c) {
+        if (!(push >> c & 1u)) continue;
+        const VContact ci = J.pool[b + c];
+        f3 n = mk(ci.nx, ci.ny, ci.nz);
+        n = n * (1.0f / sqrtf(dot(n, n)));
+        xb = xb - n * dot(n, axi);
+    }
+    const f3 fb = vb * ((A.subh / mass) * mask);
+    J.xbar[g] = make_float4(xb.x, xb.y, xb.z, 0.f);
+    J.vbar[g] = make_float4(vb.x, vb.y, vb.z, 0.f);
+    J.fbar[g] = make_float4(fb.x, fb.y, fb.z, 0.f);
+}
+
+__global__ void __launch_bounds__(128) k_adj_springs(StepArgs A, AdjArgs J, u32 m) {
+    const u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= J.nV) return;
+    const u32 g = J.voff + i;
+    const MeshDev M = A.meshes[m];
+    const int N = (int)J.N, row = (int)(i / J.N), col = (int)(i % J.N);
+    const f3 p = ld(J.x, g), w = ld(J.v, g), fi = ld(J.fbar, g);
+    const float kd = A.kd;
+    f3 dxb = mk(0.f, 0.f, 0.f), dvb = mk(0.f, 0.f, 0.f);
+    grid_stencil(N, row, col, [&](int r, int c, int fam, u32 sid) {
+        float k, rest;
+        grid_spring_kL(A, M, fam, sid, k, rest);
+        const u32 jl = (u32)(r * N + c), j = J.voff + jl;
+        const f3 dx = ld(J.x, j) - p, dv = ld(J.v, j) - w;
+        const float l = sqrtf(dot(dx, dx));
+        if (l < 1e-7f) return;
+        const f3 nd = dx / l;
+        const float a = k * (l - rest) + kd * dot(dv, nd);
+        const f3 gdir = fi - ld(J.fbar, j);
+        const float ng = dot(nd, gdir);
+        const f3 dvp = dv - nd * dot(nd, dv), gp = gdir - nd * ng;
+        const f3 ddx = nd * (k * ng) + dvp * (kd * ng / l) + gp * (a / l);
+        dxb = dxb - ddx;
+        dvb = dvb - nd * (kd * ng);
+        if (i < jl) {  // one owner per spring: no race on the accumulators
+            J.gk[sid] += (l - rest) * ng;
+            J.gL[sid] += -k * ng;
+        }
+    });
+    const f3 xb = ld(J.xbar, g) + dxb;
+    const f3 vb = ld(J.vbar, g) + dvb + fi * A.kair;
+    J.ax_out[g] = make_float4(xb.x, xb.y, xb.z, 0.f);
+    J.av_out[g] = make_float4(vb.x, vb.y, vb.z, 0.f);
+}
+
+__global__ void k_mesh_pack4(const float* __restrict__ in, float4* __restrict__ out, u32 voff, u32 n) {
+    u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[voff + i] = make_float4(in[3 * i], in[3 * i + 1], in[3 * i + 2], 0.f);
+}
+__global__ void k_mesh_unpack4(const float4* __restrict__ in, float* __restrict__ out, u32 voff, u32 n) {
+    u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) { float4 q = in[voff + i]; out[3 * i] = q.x; out[3 * i + 1] = q.y; out[3 * i + 2] = q.z; }
+}
+
+}  // namespace ys
+
+struct ys_adjoint {
+    ys_scene* s = nullptr;
+    int mesh = 0;
+    u32 T = 0, K = 0, nseg = 0, nV = 0, voff = 0, S = 0, N = 0;
+    // initial scene state and checkpoints (whole-scene arrays)
+    DBuf<float4> x0, v0;
+    std::vector<DBuf<float4>> ck_x, ck_xp, ck_v;
+    std::vector<uint64_t> ck_frame;
+    std::vector<u32> ck_cursor;
+    // one segment of replayed steps
+    std::vector<DBuf<float4>> st_x, st_v;
+    std::vector<DBuf<u32>> st_vstart, st_vcount;
+    std::vector<DBuf<VContact>> st_pool;
+    DBuf<float4> ax, av, ax2, av2, xbar, vbar, fbar;
+    bool forward_done = false;
+};
+
+namespace {
+
+void restore_state(ys_scene* s, const float4* x, const float4* xp, const float4* v, uint64_t frame, u32 cursor) {
+    const size_t bytes = sizeof(float4) * s->nV;
+    cudaMemcpyAsync(s->X[s->cur].p, x, bytes, cudaMemcpyDeviceToDevice, s->stream);
+    cudaMemcpyAsync(s->X[s->prev].p, xp, bytes, cudaMemcpyDeviceToDevice, s->stream);
+    cudaMemcpyAsync(s->V[s->cv].p, v, bytes, cudaMemcpyDeviceToDevice, s->stream);
+    // vertices that no substep rewrites keep one value in every buffer
+    const int third = 3 - s->cur - s->prev;
+    cudaMemcpyAsync(s->X[third].p, x, bytes, cudaMemcpyDeviceToDevice, s->stream);
+    cudaMemcpyAsync(s->V[1 - s->cv].p, v, bytes, cudaMemcpyDeviceToDevice, s->stream);
+    s->frame = frame;
+    s->cursor = cursor;
+    s->snapshot_pending = false;
+}
+
+}  // namespace
+
+extern "C" {
+
+ys_status ys_scene_set_grid_springs(ys_scene* s, int mesh, const float* d_k, const float* d_L) {
+    ys_status r = check_scene(s);
+    if (r) return r;
+    if (mesh < 0 || (size_t)mesh >= s->meshes.size()) return fail(YS_ERR_BAD_ARG, "bad mesh index");
+    HostMesh& H = s->meshes[mesh];
+    if (H.d.behavior != YS_FAST_GRID_CLOTH) return fail(YS_ERR_BAD_ARG, "per-spring parameters need a FastGridCloth");
+    const u32 n = H.d.grid_n;
+    const size_t S = 2 * (size_t)n * (n - 1) + 2 * (size_t)(n - 1) * (n - 1) + 2 * (size_t)n * (n - 2);
+    if (!s->gk.p) {
+        size_t total = 0;
+        for (auto& M : s->meshes)
+            if (M.d.behavior == YS_FAST_GRID_CLOTH) {
+                const size_t q = M.d.grid_n;
+                total += 2 * q * (q - 1) + 2 * (q - 1) * (q - 1) + 2 * q * (q - 2);
+            }
+        YS_CK(s->gk.alloc(total));
+        YS_CK(s->gL.alloc(total));
+        size_t off = 0;
+        for (size_t m = 0; m < s->meshes.size(); ++m)
+            if (s->meshes[m].d.behavior == YS_FAST_GRID_CLOTH) {
+                s->hmeshes[m].gspr = (u32)off;
+                const size_t q = s->meshes[m].d.grid_n;
+                off += 2 * q * (q - 1) + 2 * (q - 1) * (q - 1) + 2 * q * (q - 2);
+            }
+        // a mesh switches to its per-spring arrays once they are set
+    }
+    const u32 base = s->hmeshes[mesh].gspr;
+    if (d_k) YS_CK(cudaMemcpyAsync(s->gk.p + base, d_k, 4 * S, cudaMemcpyDeviceToDevice, s->stream));
+    if (d_L) YS_CK(cudaMemcpyAsync(s->gL.p + base, d_L, 4 * S, cudaMemcpyDeviceToDevice, s->stream));
+    std::vector<MeshDev> md = s->hmeshes;
+    for (size_t m = 0; m < md.size(); ++m)
+        if ((int)m != mesh && md[m].gspr != NO_SPRINGS && !s->meshes[m].grid_springs_on) md[m].gspr = NO_SPRINGS;
+    H.grid_springs_on = true;
+    YS_CK(cudaMemcpyAsync(s->dmeshes.p, md.data(), sizeof(MeshDev) * md.size(), cudaMemcpyHostToDevice, s->stream));
+    YS_CK(cudaStreamSynchronize(s->stream));
+    drop_graphs(s);
+    return YS_OK;
+}
+
+ys_status ys_adjoint_create(ys_adjoint** out, ys_scene* s, int mesh, uint32_t steps, uint32_t checkpoint_every) {
+    ys_status r = check_scene(s);
+    if (r) return r;
+    if (!out || steps == 0 || checkpoint_every == 0) return fail(YS_ERR_BAD_ARG, "bad argument");
+    if (mesh < 0 || (size_t)mesh >= s->meshes.size()) return fail(YS_ERR_BAD_ARG, "bad mesh index");
+    HostMesh& H = s->meshes[mesh];
+    if (H.d.behavior != YS_FAST_GRID_CLOTH) return fail(YS_ERR_BAD_ARG, "the adjoint covers FastGridCloth meshes");
+    for (size_t m = 0; m < s->meshes.size(); ++m)
+        if ((int)m != mesh && (s->meshes[m].flags & MF_CLOTH))
+            return fail(YS_ERR_BAD_ARG, "the adjoint scene holds one cloth (obstacles are static)");
+    if (s->P.self_mode != YS_SELF_OFF) return fail(YS_ERR_BAD_ARG, "the adjoint needs self-collision off");
+    ys_adjoint* a = new ys_adjoint();
+    a->s = s; a->mesh = mesh; a->T = steps; a->K = checkpoint_every;
+    a->nseg = (steps + checkpoint_every - 1) / checkpoint_every;
+    a->nV = H.d.num_vertices; a->voff = H.voff; a->N = H.d.grid_n;
+    const u32 n = a->N;
+    a->S = 2 * n * (n - 1) + 2 * (n - 1) * (n - 1) + 2 * n * (n - 2);
+    auto fail_free = [&](cudaError_t e) { delete a; return fail(YS_ERR_CUDA, cudaGetErrorString(e)); };
+    cudaError_t e;
+    if ((e = a->x0.alloc(s->nV)) || (e = a->v0.alloc(s->nV))) return fail_free(e);
+    a->ck_x.resize(a->nseg); a->ck_xp.resize(a->nseg); a->ck_v.resize(a->nseg);
+    a->ck_frame.resize(a->nseg); a->ck_cursor.resize(a->nseg);
+    for (u32 i = 0; i < a->nseg; ++i)
+        if ((e = a->ck_x[i].alloc(s->nV)) || (e = a->ck_xp[i].alloc(s->nV)) || (e = a->ck_v[i].alloc(s->nV)))
+            return fail_free(e);
+    a->st_x.resize(a->K); a->st_v.resize(a->K); a->st_vstart.resize(a->K); a->st_vcount.resize(a->K);
+    a->st_pool.resize(a->K);
+    for (u32 i = 0; i < a->K; ++i)
+        if ((e = a->st_x[i].alloc(s->nV)) || (e = a->st_v[i].alloc(s->nV)) || (e = a->st_vstart[i].alloc(s->nV)) ||
+            (e = a->st_vcount[i].alloc(s->nV)) || (e = a->st_pool[i].alloc(s->cap)))
+            return fail_free(e);
+    if ((e = a->ax.alloc(s->nV)) || (e = a->av.alloc(s->nV)) || (e = a->ax2.alloc(s->nV)) || (e = a->av2.alloc(s->nV)) ||
+        (e = a->xbar.alloc(s->nV)) || (e = a->vbar.alloc(s->nV)) || (e = a->fbar.alloc(s->nV)))
+        return fail_free(e);
+    // the rollout starts from the scene's current state
+    YS_CK(cudaMemcpyAsync(a->x0.p, s->X[s->cur].p, sizeof(float4) * s->nV, cudaMemcpyDeviceToDevice, s->stream));
+    YS_CK(cudaMemcpyAsync(a->v0.p, s->V[s->cv].p, sizeof(float4) * s->nV, cudaMemcpyDeviceToDevice, s->stream));
+    YS_CK(cudaStreamSynchronize(s->stream));
+    *out = a;
+    return YS_OK;
+}
+
+ys_status ys_adjoint_destroy(ys_adjoint* a) {
+    if (!a) return YS_OK;
+    cudaStreamSynchronize(a->s->stream);
+    for (auto* v : {&a->ck_x, &a->ck_xp, &a->ck_v, &a->st_x, &a->st_v}) for (auto& b : *v) b.free();
+    for (auto& b : a->st_vstart) b.free();
+    for (auto& b : a->st_vcount) b.free();
+    for (auto& b : a->st_pool) b.free();
+    a->x0.free(); a->v0.free(); a->ax.free(); a->av.free(); a->ax2.free(); a->av2.free();
+    a->xbar.free(); a->vbar.free(); a->fbar.free();
+    delete a;
+    return YS_OK;
+}
+
+uint32_t ys_adjoint_num_springs(ys_adjoint* a) { return a ? a->S : 0; }
+
+// Set the rollout's parameters (device pointers, any may be NULL to keep):
+// per-spring stiffness and rest length (canonical spring order), and the
+// cloth's initial velocity (3 floats per vertex).
+ys_status ys_adjoint_set_params(ys_adjoint* a, const float* d_k, const float* d_L, const float* d_v0) {
+    if (!a) return fail(YS_ERR_BAD_ARG, "null adjoint");
+    ys_scene* s = a->s;
+    if (d_k || d_L) {
+        ys_status r = ys_scene_set_grid_springs(s, a->mesh, d_k, d_L);
+        if (r) return r;
+    }
+    if (d_v0) k_mesh_pack4<<<ceil_div(a->nV, 256), 256, 0, s->stream>>>(d_v0, a->v0.p, a->voff, a->nV);
+    YS_CK(cudaGetLastError());
+    a->forward_done = false;
+    return YS_OK;
+}
+
+// Forward rollout of T substeps from the initial state; x_T of the cloth
+// (3 floats per vertex) into d_xT.
+ys_status ys_adjoint_forward(ys_adjoint* a, float* d_xT) {
+    if (!a) return fail(YS_ERR_BAD_ARG, "null adjoint");
+    ys_scene* s = a->s;
+    restore_state(s, a->x0.p, a->x0.p, a->v0.p, 0, 0);
+    const bool rec = s->record;
+    s->record = false;
+    ys_status r = YS_OK;
+    for (u32 t = 0; t < a->T && !r; ++t) {
+        if (t % a->K == 0) {
+            const u32 i = t / a->K;
+            const size_t bytes = sizeof(float4) * s->nV;
+            const float4* xp = s->snapshot_pending ? s->X[s->cur].p : s->X[s->prev].p;
+            YS_CK(cudaMemcpyAsync(a->ck_x[i].p, s->X[s->cur].p, bytes, cudaMemcpyDeviceToDevice, s->stream));
+            YS_CK(cudaMemcpyAsync(a->ck_xp[i].p, xp, bytes, cudaMemcpyDeviceToDevice, s->stream));
+            YS_CK(cudaMemcpyAsync(a->ck_v[i].p, s->V[s->cv].p, bytes, cudaMemcpyDeviceToDevice, s->stream));
+            a->ck_frame[i] = s->frame;
+            a->ck_cursor[i] = s->cursor;
+        }
+        r = fused_substep(s);
+    }
+    s->record = rec;
+    if (r) return r;
+    if (d_xT) k_mesh_unpack4<<<ceil_div(a->nV, 256), 256, 0, s->stream>>>(s->X[s->cur].p, d_xT, a->voff, a->nV);
+    YS_CK(cudaGetLastError());
+    a->forward_done = true;
+    return YS_OK;
+}
+
+// Reverse pass: dL/dx_T of the cloth in, gradients w.r.t. per-spring
+// stiffness, rest length and the initial velocity out (device pointers).
+ys_status ys_adjoint_backward(ys_adjoint* a, const float* d_dLdx, float* d_gk, float* d_gL, float* d_gv0) {
+    if (!a || !d_dLdx || !d_gk || !d_gL || !d_gv0) return fail(YS_ERR_BAD_ARG, "null argument");
+    if (!a->forward_done) return fail(YS_ERR_STATE, "run ys_adjoint_forward first");
+    ys_scene* s = a->s;
+    cudaStream_t st = s->stream;
+    const size_t bytes = sizeof(float4) * s->nV;
+    YS_CK(cudaMemsetAsync(a->ax.p, 0, bytes, st));
+    YS_CK(cudaMemsetAsync(a->av.p, 0, bytes, st));
+    k_mesh_pack4<<<ceil_div(a->nV, 256), 256, 0, st>>>(d_dLdx, a->ax.p, a->voff, a->nV);
+    YS_CK(cudaMemsetAsync(d_gk, 0, 4 * (size_t)a->S, st));
+    YS_CK(cudaMemsetAsync(d_gL, 0, 4 * (size_t)a->S, st));
+    ys_status r = YS_OK;
+    const bool rec = s->record;
+    VContact* keep_pool = s->pool.p;
+    u32* keep_vs = s->vstart.p;
+    u32* keep_vc = s->vcount.p;
+    if ((r = ensure_record(s))) return r;
+    keep_pool = s->pool.p; keep_vs = s->vstart.p; keep_vc = s->vcount.p;
+    for (int seg = (int)a->nseg - 1; seg >= 0 && !r; --seg) {
+        const u32 t0 = (u32)seg * a->K, t1 = std::min(a->T, t0 + a->K);
+        restore_state(s, a->ck_x[seg].p, a->ck_xp[seg].p, a->ck_v[seg].p, a->ck_frame[seg], a->ck_cursor[seg]);
+        s->record = true;
+        for (u32 t = t0; t < t1 && !r; ++t) {
+            const u32 k = t - t0;
+            YS_CK(cudaMemcpyAsync(a->st_x[k].p, s->X[s->cur].p, bytes, cudaMemcpyDeviceToDevice, st));
+            YS_CK(cudaMemcpyAsync(a->st_v[k].p, s->V[s->cv].p, bytes, cudaMemcpyDeviceToDevice, st));
+            s->pool.p = a->st_pool[k].p;
+            s->vstart.p = a->st_vstart[k].p;
+            s->vcount.p = a->st_vcount[k].p;
+            r = fused_substep(s);
+        }
+        s->pool.p = keep_pool; s->vstart.p = keep_vs; s->vcount.p = keep_vc;
+        s->record = rec;
+        if (r) break;
+        for (int t = (int)t1 - 1; t >= (int)t0; --t) {
+            const u32 k = (u32)t - t0;
+            StepArgs A = make_args(s);
+            AdjArgs J;
+            J.x = a->st_x[k].p; J.v = a->st_v[k].p;
+            J.vstart = a->st_vstart[k].p; J.vcount = a->st_vcount[k].p; J.pool = a->st_pool[k].p;
+            J.ax = a->ax.p; J.av = a->av.p; J.xbar = a->xbar.p; J.vbar = a->vbar.p; J.fbar = a->fbar.p;
+            J.ax_out = a->ax2.p; J.av_out = a->av2.p;
+            J.gk = d_gk; J.gL = d_gL;
+            J.voff = a->voff; J.nV = a->nV; J.N = a->N;
+            // forces at step t read the step's own state
+            A.x = J.x; A.v = J.v;
+            k_adj_vertex<<<ceil_div(a->nV, 128), 128, 0, st>>>(A, J, (u32)a->mesh);
+            k_adj_springs<<<ceil_div(a->nV, 128), 128, 0, st>>>(A, J, (u32)a->mesh);
+            YS_CK(cudaGetLastError());
+            std::swap(a->ax.p, a->ax2.p);
+            std::swap(a->av.p, a->av2.p);
+        }
+    }
+    if (r) return r;
+    k_mesh_unpack4<<<ceil_div(a->nV, 256), 256, 0, st>>>(a->av.p, d_gv0, a->voff, a->nV);
+    YS_CK(cudaGetLastError());
+    YS_CK(cudaStreamSynchronize(st));
     return YS_OK;
 }
 

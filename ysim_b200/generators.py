@@ -205,28 +205,36 @@ def config_c1(seed: int = 1, P: int = 64, level: int = 4, height: float = 1.0) -
     return SceneSpec("c1_fastgrid64_ico4", Params(subh=1.0 / 6000.0, substeps=10), [cloth, obst], seed)
 
 
-def config_c2(seed: int = 2, P: int = 512, level: int = 7, height: float = 0.40, self_mode: int = 1,
-              obstacle: bool = True) -> SceneSpec:
-    """Plain TriangularCloth 512x512 (262,144 v, 522,242 tris), jitter
+def config_c2(seed: int = 2, P: int = 512, level: int = 7, height: float = 0.37, self_mode: int = 1,
+              obstacle: bool = True, size: float = 1.0, kstretch: float = 1e3, kbend: float = 1e1,
+              gravity: float = -1.0) -> SceneSpec:
+    """Plain TriangularCloth P x P (512: 262,144 v, 522,242 tris), jitter
     U(-0.1s, 0.1s) on all axes, self-collision on, over a static displaced
-    level-7 icosphere (r 0.3, radial noise amplitude 0.05); subh 1/1200,
-    20 substeps/frame.  Margin and radius are the reference defaults scaled by
-    the grid-spacing ratio (1/511)/(1/63) so the contact band stays about one
-    edge length, as in the reference's 64-grid scenes; the contact thickness
-    is C1's 1e-3 scaled the same way (about 6% of an edge)."""
+    level-7 icosphere (radius 0.3 size, radial noise amplitude 0.05 size);
+    subh 1/1200, 20 substeps/frame.  Margin, radius and contact thickness are
+    the reference defaults (0.015, 0.012) and C1's thickness (1e-3) scaled by
+    the grid-spacing ratio so the contact band stays about one edge length, as
+    in the reference's 64-grid scenes.  `size` scales the whole scene.
+    Gravity is 1 m/s^2: at this resolution and step the explicit integrator's
+    stability bound (k/m below about 0.67/subh^2) leaves a 1 m sheet under
+    9.81 m/s^2 stretched by several hundred percent under its own weight; it
+    then crumples through itself and the reference's self-contact push blows
+    it up (measured: every stiffness / damping variant at 9.81 diverges within
+    about 10 frames of contact)."""
     from ._lib import MESH_COLLIDABLE, MESH_SELF_COLLIDE, TRIANGULAR_CLOTH
     rng = np.random.Generator(np.random.PCG64(seed))
-    s = 1.0 / (P - 1)
-    x, f = grid_cloth(P, 1.0, (0.0, height, 0.0))
+    s = size / (P - 1)
+    x, f = grid_cloth(P, size, (0.0, height * size, 0.0))
     x = (x + rng.uniform(-0.1 * s, 0.1 * s, x.shape).astype(F32)).astype(F32)
+    scale = s / (1.0 / 63.0)
     cloth = Mesh(behavior=TRIANGULAR_CLOTH, flags=MESH_COLLIDABLE | MESH_SELF_COLLIDE, x=x, facets=f,
-                 v=np.zeros_like(x), mass=np.full(P * P, 1e-2, F32), mask=np.ones(P * P, F32), kstretch=1e3,
-                 kshear=5e2, kbend=1e1, thickness=1e-3 * (63.0 / (P - 1)))
-    scale = (1.0 / (P - 1)) / (1.0 / 63.0)
-    prm = Params(subh=1.0 / 1200.0, substeps=20, margin=0.015 * scale, radius=0.012 * scale, self_mode=self_mode)
+                 v=np.zeros_like(x), mass=np.full(P * P, 1e-2, F32), mask=np.ones(P * P, F32), kstretch=kstretch,
+                 kshear=5e2, kbend=kbend, thickness=1e-3 * scale)
+    prm = Params(subh=1.0 / 1200.0, substeps=20, margin=0.015 * scale, radius=0.012 * scale, self_mode=self_mode,
+                 gravity=(0.0, gravity, 0.0))
     meshes = [cloth]
     if obstacle:
-        meshes.append(obstacle_sphere(level, 0.3, amplitude=0.05, seed=seed + 1000))
+        meshes.append(obstacle_sphere(level, 0.3 * size, amplitude=0.05 * size, seed=seed + 1000))
     return SceneSpec(f"c2_tricloth{P}_ico{level}", prm, meshes, seed)
 
 
