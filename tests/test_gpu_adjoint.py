@@ -36,65 +36,107 @@ def test_uniform_grid_springs_reproduce_fastgrid(cuda_lib):
         b.close()
 
 
-def _problem(spec, T, seed=0):
-    import torch
+def _problem(spec, seed=0):
+    """Uniform FastGrid springs, a random initial velocity and a linear loss
+    sum(w * x_T).  The loss is linear so that its gradient (the adjoint seed)
+    is the same exact array in FP32 and FP64: a quadratic loss seeded with
+    2 (x_T - x*) would carry the FP32 quantisation of x_T (~3e-8 at |x| ~ 0.5)
+    into a seed whose entries are themselves ~1e-6, i.e. percent-level noise
+    before the adjoint even starts."""
     from ysim_b200 import generators as G
     from oracle import oracle as O
     c = spec.meshes[0]
     k, L = G.grid_spring_params(c.grid_n, c.grid_rest, (c.kstretch, c.kshear, c.kbend))
     rng = np.random.default_rng(seed)
-    kt = (k * np.exp(rng.normal(0, 0.3, len(k)))).astype(np.float64)
     v0 = rng.normal(0, 0.02, (c.nV, 3)).astype(np.float32)
-    R = O.Rollout(spec, kt, L, v0=v0)
-    xstar, _ = R.forward(T)
-    R.set(k, L)
-    return k, L, v0, xstar, R
+    w = (rng.normal(0, 1, (c.nV, 3)) / c.nV).astype(np.float32)
+    R = O.Rollout(spec, k, L, v0=v0)
+    return k, L, v0, w, R
 
 
-def test_adjoint_matches_fp64_reference_and_fd(cuda_lib):
+# Windows on which the rollout is a smooth function of the parameters and the
+# FP32 and FP64 forwards take the same branch at every step.  The contact
+# response pushes a penetrating vertex out to the thickness along the contact
+# normal and removes its approaching normal velocity, so on the next step that
+# vertex is re-tested `d < thickness` with d on the boundary itself: FP32 and
+# FP64 (and any finite-difference perturbation) pick "push again" or "release"
+# by round-off, after which the rollouts are different branches of a
+# piecewise-smooth map.  The contact window therefore ends at the first step
+# with a push (found with the FP32 oracle, whose forward is bit-identical to
+# the CUDA one); the contact-free window runs 40 steps of springs and
+# integration alone.
+WINDOWS = [pytest.param(0.5, False, id="contact_free_40"),
+           pytest.param(0.2995, True, id="contacts_to_first_push")]
+
+
+def _window(spec, v0, contacts):
+    if not contacts:
+        return 40
+    from oracle import oracle as O
+    S = O.OracleScene(spec)
+    v = S.get("v")
+    v[: len(v0)] = v0
+    S.set("v", v)
+    thickness = spec.meshes[0].thickness
+    for t in range(1, 41):
+        S.step(1)
+        off, c = S.contacts()
+        if (c["d"][: int(off[len(v0)])] < thickness).any():
+            return t
+    raise AssertionError("no contact push within 40 steps")
+
+
+@pytest.mark.parametrize("height,contacts", WINDOWS)
+def test_adjoint_matches_fp64_reference_and_fd(cuda_lib, height, contacts):
     import torch
     from ysim_b200.adjoint import ClothRollout
-    spec = _small()
-    T = 40
-    k, L, v0, xstar, R = _problem(spec, T)
+    spec = _small(height=height)
+    k, L, v0, w, R = _problem(spec)
+    T = _window(spec, v0, contacts)
     V = spec.meshes[0].nV
+    w64 = w.astype(np.float64)
     # FP64 reference adjoint
     x64, ncontacts = R.forward(T, keep=True)
-    assert ncontacts > 0
-    gk64, gL64, gv64 = R.backward(T, 2.0 * (x64 - xstar) / V)
+    assert (ncontacts > 0) == contacts
+    gk64, gL64, gv64 = R.backward(T, w64)
     # CUDA adjoint through torch.autograd
-    roll = ClothRollout(spec, steps=T, checkpoint_every=10)
+    roll = ClothRollout(spec, steps=T, checkpoint_every=5)
     try:
         kt = torch.tensor(k, device="cuda", requires_grad=True)
         Lt = torch.tensor(L, device="cuda", requires_grad=True)
         vt = torch.tensor(v0, device="cuda", requires_grad=True)
         xT = roll(kt, Lt, vt)
-        target = torch.tensor(xstar, dtype=torch.float32, device="cuda")
-        loss = ((xT - target) ** 2).sum(1).mean()
+        loss = (xT * torch.tensor(w, device="cuda")).sum()
         loss.backward()
         gk, gL, gv = kt.grad.cpu().numpy(), Lt.grad.cpu().numpy(), vt.grad.cpu().numpy()
-        # FP32 rollout vs the FP64 one: round-off only (40 steps, with contacts)
-        assert np.abs(xT.detach().cpu().numpy() - x64).max() < 5e-4
-        for g32, g64 in ((gk, gk64), (gL, gL64), (gv, gv64)):
-            rel = np.linalg.norm(g32 - g64) / max(np.linalg.norm(g64), 1e-30)
-            assert rel < 1e-3, rel
-        # FP64 central differences on a few parameters (eps 1e-6)
+        # FP32 rollout vs the FP64 one: round-off only on a branch-stable window
+        assert np.abs(xT.detach().cpu().numpy() - x64).max() < 1e-6
+        # FP32 adjoint vs FP64 adjoint, norm-relative per parameter group
+        rels = {name: np.linalg.norm(g32 - g64) / max(np.linalg.norm(g64), 1e-30)
+                for name, g32, g64 in (("k", gk, gk64), ("L", gL, gL64), ("v0", gv, gv64))}
+        print("adjoint rel err", rels)
+        assert max(rels.values()) < 1e-3, rels
+        # FP64 central differences (step 1e-6 relative for k, 1e-6 absolute for L, v0)
         rng = np.random.default_rng(3)
-        loss64 = lambda x: float(((x - xstar) ** 2).sum(1).mean())
-        eps = 1e-6
+        loss64 = lambda x: float((x * w64).sum())
         checks = []
         for _ in range(3):
             i = int(rng.integers(len(k)))
+            eps = 1e-6 * float(k[i])
             kk = k.astype(np.float64).copy(); kk[i] += eps; R.set(kk, L); lp = loss64(R.forward(T)[0])
             kk[i] -= 2 * eps; R.set(kk, L); lm = loss64(R.forward(T)[0]); R.set(k, L)
-            checks.append((gk[i], (lp - lm) / (2 * eps)))
+            checks.append((gk[i], (lp - lm) / (2 * eps), np.abs(gk64).max()))
+            i = int(rng.integers(len(L)))
+            eps = 1e-6
+            ll = L.astype(np.float64).copy(); ll[i] += eps; R.set(k, ll); lp = loss64(R.forward(T)[0])
+            ll[i] -= 2 * eps; R.set(k, ll); lm = loss64(R.forward(T)[0]); R.set(k, L)
+            checks.append((gL[i], (lp - lm) / (2 * eps), np.abs(gL64).max()))
             j = int(rng.integers(3 * V))
             vv = v0.reshape(-1).astype(np.float64).copy(); vv[j] += eps; R.set(v0=vv); lp = loss64(R.forward(T)[0])
             vv[j] -= 2 * eps; R.set(v0=vv); lm = loss64(R.forward(T)[0]); R.set(v0=v0.reshape(-1))
-            checks.append((gv.reshape(-1)[j], (lp - lm) / (2 * eps)))
-        scale = max(abs(fd) for _, fd in checks)
-        for g, fd in checks:
-            assert abs(g - fd) <= 1e-3 * scale + 1e-3 * abs(fd), (g, fd)
+            checks.append((gv.reshape(-1)[j], (lp - lm) / (2 * eps), np.abs(gv64).max()))
+        for g, fd, scale in checks:
+            assert abs(g - fd) <= 1e-3 * scale + 1e-2 * abs(fd), (g, fd, scale)
     finally:
         roll.close()
 
@@ -104,7 +146,7 @@ def test_checkpoint_interval_does_not_change_gradients(cuda_lib):
     from ysim_b200.adjoint import ClothRollout
     spec = _small()
     T = 24
-    k, L, v0, xstar, _ = _problem(spec, T, seed=1)
+    k, L, v0, w, _ = _problem(spec, seed=1)
     out = []
     for K in (1, 5, 24):
         roll = ClothRollout(spec, steps=T, checkpoint_every=K)
@@ -112,7 +154,7 @@ def test_checkpoint_interval_does_not_change_gradients(cuda_lib):
             kt = torch.tensor(k, device="cuda", requires_grad=True)
             Lt = torch.tensor(L, device="cuda", requires_grad=True)
             vt = torch.tensor(v0, device="cuda", requires_grad=True)
-            loss = ((roll(kt, Lt, vt) - torch.tensor(xstar, dtype=torch.float32, device="cuda")) ** 2).sum(1).mean()
+            loss = (roll(kt, Lt, vt) * torch.tensor(w, device="cuda")).sum()
             loss.backward()
             out.append((kt.grad.cpu().numpy(), Lt.grad.cpu().numpy(), vt.grad.cpu().numpy()))
         finally:
