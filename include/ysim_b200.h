@@ -243,6 +243,18 @@ ys_status ys_morton_codes(const float* d_x, uint32_t num_vertices, const uint32_
  * ys_radix_sort_scratch_bytes(n) bytes. */
 size_t ys_radix_sort_scratch_bytes(uint32_t n);
 ys_status ys_radix_sort_pairs(uint32_t* d_keys, uint32_t* d_vals, uint32_t n, void* d_scratch, void* stream);
+/* The same sort for callers that cannot allocate device memory: code running
+ * under CUDA-graph capture or in an allocation-free real-time loop, hosts
+ * whose device memory belongs to another allocator, plugins that must not
+ * grow the process's device footprint.  It calls no cudaMalloc / cudaFree and
+ * no allocating library routine; its scratch is a fixed 8,651,776-byte
+ * __device__ array that every GPU loading this library holds until exit.
+ * At most 1,048,576 pairs (larger n returns YS_ERR_CAPACITY).  The first call
+ * on a device looks up that array's device address, so make it before any
+ * stream capture.  All calls share the one array: calls that overlap on the
+ * GPU (different streams or threads without ordering) race.  Asynchronous on
+ * `stream`.  Has no counterpart in the reference. */
+ys_status ys_radix_sort_pairs_noalloc(uint32_t* d_keys, uint32_t* d_vals, uint32_t n, void* stream);
 
 #ifdef __cplusplus
 }

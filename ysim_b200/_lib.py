@@ -119,6 +119,7 @@ _PROTOS = {
                                   C.c_void_p]),
     "ys_radix_sort_scratch_bytes": (C.c_size_t, [C.c_uint32]),
     "ys_radix_sort_pairs": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p]),
+    "ys_radix_sort_pairs_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p]),
 }
 
 # every symbol the header declares (tests check the library exports them all)

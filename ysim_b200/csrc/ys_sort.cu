@@ -168,3 +168,62 @@ cudaError_t radix_sort_pairs(u32* keys, u32* vals, u32 n, void* scratch, int beg
 }
 
 }  // namespace ys
+
+// ---------------------------------------------------------------------------
+// Sort with no allocation at all, for callers that cannot call cudaMalloc:
+// code that runs inside a CUDA-graph capture or an allocation-free real-time
+// loop, hosts whose device memory is owned by another allocator (a game
+// engine's or a framework's pool), and plugins that must not grow the
+// process's device footprint behind the host's back.  The scratch lives in a
+// file-scope __device__ array of fixed size, reserved on every GPU that loads
+// this library until the process exits.
+#include <mutex>
+#include <string>
+
+#include "ysim_b200.h"
+
+namespace ys {
+ys_status fail(ys_status code, const std::string& msg);
+
+static constexpr u32 NOALLOC_MAX_PAIRS = 1u << 20;  // 1,048,576 pairs
+static constexpr size_t NOALLOC_SCRATCH_BYTES =
+    (size_t)256 * (NOALLOC_MAX_PAIRS / TILE) * 4 + 256 * 4 + (size_t)2 * NOALLOC_MAX_PAIRS * 4;  // 8,651,776 B
+static __device__ __align__(256) unsigned char g_noalloc_sort_scratch[NOALLOC_SCRATCH_BYTES];
+
+static std::mutex g_noalloc_mutex;
+static void* g_noalloc_addr[64] = {};
+}  // namespace ys
+
+extern "C" ys_status ys_radix_sort_pairs_noalloc(uint32_t* d_keys, uint32_t* d_vals, uint32_t n, void* stream) {
+    using namespace ys;
+    if (n > NOALLOC_MAX_PAIRS)
+        return fail(YS_ERR_CAPACITY, "ys_radix_sort_pairs_noalloc: n = " + std::to_string(n) +
+                                         " exceeds the fixed scratch capacity of " +
+                                         std::to_string(NOALLOC_MAX_PAIRS) + " pairs");
+    if (n > 1 && (!d_keys || !d_vals)) return fail(YS_ERR_BAD_ARG, "ys_radix_sort_pairs_noalloc: null array");
+    if (n <= 1) return YS_OK;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return fail(YS_ERR_CUDA, std::string("cudaGetDevice: ") + cudaGetErrorString(e));
+    if (dev < 0 || dev >= 64) return fail(YS_ERR_BAD_ARG, "device index out of range");
+    void* scratch = nullptr;
+    {
+        // first call on this device: look up the device address of the array
+        // (its host-side name is only a stand-in and must never reach a kernel)
+        std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+        if (!g_noalloc_addr[dev]) {
+            void* p = nullptr;
+            e = cudaGetSymbolAddress(&p, g_noalloc_sort_scratch);
+            if (e != cudaSuccess)
+                return fail(YS_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+            g_noalloc_addr[dev] = p;
+        }
+        scratch = g_noalloc_addr[dev];
+    }
+    // Every pass overwrites the whole histogram / totals region it reads and
+    // the ping-pong halves are written before they are read, so nothing left
+    // by an earlier call needs clearing.  4 passes end in the caller's arrays.
+    e = radix_sort_pairs(d_keys, d_vals, n, scratch, 0, 32, (cudaStream_t)stream);
+    if (e != cudaSuccess) return fail(YS_ERR_CUDA, std::string("radix sort: ") + cudaGetErrorString(e));
+    return YS_OK;
+}
