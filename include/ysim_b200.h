@@ -56,6 +56,18 @@ typedef int ys_status;
 #define YS_SELF_HASH 1u
 #define YS_SELF_BVH 2u
 
+/* Morton normalisation of the scene's trees.  REFERENCE scales each axis by
+ * the mesh box's own width (fillMortons_Tri, src/metal/bvh.metal:42-63), which
+ * reproduces the reference's tree node for node.  CUBE (the default) scales
+ * all axes by the largest width: on a flat, jittered sheet the per-axis form
+ * spreads the thin axis's jitter over all ten of its bits, so the tree splits
+ * on it at every third level into siblings covering the same area, and each
+ * query descends both.  The candidate sets, contacts and positions are the
+ * same under both layouts (every leaf box is the same; only the order of the
+ * descent changes). */
+#define YS_TREE_REFERENCE 0
+#define YS_TREE_CUBE 1
+
 /* Simulator / SymplecticSystem parameters: subh, kair, kd
  * (symplectic_system.hpp:191-198), gravity (Scene::environment), margin and
  * radius (simulator.hpp:180-181), substeps per frame, BVH rebuild period in
@@ -136,6 +148,10 @@ ys_status ys_scene_set_record(ys_scene* s, int record);
 /* Replay each fused substep as a captured CUDA graph (default on; substeps
  * that rebuild trees, record contacts or time kernels run eagerly). */
 ys_status ys_scene_set_graphs(ys_scene* s, int on);
+/* Tree layout (YS_TREE_REFERENCE / YS_TREE_CUBE) for every tree the scene
+ * builds; call between ys_scene_create and ys_scene_pack.  Replaces the
+ * Morton normalisation inside BVH<..>::build (include/sim/bvh.hpp:1194-1301). */
+ys_status ys_scene_set_tree_layout(ys_scene* s, int layout);
 ys_status ys_scene_sync(ys_scene* s);
 /* CUDA stream of the scene (cudaStream_t) as void*. */
 ys_status ys_scene_stream(ys_scene* s, void** stream_out);

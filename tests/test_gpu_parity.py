@@ -169,13 +169,17 @@ def _advance_to_contact(spec, frames):
     return o
 
 
+@pytest.mark.parametrize("layout", [0, 1], ids=["reference_tree", "cube_tree"])
 @pytest.mark.parametrize("name", ["c1", "c2hash", "c2bvh"])
-def test_scene_staged_and_fused_match_oracle(cuda_lib, oracle, name):
+def test_scene_staged_and_fused_match_oracle(cuda_lib, oracle, name, layout):
+    """Rows, contacts and states equal the oracle's (which builds the
+    reference's trees) under both tree layouts: the layout changes the descent
+    order, never a candidate set."""
     from ysim_b200.scene import Scene
     spec = _small_specs()[name]
     o = _advance_to_contact(spec, 3)
     x0, v0, xp0 = o.get("x"), o.get("v"), o.get("xprev")
-    s = Scene(spec)
+    s = Scene(spec, tree_layout=layout)
     try:
         # both sides start at frame 0 from the same mid-drape state, so the
         # frame-0 preamble rebuilds every non-Float tree from x0 on both
@@ -211,7 +215,7 @@ def test_scene_staged_and_fused_match_oracle(cuda_lib, oracle, name):
     finally:
         s.close()
     # fused path from the same state
-    s = Scene(spec)
+    s = Scene(spec, tree_layout=layout)
     try:
         s.set("x", x0); s.set("v", v0); s.set("xprev", xp0)
         s.set_record(True)
@@ -233,9 +237,12 @@ def test_scene_staged_and_fused_match_oracle(cuda_lib, oracle, name):
 
 
 def test_scene_tree_matches_oracle(cuda_lib, oracle):
+    """With the reference layout the scene's trees are the reference's, node
+    for node (codes, order, parents, boxes)."""
+    from ysim_b200 import _lib
     from ysim_b200.scene import Scene
     spec = _small_specs()["c2hash"]
-    s = Scene(spec)
+    s = Scene(spec, tree_layout=_lib.TREE_REFERENCE)
     o = oracle.OracleScene(spec)
     o.stage(0)
     try:

@@ -33,6 +33,8 @@ MESH_SELF_COLLIDE = 4
 SELF_OFF = 0
 SELF_HASH = 1
 SELF_BVH = 2
+TREE_REFERENCE = 0  # Morton normalisation per axis, node for node the reference's tree
+TREE_CUBE = 1       # one scale for all axes (default)
 
 
 class SimParams(C.Structure):
@@ -79,6 +81,7 @@ _PROTOS = {
     "ys_scene_step": (C.c_int, [C.c_void_p, C.c_uint32]),
     "ys_scene_set_record": (C.c_int, [C.c_void_p, C.c_int]),
     "ys_scene_set_graphs": (C.c_int, [C.c_void_p, C.c_int]),
+    "ys_scene_set_tree_layout": (C.c_int, [C.c_void_p, C.c_int]),
     "ys_scene_sync": (C.c_int, [C.c_void_p]),
     "ys_scene_stream": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
     "ys_scene_get_state": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),

@@ -69,15 +69,23 @@ __device__ __forceinline__ float clamp01023(float v) { return fminf(fmaxf(v, 0.f
 
 // fillMortons_Tri (bvh.metal:42-63): centroid ((x0+x1)+x2)/3, normalised by
 // the scene box (width clamped to >= 1e-8), 10 bits per axis, code = x*4+y*2+z.
+// cube != 0 normalises all three axes by the box's largest width instead of
+// each axis by its own: a flat sheet's thin axis then keeps its few high bits
+// constant rather than spreading its jitter over all ten, which would split the
+// tree on that axis at every third level into siblings covering the same area.
 __global__ void __launch_bounds__(256) k_morton(const float4* x4, const float* x3, u32 voff, const u32* __restrict__ F,
                                                 u32 nF, const u32* __restrict__ box, u32* __restrict__ codes,
-                                                u32* __restrict__ idx) {
+                                                u32* __restrict__ idx, int cube) {
     u32 i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= nF) return;
     f3 bmin = mk(funord(box[0]), funord(box[1]), funord(box[2]));
     f3 bmax = mk(funord(box[3]), funord(box[4]), funord(box[5]));
     f3 w = bmax - bmin;
     w = mk(fmaxf(w.x, 1e-8f), fmaxf(w.y, 1e-8f), fmaxf(w.z, 1e-8f));
+    if (cube) {
+        const float W = fmaxf(w.x, fmaxf(w.y, w.z));
+        w = mk(W, W, W);
+    }
     f3 c = (load_pos(x4, x3, voff + F[3 * i]) + load_pos(x4, x3, voff + F[3 * i + 1]) +
             load_pos(x4, x3, voff + F[3 * i + 2])) / 3.0f;
     c = (c - bmin) / w;
@@ -88,9 +96,9 @@ __global__ void __launch_bounds__(256) k_morton(const float4* x4, const float* x
 }
 
 void launch_morton(const float4* x4, const float* x3, u32 voff, const u32* facets, u32 nF, const u32* box, u32* codes,
-                   u32* idx, cudaStream_t s) {
+                   u32* idx, cudaStream_t s, bool cube) {
     if (nF == 0) return;
-    k_morton<<<ceil_div(nF, 256), 256, 0, s>>>(x4, x3, voff, facets, nF, box, codes, idx);
+    k_morton<<<ceil_div(nF, 256), 256, 0, s>>>(x4, x3, voff, facets, nF, box, codes, idx, cube ? 1 : 0);
 }
 
 // ------------------------------------------------------------------ Karras

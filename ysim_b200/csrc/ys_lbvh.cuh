@@ -33,9 +33,10 @@ struct RefitJob {
 // bits stored via ordered-int atomics; call box_init first).
 void launch_box_init(u32* box, cudaStream_t s);
 void launch_box(const float4* x4, const float* x3, u32 voff, u32 nV, u32* box, cudaStream_t s);
-// Morton code per face from the scene box (fillMortons_Tri, bvh.metal:42-63).
+// Morton code per face from the scene box (fillMortons_Tri, bvh.metal:42-63);
+// cube = one scale for all axes (the box's largest width) instead of per axis.
 void launch_morton(const float4* x4, const float* x3, u32 voff, const u32* facets, u32 nF, const u32* box, u32* codes,
-                   u32* idx, cudaStream_t s);
+                   u32* idx, cudaStream_t s, bool cube = false);
 // Karras topology (buildTree_Tri, bvh.metal:352-393); zeroes visit counters.
 // Runs of three or more equal Morton codes make the reference's topology
 // inconsistent (findSplit splits them at the midpoint, bvh.metal:204, while

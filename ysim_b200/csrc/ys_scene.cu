@@ -217,36 +217,219 @@ __device__ __forceinline__ void warp_count(unsigned long long* ctr, u32 v) {
 }
 
 // ------------------------------------------------------------------ fused
+// One thread per vertex, but the per-candidate work (the H1 face test with its
+// two point-triangle distances, and the narrow test) is not done inside the
+// thread's own tree descent, where a warp would run it with the few lanes that
+// reached a leaf on that iteration.  Descents only push (owner lane, mesh,
+// face) into a per-warp queue in shared memory; whenever 32 candidates wait,
+// the whole warp takes one each, fetching the owner's positions by shuffle.
+// Contacts go back to their owner through a per-warp buffer and are inserted
+// into the owner's sorted list, which keeps the MAXC smallest (mesh, face)
+// keys whatever the arrival order -- so results are those of a per-vertex
+// loop over candidates in descent order.
+static constexpr int FUSED_WARPS = 4;  // 128-thread blocks
+static constexpr u32 WQ_CAP = 64;      // candidate queue: < 32 left over + 32 new
+static constexpr u32 WC_CAP = 64;      // contact buffer between flushes
+static constexpr u32 KEY_SELF = 32u;   // queue key: (mesh << 6) | KEY_SELF? | owner lane
+static constexpr unsigned FULL_MASK = 0xFFFFFFFFu;
+
+struct WarpWork {
+    u32 qf[WQ_CAP];
+    u32 qk[WQ_CAP];
+    VContact cb[WC_CAP];
+    unsigned char co[WC_CAP];
+};
+
+__device__ __forceinline__ void insert_contact(VContact (&buf)[MAXC], int& nc, u32& st, const VContact& c) {
+    if (nc == MAXC) {
+        st |= ST_CONTACT_OVF;
+        if (!key_less(c.tobj, c.tri, buf[MAXC - 1].tobj, buf[MAXC - 1].tri)) return;
+        --nc;
+    }
+    int i = nc;
+    while (i > 0 && key_less(c.tobj, c.tri, buf[i - 1].tobj, buf[i - 1].tri)) { buf[i] = buf[i - 1]; --i; }
+    buf[i] = c;
+    ++nc;
+}
+
 __global__ void __launch_bounds__(128) k_fused(StepArgs A) {
+    __shared__ WarpWork wq[FUSED_WARPS];
+    const u32 lane = threadIdx.x & 31u;
+    WarpWork& Q = wq[threadIdx.x >> 5];
     const u32 g = blockIdx.x * blockDim.x + threadIdx.x;
-    if (g >= A.nV) return;
-    const u32 m = A.vobj[g];
+    const bool valid = g < A.nV;
+    const u32 m = valid ? A.vobj[g] : 0u;
     const MeshDev M = A.meshes[m];
-    const f3 xc = ld(A.x, g);
+    const f3 xc = valid ? ld(A.x, g) : mk(0.f, 0.f, 0.f);
+    const bool query = valid && (M.flags & MF_QUERY) && (M.flags & MF_TREE);
+    const f3 xpv = query ? ld(A.xp, g) : xc;
+    const float mg = A.margin;
+    u32 st = 0, rows = 0;
+
+    // ---- descent state: stage 0 = own tree, 1 + k = target k
+    float inv = 0.f;
+    bool selfOK = false;
+    f3 smn = xc, smx = xc;
+    if (query) {
+        if (A.self_mode == YS_SELF_HASH && (M.flags & MF_CLOTH) && (M.flags & MF_SELF)) {
+            float mx = __uint_as_float(A.maxext[m]);
+            float cs = (mx > 1e-5f) ? mx : 1e-5f;
+            inv = 1.f / cs;
+            H1Vertex h;
+            if (h1_vertex(xc, xpv, inv, h)) { selfOK = true; h1_query_box(h, mg, smn, smx); }
+        } else if (A.self_mode == YS_SELF_BVH) {
+            selfOK = true;
+            smn = xc - mk(mg, mg, mg);
+            smx = xc + mk(mg, mg, mg);
+        }
+    }
+    const u32 nstage = query ? 1u + (M.tgt_end - M.tgt_begin) : 0u;
+    u32 stage = 0;
+    int stack[STACK_DEPTH];
+    int sp = 0;
+    u32 visited = 0, nn = 0, key = 0;
+    const Node* nodes = A.nodes;
+    f3 qmn = xc, qmx = xc;
+    auto next_tree = [&]() -> bool {
+        while (stage < nstage) {
+            const u32 s = stage++;
+            if (s == 0) {
+                if (!selfOK || M.nF == 0) continue;
+                nodes = A.nodes + M.node_off;
+                nn = 2 * M.nF - 1;
+                qmn = smn;
+                qmx = smx;
+                key = (m << 6) | KEY_SELF | lane;
+            } else {
+                const u32 t = A.targets[M.tgt_begin + s - 1];
+                const u32 tno = A.meshes[t].node_off, tnf = A.meshes[t].nF;
+                if (tnf == 0 || !root_overlap(A.nodes + M.node_off, A.nodes + tno)) continue;
+                nodes = A.nodes + tno;
+                nn = 2 * tnf - 1;
+                qmn = xc - mk(mg, mg, mg);
+                qmx = xc + mk(mg, mg, mg);
+                key = (t << 6) | lane;
+            }
+            stack[0] = 0;
+            sp = 1;
+            visited = 0;
+            return true;
+        }
+        return false;
+    };
+
     VContact buf[MAXC];
     int nc = 0;
-    u32 nrows = 0, st = 0;
-    if (M.flags & MF_QUERY) {
-        const f3 xpv = ld(A.xp, g);
-        st |= query_vertex(A, g, m, M, xc, xpv, [&](u32 t, u32 f, uint4 tri, u32 tvoff) {
-            ++nrows;
-            f3 n;
-            float d;
-            if (!narrow_one(xc, xpv, ld(A.x, tvoff + tri.x), ld(A.x, tvoff + tri.y), ld(A.x, tvoff + tri.z), A.band, n,
-                            d))
-                return;
-            if (nc == MAXC) {
-                st |= ST_CONTACT_OVF;
-                if (!key_less(t, f, buf[MAXC - 1].tobj, buf[MAXC - 1].tri)) return;
-                --nc;
+    u32 qn = 0, cn = 0;  // warp-uniform fill of the queue and of the contact buffer
+
+    auto flush = [&]() {
+        __syncwarp();
+        for (u32 i = 0; i < cn; ++i)
+            if (Q.co[i] == lane) insert_contact(buf, nc, st, Q.cb[i]);
+        __syncwarp();
+        cn = 0;
+    };
+    // Process queue entries [base, base + cnt), cnt <= 32: lane i takes entry base + i.
+    auto drain = [&](u32 base, u32 cnt) {
+        __syncwarp();
+        const bool has = lane < cnt;
+        u32 f = 0, k = 0;
+        if (has) { f = Q.qf[base + lane]; k = Q.qk[base + lane]; }
+        __syncwarp();
+        const int owner = (int)(k & 31u);
+        const f3 oxc = mk(__shfl_sync(FULL_MASK, xc.x, owner), __shfl_sync(FULL_MASK, xc.y, owner),
+                          __shfl_sync(FULL_MASK, xc.z, owner));
+        const f3 oxp = mk(__shfl_sync(FULL_MASK, xpv.x, owner), __shfl_sync(FULL_MASK, xpv.y, owner),
+                          __shfl_sync(FULL_MASK, xpv.z, owner));
+        const u32 og = __shfl_sync(FULL_MASK, g, owner);
+        const float oinv = __shfl_sync(FULL_MASK, inv, owner);
+        bool hit = false;
+        VContact c;
+        if (has) {
+            const u32 t = k >> 6;
+            const u32 tvo = A.meshes[t].voff;
+            const uint4 tri = A.F[A.meshes[t].foff + f];
+            bool row = true;
+            if (k & KEY_SELF) {
+                if (A.self_mode == YS_SELF_HASH) {
+                    H1Vertex h;
+                    h1_vertex(oxc, oxp, oinv, h);  // accepted for the owner already
+                    row = h1_face(A.x, tvo, tri, og - tvo, mg, oinv, h);
+                } else {
+                    const u32 lid = og - tvo;
+                    row = !(tri.x == lid || tri.y == lid || tri.z == lid);
+                }
             }
-            int i = nc;
-            while (i > 0 && key_less(t, f, buf[i - 1].tobj, buf[i - 1].tri)) { buf[i] = buf[i - 1]; --i; }
-            buf[i] = VContact{t, f, n.x, n.y, n.z, d};
-            ++nc;
-        });
+            if (row) {
+                ++rows;
+                f3 n;
+                float d;
+                if (narrow_one(oxc, oxp, ld(A.x, tvo + tri.x), ld(A.x, tvo + tri.y), ld(A.x, tvo + tri.z), A.band, n,
+                               d)) {
+                    hit = true;
+                    c = VContact{t, f, n.x, n.y, n.z, d};
+                }
+            }
+        }
+        const unsigned hm = __ballot_sync(FULL_MASK, hit);
+        if (hm) {
+            if (cn + (u32)__popc(hm) > WC_CAP) flush();
+            if (hit) {
+                const u32 slot = cn + (u32)__popc(hm & ((1u << lane) - 1u));
+                Q.cb[slot] = c;
+                Q.co[slot] = (unsigned char)owner;
+            }
+            cn += (u32)__popc(hm);
+        }
+        __syncwarp();
+    };
+
+    bool active = query && next_tree();
+    while (true) {
+        if (active && sp == 0) active = next_tree();
+        if (!__ballot_sync(FULL_MASK, active)) break;
+        int leaf = -1;
+        if (active) {
+            if (++visited > VISIT_CAP) {
+                st |= ST_STACK_OVF;
+                sp = 0;
+            } else {
+                const int id = stack[--sp];
+                if (id >= 0 && (u32)id < nn) {
+                    const float4* p = reinterpret_cast<const float4*>(nodes + id);
+                    const float4 n0 = __ldg(p), n1 = __ldg(p + 1);
+                    if (overlap(qmn, qmx, n0, n1)) {
+                        const int a = __float_as_int(n0.w), b = __float_as_int(n1.w);
+                        if (a < 0) {
+                            leaf = b;
+                        } else if (sp + 2 > STACK_DEPTH) {
+                            st |= ST_STACK_OVF;
+                        } else {
+                            stack[sp++] = a;
+                            stack[sp++] = b;
+                        }
+                    }
+                }
+            }
+        }
+        const unsigned lm = __ballot_sync(FULL_MASK, leaf >= 0);
+        if (lm) {
+            if (leaf >= 0) {
+                const u32 slot = qn + (u32)__popc(lm & ((1u << lane) - 1u));
+                Q.qf[slot] = (u32)leaf;
+                Q.qk[slot] = key;
+            }
+            qn += (u32)__popc(lm);
+            if (qn >= 32) {
+                drain(qn - 32, 32);
+                qn -= 32;
+            }
+        }
     }
-    if (M.flags & MF_CLOTH) {
+    if (qn) drain(0, qn);
+    if (cn) flush();
+
+    if (valid && (M.flags & MF_CLOTH)) {
         f3 vel = ld(A.v, g);
         const float mass = A.mass[g], mask = A.mask[g];
         const f3 force = vertex_force(A, M, g, xc, vel, mass);
@@ -257,12 +440,12 @@ __global__ void __launch_bounds__(128) k_fused(StepArgs A) {
         if (sanitize(pos, vel, xc)) st |= ST_NONFINITE;
         A.xn[g] = make_float4(pos.x, pos.y, pos.z, 0.f);
         A.vn[g] = make_float4(vel.x, vel.y, vel.z, 0.f);
-    } else if (!(M.flags & MF_STATIC)) {
+    } else if (valid && !(M.flags & MF_STATIC)) {
         // not integrated (Rigid / Float / Kinematic): carry the state over
         A.xn[g] = A.x[g];
         A.vn[g] = A.v[g];
     }
-    if (A.record) {
+    if (valid && A.record) {
         u32 base = (u32)atomicAdd(&A.counters[2], (unsigned long long)nc);
         if (base + (u32)nc > A.cap) {
             st |= ST_PAIR_OVF;
@@ -274,7 +457,7 @@ __global__ void __launch_bounds__(128) k_fused(StepArgs A) {
             A.vcount[g] = (u32)nc;
         }
     }
-    warp_count(&A.counters[0], nrows);
+    warp_count(&A.counters[0], rows);
     warp_count(&A.counters[1], (u32)nc);
     if (st) atomicOr(A.status, st);
 }
@@ -526,6 +709,7 @@ struct ys_scene {
     // refit + fused substep replayed without host launch overhead
     bool use_graphs = true;
     cudaGraphExec_t graphs[18] = {};
+    int tree_layout = YS_TREE_CUBE;  // Morton normalisation of the scene trees
     DBuf<char> sortScratch, scanScratch;
     // staged / record buffers
     u32 cap = 0;
@@ -613,7 +797,8 @@ ys_status build_tree(ys_scene* s, HostMesh& H) {
     u32* idx = s->idx.p + H.foff;
     launch_box_init(s->box.p, st);
     launch_box(s->X[s->cur].p, nullptr, H.voff, H.d.num_vertices, s->box.p, st);
-    launch_morton(s->X[s->cur].p, nullptr, H.voff, s->F3.p + 3 * (size_t)H.foff, n, s->box.p, codes, idx, st);
+    launch_morton(s->X[s->cur].p, nullptr, H.voff, s->F3.p + 3 * (size_t)H.foff, n, s->box.p, codes, idx, st,
+                  s->tree_layout == YS_TREE_CUBE);
     YS_CK(radix_sort_pairs(codes, idx, n, s->sortScratch.p, 0, 32, st));
     launch_karras(codes, idx, n, s->nodes.p + H.node_off, s->parent.p + H.node_off, s->parent2.p + H.node_off,
                   s->visits.p + H.foff, st);
@@ -1088,6 +1273,14 @@ ys_status ys_scene_step(ys_scene* s, uint32_t n) {
 ys_status ys_scene_set_record(ys_scene* s, int record) {
     if (!s) return fail(YS_ERR_BAD_ARG, "null scene");
     s->record = record != 0;
+    return YS_OK;
+}
+
+ys_status ys_scene_set_tree_layout(ys_scene* s, int layout) {
+    if (!s) return fail(YS_ERR_BAD_ARG, "null scene");
+    if (s->packed) return fail(YS_ERR_STATE, "ys_scene_set_tree_layout: call before ys_scene_pack");
+    if (layout != YS_TREE_REFERENCE && layout != YS_TREE_CUBE) return fail(YS_ERR_BAD_ARG, "unknown tree layout");
+    s->tree_layout = layout;
     return YS_OK;
 }
 

@@ -68,7 +68,7 @@ class _System:
 class Scene:
     """A packed scene on one GPU (one CUDA stream)."""
 
-    def __init__(self, spec: SceneSpec, device: int = 0, pack: bool = True):
+    def __init__(self, spec: SceneSpec, device: int = 0, pack: bool = True, tree_layout: Optional[int] = None):
         self.lib = _lib.load()
         self.spec = spec
         p = spec.params
@@ -89,6 +89,8 @@ class Scene:
                               (C.c_float * 6)(*m.grid_rest), m.group)
             idx = C.c_int()
             _lib.check(self.lib.ys_scene_add_mesh(self.h, C.byref(d), C.byref(idx)), "ys_scene_add_mesh")
+        if tree_layout is not None:
+            _lib.check(self.lib.ys_scene_set_tree_layout(self.h, int(tree_layout)), "ys_scene_set_tree_layout")
         self.nV = spec.nV
         self.broad_phase = _BroadPhase(self)
         self.narrow_phase = _NarrowPhase(self)
