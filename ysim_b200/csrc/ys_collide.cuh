@@ -46,6 +46,66 @@ __device__ __forceinline__ u32 traverse(const Node* __restrict__ nodes, u32 numN
     return st;
 }
 
+__device__ __forceinline__ bool overlap_xyz(f3 qmn, f3 qmx, float lx, float ly, float lz, float hx, float hy,
+                                            float hz) {
+    if (qmx.x < lx || qmn.x > hx) return false;
+    if (qmx.y < ly || qmn.y > hy) return false;
+    if (qmx.z < lz || qmn.z > hz) return false;
+    return true;
+}
+
+// One step of a 4-wide descent: the node's four child boxes against the
+// query; internal children are pushed, leaves reported through leaf(slot,
+// face).  Returns status bits (stack full).
+template <class Leaf>
+__device__ __forceinline__ u32 wide_step(const Wide4* __restrict__ w4, int w, f3 qmn, f3 qmx, int* stack, int& sp,
+                                         Leaf&& leaf) {
+    const float4* p = reinterpret_cast<const float4*>(w4 + w);
+    const float4 lx = __ldg(p), ly = __ldg(p + 1), lz = __ldg(p + 2);
+    const float4 hx = __ldg(p + 3), hy = __ldg(p + 4), hz = __ldg(p + 5);
+    const int4 ch = __ldg(reinterpret_cast<const int4*>(p + 6));
+    const float LX[4] = {lx.x, lx.y, lx.z, lx.w}, LY[4] = {ly.x, ly.y, ly.z, ly.w}, LZ[4] = {lz.x, lz.y, lz.z, lz.w};
+    const float HX[4] = {hx.x, hx.y, hx.z, hx.w}, HY[4] = {hy.x, hy.y, hy.z, hy.w}, HZ[4] = {hz.x, hz.y, hz.z, hz.w};
+    const int C[4] = {ch.x, ch.y, ch.z, ch.w};
+    u32 st = 0;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const int c = C[k];
+        if (c == W4_EMPTY || !overlap_xyz(qmn, qmx, LX[k], LY[k], LZ[k], HX[k], HY[k], HZ[k])) continue;
+        if (c < 0) {
+            leaf(k, (u32)~c);
+        } else if (sp < STACK_DEPTH) {
+            stack[sp++] = c;
+        } else {
+            st |= ST_STACK_OVF;
+        }
+    }
+    return st;
+}
+
+// Descent of the 4-wide form of a tree (same leaves as traverse on the binary
+// form): the root box first (binary root node), then wide nodes from 0.
+template <class Fn>
+__device__ __forceinline__ u32 traverse_wide(const Node* __restrict__ root, const Wide4* __restrict__ w4, u32 cap,
+                                             f3 qmn, f3 qmx, Fn&& fn) {
+    if (cap == 0) return 0;
+    {
+        const float4* p = reinterpret_cast<const float4*>(root);
+        if (!overlap(qmn, qmx, __ldg(p), __ldg(p + 1))) return 0;
+    }
+    int stack[STACK_DEPTH];
+    int sp = 0;
+    stack[sp++] = 0;
+    u32 visited = 0, st = 0;
+    while (sp > 0) {
+        if (++visited > VISIT_CAP) { st |= ST_STACK_OVF; break; }
+        const int w = stack[--sp];
+        if (w < 0 || (u32)w >= cap) continue;
+        st |= wide_step(w4, w, qmn, qmx, stack, sp, [&](int, u32 f) { fn(f); });
+    }
+    return st;
+}
+
 __device__ __forceinline__ bool root_overlap(const Node* __restrict__ a, const Node* __restrict__ b) {
     const float4* pa = reinterpret_cast<const float4*>(a);
     const float4* pb = reinterpret_cast<const float4*>(b);
@@ -147,6 +207,18 @@ __device__ __forceinline__ bool h1_vertex(f3 x, f3 xp, float inv, H1Vertex& h) {
     }
     return true;
 }
+// The box part of h1_vertex for a vertex that already passed its 64-cell check.
+__device__ __forceinline__ void h1_vertex_box(f3 x, f3 xp, H1Vertex& h) {
+    const float xc[3] = {x.x, x.y, x.z}, xq[3] = {xp.x, xp.y, xp.z};
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        float pc = xc[a], pp = xq[a];
+        if (!isfinite(pp) || fabsf(pp - pc) > 1.f) pp = pc;
+        h.pc[a] = pc; h.pp[a] = pp;
+        h.lo[a] = (pp < pc) ? pp : pc;
+        h.hi[a] = (pc < pp) ? pp : pc;
+    }
+}
 // Traversal box that contains every face box the exact test can accept: the
 // vertex box grown by m plus a few ulps of slack, so the BVH never prunes a
 // row the grid would have produced.
@@ -161,8 +233,11 @@ __device__ __forceinline__ void h1_query_box(const H1Vertex& h, float m, f3& qmn
 // AABB +- m, collectFaceBoxes spatial_hash.hpp:1625-1643) overlaps the swept
 // vertex box, the face does not contain the vertex, and the point-triangle
 // distance^2 at x or xPrev is <= m^2 (spatial_hash.hpp:1804-1846).
+// span_check = false skips the face's 64-cell test, for callers whose cell
+// size is this mesh's largest key-box extent computed from the same positions
+// (the refit's H1 extent): every key box then spans at most two cells.
 __device__ __forceinline__ bool h1_face(const float4* __restrict__ X, u32 voff, uint4 tri, u32 v, float m, float inv,
-                                        const H1Vertex& h) {
+                                        const H1Vertex& h, bool span_check = true) {
     if (tri.x == v || tri.y == v || tri.z == v) return false;
     f3 P0 = ld(X, voff + tri.x), P1 = ld(X, voff + tri.y), P2 = ld(X, voff + tri.z);
     const float A[3] = {P0.x, P0.y, P0.z}, B[3] = {P1.x, P1.y, P1.z}, C[3] = {P2.x, P2.y, P2.z};
@@ -181,10 +256,12 @@ __device__ __forceinline__ bool h1_face(const float4* __restrict__ X, u32 voff, 
         bmn[a] = lo - m;
         bmx[a] = hi + m;
     }
+    if (span_check) {
 #pragma unroll
-    for (int a = 0; a < 3; ++a) {
-        int l = (int)floorf(bmn[a] * inv), u = (int)floorf(bmx[a] * inv);
-        if (u - l > 64) return false;  // face never entered the grid
+        for (int a = 0; a < 3; ++a) {
+            int l = (int)floorf(bmn[a] * inv), u = (int)floorf(bmx[a] * inv);
+            if (u - l > 64) return false;  // face never entered the grid
+        }
     }
     if (h.hi[0] < bmn[0] || h.lo[0] > bmx[0] || h.hi[1] < bmn[1] || h.lo[1] > bmx[1] || h.hi[2] < bmn[2] ||
         h.lo[2] > bmx[2])

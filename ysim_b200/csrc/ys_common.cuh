@@ -33,6 +33,23 @@ struct __align__(16) Node {
 };
 static_assert(sizeof(Node) == 32, "Node must be 32 bytes");
 
+// 4-wide node of the scene trees in the cube layout: the boxes of up to four
+// children side by side (one 128-byte line holds everything a descent step
+// tests), the child words, the child count and the link to the parent's slot.
+// child >= 0: a wide node; child < 0: a leaf, ~child = face; W4_EMPTY: unused
+// slot (its box is inverted so it never overlaps).
+struct __align__(128) Wide4 {
+    float lox[4], loy[4], loz[4];
+    float hix[4], hiy[4], hiz[4];
+    i32 child[4];
+    u32 nchild;
+    i32 parent;  // wide parent, -1 at the root
+    u32 slot;    // this node's slot in the parent
+    u32 pad;
+};
+static_assert(sizeof(Wide4) == 128, "Wide4 must be 128 bytes");
+static constexpr i32 W4_EMPTY = 0x7FFFFFFF;
+
 // BroadCollision (collision_pod.hpp:256-261), 32 B.
 struct Row { u32 point, tri, qobj, tobj, qbeh, tbeh, qshape, tshape; };
 static_assert(sizeof(Row) == 32, "Row must be 32 bytes");

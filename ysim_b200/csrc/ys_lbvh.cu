@@ -1,4 +1,6 @@
 // ys_lbvh.cu -- Morton codes, Karras LBVH topology and the fused swept refit.
+#include <utility>
+
 #include "ys_lbvh.cuh"
 
 namespace ys {
@@ -122,7 +124,8 @@ __global__ void k_parent_init(i32* __restrict__ parent, i32* __restrict__ parent
 
 __global__ void __launch_bounds__(256) k_karras(const u32* __restrict__ codes, const u32* __restrict__ idx, u32 n,
                                                 Node* __restrict__ nodes, i32* __restrict__ parent,
-                                                i32* __restrict__ parent2, u32* __restrict__ visits) {
+                                                i32* __restrict__ parent2, u32* __restrict__ visits,
+                                                int consistent) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= (int)n) return;
     KarrasView K{codes, idx, (int)n};
@@ -143,7 +146,17 @@ __global__ void __launch_bounds__(256) k_karras(const u32* __restrict__ codes, c
     // findSplit
     u32 c0 = codes[first], c1 = codes[last];
     u32 split;
-    if (c0 == c1) {
+    if (consistent) {
+        // largest s in [first, last) sharing more key bits with first than last does
+        const int dnode = K.delta(first, last);
+        int sp = first, step = last - first;
+        do {
+            step = (step + 1) >> 1;
+            const int ns = sp + step;
+            if (ns < last && K.delta(first, ns) > dnode) sp = ns;
+        } while (step > 1);
+        split = (u32)sp;
+    } else if (c0 == c1) {
         split = (u32)((first + last) >> 1);
     } else {
         int prefix = clz32(c0 ^ c1);
@@ -167,10 +180,142 @@ __global__ void __launch_bounds__(256) k_karras(const u32* __restrict__ codes, c
 }
 
 void launch_karras(const u32* codes, const u32* idx, u32 n, Node* nodes, i32* parent, i32* parent2, u32* visits,
-                   cudaStream_t s) {
+                   cudaStream_t s, bool consistent) {
     if (n == 0) return;
     k_parent_init<<<ceil_div(2 * n - 1, 256), 256, 0, s>>>(parent, parent2, 2 * n - 1);
-    k_karras<<<ceil_div(n, 256), 256, 0, s>>>(codes, idx, n, nodes, parent, parent2, visits);
+    k_karras<<<ceil_div(n, 256), 256, 0, s>>>(codes, idx, n, nodes, parent, parent2, visits, consistent ? 1 : 0);
+}
+
+// ------------------------------------------------------------------ 4-wide
+// Depth of every binary node by pointer jumping: after round r, anc[i] is the
+// 2^r-th ancestor (or -1) and dep[i] the distance to it.
+__global__ void k_depth_init(const i32* __restrict__ parent, u32 m, i32* __restrict__ anc, i32* __restrict__ dep) {
+    const u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m) return;
+    const i32 p = parent[i];
+    anc[i] = p;
+    dep[i] = p >= 0 ? 1 : 0;
+}
+__global__ void k_depth_jump(const i32* __restrict__ anc, const i32* __restrict__ dep, i32* __restrict__ anc2,
+                             i32* __restrict__ dep2, u32 m) {
+    const u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m) return;
+    const i32 a = anc[i];
+    if (a >= 0 && (u32)a < m) {
+        dep2[i] = dep[i] + dep[a];
+        anc2[i] = anc[a];
+    } else {
+        dep2[i] = dep[i];
+        anc2[i] = -1;
+    }
+}
+__global__ void k_wide_flag(const i32* __restrict__ dep, u32 nInner, u32* __restrict__ flag) {
+    const u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < nInner) flag[i] = (dep[i] & 1) == 0 ? 1u : 0u;
+}
+__device__ __forceinline__ void w4_empty_boxes(Wide4& o) {
+    const float inf = __int_as_float(0x7f800000);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        o.lox[k] = inf; o.loy[k] = inf; o.loz[k] = inf;
+        o.hix[k] = -inf; o.hiy[k] = -inf; o.hiz[k] = -inf;
+        o.child[k] = W4_EMPTY;
+    }
+}
+// One thread per even-depth internal node i: wide node widx[i] takes i's
+// children, each internal child replaced by its own two children.
+__global__ void k_wide_fill(const Node* __restrict__ nodes, const i32* __restrict__ dep, const u32* __restrict__ widx,
+                            u32 n, Wide4* __restrict__ w4, int2* __restrict__ leafW, u32* __restrict__ warrive) {
+    const u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+    const u32 nInner = n - 1;
+    if (i >= nInner || (dep[i] & 1)) return;
+    const u32 W = widx[i];
+    i32 kids[4];
+    int nk = 0;
+    const i32 ab[2] = {nodes[i].a, nodes[i].b};
+#pragma unroll
+    for (int c = 0; c < 2; ++c) {
+        const i32 x = ab[c];
+        if (x >= 0 && (u32)x < nInner) {
+            kids[nk++] = nodes[x].a;
+            kids[nk++] = nodes[x].b;
+        } else {
+            kids[nk++] = x;
+        }
+    }
+    Wide4 o;
+    w4_empty_boxes(o);
+    for (int k = 0; k < nk; ++k) {
+        const i32 x = kids[k];
+        if (x >= 0 && (u32)x < nInner) {
+            const u32 cw = widx[x];
+            o.child[k] = (i32)cw;
+            w4[cw].parent = (i32)W;  // the child's own thread never writes these two words
+            w4[cw].slot = (u32)k;
+        } else {
+            o.child[k] = ~nodes[x].b;
+            leafW[(u32)x - nInner] = make_int2((i32)W, k);
+        }
+    }
+    float4* dst = reinterpret_cast<float4*>(&w4[W]);
+    const float4* src = reinterpret_cast<const float4*>(&o);
+#pragma unroll
+    for (int k = 0; k < 7; ++k) dst[k] = src[k];  // boxes + child words
+    w4[W].nchild = (u32)nk;
+    if (i == 0) { w4[W].parent = -1; w4[W].slot = 0; }
+    warrive[W] = 0;
+}
+// A tree of one leaf (binary node 0 is the leaf): one wide node, one slot.
+__global__ void k_wide_single(const Node* __restrict__ nodes, Wide4* __restrict__ w4, int2* __restrict__ leafW,
+                              u32* __restrict__ warrive) {
+    Wide4 o;
+    w4_empty_boxes(o);
+    o.child[0] = ~nodes[0].b;
+    o.nchild = 1;
+    o.parent = -1;
+    o.slot = 0;
+    o.pad = 0;
+    w4[0] = o;
+    leafW[0] = make_int2(0, 0);
+    warrive[0] = 0;
+}
+
+size_t wide_build_scratch_bytes(u32 n) {
+    const size_t m = n ? 2 * (size_t)n - 1 : 1;
+    return 4 * m * sizeof(i32) + 256 + (size_t)n * sizeof(u32) + 256 + scan_scratch_bytes(n ? n : 1);
+}
+
+cudaError_t launch_wide_build(const Node* nodes, const i32* parent, u32 n, Wide4* w4, int2* leafW, u32* warrive,
+                              void* scratch, cudaStream_t s) {
+    if (n == 0) return cudaSuccess;
+    if (n == 1) {
+        k_wide_single<<<1, 1, 0, s>>>(nodes, w4, leafW, warrive);
+        return cudaGetLastError();
+    }
+    const u32 m = 2 * n - 1;
+    char* base = static_cast<char*>(scratch);
+    i32* anc = reinterpret_cast<i32*>(base);
+    i32* dep = anc + m;
+    i32* anc2 = dep + m;
+    i32* dep2 = anc2 + m;
+    size_t off = ((4 * (size_t)m * sizeof(i32)) + 255) & ~(size_t)255;
+    u32* widx = reinterpret_cast<u32*>(base + off);
+    off = (off + (size_t)n * sizeof(u32) + 255) & ~(size_t)255;
+    void* scanScratch = base + off;
+    k_depth_init<<<ceil_div(m, 256), 256, 0, s>>>(parent, m, anc, dep);
+    // enough rounds for any depth below m
+    int rounds = 1;
+    while ((1u << rounds) < m && rounds < 31) ++rounds;
+    for (int r = 0; r < rounds; ++r) {
+        k_depth_jump<<<ceil_div(m, 256), 256, 0, s>>>(anc, dep, anc2, dep2, m);
+        std::swap(anc, anc2);
+        std::swap(dep, dep2);
+    }
+    k_wide_flag<<<ceil_div(n - 1, 256), 256, 0, s>>>(dep, n - 1, widx);
+    cudaError_t e = exclusive_scan(widx, n - 1, scanScratch, s);
+    if (e != cudaSuccess) return e;
+    k_wide_fill<<<ceil_div(n - 1, 256), 256, 0, s>>>(nodes, dep, widx, n, w4, leafW, warrive);
+    return cudaGetLastError();
 }
 
 // ------------------------------------------------------------------ refit
@@ -181,15 +326,67 @@ void launch_karras(const u32* codes, const u32* idx, u32 n, Node* nodes, i32* pa
 // internal node receives exactly two arrivals per refit (one per child it
 // lists), so an even old value means "first", odd means "second".  Karras
 // zeroes them at build.
-// Memory order: box store -> __threadfence -> atomicAdd (release); atomicAdd
-// -> __threadfence -> L1-bypassing loads of the children (acquire).
+// Memory order: the arrival is an acq_rel atomic at GPU scope: it releases
+// this thread's box stores and acquires the sibling's; the children are then
+// read with L1-bypassing loads.
+// Box coordinates only: the child / face words (w) are left alone, so no
+// read-modify-write is needed.
 __device__ __forceinline__ void store_box(Node* nd, f3 lo, f3 hi) {
-    float4* p = reinterpret_cast<float4*>(nd);
-    float4 a = __ldcg(p), b = __ldcg(p + 1);
-    a.x = lo.x; a.y = lo.y; a.z = lo.z;
-    b.x = hi.x; b.y = hi.y; b.z = hi.z;
-    __stcg(p, a);
-    __stcg(p + 1, b);
+    float* p = reinterpret_cast<float*>(nd);
+    __stcg(reinterpret_cast<float2*>(p), make_float2(lo.x, lo.y));
+    __stcg(p + 2, lo.z);
+    __stcg(reinterpret_cast<float2*>(p + 4), make_float2(hi.x, hi.y));
+    __stcg(p + 6, hi.z);
+}
+
+__device__ __forceinline__ u32 arrive_acq_rel(u32* counter) {
+    u32 old;
+    asm volatile("atom.add.acq_rel.gpu.global.u32 %0, [%1], 1;" : "=r"(old) : "l"(counter) : "memory");
+    return old;
+}
+
+// Arrival at a wide node: counts 0 .. wrap, then back to 0 (no reset needed
+// between refits); acq_rel as arrive_acq_rel.
+__device__ __forceinline__ u32 arrive_inc_acq_rel(u32* counter, u32 wrap) {
+    u32 old;
+    asm volatile("atom.inc.acq_rel.gpu.global.u32 %0, [%1], %2;" : "=r"(old) : "l"(counter), "r"(wrap) : "memory");
+    return old;
+}
+
+// Wide climb: write this box into the parent's slot; the last of the node's
+// children to arrive takes the union of its slots (in slot order) to the
+// grandparent, and the root's union becomes the binary root box.
+__device__ __forceinline__ void climb_wide(const RefitJob& J, u32 i, f3 lo, f3 hi, u32* status) {
+    const int2 ws = J.leafW[i];
+    i32 w = ws.x;
+    u32 s = (u32)ws.y;
+    const u32 cap = J.n > 1 ? J.n - 1 : 1;
+    for (u32 step = 0; step < 128; ++step) {
+        if (w < 0 || (u32)w >= cap || s > 3) break;
+        Wide4* W = J.w4 + w;
+        __stcg(&W->lox[s], lo.x); __stcg(&W->loy[s], lo.y); __stcg(&W->loz[s], lo.z);
+        __stcg(&W->hix[s], hi.x); __stcg(&W->hiy[s], hi.y); __stcg(&W->hiz[s], hi.z);
+        const u32 nc = __ldcg(&W->nchild);
+        const i32 par = __ldcg(&W->parent);
+        const u32 ps = __ldcg(&W->slot);
+        if (nc == 0 || nc > 4) break;
+        if (arrive_inc_acq_rel(&J.warrive[w], nc - 1) != nc - 1) return;
+        const float4* p = reinterpret_cast<const float4*>(W);
+        const float4 lx = __ldcg(p), ly = __ldcg(p + 1), lz = __ldcg(p + 2);
+        const float4 hx = __ldcg(p + 3), hy = __ldcg(p + 4), hz = __ldcg(p + 5);
+        lo = mk(lx.x, ly.x, lz.x);
+        hi = mk(hx.x, hy.x, hz.x);
+        if (nc > 1) { lo = vmin(lo, mk(lx.y, ly.y, lz.y)); hi = vmax(hi, mk(hx.y, hy.y, hz.y)); }
+        if (nc > 2) { lo = vmin(lo, mk(lx.z, ly.z, lz.z)); hi = vmax(hi, mk(hx.z, hy.z, hz.z)); }
+        if (nc > 3) { lo = vmin(lo, mk(lx.w, ly.w, lz.w)); hi = vmax(hi, mk(hx.w, hy.w, hz.w)); }
+        if (par < 0) {
+            store_box(&J.nodes[0], lo, hi);
+            return;
+        }
+        w = par;
+        s = ps;
+    }
+    atomicOr(status, ST_ITER_CAP);
 }
 
 __global__ void __launch_bounds__(256) k_refit(const RefitJob* __restrict__ jobs, u32 numJobs, u32 totalLeaves,
@@ -260,51 +457,72 @@ __global__ void __launch_bounds__(256) k_refit(const RefitJob* __restrict__ jobs
         const u32 e = __reduce_max_sync(peers, __float_as_uint(ext));
         if (J.selfMargin > 0.f && (threadIdx.x & 31) == (unsigned)(__ffs(peers) - 1)) atomicMax(J.maxExt, e);
     }
+    if (J.w4) {
+        climb_wide(J, i, lo, hi, status);
+        return;
+    }
     store_box(&nodes[leaf], lo, hi);
     if (n == 1) return;
     const u32 numInner = n - 1;
     // Climb: deliver this node's arrival to every internal node that claims
     // it as a child (one claimant in a consistent tree); the second arrival
     // at a claimant combines it and climbs on from there.  Extra climbs (a
-    // node with two claimants) wait in a small pending list.
+    // node with two claimants) wait in a small pending list.  The climbing
+    // thread keeps the box of the node it carries in registers and, at a
+    // claimant, loads only the other child's box; the claimant's child words
+    // are read before the arrival atomic (they do not change during a refit).
     u32 pending[4];
     int np = 0;
     u32 child = leaf;
-    __threadfence();
+    f3 clo = lo, chi = hi;
+    bool have_box = true;  // clo/chi hold child's box (false for a resumed pending node)
     for (u32 step = 0; step < 2 * n; ++step) {
         const i32 p1 = __ldcg(&J.parent[child]);
         const i32 p2 = __ldcg(&J.parent2[child]);
         i32 claim[2] = {p1, (p2 != p1 && p2 != 0x7FFFFFFF) ? p2 : -1};
         i32 next = -1;
+        f3 nlo = clo, nhi = chi;
 #pragma unroll
         for (int c = 0; c < 2; ++c) {
             const i32 par = claim[c];
             if (par < 0) continue;
             if ((u32)par >= numInner) { atomicOr(status, ST_ITER_CAP); continue; }
-            u32 old = atomicAdd(&J.visits[par], 1u);
+            const i32 ca = __ldcg(&nodes[par].a), cb = __ldcg(&nodes[par].b);
+            u32 old = arrive_acq_rel(&J.visits[par]);
             if ((old & 1u) == 0u) continue;  // first arrival: the sibling's thread combines
-            __threadfence();
-            const float4* pn = reinterpret_cast<const float4*>(&nodes[par]);
-            const float4 h0 = __ldcg(pn), h1 = __ldcg(pn + 1);
-            const i32 ca = __float_as_int(h0.w), cb = __float_as_int(h1.w);
             if (ca < 0 || (u32)ca >= 2 * n - 1 || cb < 0 || (u32)cb >= 2 * n - 1) {
                 atomicOr(status, ST_ITER_CAP);
                 continue;
             }
-            const float4* A = reinterpret_cast<const float4*>(&nodes[ca]);
-            const float4* B = reinterpret_cast<const float4*>(&nodes[cb]);
-            float4 a0 = __ldcg(A), a1 = __ldcg(A + 1), b0 = __ldcg(B), b1 = __ldcg(B + 1);
-            f3 plo = vmin(mk(a0.x, a0.y, a0.z), mk(b0.x, b0.y, b0.z));
-            f3 phi = vmax(mk(a1.x, a1.y, a1.z), mk(b1.x, b1.y, b1.z));
+            f3 plo, phi;
+            const bool mineA = have_box && (u32)ca == child, mineB = have_box && (u32)cb == child;
+            if (mineA || mineB) {
+                const float4* O = reinterpret_cast<const float4*>(&nodes[mineA ? cb : ca]);
+                const float4 o0 = __ldcg(O), o1 = __ldcg(O + 1);
+                const f3 olo = mk(o0.x, o0.y, o0.z), ohi = mk(o1.x, o1.y, o1.z);
+                // operands in (a, b) order, as the combine of two loaded boxes
+                plo = mineA ? vmin(clo, olo) : vmin(olo, clo);
+                phi = mineA ? vmax(chi, ohi) : vmax(ohi, chi);
+            } else {
+                const float4* A = reinterpret_cast<const float4*>(&nodes[ca]);
+                const float4* B = reinterpret_cast<const float4*>(&nodes[cb]);
+                float4 a0 = __ldcg(A), a1 = __ldcg(A + 1), b0 = __ldcg(B), b1 = __ldcg(B + 1);
+                plo = vmin(mk(a0.x, a0.y, a0.z), mk(b0.x, b0.y, b0.z));
+                phi = vmax(mk(a1.x, a1.y, a1.z), mk(b1.x, b1.y, b1.z));
+            }
             store_box(&nodes[par], plo, phi);
-            __threadfence();
-            if (next < 0) next = par;
+            if (next < 0) { next = par; nlo = plo; nhi = phi; }
             else if (np < 4) pending[np++] = (u32)par;
             else atomicOr(status, ST_ITER_CAP);
         }
         if (next < 0) {
             if (np == 0) return;  // root reached, first arrival, or an unclaimed node
             next = (i32)pending[--np];
+            have_box = false;     // its box is in memory (stored above)
+        } else {
+            have_box = true;
+            clo = nlo;
+            chi = nhi;
         }
         child = (u32)next;
     }

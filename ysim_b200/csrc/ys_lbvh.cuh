@@ -4,6 +4,7 @@
 // at slot 0, leaves at [N-1, 2N-2].
 #pragma once
 #include "ys_common.cuh"
+#include "ys_scan.cuh"
 
 namespace ys {
 
@@ -27,6 +28,11 @@ struct RefitJob {
     u32 swept;
     float selfMargin;       // > 0: also reduce the H1 grid extent into *maxExt
     u32* maxExt;            // float bits, atomicMax (positive floats order as ints)
+    // 4-wide form (cube layout): when set the refit fills the wide nodes'
+    // child slots and the binary root box instead of the binary nodes
+    Wide4* w4;
+    const int2* leafW;      // per leaf: (wide node, slot)
+    u32* warrive;           // per wide node: arrivals this refit (self-resetting)
 };
 
 // Scene box of a mesh (min/max over all its vertices) into box[6] (float
@@ -44,8 +50,18 @@ void launch_morton(const float4* x4, const float* x3, u32 voff, const u32* facet
 // by two internal nodes, or by none.  Child arrays stay exactly the
 // reference's; parent keeps the largest claimant (what a serial build loop
 // leaves behind) and parent2 the smallest, so the refit reaches every claimant.
+// consistent = true splits runs of equal codes by the (code, index) key that
+// determineRange already orders them by, so every node has one parent (the
+// cube layout); false keeps the reference's midpoint split.
 void launch_karras(const u32* codes, const u32* idx, u32 n, Node* nodes, i32* parent, i32* parent2, u32* visits,
-                   cudaStream_t s);
+                   cudaStream_t s, bool consistent = false);
+// 4-wide form of a consistent binary tree of n leaves: internal nodes at even
+// depth become wide nodes (numbered by an exclusive scan), their children and
+// grandchildren their slots.  w4 and warrive need max(n - 1, 1) entries,
+// leafW n, scratch wide_build_scratch_bytes(n).  Boxes are filled by a refit.
+size_t wide_build_scratch_bytes(u32 n);
+cudaError_t launch_wide_build(const Node* nodes, const i32* parent, u32 n, Wide4* w4, int2* leafW, u32* warrive,
+                              void* scratch, cudaStream_t s);
 // Leaves + bottom-up for every job (jobs in device memory, jobsHost mirrors
 // them for the launch size).
 void launch_refit(const RefitJob* jobsDev, u32 numJobs, u32 totalLeaves, u32* status, cudaStream_t s);

@@ -49,6 +49,7 @@ struct MeshDev {
     float rest[6];
     u32 tgt_begin, tgt_end;
     u32 gspr;  // FastGridCloth: offset of this mesh's per-spring k / L arrays, or NO_SPRINGS
+    u32 w4_off, w4_cap;  // wide nodes of this mesh's tree (cube layout)
 };
 static constexpr u32 NO_SPRINGS = 0xFFFFFFFFu;
 
@@ -65,6 +66,8 @@ struct StepArgs {
     const u32* targets;
     const uint4* F;
     const Node* nodes;
+    const Wide4* w4;  // 4-wide form of the trees (wide != 0)
+    u32 wide;
     const u32* spr_off;
     const u32* spr_split;
     const u32* spr_nbr;
@@ -96,6 +99,13 @@ struct StepArgs {
 // BroadPhase::detectCollisions for one query vertex (bvh.hpp:2853-2949 and
 // the hybrid self pass, simulator.hpp:3678-3701): self rows first, then every
 // target mesh whose root box overlaps this mesh's root box.
+// Leaves of mesh t's tree overlapping [qmn, qmx], binary or 4-wide form.
+template <class Fn>
+__device__ __forceinline__ u32 descend(const StepArgs& A, const MeshDev& T, f3 qmn, f3 qmx, Fn&& fn) {
+    if (A.wide) return traverse_wide(A.nodes + T.node_off, A.w4 + T.w4_off, T.w4_cap, qmn, qmx, fn);
+    return traverse(A.nodes + T.node_off, 2 * T.nF - 1, qmn, qmx, fn);
+}
+
 template <class Sink>
 __device__ __forceinline__ u32 query_vertex(const StepArgs& A, u32 g, u32 m, const MeshDev& M, f3 xc, f3 xpv,
                                             Sink&& sink) {
@@ -111,14 +121,14 @@ __device__ __forceinline__ u32 query_vertex(const StepArgs& A, u32 g, u32 m, con
         if (h1_vertex(xc, xpv, inv, h)) {
             f3 qmn, qmx;
             h1_query_box(h, mg, qmn, qmx);
-            st |= traverse(A.nodes + M.node_off, 2 * M.nF - 1, qmn, qmx, [&](u32 f) {
+            st |= descend(A, M, qmn, qmx, [&](u32 f) {
                 uint4 tri = A.F[M.foff + f];
                 if (h1_face(A.x, M.voff, tri, lid, mg, inv, h)) sink(m, f, tri, M.voff);
             });
         }
     } else if (A.self_mode == YS_SELF_BVH) {
         f3 qmn = xc - mk(mg, mg, mg), qmx = xc + mk(mg, mg, mg);
-        st |= traverse(A.nodes + M.node_off, 2 * M.nF - 1, qmn, qmx, [&](u32 f) {
+        st |= descend(A, M, qmn, qmx, [&](u32 f) {
             uint4 tri = A.F[M.foff + f];
             if (tri.x == lid || tri.y == lid || tri.z == lid) return;
             sink(m, f, tri, M.voff);
@@ -126,12 +136,12 @@ __device__ __forceinline__ u32 query_vertex(const StepArgs& A, u32 g, u32 m, con
     }
     for (u32 k = M.tgt_begin; k < M.tgt_end; ++k) {
         const u32 t = A.targets[k];
-        const u32 tno = A.meshes[t].node_off, tnf = A.meshes[t].nF, tfo = A.meshes[t].foff, tvo = A.meshes[t].voff;
-        if (!root_overlap(A.nodes + M.node_off, A.nodes + tno)) continue;
+        const MeshDev T = A.meshes[t];
+        if (!root_overlap(A.nodes + M.node_off, A.nodes + T.node_off)) continue;
         f3 qmn = xc - mk(mg, mg, mg), qmx = xc + mk(mg, mg, mg);
-        st |= traverse(A.nodes + tno, 2 * tnf - 1, qmn, qmx, [&](u32 f) {
-            uint4 tri = A.F[tfo + f];
-            sink(t, f, tri, tvo);
+        st |= descend(A, T, qmn, qmx, [&](u32 f) {
+            uint4 tri = A.F[T.foff + f];
+            sink(t, f, tri, T.voff);
         });
     }
     return st;
@@ -228,7 +238,7 @@ __device__ __forceinline__ void warp_count(unsigned long long* ctr, u32 v) {
 // keys whatever the arrival order -- so results are those of a per-vertex
 // loop over candidates in descent order.
 static constexpr int FUSED_WARPS = 4;  // 128-thread blocks
-static constexpr u32 WQ_CAP = 64;      // candidate queue: < 32 left over + 32 new
+static constexpr u32 WQ_CAP = 160;     // candidate queue: < 32 left over + up to 4 leaves per lane
 static constexpr u32 WC_CAP = 64;      // contact buffer between flushes
 static constexpr u32 KEY_SELF = 32u;   // queue key: (mesh << 6) | KEY_SELF? | owner lane
 static constexpr unsigned FULL_MASK = 0xFFFFFFFFu;
@@ -252,68 +262,74 @@ __device__ __forceinline__ void insert_contact(VContact (&buf)[MAXC], int& nc, u
     ++nc;
 }
 
-__global__ void __launch_bounds__(128) k_fused(StepArgs A) {
+// WIDE: descend the 4-wide form of the trees (cube layout), else the binary one.
+template <bool WIDE>
+__global__ void __launch_bounds__(128, 8) k_fused(StepArgs A) {
     __shared__ WarpWork wq[FUSED_WARPS];
     const u32 lane = threadIdx.x & 31u;
     WarpWork& Q = wq[threadIdx.x >> 5];
     const u32 g = blockIdx.x * blockDim.x + threadIdx.x;
     const bool valid = g < A.nV;
     const u32 m = valid ? A.vobj[g] : 0u;
-    const MeshDev M = A.meshes[m];
+    const MeshDev* __restrict__ Mp = A.meshes + m;
+    const u32 mflags = Mp->flags;
     const f3 xc = valid ? ld(A.x, g) : mk(0.f, 0.f, 0.f);
-    const bool query = valid && (M.flags & MF_QUERY) && (M.flags & MF_TREE);
+    const bool query = valid && (mflags & MF_QUERY) && (mflags & MF_TREE);
     const f3 xpv = query ? ld(A.xp, g) : xc;
     const float mg = A.margin;
     u32 st = 0, rows = 0;
 
-    // ---- descent state: stage 0 = own tree, 1 + k = target k
+    // ---- descent state: the own tree first (set up here), then the targets
+    int stack[STACK_DEPTH];
+    int sp = 0;
+    u32 visited = 0, nn = 0, key = 0;
+    const Node* nodes = A.nodes;  // binary form
+    const Wide4* wn = A.w4;       // wide form
+    f3 qmn = xc, qmx = xc;
     float inv = 0.f;
-    bool selfOK = false;
-    f3 smn = xc, smx = xc;
-    if (query) {
-        if (A.self_mode == YS_SELF_HASH && (M.flags & MF_CLOTH) && (M.flags & MF_SELF)) {
+    // start a descent of mesh t's tree unless the query misses its root box
+    auto start = [&](u32 t, u32 k) {
+        const MeshDev* T = A.meshes + t;
+        key = k;
+        visited = 0;
+        if (WIDE) {
+            const float4* r = reinterpret_cast<const float4*>(A.nodes + T->node_off);
+            if (!overlap(qmn, qmx, __ldg(r), __ldg(r + 1))) return;
+            wn = A.w4 + T->w4_off;
+            nn = T->w4_cap;
+        } else {
+            nodes = A.nodes + T->node_off;
+            nn = 2 * T->nF - 1;
+        }
+        stack[0] = 0;
+        sp = 1;
+    };
+    if (query && Mp->nF) {
+        bool selfOK = false;
+        if (A.self_mode == YS_SELF_HASH && (mflags & MF_CLOTH) && (mflags & MF_SELF)) {
             float mx = __uint_as_float(A.maxext[m]);
             float cs = (mx > 1e-5f) ? mx : 1e-5f;
             inv = 1.f / cs;
             H1Vertex h;
-            if (h1_vertex(xc, xpv, inv, h)) { selfOK = true; h1_query_box(h, mg, smn, smx); }
+            if (h1_vertex(xc, xpv, inv, h)) { selfOK = true; h1_query_box(h, mg, qmn, qmx); }
         } else if (A.self_mode == YS_SELF_BVH) {
             selfOK = true;
-            smn = xc - mk(mg, mg, mg);
-            smx = xc + mk(mg, mg, mg);
+            qmn = xc - mk(mg, mg, mg);
+            qmx = xc + mk(mg, mg, mg);
         }
+        if (selfOK) start(m, (m << 6) | KEY_SELF | lane);
     }
-    const u32 nstage = query ? 1u + (M.tgt_end - M.tgt_begin) : 0u;
-    u32 stage = 0;
-    int stack[STACK_DEPTH];
-    int sp = 0;
-    u32 visited = 0, nn = 0, key = 0;
-    const Node* nodes = A.nodes;
-    f3 qmn = xc, qmx = xc;
+    const u32 te = query ? Mp->tgt_end : 0u;
+    u32 tk = query ? Mp->tgt_begin : 0u;  // next target
     auto next_tree = [&]() -> bool {
-        while (stage < nstage) {
-            const u32 s = stage++;
-            if (s == 0) {
-                if (!selfOK || M.nF == 0) continue;
-                nodes = A.nodes + M.node_off;
-                nn = 2 * M.nF - 1;
-                qmn = smn;
-                qmx = smx;
-                key = (m << 6) | KEY_SELF | lane;
-            } else {
-                const u32 t = A.targets[M.tgt_begin + s - 1];
-                const u32 tno = A.meshes[t].node_off, tnf = A.meshes[t].nF;
-                if (tnf == 0 || !root_overlap(A.nodes + M.node_off, A.nodes + tno)) continue;
-                nodes = A.nodes + tno;
-                nn = 2 * tnf - 1;
-                qmn = xc - mk(mg, mg, mg);
-                qmx = xc + mk(mg, mg, mg);
-                key = (t << 6) | lane;
-            }
-            stack[0] = 0;
-            sp = 1;
-            visited = 0;
-            return true;
+        while (tk < te) {
+            const u32 t = A.targets[tk++];
+            const u32 tno = A.meshes[t].node_off, tnf = A.meshes[t].nF;
+            if (tnf == 0 || !root_overlap(A.nodes + Mp->node_off, A.nodes + tno)) continue;
+            qmn = xc - mk(mg, mg, mg);
+            qmx = xc + mk(mg, mg, mg);
+            start(t, (t << 6) | lane);
+            if (sp) return true;
         }
         return false;
     };
@@ -352,9 +368,11 @@ __global__ void __launch_bounds__(128) k_fused(StepArgs A) {
             bool row = true;
             if (k & KEY_SELF) {
                 if (A.self_mode == YS_SELF_HASH) {
+                    // the owner passed its 64-cell check; the cell size is the
+                    // extent the refit just took from these positions
                     H1Vertex h;
-                    h1_vertex(oxc, oxp, oinv, h);  // accepted for the owner already
-                    row = h1_face(A.x, tvo, tri, og - tvo, mg, oinv, h);
+                    h1_vertex_box(oxc, oxp, h);
+                    row = h1_face(A.x, tvo, tri, og - tvo, mg, oinv, h, false);
                 } else {
                     const u32 lid = og - tvo;
                     row = !(tri.x == lid || tri.y == lid || tri.z == lid);
@@ -383,64 +401,84 @@ __global__ void __launch_bounds__(128) k_fused(StepArgs A) {
         }
         __syncwarp();
     };
+    // warp-aggregated append of this lane's leaf (face >= 0) to the queue
+    auto enqueue = [&](int face) {
+        const unsigned lm = __ballot_sync(FULL_MASK, face >= 0);
+        if (lm) {
+            if (face >= 0) {
+                const u32 slot = qn + (u32)__popc(lm & ((1u << lane) - 1u));
+                Q.qf[slot] = (u32)face;
+                Q.qk[slot] = key;
+            }
+            qn += (u32)__popc(lm);
+        }
+    };
 
-    bool active = query && next_tree();
+    bool active = sp > 0 || next_tree();
     while (true) {
         if (active && sp == 0) active = next_tree();
         if (!__ballot_sync(FULL_MASK, active)) break;
-        int leaf = -1;
-        if (active) {
-            if (++visited > VISIT_CAP) {
-                st |= ST_STACK_OVF;
-                sp = 0;
-            } else {
-                const int id = stack[--sp];
-                if (id >= 0 && (u32)id < nn) {
-                    const float4* p = reinterpret_cast<const float4*>(nodes + id);
-                    const float4 n0 = __ldg(p), n1 = __ldg(p + 1);
-                    if (overlap(qmn, qmx, n0, n1)) {
-                        const int a = __float_as_int(n0.w), b = __float_as_int(n1.w);
-                        if (a < 0) {
-                            leaf = b;
-                        } else if (sp + 2 > STACK_DEPTH) {
-                            st |= ST_STACK_OVF;
-                        } else {
-                            stack[sp++] = a;
-                            stack[sp++] = b;
+        if (WIDE) {
+            int lf[4] = {-1, -1, -1, -1};
+            if (active) {
+                if (++visited > VISIT_CAP) {
+                    st |= ST_STACK_OVF;
+                    sp = 0;
+                } else {
+                    const int w = stack[--sp];
+                    if (w >= 0 && (u32)w < nn)
+                        st |= wide_step(wn, w, qmn, qmx, stack, sp, [&](int s, u32 f) { lf[s] = (int)f; });
+                }
+            }
+#pragma unroll
+            for (int s = 0; s < 4; ++s) enqueue(lf[s]);
+        } else {
+            int leaf = -1;
+            if (active) {
+                if (++visited > VISIT_CAP) {
+                    st |= ST_STACK_OVF;
+                    sp = 0;
+                } else {
+                    const int id = stack[--sp];
+                    if (id >= 0 && (u32)id < nn) {
+                        const float4* p = reinterpret_cast<const float4*>(nodes + id);
+                        const float4 n0 = __ldg(p), n1 = __ldg(p + 1);
+                        if (overlap(qmn, qmx, n0, n1)) {
+                            const int a = __float_as_int(n0.w), b = __float_as_int(n1.w);
+                            if (a < 0) {
+                                leaf = b;
+                            } else if (sp + 2 > STACK_DEPTH) {
+                                st |= ST_STACK_OVF;
+                            } else {
+                                stack[sp++] = a;
+                                stack[sp++] = b;
+                            }
                         }
                     }
                 }
             }
+            enqueue(leaf);
         }
-        const unsigned lm = __ballot_sync(FULL_MASK, leaf >= 0);
-        if (lm) {
-            if (leaf >= 0) {
-                const u32 slot = qn + (u32)__popc(lm & ((1u << lane) - 1u));
-                Q.qf[slot] = (u32)leaf;
-                Q.qk[slot] = key;
-            }
-            qn += (u32)__popc(lm);
-            if (qn >= 32) {
-                drain(qn - 32, 32);
-                qn -= 32;
-            }
+        while (qn >= 32) {
+            drain(qn - 32, 32);
+            qn -= 32;
         }
     }
     if (qn) drain(0, qn);
     if (cn) flush();
 
-    if (valid && (M.flags & MF_CLOTH)) {
+    if (valid && (mflags & MF_CLOTH)) {
         f3 vel = ld(A.v, g);
         const float mass = A.mass[g], mask = A.mask[g];
-        const f3 force = vertex_force(A, M, g, xc, vel, mass);
+        const f3 force = vertex_force(A, *Mp, g, xc, vel, mass);
         f3 pos = xc;
         vel = vel + ((force * A.subh) / mass) * mask;
-        contact_response(pos, vel, nc, M.thickness, [&](int i) { return buf[i]; });
+        contact_response(pos, vel, nc, Mp->thickness, [&](int i) { return buf[i]; });
         pos = pos + (vel * A.subh) * mask;
         if (sanitize(pos, vel, xc)) st |= ST_NONFINITE;
         A.xn[g] = make_float4(pos.x, pos.y, pos.z, 0.f);
         A.vn[g] = make_float4(vel.x, vel.y, vel.z, 0.f);
-    } else if (valid && !(M.flags & MF_STATIC)) {
+    } else if (valid && !(mflags & MF_STATIC)) {
         // not integrated (Rigid / Float / Kinematic): carry the state over
         A.xn[g] = A.x[g];
         A.vn[g] = A.v[g];
@@ -460,6 +498,11 @@ __global__ void __launch_bounds__(128) k_fused(StepArgs A) {
     warp_count(&A.counters[0], rows);
     warp_count(&A.counters[1], (u32)nc);
     if (st) atomicOr(A.status, st);
+}
+
+void launch_fused(const StepArgs& A, u32 nV, cudaStream_t st) {
+    if (A.wide) k_fused<true><<<ceil_div(nV, 128), 128, 0, st>>>(A);
+    else k_fused<false><<<ceil_div(nV, 128), 128, 0, st>>>(A);
 }
 
 // ------------------------------------------------------------------ staged
@@ -580,6 +623,7 @@ struct HostMesh {
     std::vector<float> x, v, mass, mask;
     std::vector<u32> F;
     u32 voff = 0, foff = 0, node_off = 0, flags = 0;
+    u32 w4_off = 0, w4_cap = 0;
     bool built = false;
     // TriangularCloth springs (mesh-local ids)
     std::vector<u32> spr_off, spr_split, spr_nbr, vaf_off, vaf;
@@ -690,6 +734,10 @@ struct ys_scene {
     DBuf<u32> F3;  // packed facets (3 per face) for the refit kernel
     DBuf<Node> nodes;
     DBuf<i32> parent, parent2;
+    DBuf<Wide4> w4;                  // cube layout: 4-wide trees used by every query and refit
+    DBuf<int2> leafW;
+    DBuf<u32> warrive;
+    DBuf<char> wideScratch;
     DBuf<MeshDev> dmeshes;
     DBuf<RefitJob> jobs;            // 6 tables (cur x cv) of njobs, then one build slot
     std::vector<RefitJob> hjobs;
@@ -749,6 +797,8 @@ StepArgs make_args(ys_scene* s) {
     A.targets = s->targets.p;
     A.F = s->F4.p;
     A.nodes = s->nodes.p;
+    A.w4 = s->w4.p;
+    A.wide = s->tree_layout == YS_TREE_CUBE ? 1u : 0u;
     A.spr_off = s->spr_off.p;
     A.spr_split = s->spr_split.p;
     A.spr_nbr = s->spr_nbr.p;
@@ -800,8 +850,12 @@ ys_status build_tree(ys_scene* s, HostMesh& H) {
     launch_morton(s->X[s->cur].p, nullptr, H.voff, s->F3.p + 3 * (size_t)H.foff, n, s->box.p, codes, idx, st,
                   s->tree_layout == YS_TREE_CUBE);
     YS_CK(radix_sort_pairs(codes, idx, n, s->sortScratch.p, 0, 32, st));
+    const bool cube = s->tree_layout == YS_TREE_CUBE;
     launch_karras(codes, idx, n, s->nodes.p + H.node_off, s->parent.p + H.node_off, s->parent2.p + H.node_off,
-                  s->visits.p + H.foff, st);
+                  s->visits.p + H.foff, st, cube);
+    if (cube)
+        YS_CK(launch_wide_build(s->nodes.p + H.node_off, s->parent.p + H.node_off, n, s->w4.p + H.w4_off,
+                                s->leafW.p + H.foff, s->warrive.p + H.w4_off, s->wideScratch.p, st));
     RefitJob J;
     memset(&J, 0, sizeof(J));
     J.nodes = s->nodes.p + H.node_off;
@@ -819,7 +873,15 @@ ys_status build_tree(ys_scene* s, HostMesh& H) {
     RefitJob* slot = s->jobs.p + 6 * (size_t)s->njobs;
     YS_CK(cudaMemcpyAsync(slot, &J, sizeof(J), cudaMemcpyHostToDevice, st));
     launch_refit(slot, 1, n, s->status.p, st);
-    YS_CK(cudaStreamSynchronize(st));  // J lives on the host stack
+    RefitJob JW = J;  // the wide boxes (and the root box) from the same positions
+    if (cube) {
+        JW.w4 = s->w4.p + H.w4_off;
+        JW.leafW = s->leafW.p + H.foff;
+        JW.warrive = s->warrive.p + H.w4_off;
+        YS_CK(cudaMemcpyAsync(slot + 1, &JW, sizeof(JW), cudaMemcpyHostToDevice, st));
+        launch_refit(slot + 1, 1, n, s->status.p, st);
+    }
+    YS_CK(cudaStreamSynchronize(st));  // J, JW live on the host stack
     H.built = true;
     return YS_OK;
 }
@@ -931,7 +993,7 @@ ys_status enqueue_fused(ys_scene* s) {
     if (r) return r;
     YS_CK(cudaMemsetAsync(s->counters.p, 0, s->record ? 24 : 16, s->stream));
     StepArgs A = make_args(s);
-    k_fused<<<ceil_div(s->nV, 128), 128, 0, s->stream>>>(A);
+    launch_fused(A, s->nV, s->stream);
     YS_CK(cudaGetLastError());
     return YS_OK;
 }
@@ -988,7 +1050,7 @@ ys_status fused_substep(ys_scene* s) {
         s->evFused.push_back(s->evUsed);
         YS_CK(cudaEventRecord(next_event(s), s->stream));
     }
-    k_fused<<<ceil_div(s->nV, 128), 128, 0, s->stream>>>(A);
+    launch_fused(A, s->nV, s->stream);
     YS_CK(cudaGetLastError());
     if (s->timing) YS_CK(cudaEventRecord(next_event(s), s->stream));
     s->snapshot_pending = true;
@@ -1029,6 +1091,7 @@ ys_status ys_scene_destroy(ys_scene* s) {
     s->spr_split.free(); s->spr_nbr.free(); s->vaf_off.free(); s->vaf.free(); s->maxext.free(); s->status.free();
     s->codes.free(); s->idx.free(); s->visits.free(); s->box.free(); s->spr_rest.free(); s->scratch3.free(); s->gk.free(); s->gL.free(); s->F4.free(); s->F3.free();
     s->nodes.free(); s->parent.free(); s->parent2.free(); s->dmeshes.free(); s->jobs.free(); s->counters.free(); s->sortScratch.free();
+    s->w4.free(); s->leafW.free(); s->warrive.free(); s->wideScratch.free();
     s->scanScratch.free(); s->rows.free(); s->contacts.free(); s->csr.free(); s->pool.free(); s->bucket.free();
     drop_graphs(s);
     s->csr_off.free(); s->vstart.free(); s->vcount.free(); s->ext.free();
@@ -1069,9 +1132,12 @@ ys_status ys_scene_pack(ys_scene* s) {
     if (s->packed) return fail(YS_ERR_STATE, "already packed");
     if (s->meshes.empty()) return fail(YS_ERR_BAD_ARG, "empty scene");
     YS_CK(cudaSetDevice(s->device));
-    u32 nV = 0, nF = 0, nNodes = 0, maxF = 1;
+    u32 nV = 0, nF = 0, nNodes = 0, maxF = 1, nW4 = 0;
     for (auto& H : s->meshes) {
         H.voff = nV; H.foff = nF; H.node_off = nNodes;
+        H.w4_off = nW4;
+        H.w4_cap = H.d.num_facets ? std::max(H.d.num_facets - 1, 1u) : 0u;
+        nW4 += H.w4_cap;
         nV += H.d.num_vertices;
         nF += H.d.num_facets;
         nNodes += H.d.num_facets ? 2 * H.d.num_facets - 1 : 0;
@@ -1139,6 +1205,8 @@ ys_status ys_scene_pack(ys_scene* s) {
             }
         D.tgt_end = (u32)targets.size();
         D.gspr = NO_SPRINGS;
+        D.w4_off = H.w4_off;
+        D.w4_cap = H.w4_cap;
         md[m] = D;
     }
     spr_off[nV] = (u32)spr_nbr.size();
@@ -1157,7 +1225,11 @@ ys_status ys_scene_pack(ys_scene* s) {
     YS_CK(s->F4.alloc(std::max(nF, 1u))); YS_CK(s->F3.alloc(3 * (size_t)std::max(nF, 1u)));
     YS_CK(s->nodes.alloc(std::max(nNodes, 1u))); YS_CK(s->parent.alloc(std::max(nNodes, 1u)));
     YS_CK(s->parent2.alloc(std::max(nNodes, 1u)));
-    YS_CK(s->dmeshes.alloc(md.size())); YS_CK(s->jobs.alloc(6 * s->meshes.size() + 1));
+    YS_CK(s->dmeshes.alloc(md.size())); YS_CK(s->jobs.alloc(6 * s->meshes.size() + 2));
+    if (s->tree_layout == YS_TREE_CUBE) {
+        YS_CK(s->w4.alloc(std::max(nW4, 1u))); YS_CK(s->leafW.alloc(std::max(nF, 1u)));
+        YS_CK(s->warrive.alloc(std::max(nW4, 1u))); YS_CK(s->wideScratch.alloc(wide_build_scratch_bytes(maxF)));
+    }
     YS_CK(s->counters.alloc(8));
     YS_CK(s->sortScratch.alloc(sort_scratch_bytes(maxF)));
     // uploads
@@ -1215,6 +1287,11 @@ ys_status ys_scene_pack(ys_scene* s) {
         J.swept = (H.flags & MF_STATIC) ? 0u : 1u;
         J.selfMargin = selfHash ? s->P.margin : 0.f;
         J.maxExt = s->maxext.p + m;
+        if (s->tree_layout == YS_TREE_CUBE) {
+            J.w4 = s->w4.p + H.w4_off;
+            J.leafW = s->leafW.p + H.foff;
+            J.warrive = s->warrive.p + H.w4_off;
+        }
         s->hjobs.push_back(J);
         leaves += J.n;
     }
@@ -1507,6 +1584,28 @@ ys_status ys_scene_tree(ys_scene* s, int mesh, void* nodes, int32_t* parent, uin
     YS_CK(cudaStreamSynchronize(s->stream));
     if (n == 0) return YS_OK;
     const size_t nn = 2 * (size_t)n - 1;
+    if (nodes && s->tree_layout == YS_TREE_CUBE) {
+        // the cube layout refits the wide form only; give the binary form the
+        // boxes of a refit from the current state (swept for moving meshes)
+        RefitJob J;
+        memset(&J, 0, sizeof(J));
+        J.nodes = s->nodes.p + H.node_off;
+        J.parent = s->parent.p + H.node_off;
+        J.parent2 = s->parent2.p + H.node_off;
+        J.visits = s->visits.p + H.foff;
+        J.facets = s->F3.p + 3 * (size_t)H.foff;
+        J.x4 = s->X[s->cur].p;
+        J.v4 = s->V[s->cv].p;
+        J.voff = H.voff;
+        J.n = n;
+        J.dt = s->P.subh;
+        J.swept = (H.flags & MF_STATIC) ? 0u : 1u;
+        J.maxExt = s->maxext.p;  // unused (selfMargin == 0)
+        RefitJob* slot = s->jobs.p + 6 * (size_t)s->njobs;
+        YS_CK(cudaMemcpyAsync(slot, &J, sizeof(J), cudaMemcpyHostToDevice, s->stream));
+        launch_refit(slot, 1, n, s->status.p, s->stream);
+        YS_CK(cudaStreamSynchronize(s->stream));
+    }
     if (nodes) YS_CK(cudaMemcpy(nodes, s->nodes.p + H.node_off, 32 * nn, cudaMemcpyDeviceToHost));
     if (parent) YS_CK(cudaMemcpy(parent, s->parent.p + H.node_off, 4 * nn, cudaMemcpyDeviceToHost));
     if (codes) YS_CK(cudaMemcpy(codes, s->codes.p + H.foff, 4 * (size_t)n, cudaMemcpyDeviceToHost));
