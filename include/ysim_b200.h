@@ -219,6 +219,15 @@ ys_status ys_adjoint_backward(ys_adjoint* a, const float* d_dLdx, float* d_gk, f
  * bvh.hpp:141-2308).  Device pointers; x / v packed xyz floats. ---------- */
 ys_status ys_lbvh_create(ys_lbvh** out, uint32_t max_prims, int device, void* stream);
 ys_status ys_lbvh_destroy(ys_lbvh* t);
+/* Split of a run of equal Morton codes in the next builds.  0 (default): the
+ * reference's midpoint split (findSplit, src/metal/bvh.metal:197-223), the
+ * reference's tree node for node.  With three or more equal codes that tree
+ * is inconsistent with determineRange's ordering: a node can be the child of
+ * two internal nodes or of none, so a query reports some leaves twice and
+ * never reaches others, as the reference does.  1: split by the (code,
+ * index) key determineRange already orders by, so every node has one parent
+ * and a query reports every overlapping leaf exactly once. */
+ys_status ys_lbvh_set_split(ys_lbvh* t, int consistent);
 /* build(): scene box, Morton, radix sort, Karras, leaves, bottom-up
  * (bvh.hpp:1194-1301). */
 ys_status ys_lbvh_build(ys_lbvh* t, const float* d_x, uint32_t num_vertices, const uint32_t* d_facets,

@@ -59,10 +59,12 @@ def test_radix_sort_bit_exact(cuda_lib, oracle, n):
     assert np.array_equal(rk, keys[o]) and np.array_equal(rv, vals[o])
 
 
-def _lbvh(cuda_lib, x, f):
+def _lbvh(cuda_lib, x, f, consistent=False):
     from ysim_b200 import _lib
     h = C.c_void_p()
     _lib.check(cuda_lib.ys_lbvh_create(C.byref(h), len(f), 0, None))
+    if consistent:
+        _lib.check(cuda_lib.ys_lbvh_set_split(h, 1))
     dx, df = _dev(x.reshape(-1)), _dev(f.reshape(-1).astype(np.int32))
     _lib.check(cuda_lib.ys_lbvh_build(h, _p(dx), len(x), _p(df), len(f)))
     return h, dx, df
@@ -310,3 +312,133 @@ def test_spatial_hash_equals_lbvh_query(cuda_lib, oracle, case):
     assert len(got) > 0
     assert np.array_equal(got, bvh)
     assert np.array_equal(got, canon_pairs(oracle.brute_q1(x, f, q, float(h_margin), False)))
+
+
+def _dup_code_soup(seed=7):
+    """Triangles in clusters of 20 around 300 centres, each cluster far inside
+    one Morton cell (1/1024 of the box): long runs of equal codes."""
+    rng = np.random.default_rng(seed)
+    centres = rng.uniform(0.05, 0.95, (300, 3))
+    c = np.repeat(centres, 20, axis=0) + rng.uniform(-5e-5, 5e-5, (6000, 3))
+    x = (c[:, None, :] + rng.normal(0, 1e-4, (6000, 3, 3))).reshape(-1, 3).astype(np.float32)
+    # two far corners fix the box so every cluster stays inside its cell
+    x = np.concatenate([x, np.array([[0, 0, 0], [1e-6, 0, 0], [0, 1e-6, 0], [1, 1, 1], [1, 1 - 1e-6, 1],
+                                     [1 - 1e-6, 1, 1]], np.float32)])
+    f = np.arange(len(x), dtype=np.uint32).reshape(-1, 3)
+    q = (np.repeat(centres, 10, axis=0) + rng.uniform(-1e-3, 1e-3, (3000, 3))).astype(np.float32)
+    return x, f, q
+
+
+def _query_pairs(cuda_lib, h, q, margin):
+    import torch
+    from ysim_b200 import _lib
+    dq = _dev(q.reshape(-1))
+    cap = 1 << 22
+    pairs = torch.empty(2 * cap, dtype=torch.int32, device="cuda")
+    cnt = torch.zeros(1, dtype=torch.int64, device="cuda")
+    _lib.check(cuda_lib.ys_lbvh_query(h, _p(dq), len(q), margin, 0, _p(pairs), cap, _p(cnt)))
+    n = int(cnt.item())
+    return canon_pairs(pairs[: 2 * n].cpu().numpy().view(np.uint32))
+
+
+def test_equal_code_runs_reference_and_consistent_split(cuda_lib, oracle):
+    """Runs of equal Morton codes.  The reference's split: the GPU tree and
+    its query equal the oracle's (the reference's) node for node and pair for
+    pair, leaves reached twice or never included.  The (code, index) split:
+    one parent per node, and the query equals brute force and the spatial hash
+    exactly (no duplicate, nothing missing)."""
+    import torch
+    from ysim_b200 import _lib
+    x, f, q = _dup_code_soup()
+    margin = np.float32(1e-3)
+    onodes, oparent, ocodes, oidx = oracle.build_tree(x, f)
+    _, counts = np.unique(ocodes, return_counts=True)
+    assert (counts >= 3).sum() > 100
+    brute = canon_pairs(oracle.brute_q1(x, f, q, float(margin), False))
+    # reference split
+    h, dx, df = _lbvh(cuda_lib, x, f)
+    try:
+        nodes, parent, codes, idx = tree_arrays(cuda_lib, h)
+        assert np.array_equal(codes, ocodes) and np.array_equal(idx, oidx)
+        assert np.array_equal(nodes["a"], onodes["a"]) and np.array_equal(nodes["b"], onodes["b"])
+        ref = _query_pairs(cuda_lib, h, q, margin)
+        assert np.array_equal(ref, canon_pairs(oracle.query_points(onodes, f, q, float(margin))))
+        assert not np.array_equal(ref, brute)  # the inconsistent topology shows
+    finally:
+        _lib.check(cuda_lib.ys_lbvh_destroy(h))
+    # consistent split
+    h, dx, df = _lbvh(cuda_lib, x, f, consistent=True)
+    try:
+        nodes, parent, codes, idx = tree_arrays(cuda_lib, h)
+        claims = np.zeros(len(nodes), np.int64)
+        inner = nodes["a"] >= 0
+        np.add.at(claims, nodes["a"][inner], 1)
+        np.add.at(claims, nodes["b"][inner], 1)
+        assert claims[0] == 0 and (claims[1:] == 1).all()
+        cons = _query_pairs(cuda_lib, h, q, margin)
+        assert np.array_equal(cons, brute)
+    finally:
+        _lib.check(cuda_lib.ys_lbvh_destroy(h))
+    sh = C.c_void_p()
+    _lib.check(cuda_lib.ys_shash_create(C.byref(sh), len(f), 64 * len(f), 0, None))
+    try:
+        dq = _dev(q.reshape(-1))
+        _lib.check(cuda_lib.ys_shash_build(sh, _p(dx), _p(df), len(f), np.float32(2 * margin)))
+        cap = 1 << 22
+        pairs = torch.empty(2 * cap, dtype=torch.int32, device="cuda")
+        cnt = torch.zeros(1, dtype=torch.int64, device="cuda")
+        _lib.check(cuda_lib.ys_shash_query(sh, _p(dq), len(q), margin, _p(pairs), cap, _p(cnt)))
+        n = int(cnt.item())
+        assert np.array_equal(canon_pairs(pairs[: 2 * n].cpu().numpy().view(np.uint32)), brute)
+    finally:
+        _lib.check(cuda_lib.ys_shash_destroy(sh))
+
+
+def _teschner(x, y, z, mask):
+    return ((x * 73856093) ^ (y * 19349663) ^ (z * 83492791)) & 0xFFFFFFFF & mask
+
+
+def test_spatial_hash_bucket_collision_inside_one_triangle(cuda_lib):
+    """Two cells of one triangle that share a hash bucket, both inside one
+    query's range: the pair is reported once (the entry is matched to the cell
+    it was binned for, not to any cell of the bucket)."""
+    import torch
+    from ysim_b200 import _lib
+    max_entries = 1024
+    T = 1
+    while T < 2 * max_entries:
+        T <<= 1
+    mask = T - 1
+    found = None
+    for x in range(100, 400):
+        for y in range(100, 140):
+            for z in range(100, 110):
+                h0 = _teschner(x, y, z, mask)
+                if any(_teschner(x + dx, y + dy, z + dz, mask) == h0
+                       for dx in (0, 1) for dy in (0, 1) for dz in (0, 1) if (dx, dy, dz) != (0, 0, 0)):
+                    found = (x, y, z)
+                    break
+            if found:
+                break
+        if found:
+            break
+    assert found is not None
+    c = np.float32(2e-3)
+    x0, y0, z0 = found
+    lo = np.array([x0, y0, z0], np.float64) * float(c) + 1e-4
+    hi = (np.array([x0, y0, z0], np.float64) + 2) * float(c) - 1e-4
+    tri = np.array([[lo[0], lo[1], lo[2]], [hi[0], lo[1], hi[2]], [lo[0], hi[1], hi[2]]], np.float32)
+    f = np.arange(3, dtype=np.uint32).reshape(1, 3)
+    q = ((np.array([[x0, y0, z0]], np.float64) + 1) * float(c)).astype(np.float32)
+    dx, df, dq = _dev(tri.reshape(-1)), _dev(f.reshape(-1).astype(np.int32)), _dev(q.reshape(-1))
+    sh = C.c_void_p()
+    _lib.check(cuda_lib.ys_shash_create(C.byref(sh), 1, max_entries, 0, None))
+    try:
+        _lib.check(cuda_lib.ys_shash_build(sh, _p(dx), _p(df), 1, c))
+        pairs = torch.zeros(64, dtype=torch.int32, device="cuda")
+        cnt = torch.zeros(1, dtype=torch.int64, device="cuda")
+        _lib.check(cuda_lib.ys_shash_query(sh, _p(dq), 1, np.float32(c / 2), _p(pairs), 32, _p(cnt)))
+        assert int(cnt.item()) == 1
+        assert pairs[:2].cpu().tolist() == [0, 0]
+    finally:
+        _lib.check(cuda_lib.ys_shash_destroy(sh))

@@ -41,11 +41,14 @@ struct ys_lbvh {
     u32 maxPrims = 0, n = 0;
     Node* nodes = nullptr;
     i32* parent = nullptr;
-    i32* parent2 = nullptr;
+    u32* claimOff = nullptr;  // claimant lists (2N + 1 entries) and ids (2N)
+    i32* claims = nullptr;
+    void* karrasScratch = nullptr;
     u32 *codes = nullptr, *idx = nullptr, *visits = nullptr, *box = nullptr, *status = nullptr;
     void* scratch = nullptr;
     RefitJob* job = nullptr;
     const u32* facets = nullptr;
+    bool consistent = false;  // Karras split of runs of equal codes (ys_lbvh_set_split)
 };
 
 #define YS_CK2(call)                                                                                   \
@@ -67,7 +70,9 @@ ys_status ys_lbvh_create(ys_lbvh** out, uint32_t maxPrims, int device, void* str
     cudaError_t e = cudaSuccess;
     if (e == cudaSuccess) e = cudaMalloc((void**)&t->nodes, nn * sizeof(Node));
     if (e == cudaSuccess) e = cudaMalloc((void**)&t->parent, nn * 4);
-    if (e == cudaSuccess) e = cudaMalloc((void**)&t->parent2, nn * 4);
+    if (e == cudaSuccess) e = cudaMalloc((void**)&t->claimOff, (nn + 2) * 4);
+    if (e == cudaSuccess) e = cudaMalloc((void**)&t->claims, (nn + 1) * 4);
+    if (e == cudaSuccess) e = cudaMalloc(&t->karrasScratch, karras_scratch_bytes(maxPrims));
     if (e == cudaSuccess) e = cudaMalloc((void**)&t->codes, (size_t)maxPrims * 4);
     if (e == cudaSuccess) e = cudaMalloc((void**)&t->idx, (size_t)maxPrims * 4);
     if (e == cudaSuccess) e = cudaMalloc((void**)&t->visits, (size_t)maxPrims * 4);
@@ -88,7 +93,7 @@ ys_status ys_lbvh_destroy(ys_lbvh* t) {
     if (!t) return YS_OK;
     cudaSetDevice(t->device);
     cudaStreamSynchronize(t->stream);
-    cudaFree(t->nodes); cudaFree(t->parent); cudaFree(t->parent2); cudaFree(t->codes); cudaFree(t->idx); cudaFree(t->visits);
+    cudaFree(t->nodes); cudaFree(t->parent); cudaFree(t->claimOff); cudaFree(t->claims); cudaFree(t->karrasScratch); cudaFree(t->codes); cudaFree(t->idx); cudaFree(t->visits);
     cudaFree(t->box); cudaFree(t->status); cudaFree(t->scratch); cudaFree(t->job);
     delete t;
     return YS_OK;
@@ -97,13 +102,19 @@ ys_status ys_lbvh_destroy(ys_lbvh* t) {
 static ys_status run_refit(ys_lbvh* t, const float* x, const float* v, float dt, int swept) {
     RefitJob J;
     memset(&J, 0, sizeof(J));
-    J.nodes = t->nodes; J.parent = t->parent; J.parent2 = t->parent2; J.visits = t->visits; J.facets = t->facets;
+    J.nodes = t->nodes; J.parent = t->parent; J.claimOff = t->claimOff; J.claims = t->claims; J.visits = t->visits; J.facets = t->facets;
     J.x3 = x; J.v3 = v; J.voff = 0; J.n = t->n; J.leafBase = 0; J.dt = dt; J.swept = swept ? 1u : 0u;
     J.selfMargin = 0.f; J.maxExt = t->box;
     YS_CK2(cudaMemcpyAsync(t->job, &J, sizeof(J), cudaMemcpyHostToDevice, t->stream));
     launch_refit(t->job, 1, t->n, t->status, t->stream);
     YS_CK2(cudaGetLastError());
     YS_CK2(cudaStreamSynchronize(t->stream));
+    return YS_OK;
+}
+
+ys_status ys_lbvh_set_split(ys_lbvh* t, int consistent) {
+    if (!t) return fail(YS_ERR_BAD_ARG, "null tree");
+    t->consistent = consistent != 0;
     return YS_OK;
 }
 
@@ -116,7 +127,8 @@ ys_status ys_lbvh_build(ys_lbvh* t, const float* x, uint32_t nV, const uint32_t*
     launch_box(nullptr, x, 0, nV, t->box, t->stream);
     launch_morton(nullptr, x, 0, F, nF, t->box, t->codes, t->idx, t->stream);
     YS_CK2(radix_sort_pairs(t->codes, t->idx, nF, t->scratch, 0, 32, t->stream));
-    launch_karras(t->codes, t->idx, nF, t->nodes, t->parent, t->parent2, t->visits, t->stream);
+    YS_CK2(launch_karras(t->codes, t->idx, nF, t->nodes, t->parent, t->claimOff, t->claims, t->visits,
+                         t->karrasScratch, t->stream, t->consistent));
     YS_CK2(cudaGetLastError());
     return run_refit(t, x, nullptr, 0.f, 0);
 }

@@ -117,14 +117,26 @@ struct KarrasView {
     }
 };
 
-__global__ void k_parent_init(i32* __restrict__ parent, i32* __restrict__ parent2, u32 numNodes) {
+__global__ void k_parent_init(i32* __restrict__ parent, u32* __restrict__ claimOff, u32 numNodes) {
     u32 i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < numNodes) { parent[i] = -1; parent2[i] = 0x7FFFFFFF; }
+    if (i < numNodes) parent[i] = -1;
+    if (i <= numNodes) claimOff[i] = 0;
+}
+// After the exclusive scan of the claim counts: every internal node enters
+// itself in its two children's claimant lists.  The cursor is the list start
+// itself, so afterwards claimOff[c] is the end of c's list and the start is
+// claimOff[c - 1] (0 for c = 0).
+__global__ void k_claim_fill(const Node* __restrict__ nodes, u32 nInner, u32* __restrict__ claimOff,
+                             i32* __restrict__ claims) {
+    const u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nInner) return;
+    claims[atomicAdd(&claimOff[nodes[i].a], 1u)] = (i32)i;
+    claims[atomicAdd(&claimOff[nodes[i].b], 1u)] = (i32)i;
 }
 
 __global__ void __launch_bounds__(256) k_karras(const u32* __restrict__ codes, const u32* __restrict__ idx, u32 n,
                                                 Node* __restrict__ nodes, i32* __restrict__ parent,
-                                                i32* __restrict__ parent2, u32* __restrict__ visits,
+                                                u32* __restrict__ claimCount, u32* __restrict__ visits,
                                                 int consistent) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= (int)n) return;
@@ -174,16 +186,22 @@ __global__ void __launch_bounds__(256) k_karras(const u32* __restrict__ codes, c
     nodes[i].a = ca;
     nodes[i].b = cb;
     atomicMax(&parent[ca], i);
-    atomicMin(&parent2[ca], i);
+    atomicAdd(&claimCount[ca], 1u);
     atomicMax(&parent[cb], i);
-    atomicMin(&parent2[cb], i);
+    atomicAdd(&claimCount[cb], 1u);
 }
 
-void launch_karras(const u32* codes, const u32* idx, u32 n, Node* nodes, i32* parent, i32* parent2, u32* visits,
-                   cudaStream_t s, bool consistent) {
-    if (n == 0) return;
-    k_parent_init<<<ceil_div(2 * n - 1, 256), 256, 0, s>>>(parent, parent2, 2 * n - 1);
-    k_karras<<<ceil_div(n, 256), 256, 0, s>>>(codes, idx, n, nodes, parent, parent2, visits, consistent ? 1 : 0);
+size_t karras_scratch_bytes(u32 n) { return scan_scratch_bytes(n ? 2 * n : 1); }
+
+cudaError_t launch_karras(const u32* codes, const u32* idx, u32 n, Node* nodes, i32* parent, u32* claimOff,
+                          i32* claims, u32* visits, void* scratch, cudaStream_t s, bool consistent) {
+    if (n == 0) return cudaSuccess;
+    k_parent_init<<<ceil_div(2 * n, 256), 256, 0, s>>>(parent, claimOff, 2 * n - 1);
+    k_karras<<<ceil_div(n, 256), 256, 0, s>>>(codes, idx, n, nodes, parent, claimOff, visits, consistent ? 1 : 0);
+    cudaError_t e = exclusive_scan(claimOff, 2 * n, scratch, s);
+    if (e != cudaSuccess) return e;
+    if (n > 1) k_claim_fill<<<ceil_div(n - 1, 256), 256, 0, s>>>(nodes, n - 1, claimOff, claims);
+    return cudaGetLastError();
 }
 
 // ------------------------------------------------------------------ 4-wide
@@ -409,7 +427,7 @@ __global__ void __launch_bounds__(256) k_refit(const RefitJob* __restrict__ jobs
     const u32 i = g - J.leafBase;
     Node* nodes = J.nodes;
     const u32 leaf = n - 1 + i;
-    const u32 f = (u32)__ldcg(&nodes[leaf].b);
+    const u32 f = J.rootOnly ? i : (u32)__ldcg(&nodes[leaf].b);  // root only: the tree is not built
     const u32 vid[3] = {J.facets[3 * f], J.facets[3 * f + 1], J.facets[3 * f + 2]};
     f3 lo, hi;
     float ext = 0.f;
@@ -457,6 +475,26 @@ __global__ void __launch_bounds__(256) k_refit(const RefitJob* __restrict__ jobs
         const u32 e = __reduce_max_sync(peers, __float_as_uint(ext));
         if (J.selfMargin > 0.f && (threadIdx.x & 31) == (unsigned)(__ffs(peers) - 1)) atomicMax(J.maxExt, e);
     }
+    if (J.rootOnly) {
+        // union of the leaf boxes, one atomic per warp and job
+        const unsigned act = __activemask();
+        const unsigned peers = __match_any_sync(act, (unsigned long long)J.rootAcc);
+        const u32 v[6] = {ford(lo.x), ford(lo.y), ford(lo.z), ford(hi.x), ford(hi.y), ford(hi.z)};
+        u32 r[6];
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            r[k] = __reduce_min_sync(peers, v[k]);
+            r[3 + k] = __reduce_max_sync(peers, v[3 + k]);
+        }
+        if ((threadIdx.x & 31) == (unsigned)(__ffs(peers) - 1)) {
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                atomicMin(&J.rootAcc[k], r[k]);
+                atomicMax(&J.rootAcc[3 + k], r[3 + k]);
+            }
+        }
+        return;
+    }
     if (J.w4) {
         climb_wide(J, i, lo, hi, status);
         return;
@@ -465,28 +503,28 @@ __global__ void __launch_bounds__(256) k_refit(const RefitJob* __restrict__ jobs
     if (n == 1) return;
     const u32 numInner = n - 1;
     // Climb: deliver this node's arrival to every internal node that claims
-    // it as a child (one claimant in a consistent tree); the second arrival
-    // at a claimant combines it and climbs on from there.  Extra climbs (a
-    // node with two claimants) wait in a small pending list.  The climbing
-    // thread keeps the box of the node it carries in registers and, at a
-    // claimant, loads only the other child's box; the claimant's child words
-    // are read before the arrival atomic (they do not change during a refit).
-    u32 pending[4];
+    // it as a child (one claimant in a consistent tree, any number in the
+    // reference's tree over runs of equal codes); the second arrival at a
+    // claimant combines it and climbs on from there.  Further completed
+    // claimants wait in a bounded pending list.  The climbing thread keeps
+    // the box of the node it carries in registers and, at a claimant, loads
+    // only the other child's box.
+    constexpr int PENDING = 16;
+    u32 pending[PENDING];
     int np = 0;
     u32 child = leaf;
     f3 clo = lo, chi = hi;
     bool have_box = true;  // clo/chi hold child's box (false for a resumed pending node)
+    const u32 nClaims = 2 * (n - 1);
     for (u32 step = 0; step < 2 * n; ++step) {
-        const i32 p1 = __ldcg(&J.parent[child]);
-        const i32 p2 = __ldcg(&J.parent2[child]);
-        i32 claim[2] = {p1, (p2 != p1 && p2 != 0x7FFFFFFF) ? p2 : -1};
+        const u32 cs = child ? __ldcg(&J.claimOff[child - 1]) : 0u;
+        const u32 ce = __ldcg(&J.claimOff[child]);
         i32 next = -1;
         f3 nlo = clo, nhi = chi;
-#pragma unroll
-        for (int c = 0; c < 2; ++c) {
-            const i32 par = claim[c];
-            if (par < 0) continue;
-            if ((u32)par >= numInner) { atomicOr(status, ST_ITER_CAP); continue; }
+        if (ce < cs || ce > nClaims) { atomicOr(status, ST_ITER_CAP); return; }
+        for (u32 k = cs; k < ce; ++k) {
+            const i32 par = __ldcg(&J.claims[k]);
+            if (par < 0 || (u32)par >= numInner) { atomicOr(status, ST_ITER_CAP); continue; }
             const i32 ca = __ldcg(&nodes[par].a), cb = __ldcg(&nodes[par].b);
             u32 old = arrive_acq_rel(&J.visits[par]);
             if ((old & 1u) == 0u) continue;  // first arrival: the sibling's thread combines
@@ -512,7 +550,7 @@ __global__ void __launch_bounds__(256) k_refit(const RefitJob* __restrict__ jobs
             }
             store_box(&nodes[par], plo, phi);
             if (next < 0) { next = par; nlo = plo; nhi = phi; }
-            else if (np < 4) pending[np++] = (u32)par;
+            else if (np < PENDING) pending[np++] = (u32)par;
             else atomicOr(status, ST_ITER_CAP);
         }
         if (next < 0) {
@@ -527,6 +565,61 @@ __global__ void __launch_bounds__(256) k_refit(const RefitJob* __restrict__ jobs
         child = (u32)next;
     }
     atomicOr(status, ST_ITER_CAP);
+}
+
+__global__ void k_refit_roots(const RefitJob* __restrict__ jobs, u32 numJobs) {
+    const u32 j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= numJobs || !jobs[j].rootOnly || jobs[j].n == 0) return;
+    u32* a = jobs[j].rootAcc;
+    store_box(jobs[j].nodes, mk(funord(a[0]), funord(a[1]), funord(a[2])), mk(funord(a[3]), funord(a[4]), funord(a[5])));
+    // ready for the next refit
+    a[0] = a[1] = a[2] = 0xFFFFFFFFu;
+    a[3] = a[4] = a[5] = 0u;
+}
+
+void launch_refit_roots(const RefitJob* jobsDev, u32 numJobs, cudaStream_t s) {
+    if (numJobs) k_refit_roots<<<ceil_div(numJobs, 128), 128, 0, s>>>(jobsDev, numJobs);
+}
+
+__global__ void __launch_bounds__(256) k_root_boxes(const RefitJob* __restrict__ jobs, const uint2* __restrict__ chunks) {
+    __shared__ u32 red[8][6];
+    const uint2 c = chunks[blockIdx.x];
+    const RefitJob& J = jobs[c.x];
+    const u32 end = min(c.y + ROOT_CHUNK, J.nVert);
+    u32 r[6] = {0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu, 0u, 0u, 0u};
+    for (u32 i = c.y + threadIdx.x; i < end; i += blockDim.x) {
+        const f3 p = ld(J.x4, J.voff + i);
+        f3 a = p, b = p;
+        if (J.swept) {
+            const f3 sp = p + ld(J.v4, J.voff + i) * J.dt;  // the swept leaf's x + v dt
+            a = vmin(p, sp);
+            b = vmax(p, sp);
+        }
+        r[0] = min(r[0], ford(a.x)); r[1] = min(r[1], ford(a.y)); r[2] = min(r[2], ford(a.z));
+        r[3] = max(r[3], ford(b.x)); r[4] = max(r[4], ford(b.y)); r[5] = max(r[5], ford(b.z));
+    }
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        r[k] = __reduce_min_sync(0xFFFFFFFFu, r[k]);
+        r[3 + k] = __reduce_max_sync(0xFFFFFFFFu, r[3 + k]);
+    }
+    const u32 w = threadIdx.x >> 5;
+    if ((threadIdx.x & 31) == 0)
+        for (int k = 0; k < 6; ++k) red[w][k] = r[k];
+    __syncthreads();
+    if (threadIdx.x < 6) {
+        const u32 k = threadIdx.x;
+        u32 v = red[0][k];
+        for (u32 q = 1; q < (blockDim.x >> 5); ++q) v = k < 3 ? min(v, red[q][k]) : max(v, red[q][k]);
+        if (k < 3) atomicMin(&J.rootAcc[k], v);
+        else atomicMax(&J.rootAcc[k], v);
+    }
+}
+
+void launch_root_boxes(const RefitJob* jobsDev, u32 numJobs, const uint2* chunks, u32 numChunks, cudaStream_t s) {
+    if (!numJobs || !numChunks) return;
+    k_root_boxes<<<numChunks, 256, 0, s>>>(jobsDev, chunks);
+    k_refit_roots<<<ceil_div(numJobs, 128), 128, 0, s>>>(jobsDev, numJobs);
 }
 
 void launch_refit(const RefitJob* jobsDev, u32 numJobs, u32 totalLeaves, u32* status, cudaStream_t s) {

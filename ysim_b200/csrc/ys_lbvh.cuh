@@ -14,7 +14,8 @@ namespace ys {
 struct RefitJob {
     Node* nodes;            // 2N-1 nodes
     const i32* parent;      // 2N-1: largest internal node claiming the node as a child (-1: none)
-    const i32* parent2;     // 2N-1: smallest claimant (== parent when one claimant, INT_MAX when none)
+    const u32* claimOff;    // claimant lists: node c's are claims[claimOff[c-1] (0 for c = 0) .. claimOff[c])
+    const i32* claims;      // 2N-2 internal node ids
     u32* visits;            // N-1 per-internal-node arrival counters
     const u32* facets;      // 3 local vertex ids per face (packed)
     const float4* x4;       // positions (float4) or nullptr
@@ -33,6 +34,14 @@ struct RefitJob {
     Wide4* w4;
     const int2* leafW;      // per leaf: (wide node, slot)
     u32* warrive;           // per wide node: arrivals this refit (self-resetting)
+    // root only: no query descends this tree, only its root box is used (the
+    // inter-object cull); the leaves (face i for thread i, the tree need not
+    // be built) are reduced straight into rootAcc (3 ordered-int minima, then
+    // 3 maxima) and launch_refit_roots writes the root node and resets
+    // rootAcc to (~0, ~0, ~0, 0, 0, 0) for the next refit.
+    u32 rootOnly;
+    u32* rootAcc;
+    u32 nVert;              // vertices of the mesh (vertex form of the root box)
 };
 
 // Scene box of a mesh (min/max over all its vertices) into box[6] (float
@@ -47,14 +56,16 @@ void launch_morton(const float4* x4, const float* x3, u32 voff, const u32* facet
 // Runs of three or more equal Morton codes make the reference's topology
 // inconsistent (findSplit splits them at the midpoint, bvh.metal:204, while
 // determineRange orders them by index): a node can then be claimed as a child
-// by two internal nodes, or by none.  Child arrays stay exactly the
+// by several internal nodes, or by none.  Child arrays stay exactly the
 // reference's; parent keeps the largest claimant (what a serial build loop
-// leaves behind) and parent2 the smallest, so the refit reaches every claimant.
+// leaves behind) and the claimant lists (claimOff, 2N entries; claims, 2N - 2)
+// hold every claimant, so the refit reaches all of them.
 // consistent = true splits runs of equal codes by the (code, index) key that
 // determineRange already orders them by, so every node has one parent (the
 // cube layout); false keeps the reference's midpoint split.
-void launch_karras(const u32* codes, const u32* idx, u32 n, Node* nodes, i32* parent, i32* parent2, u32* visits,
-                   cudaStream_t s, bool consistent = false);
+size_t karras_scratch_bytes(u32 n);
+cudaError_t launch_karras(const u32* codes, const u32* idx, u32 n, Node* nodes, i32* parent, u32* claimOff,
+                          i32* claims, u32* visits, void* scratch, cudaStream_t s, bool consistent = false);
 // 4-wide form of a consistent binary tree of n leaves: internal nodes at even
 // depth become wide nodes (numbered by an exclusive scan), their children and
 // grandchildren their slots.  w4 and warrive need max(n - 1, 1) entries,
@@ -65,5 +76,13 @@ cudaError_t launch_wide_build(const Node* nodes, const i32* parent, u32 n, Wide4
 // Leaves + bottom-up for every job (jobs in device memory, jobsHost mirrors
 // them for the launch size).
 void launch_refit(const RefitJob* jobsDev, u32 numJobs, u32 totalLeaves, u32* status, cudaStream_t s);
+// Root boxes of the root-only jobs from their accumulators (after launch_refit).
+void launch_refit_roots(const RefitJob* jobsDev, u32 numJobs, cudaStream_t s);
+// Root boxes from vertices, for meshes whose every vertex belongs to a face
+// (then the union of the swept leaf boxes is the union of {x, x + v dt} over
+// the vertices): one block per chunk (job, first vertex) of ROOT_CHUNK
+// vertices, then launch_refit_roots on the same jobs.
+static constexpr u32 ROOT_CHUNK = 2048;
+void launch_root_boxes(const RefitJob* jobsDev, u32 numJobs, const uint2* chunks, u32 numChunks, cudaStream_t s);
 
 }  // namespace ys

@@ -625,6 +625,9 @@ struct HostMesh {
     u32 voff = 0, foff = 0, node_off = 0, flags = 0;
     u32 w4_off = 0, w4_cap = 0;
     bool built = false;
+    // the tree is descended by some query (a target of a query mesh, or
+    // self-queried), or is a static query mesh's (root box for the cull)
+    bool needs_tree = true;
     // TriangularCloth springs (mesh-local ids)
     std::vector<u32> spr_off, spr_split, spr_nbr, vaf_off, vaf;
     std::vector<float> spr_rest;
@@ -733,7 +736,16 @@ struct ys_scene {
     DBuf<uint4> F4;
     DBuf<u32> F3;  // packed facets (3 per face) for the refit kernel
     DBuf<Node> nodes;
-    DBuf<i32> parent, parent2;
+    DBuf<i32> parent, claims;        // largest claimant per node; claimant lists (offset node_off)
+    DBuf<u32> claimOff;              // per mesh 2N entries at node_off + mesh index
+    DBuf<u32> rootAcc;               // 32 per refit job (root-only jobs' leaf-box union, one line each)
+    u32 nRootOnly = 0;
+    // root-only jobs of meshes whose every vertex is on a face: root box by a
+    // chunked vertex reduction (6 tables (cur x cv) of nrjobs, like jobs)
+    DBuf<RefitJob> rjobs;
+    DBuf<uint2> rchunks;
+    u32 nrjobs = 0, nrchunks = 0;
+    DBuf<char> karrasScratch;
     DBuf<Wide4> w4;                  // cube layout: 4-wide trees used by every query and refit
     DBuf<int2> leafW;
     DBuf<u32> warrive;
@@ -839,6 +851,12 @@ void rotate(ys_scene* s) {
 }
 
 // BVH<..,LINEAR,TRIANGLE>::build for one mesh on the current positions.
+// Claimant-list offsets of mesh H's tree (2N entries after its nodes' offset,
+// one extra slot per earlier mesh).
+u32* claim_off(ys_scene* s, const HostMesh& H) {
+    return s->claimOff.p + H.node_off + (size_t)(&H - s->meshes.data());
+}
+
 ys_status build_tree(ys_scene* s, HostMesh& H) {
     const u32 n = H.d.num_facets;
     if (n == 0) return YS_OK;
@@ -851,8 +869,8 @@ ys_status build_tree(ys_scene* s, HostMesh& H) {
                   s->tree_layout == YS_TREE_CUBE);
     YS_CK(radix_sort_pairs(codes, idx, n, s->sortScratch.p, 0, 32, st));
     const bool cube = s->tree_layout == YS_TREE_CUBE;
-    launch_karras(codes, idx, n, s->nodes.p + H.node_off, s->parent.p + H.node_off, s->parent2.p + H.node_off,
-                  s->visits.p + H.foff, st, cube);
+    YS_CK(launch_karras(codes, idx, n, s->nodes.p + H.node_off, s->parent.p + H.node_off, claim_off(s, H),
+                        s->claims.p + H.node_off, s->visits.p + H.foff, s->karrasScratch.p, st, cube));
     if (cube)
         YS_CK(launch_wide_build(s->nodes.p + H.node_off, s->parent.p + H.node_off, n, s->w4.p + H.w4_off,
                                 s->leafW.p + H.foff, s->warrive.p + H.w4_off, s->wideScratch.p, st));
@@ -860,7 +878,8 @@ ys_status build_tree(ys_scene* s, HostMesh& H) {
     memset(&J, 0, sizeof(J));
     J.nodes = s->nodes.p + H.node_off;
     J.parent = s->parent.p + H.node_off;
-    J.parent2 = s->parent2.p + H.node_off;
+    J.claimOff = claim_off(s, H);
+    J.claims = s->claims.p + H.node_off;
     J.visits = s->visits.p + H.foff;
     J.facets = s->F3.p + 3 * (size_t)H.foff;
     J.x4 = s->X[s->cur].p;
@@ -891,6 +910,7 @@ ys_status preamble(ys_scene* s) {
     if (s->P.rebuild_frames && s->frame % s->P.rebuild_frames == 0) {
         for (auto& H : s->meshes) {
             if (H.built && H.d.behavior == YS_FLOAT) continue;
+            if (!H.needs_tree) continue;  // its root box comes from the root-only refit
             ys_status r = build_tree(s, H);
             if (r) return r;
         }
@@ -900,11 +920,15 @@ ys_status preamble(ys_scene* s) {
 }
 
 ys_status refit(ys_scene* s) {
+    if (s->nrjobs)
+        launch_root_boxes(s->rjobs.p + (size_t)(s->cur * 2 + s->cv) * s->nrjobs, s->nrjobs, s->rchunks.p,
+                          s->nrchunks, s->stream);
     if (s->njobs == 0) return YS_OK;
     // the job table for the current (position, velocity) buffer pair
     const RefitJob* table = s->jobs.p + (size_t)(s->cur * 2 + s->cv) * s->njobs;
     YS_CK(cudaMemsetAsync(s->maxext.p, 0, s->maxext.n * 4, s->stream));
     launch_refit(table, s->njobs, s->refitLeaves, s->status.p, s->stream);
+    if (s->nRootOnly) launch_refit_roots(table, s->njobs, s->stream);
     return YS_OK;
 }
 
@@ -1090,7 +1114,8 @@ ys_status ys_scene_destroy(ys_scene* s) {
     s->Fbuf.free(); s->mass.free(); s->mask.free(); s->vobj.free(); s->targets.free(); s->spr_off.free();
     s->spr_split.free(); s->spr_nbr.free(); s->vaf_off.free(); s->vaf.free(); s->maxext.free(); s->status.free();
     s->codes.free(); s->idx.free(); s->visits.free(); s->box.free(); s->spr_rest.free(); s->scratch3.free(); s->gk.free(); s->gL.free(); s->F4.free(); s->F3.free();
-    s->nodes.free(); s->parent.free(); s->parent2.free(); s->dmeshes.free(); s->jobs.free(); s->counters.free(); s->sortScratch.free();
+    s->nodes.free(); s->parent.free(); s->claims.free(); s->claimOff.free(); s->karrasScratch.free(); s->rootAcc.free();
+    s->rjobs.free(); s->rchunks.free(); s->dmeshes.free(); s->jobs.free(); s->counters.free(); s->sortScratch.free();
     s->w4.free(); s->leafW.free(); s->warrive.free(); s->wideScratch.free();
     s->scanScratch.free(); s->rows.free(); s->contacts.free(); s->csr.free(); s->pool.free(); s->bucket.free();
     drop_graphs(s);
@@ -1224,7 +1249,9 @@ ys_status ys_scene_pack(ys_scene* s) {
     YS_CK(s->codes.alloc(std::max(nF, 1u))); YS_CK(s->idx.alloc(std::max(nF, 1u))); YS_CK(s->visits.alloc(std::max(nF, 1u)));
     YS_CK(s->F4.alloc(std::max(nF, 1u))); YS_CK(s->F3.alloc(3 * (size_t)std::max(nF, 1u)));
     YS_CK(s->nodes.alloc(std::max(nNodes, 1u))); YS_CK(s->parent.alloc(std::max(nNodes, 1u)));
-    YS_CK(s->parent2.alloc(std::max(nNodes, 1u)));
+    YS_CK(s->claims.alloc(std::max(nNodes, 1u)));
+    YS_CK(s->claimOff.alloc((size_t)nNodes + s->meshes.size() + 1));
+    YS_CK(s->karrasScratch.alloc(karras_scratch_bytes(maxF)));
     YS_CK(s->dmeshes.alloc(md.size())); YS_CK(s->jobs.alloc(6 * s->meshes.size() + 2));
     if (s->tree_layout == YS_TREE_CUBE) {
         YS_CK(s->w4.alloc(std::max(nW4, 1u))); YS_CK(s->leafW.alloc(std::max(nF, 1u)));
@@ -1263,21 +1290,46 @@ ys_status ys_scene_pack(ys_scene* s) {
     YS_CK(cudaMemset(s->status.p, 0, 4));
     YS_CK(cudaMemset(s->maxext.p, 0, 4 * s->meshes.size()));
     YS_CK(cudaMemset(s->counters.p, 0, 8 * s->counters.n));
-    // refit jobs: every non-static mesh with a tree, plus static cloth that
-    // needs the self-hash grid extent
+    // Which trees a query descends: the targets of every query mesh, and the
+    // self-queried meshes.  A query mesh whose own tree nothing descends
+    // still needs that tree's root box (the inter-object cull): a root-only
+    // refit (or, for a static mesh, the one build) provides it.
+    std::vector<char> descended(s->meshes.size(), 0), rootUsed(s->meshes.size(), 0);
+    for (size_t m = 0; m < s->meshes.size(); ++m) {
+        const HostMesh& H = s->meshes[m];
+        if (!(H.flags & MF_QUERY) || !(H.flags & MF_TREE)) continue;
+        const bool selfQ = s->P.self_mode == YS_SELF_BVH ||
+                           (s->P.self_mode == YS_SELF_HASH && (H.flags & MF_CLOTH) && (H.flags & MF_SELF));
+        if (selfQ) descended[m] = 1;
+        for (u32 k = md[m].tgt_begin; k < md[m].tgt_end; ++k) descended[targets[k]] = 1;
+        if (md[m].tgt_end > md[m].tgt_begin) rootUsed[m] = 1;
+    }
+    for (size_t m = 0; m < s->meshes.size(); ++m) {
+        HostMesh& H = s->meshes[m];
+        H.needs_tree = H.d.num_facets && (descended[m] || ((H.flags & MF_STATIC) && rootUsed[m]));
+    }
+    // refit jobs: every non-static tree a query descends, plus static cloth
+    // that needs the self-hash grid extent; root-only jobs for the rest whose
+    // root box the cull reads
     s->hjobs.clear();
+    std::vector<RefitJob> hr;        // vertex-form root-only jobs
+    std::vector<uint2> chunks;
     u32 leaves = 0;
+    s->nRootOnly = 0;
     for (size_t m = 0; m < s->meshes.size(); ++m) {
         HostMesh& H = s->meshes[m];
         if (!H.d.num_facets) continue;
         const bool selfHash = s->P.self_mode == YS_SELF_HASH && (H.flags & MF_CLOTH) && (H.flags & MF_SELF) &&
                               (H.flags & MF_QUERY);
         if ((H.flags & MF_STATIC) && !selfHash) continue;
+        if (!descended[m] && !rootUsed[m] && !selfHash) continue;
+        const bool rootOnly = !descended[m] && !selfHash;
         RefitJob J;
         memset(&J, 0, sizeof(J));
         J.nodes = s->nodes.p + H.node_off;
         J.parent = s->parent.p + H.node_off;
-        J.parent2 = s->parent2.p + H.node_off;
+        J.claimOff = claim_off(s, H);
+    J.claims = s->claims.p + H.node_off;
         J.visits = s->visits.p + H.foff;
         J.facets = s->F3.p + 3 * (size_t)H.foff;
         J.voff = H.voff;
@@ -1287,7 +1339,18 @@ ys_status ys_scene_pack(ys_scene* s) {
         J.swept = (H.flags & MF_STATIC) ? 0u : 1u;
         J.selfMargin = selfHash ? s->P.margin : 0.f;
         J.maxExt = s->maxext.p + m;
-        if (s->tree_layout == YS_TREE_CUBE) {
+        if (rootOnly) {
+            J.rootOnly = 1;
+            J.nVert = H.d.num_vertices;
+            std::vector<char> onFace(H.d.num_vertices, 0);
+            for (u32 v : H.F) onFace[v] = 1;
+            if (std::all_of(onFace.begin(), onFace.end(), [](char c) { return c != 0; })) {
+                for (u32 c0 = 0; c0 < J.nVert; c0 += ROOT_CHUNK) chunks.push_back(make_uint2((u32)hr.size(), c0));
+                hr.push_back(J);
+                continue;
+            }
+            ++s->nRootOnly;
+        } else if (s->tree_layout == YS_TREE_CUBE) {
             J.w4 = s->w4.p + H.w4_off;
             J.leafW = s->leafW.p + H.foff;
             J.warrive = s->warrive.p + H.w4_off;
@@ -1297,6 +1360,31 @@ ys_status ys_scene_pack(ys_scene* s) {
     }
     s->refitLeaves = leaves;
     s->njobs = (u32)s->hjobs.size();
+    s->nrjobs = (u32)hr.size();
+    s->nrchunks = (u32)chunks.size();
+    {
+        const size_t nacc = std::max<size_t>(s->njobs + s->nrjobs, 1);
+        std::vector<u32> acc(32 * nacc, 0u);
+        for (size_t j = 0; j < nacc; ++j)
+            for (int k = 0; k < 3; ++k) acc[32 * j + k] = 0xFFFFFFFFu;
+        YS_CK(s->rootAcc.alloc(acc.size()));
+        YS_CK(cudaMemcpy(s->rootAcc.p, acc.data(), 4 * acc.size(), cudaMemcpyHostToDevice));
+        for (size_t j = 0; j < s->hjobs.size(); ++j)
+            if (s->hjobs[j].rootOnly) s->hjobs[j].rootAcc = s->rootAcc.p + 32 * j;
+        for (size_t j = 0; j < hr.size(); ++j) hr[j].rootAcc = s->rootAcc.p + 32 * (s->njobs + j);
+    }
+    if (s->nrjobs) {
+        YS_CK(s->rjobs.alloc(6 * (size_t)s->nrjobs));
+        YS_CK(s->rchunks.alloc(chunks.size()));
+        YS_CK(cudaMemcpy(s->rchunks.p, chunks.data(), chunks.size() * sizeof(uint2), cudaMemcpyHostToDevice));
+        for (int c = 0; c < 3; ++c)
+            for (int w = 0; w < 2; ++w) {
+                std::vector<RefitJob> t = hr;
+                for (auto& J : t) { J.x4 = s->X[c].p; J.v4 = s->V[w].p; }
+                YS_CK(cudaMemcpy(s->rjobs.p + (size_t)(c * 2 + w) * s->nrjobs, t.data(),
+                                 t.size() * sizeof(RefitJob), cudaMemcpyHostToDevice));
+            }
+    }
     for (int c = 0; c < 3; ++c)
         for (int w = 0; w < 2; ++w) {
             std::vector<RefitJob> t = s->hjobs;
@@ -1309,6 +1397,7 @@ ys_status ys_scene_pack(ys_scene* s) {
     s->cur = 0; s->prev = 1; s->cv = 0;
     // BroadPhase::build at initialize (Simulator::initialize -> build)
     for (auto& H : s->meshes) {
+        if (!H.needs_tree) continue;
         ys_status r = build_tree(s, H);
         if (r) return r;
     }
@@ -1583,6 +1672,10 @@ ys_status ys_scene_tree(ys_scene* s, int mesh, void* nodes, int32_t* parent, uin
     if (nprims) *nprims = n;
     YS_CK(cudaStreamSynchronize(s->stream));
     if (n == 0) return YS_OK;
+    if (!H.built) {  // a tree no query descends is built only when inspected
+        r = build_tree(s, H);
+        if (r) return r;
+    }
     const size_t nn = 2 * (size_t)n - 1;
     if (nodes && s->tree_layout == YS_TREE_CUBE) {
         // the cube layout refits the wide form only; give the binary form the
@@ -1591,7 +1684,8 @@ ys_status ys_scene_tree(ys_scene* s, int mesh, void* nodes, int32_t* parent, uin
         memset(&J, 0, sizeof(J));
         J.nodes = s->nodes.p + H.node_off;
         J.parent = s->parent.p + H.node_off;
-        J.parent2 = s->parent2.p + H.node_off;
+        J.claimOff = claim_off(s, H);
+    J.claims = s->claims.p + H.node_off;
         J.visits = s->visits.p + H.foff;
         J.facets = s->F3.p + 3 * (size_t)H.foff;
         J.x4 = s->X[s->cur].p;

@@ -7,8 +7,11 @@
 // collision microbenchmark: triangles are binned by their AABB into every
 // cell it overlaps (cell edge = 2h by default), a counting sort groups the
 // entries by hash bucket, and each query point probes the <= 8 cells its box
-// [p - h, p + h] overlaps.  A pair (p, t) is emitted only from the cell that
-// is the component-wise max of the two cell ranges' lower corners, so each
+// [p - h, p + h] overlaps.  Every entry keeps the ordinal of the cell it was
+// binned for, so a bucket shared by two cells (a hash collision, possibly of
+// two cells of the same triangle) never passes an entry off as another
+// cell's.  A pair (p, t) is emitted only from the cell that is the
+// component-wise max of the two cell ranges' lower corners, so each
 // overlapping pair comes out exactly once, and the candidate set equals the
 // LBVH point query's (queryPoints, bvh.metal:1394-1412) under the same
 // inclusive AABB test.
@@ -57,8 +60,8 @@ __global__ void k_sh_bound(const float* __restrict__ x, const u32* __restrict__ 
 }
 
 __global__ void k_sh_emit(const ShTri* __restrict__ tris, const u32* __restrict__ off, u32 nF, u32 mask,
-                          u32* __restrict__ ebucket, u32* __restrict__ etri, u32* __restrict__ bhist,
-                          u32* __restrict__ big, u32* __restrict__ nbig) {
+                          u32* __restrict__ ebucket, u32* __restrict__ etri, unsigned short* __restrict__ eord,
+                          u32* __restrict__ bhist, u32* __restrict__ big, u32* __restrict__ nbig) {
     u32 t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= nF) return;
     const ShTri r = tris[t];
@@ -75,17 +78,21 @@ __global__ void k_sh_emit(const ShTri* __restrict__ tris, const u32* __restrict_
                 u32 b = cell_hash(xx, y, z, mask);
                 ebucket[k] = b;
                 etri[k] = t;
+                eord[k] = (unsigned short)(k - base);  // < MAX_CELLS
                 atomicAdd(&bhist[b], 1u);
                 ++k;
             }
 }
 
-__global__ void k_sh_scatter(const u32* __restrict__ ebucket, const u32* __restrict__ etri, u32 nE,
-                             const u32* __restrict__ bstart, u32* __restrict__ bfill, u32* __restrict__ sorted) {
+__global__ void k_sh_scatter(const u32* __restrict__ ebucket, const u32* __restrict__ etri,
+                             const unsigned short* __restrict__ eord, u32 nE, const u32* __restrict__ bstart,
+                             u32* __restrict__ bfill, u32* __restrict__ sorted, unsigned short* __restrict__ sord) {
     u32 i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= nE) return;
     u32 b = ebucket[i];
-    sorted[bstart[b] + atomicAdd(&bfill[b], 1u)] = etri[i];
+    const u32 j = bstart[b] + atomicAdd(&bfill[b], 1u);
+    sorted[j] = etri[i];
+    sord[j] = eord[i];
 }
 
 __device__ __forceinline__ bool box_hit(f3 qmn, f3 qmx, const ShTri& r) {
@@ -97,7 +104,8 @@ __device__ __forceinline__ bool box_hit(f3 qmn, f3 qmx, const ShTri& r) {
 
 __global__ void __launch_bounds__(128) k_sh_query(const float* __restrict__ qx, u32 nQ, float m, float inv, u32 mask,
                                                   const ShTri* __restrict__ tris, const u32* __restrict__ bstart,
-                                                  const u32* __restrict__ sorted, const u32* __restrict__ big,
+                                                  const u32* __restrict__ sorted,
+                                                  const unsigned short* __restrict__ sord, const u32* __restrict__ big,
                                                   const u32* __restrict__ nbig, u32* __restrict__ pairs, u64 cap,
                                                   unsigned long long* count) {
     const u32 p = blockIdx.x * blockDim.x + threadIdx.x;
@@ -122,9 +130,12 @@ __global__ void __launch_bounds__(128) k_sh_query(const float* __restrict__ qx, 
                 for (u32 k = bstart[b]; k < bstart[b + 1]; ++k) {
                     const u32 t = sorted[k];
                     const ShTri r = tris[t];
-                    // the triangle really covers this cell (not a hash collision)
+                    // the entry was binned for this very cell (not for another
+                    // cell hashing to the same bucket)
                     if (xx < r.lo[0] || xx > r.hi[0] || y < r.lo[1] || y > r.hi[1] || z < r.lo[2] || z > r.hi[2])
                         continue;
+                    const int nx = r.hi[0] - r.lo[0] + 1, ny = r.hi[1] - r.lo[1] + 1;
+                    if ((int)sord[k] != ((z - r.lo[2]) * ny + (y - r.lo[1])) * nx + (xx - r.lo[0])) continue;
                     // emit from the first common cell only
                     if (xx != max(lo[0], r.lo[0]) || y != max(lo[1], r.lo[1]) || z != max(lo[2], r.lo[2])) continue;
                     if (box_hit(qmn, qmx, r)) emit(t);
@@ -149,6 +160,7 @@ struct ys_shash {
     ShTri* tris = nullptr;
     u32 *counts = nullptr, *ebucket = nullptr, *etri = nullptr, *bstart = nullptr, *bfill = nullptr, *sorted = nullptr,
         *big = nullptr, *nbig = nullptr;
+    unsigned short *eord = nullptr, *sord = nullptr;  // cell ordinal of each entry within its triangle's range
     void* scan = nullptr;
 };
 
@@ -177,6 +189,8 @@ ys_status ys_shash_create(ys_shash** out, uint32_t max_tris, uint32_t max_entrie
     if (e == cudaSuccess) e = cudaMalloc((void**)&h->ebucket, 4 * (size_t)max_entries);
     if (e == cudaSuccess) e = cudaMalloc((void**)&h->etri, 4 * (size_t)max_entries);
     if (e == cudaSuccess) e = cudaMalloc((void**)&h->sorted, 4 * (size_t)max_entries);
+    if (e == cudaSuccess) e = cudaMalloc((void**)&h->eord, 2 * (size_t)max_entries);
+    if (e == cudaSuccess) e = cudaMalloc((void**)&h->sord, 2 * (size_t)max_entries);
     if (e == cudaSuccess) e = cudaMalloc((void**)&h->bstart, 4 * ((size_t)T + 1));
     if (e == cudaSuccess) e = cudaMalloc((void**)&h->bfill, 4 * (size_t)T);
     if (e == cudaSuccess) e = cudaMalloc((void**)&h->big, 4 * (size_t)max_tris);
@@ -195,7 +209,7 @@ ys_status ys_shash_destroy(ys_shash* h) {
     if (!h) return YS_OK;
     cudaSetDevice(h->device);
     cudaStreamSynchronize(h->stream);
-    cudaFree(h->tris); cudaFree(h->counts); cudaFree(h->ebucket); cudaFree(h->etri); cudaFree(h->sorted);
+    cudaFree(h->tris); cudaFree(h->counts); cudaFree(h->ebucket); cudaFree(h->etri); cudaFree(h->sorted); cudaFree(h->eord); cudaFree(h->sord);
     cudaFree(h->bstart); cudaFree(h->bfill); cudaFree(h->big); cudaFree(h->nbig); cudaFree(h->scan);
     delete h;
     return YS_OK;
@@ -219,11 +233,13 @@ ys_status ys_shash_build(ys_shash* h, const float* d_x, const uint32_t* d_facets
     const u32 T = h->mask + 1;
     YS_CK3(cudaMemsetAsync(h->bstart, 0, 4 * ((size_t)T + 1), s));
     YS_CK3(cudaMemsetAsync(h->nbig, 0, 4, s));
-    k_sh_emit<<<ceil_div(nF, 256), 256, 0, s>>>(h->tris, h->counts, nF, h->mask, h->ebucket, h->etri, h->bstart,
-                                                 h->big, h->nbig);
+    k_sh_emit<<<ceil_div(nF, 256), 256, 0, s>>>(h->tris, h->counts, nF, h->mask, h->ebucket, h->etri, h->eord,
+                                                 h->bstart, h->big, h->nbig);
     YS_CK3(exclusive_scan(h->bstart, T + 1, h->scan, s));
     YS_CK3(cudaMemsetAsync(h->bfill, 0, 4 * (size_t)T, s));
-    if (nE) k_sh_scatter<<<ceil_div(nE, 256), 256, 0, s>>>(h->ebucket, h->etri, nE, h->bstart, h->bfill, h->sorted);
+    if (nE)
+        k_sh_scatter<<<ceil_div(nE, 256), 256, 0, s>>>(h->ebucket, h->etri, h->eord, nE, h->bstart, h->bfill, h->sorted,
+                                                      h->sord);
     YS_CK3(cudaGetLastError());
     YS_CK3(cudaStreamSynchronize(s));
     return YS_OK;
@@ -236,7 +252,8 @@ ys_status ys_shash_query(ys_shash* h, const float* d_qx, uint32_t nQ, float marg
     cudaStream_t s = h->stream;
     YS_CK3(cudaMemsetAsync(d_count, 0, 8, s));
     if (nQ) k_sh_query<<<ceil_div(nQ, 128), 128, 0, s>>>(d_qx, nQ, margin, h->inv, h->mask, h->tris, h->bstart,
-                                                          h->sorted, h->big, h->nbig, d_pairs, cap, d_count);
+                                                          h->sorted, h->sord, h->big, h->nbig, d_pairs, cap,
+                                                          d_count);
     YS_CK3(cudaGetLastError());
     YS_CK3(cudaStreamSynchronize(s));
     return YS_OK;

@@ -192,8 +192,10 @@ def obstacle_sphere(level: int, radius: float, center=(0.0, 0.0, 0.0), amplitude
 # ---------------------------------------------------------------- configs
 def config_c1(seed: int = 1, P: int = 64, level: int = 4, height: float = 1.0) -> SceneSpec:
     """Plain FastGridCloth 64x64 over a static level-4 icosphere (r 0.3);
-    k 1e3/5e2/1e1, m 1e-3, thickness 1e-3, subh 1/600, 10 substeps/frame,
-    reference margin/radius, jiggle U[0,1e-4] on the normal axis."""
+    k 1e3/5e2/1e1, m 1e-3, thickness 1e-3, 10 substeps/frame, reference
+    margin/radius, jiggle U[0,1e-4] on the normal axis.  subh is 1/6000
+    (h = 1/600 split in 10): the 12-spring stencil's stiffness over m = 1e-3
+    puts the explicit integrator's stability limit below 1/600."""
     from ._lib import FAST_GRID_CLOTH, MESH_COLLIDABLE
     rng = np.random.Generator(np.random.PCG64(seed))
     x, f = grid_cloth(P, 1.0, (0.0, height, 0.0))
@@ -251,10 +253,13 @@ def soup(n: int, seed: int = 3, nq: Optional[int] = None):
     return x, f, q
 
 
-def config_c4(seed: int = 4, instances: int = 256, lo: int = 16, hi: int = 256, level: int = 4) -> SceneSpec:
+def config_c4(seed: int = 4, instances: int = 256, lo: int = 16, hi: int = 256, level: int = 4,
+              drop: float = 0.1) -> SceneSpec:
     """Batched: independent FastGridCloth instances (side U{lo..hi}) each over
     its own level-4 icosphere (random offset, r in [0.2, 0.5]); instances sit
-    3 m apart and only collide within their own group."""
+    3 m apart and only collide within their own group; each cloth starts
+    `drop` above its obstacle's top.  Cloth physics and step are C1's
+    (k 1e3/5e2/1e1, m 1e-3, subh 1/6000, 10 substeps/frame)."""
     from ._lib import FAST_GRID_CLOTH, MESH_COLLIDABLE
     rng = np.random.Generator(np.random.PCG64(seed))
     meshes = []
@@ -264,15 +269,24 @@ def config_c4(seed: int = 4, instances: int = 256, lo: int = 16, hi: int = 256, 
         r = float(rng.uniform(0.2, 0.5))
         off = rng.uniform(-0.2, 0.2, 3)
         base = np.array([3.0 * (i % cols), 0.0, 3.0 * (i // cols)])
-        x, f = grid_cloth(P, 1.0, tuple(base + np.array([0.0, r + 0.1, 0.0])))
+        x, f = grid_cloth(P, 1.0, tuple(base + np.array([0.0, r + drop, 0.0])))
         x[:, 1] = (x[:, 1] + rng.uniform(0.0, 1e-4, P * P).astype(F32)).astype(F32)
         cloth = Mesh(behavior=FAST_GRID_CLOTH, flags=MESH_COLLIDABLE, x=x, facets=f, v=np.zeros_like(x),
-                     mass=np.full(P * P, 1e-2, F32), mask=np.ones(P * P, F32), kstretch=1e3, kshear=5e2, kbend=1e1,
+                     mass=np.full(P * P, 1e-3, F32), mask=np.ones(P * P, F32), kstretch=1e3, kshear=5e2, kbend=1e1,
                      thickness=1e-3, grid_n=P, grid_rest=fast_grid_rest(x, P), group=i)
         ob = obstacle_sphere(level, r, center=tuple(base + off * np.array([1.0, 0.0, 1.0])))
         ob.group = i
         meshes += [cloth, ob]
-    return SceneSpec(f"c4_batched{instances}", Params(subh=1.0 / 600.0, substeps=10), meshes, seed)
+    return SceneSpec(f"c4_batched{instances}", Params(subh=1.0 / 6000.0, substeps=10), meshes, seed)
+
+
+def split_instances(spec: SceneSpec) -> List[SceneSpec]:
+    """The plain per-instance form of a batched scene: one scene per group
+    (its cloth and its obstacle), same parameters, group ids reset to 0."""
+    groups = {}
+    for m in spec.meshes:
+        groups.setdefault(m.group, []).append(dataclasses.replace(m, group=0))
+    return [SceneSpec(f"{spec.name}_inst{g}", spec.params, ms, spec.seed) for g, ms in sorted(groups.items())]
 
 
 # ---------------------------------------------------------------- adjoint
