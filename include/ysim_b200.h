@@ -244,6 +244,29 @@ ys_status ys_lbvh_query(ys_lbvh* t, const float* d_qx, uint32_t num_queries, flo
 ys_status ys_lbvh_arrays(ys_lbvh* t, void** nodes, int32_t** parent, uint32_t** codes, uint32_t** idx,
                          uint32_t* num_prims);
 
+/* ---- Face-face spatial-hash broad phase (SpatialHashing<METAL>::detectCollisions,
+ * include/sim/spatial_hash.hpp:880-960; src/metal/spatialhashing.metal:64-478):
+ * bounding spheres, a grid of cell 2*maxR + margin, a home and up to 7
+ * phantom cells per face, per-cell home-home and home-phantom pairs with the
+ * reference's marking dedup and sphere cull, 6 rows per surviving pair.  The
+ * rows are those of the reference as a multiset (emission order differs).
+ * Inputs are the packed scene (Scene::pack): positions (packed xyz), vertex
+ * offsets per mesh (num_meshes + 1), facets with mesh-local vertex ids, face
+ * offsets per mesh (num_meshes + 1), behaviour and collider kind per mesh.
+ * Device pointers; asynchronous on the stream; no host synchronisation. */
+typedef struct ys_shff ys_shff;
+ys_status ys_shff_create(ys_shff** out, uint32_t max_faces, int device, void* stream);
+ys_status ys_shff_destroy(ys_shff* h);
+/* Rows (BroadCollision layout, 32 B) into d_rows[0, cap); *d_count receives
+ * the number of rows (rows beyond cap are counted, not written). */
+ys_status ys_shff_detect(ys_shff* h, const float* d_x, uint32_t num_vertices, const uint32_t* d_state_off,
+                         const uint32_t* d_facets, const uint32_t* d_facet_off, uint32_t num_faces,
+                         const uint32_t* d_behaviors, const uint32_t* d_shapes, uint32_t num_meshes, float margin,
+                         int enable_self, void* d_rows, uint64_t cap, unsigned long long* d_count);
+/* Entries, cells, candidate pairs and grid resolution of the last detect
+ * (the reference's LastRunStats, spatial_hash.hpp:183-208); synchronises. */
+ys_status ys_shff_stats(ys_shff* h, uint32_t out6[6]);
+
 /* ---- Uniform-grid spatial-hash broad phase, point vs triangle (the
  * spatial-hash family of the reference: SpatialHashing<METAL>::detectCollisions,
  * spatial_hash.hpp:880-960, and CpuSpatialHash, spatial_hash.hpp:1547-2016).

@@ -1,8 +1,9 @@
 """Host build of the reference's own Metal compute kernels: oracle/_ref/libysref.so.
 
-TEST INFRASTRUCTURE ONLY.  Compiles oracle/ref_harness.cpp three times, each
-time including one shader of the reference checkout in place
-(src/metal/bvh.metal, bruteforce.metal, physics.metal) with oracle/ref_shim
+TEST INFRASTRUCTURE ONLY.  Compiles oracle/ref_harness.cpp once per shader,
+each time including one shader of the reference checkout in place
+(src/metal/bvh.metal, bruteforce.metal, physics.metal, spatialhashing.metal)
+with oracle/ref_shim
 standing in for <metal_stdlib>; nothing of the reference is copied into this
 repository.  Skipped (returns None) when the reference checkout is absent;
 the built library is git-ignored but travels with the working tree.
@@ -19,7 +20,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 REF = os.environ.get("YSIM_REFERENCE", "/root/reference")
 OUT_DIR = os.path.join(HERE, "_ref")
 OUT = os.path.join(OUT_DIR, "libysref.so")
-SHADERS = {"BVH": "bvh.metal", "NARROW": "bruteforce.metal", "PHYSICS": "physics.metal"}
+SHADERS = {"BVH": "bvh.metal", "NARROW": "bruteforce.metal", "PHYSICS": "physics.metal",
+           "SH": "spatialhashing.metal"}
 
 
 def available() -> bool:

@@ -64,6 +64,8 @@ def lib():
             "yso_scene_contacts": (None, [vp, vp, vp]),
             "yso_scene_tree_nodes": (C.c_uint64, [vp, C.c_int]),
             "yso_scene_tree": (None, [vp, C.c_int, vp, vp, vp, vp]),
+            "yso_sh_face_face": (C.c_uint64, [vp, vp, vp, vp, vp, vp, C.c_uint32, C.c_float, C.c_int, vp,
+                                              C.c_uint64, vp]),
         }
         for k, (r, a) in sig.items():
             f = getattr(L, k)
@@ -133,6 +135,31 @@ def query_points(nodes, F, q, margin, self_query=False, cap=None):
     out = np.zeros((n, 2), np.uint32)
     lib().yso_query_points(P(nodes), len(nodes), P(F), P(q), len(q), margin, int(self_query), P(out), n)
     return out
+
+
+def pack_meshes(meshes):
+    """Packed-scene arrays of a mesh list (Scene::pack, scene.hpp:783-1180):
+    x (V, 3), per-mesh vertex and face offsets, facets with mesh-local vertex
+    ids, behaviours, shapes (0 = triangle mesh)."""
+    x = np.concatenate([np.asarray(m.x, np.float32) for m in meshes])
+    so = np.concatenate([[0], np.cumsum([m.nV for m in meshes])]).astype(np.uint32)
+    fo = np.concatenate([[0], np.cumsum([m.nF for m in meshes])]).astype(np.uint32)
+    F = np.concatenate([np.asarray(m.facets, np.uint32) for m in meshes])
+    beh = np.array([m.behavior for m in meshes], np.uint32)
+    shape = np.zeros(len(meshes), np.uint32)
+    return x, so, fo, F, beh, shape
+
+
+def sh_face_face(x, so, fo, F, beh, shape, margin, self_rows=True):
+    """H2 rows (ROW_DTYPE) of the face-face spatial hash, and stats (entries,
+    cells, candidate pairs, grid resolution)."""
+    a = [np.ascontiguousarray(t, d) for t, d in ((x, np.float32), (so, np.uint32), (F, np.uint32), (fo, np.uint32),
+                                                  (beh, np.uint32), (shape, np.uint32))]
+    st = np.zeros(6, np.uint32)
+    n = lib().yso_sh_face_face(*[P(t) for t in a], len(beh), margin, int(self_rows), None, 0, P(st))
+    out = np.zeros(n, ROW_DTYPE)
+    lib().yso_sh_face_face(*[P(t) for t in a], len(beh), margin, int(self_rows), P(out), n, P(st))
+    return out, st
 
 
 def brute_q1(x, F, q, margin, self_query=False):

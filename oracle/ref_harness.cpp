@@ -218,6 +218,106 @@ void yref_bucket(const void* contacts, uint32_t n, const uint32_t* voff, uint32_
 }
 
 }  // extern "C"
+#elif defined(YS_REF_SH)
+#include <algorithm>
+#include <vector>
+#include YS_STR(YS_REF_SRC)
+
+static_assert(sizeof(SHEntry) == 8, "SHEntry");
+static_assert(sizeof(CellProp) == 20, "CellProp");
+static_assert(sizeof(BroadCollision) == 32, "BroadCollision");
+
+extern "C" {
+
+// SpatialHashing<METAL>::detectCollisions (spatial_hash.hpp:880-960) over a
+// packed scene: the reference's kernels sh_buildBV, sh_assignCells,
+// sh_markStarts, sh_fillCellProp, sh_computePairCount and sh_broadPhase, in
+// that order, with the host steps between them restated from
+// spatial_hash.hpp: faceObj (:255-267), the max-radius reduction (the
+// maximum of the radii, :308-341), computeGrid (:343-400), the stable
+// 4-pass radix sort by cellID (:409-412, RadixSorter), findNumValid
+// (:414-426), hostScanCellStarts (:439-449) and hostScanPairPrefix
+// (:590-602).  Returns the number of rows the kernel counted (rows past cap
+// are dropped by the kernel).  out6: numValid, numCells, numPairs, gridRes.
+uint32_t yref_sh_detect(const float* x, const uint32_t* stateOff, const uint32_t* F, const uint32_t* facetOff,
+                        const uint32_t* behaviors, const uint32_t* shapes, uint32_t numMeshes, float margin,
+                        uint32_t enableSelf, void* rows, uint32_t cap, uint32_t* out6) {
+    const uint32_t nV = stateOff[numMeshes], nF = facetOff[numMeshes];
+    for (int k = 0; k < 6; ++k) out6[k] = 0;
+    if (nF == 0 || nV == 0) return 0;
+    std::vector<uint32_t> faceObj(nF);
+    for (uint32_t m = 0; m < numMeshes; ++m)
+        for (uint32_t f = facetOff[m]; f < facetOff[m + 1]; ++f) faceObj[f] = m;
+    SHParams params;
+    std::memset(&params, 0, sizeof(params));
+    params.numFaces = nF;
+    std::vector<float> centroid(3 * (size_t)nF), radius(nF);
+    for (uint32_t i = 0; i < nF; ++i)
+        sh_buildBV((const packed_float3*)x, stateOff, (const packed_uint3*)F, faceObj.data(), params,
+                   (packed_float3*)centroid.data(), radius.data(), i);
+    float maxR = 0.0f;
+    for (uint32_t i = 0; i < nF; ++i) maxR = max(maxR, radius[i]);
+    float3 mn(x[0], x[1], x[2]), mx = mn;
+    for (uint32_t v = 0; v < nV; ++v) {
+        float3 p(x[3 * v], x[3 * v + 1], x[3 * v + 2]);
+        mn = float3(std::min(mn.x, p.x), std::min(mn.y, p.y), std::min(mn.z, p.z));
+        mx = float3(std::max(mx.x, p.x), std::max(mx.y, p.y), std::max(mx.z, p.z));
+    }
+    float cellSize = 2.0f * maxR * 1.0f + margin;
+    if (cellSize <= 0.f) cellSize = std::max(margin, 1e-6f);
+    params.cellSize = cellSize;
+    params.epsilon = margin;
+    params.originMin = packed_float3(mn.x, mn.y, mn.z);
+    for (int k = 0; k < 3; ++k) {
+        float extent = mx[k] - mn[k];
+        uint32_t r = (uint32_t)std::ceil(extent / cellSize);
+        params.gridRes[k] = r == 0 ? 1 : r;
+    }
+    std::vector<SHEntry> entries(8 * (size_t)nF);
+    std::vector<uchar> faceCB(nF);
+    for (uint32_t i = 0; i < nF; ++i)
+        sh_assignCells((const packed_float3*)centroid.data(), radius.data(), params, entries.data(), faceCB.data(), i);
+    std::stable_sort(entries.begin(), entries.end(),
+                     [](const SHEntry& a, const SHEntry& b) { return a.cellID < b.cellID; });
+    uint32_t numValid = 0;
+    while (numValid < entries.size() && entries[numValid].cellID != 0xFFFFFFFFu) ++numValid;
+    std::vector<uint32_t> flag(numValid + 1), cellIdxOf(numValid + 1);
+    for (uint32_t i = 0; i < numValid; ++i) sh_markStarts(entries.data(), numValid, flag.data(), i);
+    uint32_t numCells = 0;
+    for (uint32_t i = 0; i < numValid; ++i) {
+        numCells += flag[i];
+        cellIdxOf[i] = numCells - 1;
+    }
+    std::vector<uint32_t> cpRaw(5 * (size_t)std::max(numCells, 1u), 0u);  // CellProp: 5 words, zeroed
+    CellProp* cp = reinterpret_cast<CellProp*>(cpRaw.data());
+    for (uint32_t i = 0; i < numValid; ++i)
+        sh_fillCellProp(entries.data(), flag.data(), cellIdxOf.data(), numValid, params, cp, i);
+    for (uint32_t c = 0; c < numCells; ++c) sh_computePairCount(cp, numCells, c);
+    std::vector<uint32_t> pairPrefix(numCells + 1, 0);
+    uint64_t running = 0;
+    for (uint32_t c = 0; c < numCells; ++c) {
+        pairPrefix[c] = (uint32_t)running;
+        running += cpRaw[5 * (size_t)c + 3];  // pairCnt
+    }
+    pairPrefix[numCells] = (uint32_t)running;
+    SHBroadParams bp;
+    bp.numCandidatePairs = (uint32_t)running;
+    bp.numCells = numCells;
+    bp.maxNumCollisions = cap;
+    bp.enableSelfCollisions = enableSelf ? 1u : 0u;
+    bp.epsilon = margin;
+    atomic_uint counter;
+    counter.v.store(0);
+    for (uint32_t id = 0; id < bp.numCandidatePairs; ++id)
+        sh_broadPhase(entries.data(), cp, pairPrefix.data(), faceCB.data(), faceObj.data(), (const packed_uint3*)F,
+                      facetOff, (const packed_float3*)centroid.data(), radius.data(), behaviors, shapes, bp, &counter,
+                      (BroadCollision*)rows, id);
+    out6[0] = numValid; out6[1] = numCells; out6[2] = bp.numCandidatePairs;
+    out6[3] = params.gridRes[0]; out6[4] = params.gridRes[1]; out6[5] = params.gridRes[2];
+    return counter.v.load();
+}
+
+}  // extern "C"
 #else
-#error "select YS_REF_BVH, YS_REF_NARROW or YS_REF_PHYSICS"
+#error "select YS_REF_BVH, YS_REF_NARROW, YS_REF_PHYSICS or YS_REF_SH"
 #endif

@@ -162,6 +162,7 @@ inline float3 cross(float3 a, float3 b) {
 }
 inline float length(float2 a) { return std::sqrt(dot(a, a)); }
 inline float length(float3 a) { return std::sqrt(dot(a, a)); }
+inline float distance(float3 a, float3 b) { return length(a - b); }
 inline float3 normalize(float3 a) { return a * (1.0f / std::sqrt(dot(a, a))); }
 inline float rsqrt(float x) { return 1.0f / std::sqrt(x); }
 inline float3 mix(float3 a, float3 b, float t) { return a + (b - a) * t; }

@@ -41,6 +41,7 @@ def lib():
             "yref_grid_forces": (None, [vp, vp, vp, vp, vp, f32, f32, f32, vp, u32]),
             "yref_integrate_grid": (None, [vp, vp, vp, vp, vp, vp, vp, vp, u32, f32, vp, u32, vp]),
             "yref_bucket": (None, [vp, u32, vp, u32, vp, vp, vp]),
+            "yref_sh_detect": (u32, [vp, vp, vp, vp, vp, vp, u32, f32, u32, vp, u32, vp]),
         }
         for k, (r, a) in sig.items():
             fn = getattr(L, k)
@@ -146,3 +147,17 @@ def integrate(kind, x, v, f, mass3, mask, csr, csr_off, voff, oid, subh, params)
     fn(P(x), P(v), P(c32(f)), P(c32(mass3)), P(c32(mask)), P(np.ascontiguousarray(csr)), P(c32(csr_off, np.uint32)),
        P(c32(voff, np.uint32)), oid, subh, P(c32(params, np.float32 if kind == "tri" else np.uint32)), len(x), P(an))
     return x, v, int(an[0])
+
+
+def sh_detect(x, so, fo, F, beh, shape, margin, self_rows=True, cap=None):
+    """SpatialHashing<METAL>::detectCollisions with the reference's kernels:
+    BroadCollision rows (ROW_DTYPE, in kernel emission order) and stats."""
+    if cap is None:
+        cap = 64 * len(F) + 64
+    out = np.zeros(cap, ROW_DTYPE)
+    st = np.zeros(6, np.uint32)
+    n = lib().yref_sh_detect(P(c32(x)), P(c32(so, np.uint32)), P(c32(F, np.uint32)), P(c32(fo, np.uint32)),
+                             P(c32(beh, np.uint32)), P(c32(shape, np.uint32)), len(beh), margin, int(self_rows),
+                             P(out), cap, P(st))
+    assert n <= cap, "row capacity"
+    return out[:n], st

@@ -225,6 +225,120 @@ void bottom_up(Node* tree, u32 nNodes) {
     }
 }
 
+// ---------------------------------------------------------------- H2 GPU hash
+// SpatialHashing<METAL>::detectCollisions (spatial_hash.hpp:880-960; kernels
+// spatialhashing.metal:64-478), the Pabst face-face hash, restated per cell:
+//   * bounding sphere per face: centroid ((v0+v1)+v2)*(1/3), radius =
+//     |centroid - v0| (sh_buildBV :84-87 uses v0 only);
+//   * grid: scene box over all vertices, cell = 2*maxR*1 + margin, res =
+//     ceil(extent/cell) >= 1 per axis (computeGrid :343-400);
+//   * home cell (floor, clamped) plus the octant's phantom cells whose wall
+//     is within r (sh_assignCells :143-238); a face's type mask holds the
+//     parity types (x&1 | y&1<<1 | z&1<<2) of every cell it entered;
+//   * in each cell, home-home and home-phantom pairs (phantom-phantom pairs
+//     are not candidates, :292-301), dropped when self pairs are off and
+//     both faces share a mesh, when both meshes are Float, when the type
+//     masks share a type below the cell's (the marking dedup), or when the
+//     centroids are farther apart than rA + rB + margin; each survivor gives
+//     6 rows: A's vertices against B's face and B's against A's (:440-477).
+struct ShHit { u32 cell; u32 face; bool phantom; };
+void sh_face_face(const float* x, const u32* stateOff, const u32* F, const u32* facetOff, const u32* beh,
+                  const u32* shape, u32 nM, float margin, bool self, std::vector<Row>& rows, u32 stats[6]) {
+    for (int k = 0; k < 6; ++k) stats[k] = 0;
+    const u32 nV = stateOff[nM], nF = facetOff[nM];
+    if (nF == 0 || nV == 0) return;
+    std::vector<u32> obj(nF);
+    for (u32 m = 0; m < nM; ++m)
+        for (u32 f = facetOff[m]; f < facetOff[m + 1]; ++f) obj[f] = m;
+    std::vector<V3> c(nF);
+    std::vector<float> r(nF);
+    float maxR = 0.f;
+    for (u32 f = 0; f < nF; ++f) {
+        const u32 vb = stateOff[obj[f]];
+        const V3 a = ld3(x, vb + F[3 * f]), b = ld3(x, vb + F[3 * f + 1]), d = ld3(x, vb + F[3 * f + 2]);
+        c[f] = (a + b + d) * (1.0f / 3.0f);
+        const V3 e = c[f] - a;
+        r[f] = std::sqrt(dot(e, e));
+        maxR = tmax(maxR, r[f]);
+    }
+    V3 lo = ld3(x, 0), hi = lo;
+    for (u32 v = 0; v < nV; ++v) { lo = vmin(lo, ld3(x, v)); hi = vmax(hi, ld3(x, v)); }
+    float cs = 2.0f * maxR * 1.0f + margin;
+    if (cs <= 0.f) cs = std::max(margin, 1e-6f);
+    const float o[3] = {lo.x, lo.y, lo.z}, ext[3] = {hi.x - lo.x, hi.y - lo.y, hi.z - lo.z};
+    int res[3];
+    for (int k = 0; k < 3; ++k) {
+        u32 q = (u32)std::ceil(ext[k] / cs);
+        res[k] = (int)(q == 0 ? 1 : q);
+    }
+    std::vector<ShHit> hits;
+    std::vector<u32> mask(nF, 0u);
+    const float hcs = cs * 0.5f;
+    for (u32 f = 0; f < nF; ++f) {
+        const float cc[3] = {c[f].x, c[f].y, c[f].z};
+        int g[3], sg[3];
+        float dist[3];
+        for (int k = 0; k < 3; ++k) {
+            g[k] = (int)std::floor((cc[k] - o[k]) / cs);
+            g[k] = std::min(std::max(g[k], 0), res[k] - 1);
+            const float local = cc[k] - (o[k] + (float)g[k] * cs);
+            sg[k] = local > hcs ? 1 : -1;
+            dist[k] = sg[k] > 0 ? cs - local : local;
+        }
+        for (int i = 0; i <= 1; ++i) {
+            if (i && dist[0] > r[f]) continue;
+            for (int j = 0; j <= 1; ++j) {
+                if (j && dist[1] > r[f]) continue;
+                for (int k = 0; k <= 1; ++k) {
+                    if (k && dist[2] > r[f]) continue;
+                    const int p[3] = {g[0] + i * sg[0], g[1] + j * sg[1], g[2] + k * sg[2]};
+                    if (p[0] < 0 || p[0] >= res[0] || p[1] < 0 || p[1] >= res[1] || p[2] < 0 || p[2] >= res[2])
+                        continue;
+                    mask[f] |= 1u << ((p[0] & 1) | ((p[1] & 1) << 1) | ((p[2] & 1) << 2));
+                    const u32 id = ((u32)p[2] * (u32)res[1] + (u32)p[1]) * (u32)res[0] + (u32)p[0];
+                    hits.push_back(ShHit{id, f, (i | j | k) != 0});
+                }
+            }
+        }
+    }
+    std::stable_sort(hits.begin(), hits.end(), [](const ShHit& a, const ShHit& b) { return a.cell < b.cell; });
+    stats[0] = (u32)hits.size();
+    stats[3] = (u32)res[0]; stats[4] = (u32)res[1]; stats[5] = (u32)res[2];
+    auto emit = [&](u32 A, u32 B) {
+        const u32 oA = obj[A], oB = obj[B];
+        for (int side = 0; side < 2; ++side) {
+            const u32 P = side ? B : A, T = side ? A : B, oP = obj[P], oT = obj[T];
+            for (int k = 0; k < 3; ++k)
+                rows.push_back(Row{F[3 * P + k], T - facetOff[oT], oP, oT, beh[oP], beh[oT], shape[oP], shape[oT]});
+        }
+        (void)oA; (void)oB;
+    };
+    for (size_t b = 0; b < hits.size();) {
+        size_t e = b;
+        while (e < hits.size() && hits[e].cell == hits[b].cell) ++e;
+        ++stats[1];
+        const u32 id = hits[b].cell;
+        const u32 gx = id % (u32)res[0], gy = (id / (u32)res[0]) % (u32)res[1], gz = id / ((u32)res[0] * (u32)res[1]);
+        const u32 below = (1u << ((gx & 1u) | ((gy & 1u) << 1) | ((gz & 1u) << 2))) - 1u;
+        std::vector<u32> home, ph;
+        for (size_t q = b; q < e; ++q) (hits[q].phantom ? ph : home).push_back(hits[q].face);
+        auto test = [&](u32 A, u32 B) {
+            ++stats[2];
+            if (!self && obj[A] == obj[B]) return;
+            if (beh[obj[A]] == 4u && beh[obj[B]] == 4u) return;  // Float-Float
+            if (mask[A] & mask[B] & below) return;
+            const V3 d = c[A] - c[B];
+            if (std::sqrt(dot(d, d)) > r[A] + r[B] + margin) return;
+            emit(A, B);
+        };
+        for (size_t i = 0; i < home.size(); ++i)
+            for (size_t j = i + 1; j < home.size(); ++j) test(home[i], home[j]);
+        for (u32 h : home)
+            for (u32 p : ph) test(h, p);
+        b = e;
+    }
+}
+
 // ---------------------------------------------------------------- Q1 query
 // intersectAABB (bvh.metal:1285-1290), inclusive.
 inline bool overlap(V3 qmn, V3 qmx, const Node& n) {
@@ -986,6 +1100,15 @@ uint64_t yso_brute_h1(const float* x, const float* xp, u32 nV, const u32* F, u32
     return cnt;
 }
 float yso_point_tri_sq(const float* p, const float* a, const float* b, const float* c) { return point_tri_sq(p, a, b, c); }
+// H2 rows (Row, 32 B each); returns the row count, stats6 = entries, cells,
+// candidate pairs, grid resolution.
+uint64_t yso_sh_face_face(const float* x, const u32* stateOff, const u32* F, const u32* facetOff, const u32* beh,
+                          const u32* shape, u32 nM, float margin, int self, void* out, uint64_t cap, u32* stats6) {
+    std::vector<Row> rows;
+    sh_face_face(x, stateOff, F, facetOff, beh, shape, nM, margin, self != 0, rows, stats6);
+    std::memcpy(out, rows.data(), sizeof(Row) * std::min<uint64_t>(cap, rows.size()));
+    return rows.size();
+}
 // One narrow-phase evaluation (returns 1 on contact).
 int yso_narrow_one(const float* qcur, const float* qprev, const float* t0, const float* t1, const float* t2, float band,
                    float* n_out, float* d_out) {

@@ -42,3 +42,13 @@ def reachable(nodes) -> np.ndarray:
         if nodes["a"][i] >= 0 and i < n - 1:
             stack += [int(nodes["a"][i]), int(nodes["b"][i])]
     return seen
+
+
+def canon_rows_full(rows) -> np.ndarray:
+    """BroadCollision rows (any structured dtype with the 8 row fields) as a
+    lexicographically sorted (n, 8) uint64 array."""
+    names = ("point", "tri", "qobj", "tobj", "qbeh", "tbeh", "qshape", "tshape")
+    if len(rows) == 0:
+        return np.zeros((0, 8), np.uint64)
+    a = np.stack([np.asarray(rows[k]).astype(np.uint64) for k in names], 1)
+    return a[np.lexsort(a.T[::-1])]

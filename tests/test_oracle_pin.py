@@ -167,3 +167,24 @@ def test_bucket_kernels_partition_like_oracle(oracle):
     for g in range(spec.nV):
         a, b = out[off[g]:off[g + 1]], oc[off[g]:off[g + 1]]
         assert sorted(zip(a["tobj"], a["tri"])) == sorted(zip(b["tobj"], b["tri"]))
+
+
+def _sh_scenes():
+    from ysim_b200 import generators as G
+    return [("c1", G.config_c1(P=24, level=2, height=0.2999), 0.015),
+            ("c2", G.config_c2(P=40, level=3, height=0.33, gravity=-9.81), 0.01),
+            ("c4", G.config_c4(instances=4, lo=8, hi=20, level=2, drop=0.001), 0.015)]
+
+
+@pytest.mark.parametrize("self_rows", [True, False])
+def test_face_face_hash_matches_reference_kernels(oracle, self_rows):
+    """H2: the restated face-face hash gives the reference kernels' rows (as a
+    multiset) and the same entry / cell / pair counts and grid."""
+    from helpers import canon_rows_full
+    for name, spec, margin in _sh_scenes():
+        x, so, fo, F, beh, shape = oracle.pack_meshes(spec.meshes)
+        a, sa = oracle.sh_face_face(x, so, fo, F, beh, shape, margin, self_rows)
+        b, sb = refk.sh_detect(x, so, fo, F, beh, shape, margin, self_rows)
+        assert len(a) > 0, name
+        assert np.array_equal(sa, sb), (name, sa, sb)
+        assert np.array_equal(canon_rows_full(a), canon_rows_full(b)), name

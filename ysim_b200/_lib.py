@@ -97,6 +97,12 @@ _PROTOS = {
     "ys_scene_contacts": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint64, C.POINTER(C.c_uint64)]),
     "ys_scene_tree": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                 C.POINTER(C.c_uint32)]),
+    "ys_shff_create": (C.c_int, [C.POINTER(C.c_void_p), C.c_uint32, C.c_int, C.c_void_p]),
+    "ys_shff_destroy": (C.c_int, [C.c_void_p]),
+    "ys_shff_detect": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32,
+                                 C.c_void_p, C.c_void_p, C.c_uint32, C.c_float, C.c_int, C.c_void_p, C.c_uint64,
+                                 C.c_void_p]),
+    "ys_shff_stats": (C.c_int, [C.c_void_p, C.c_void_p]),
     "ys_lbvh_set_split": (C.c_int, [C.c_void_p, C.c_int]),
     "ys_lbvh_create": (C.c_int, [C.POINTER(C.c_void_p), C.c_uint32, C.c_int, C.c_void_p]),
     "ys_lbvh_destroy": (C.c_int, [C.c_void_p]),

@@ -243,7 +243,8 @@ __device__ __forceinline__ void w4_empty_boxes(Wide4& o) {
 // One thread per even-depth internal node i: wide node widx[i] takes i's
 // children, each internal child replaced by its own two children.
 __global__ void k_wide_fill(const Node* __restrict__ nodes, const i32* __restrict__ dep, const u32* __restrict__ widx,
-                            u32 n, Wide4* __restrict__ w4, int2* __restrict__ leafW, u32* __restrict__ warrive) {
+                            u32 n, Wide4* __restrict__ w4, int2* __restrict__ leafW, int2* __restrict__ leafWf,
+                            u32* __restrict__ warrive) {
     const u32 i = blockIdx.x * blockDim.x + threadIdx.x;
     const u32 nInner = n - 1;
     if (i >= nInner || (dep[i] & 1)) return;
@@ -273,6 +274,7 @@ __global__ void k_wide_fill(const Node* __restrict__ nodes, const i32* __restric
         } else {
             o.child[k] = ~nodes[x].b;
             leafW[(u32)x - nInner] = make_int2((i32)W, k);
+            leafWf[nodes[x].b] = make_int2((i32)W, k);
         }
     }
     float4* dst = reinterpret_cast<float4*>(&w4[W]);
@@ -285,7 +287,7 @@ __global__ void k_wide_fill(const Node* __restrict__ nodes, const i32* __restric
 }
 // A tree of one leaf (binary node 0 is the leaf): one wide node, one slot.
 __global__ void k_wide_single(const Node* __restrict__ nodes, Wide4* __restrict__ w4, int2* __restrict__ leafW,
-                              u32* __restrict__ warrive) {
+                              int2* __restrict__ leafWf, u32* __restrict__ warrive, u32* __restrict__ wcount) {
     Wide4 o;
     w4_empty_boxes(o);
     o.child[0] = ~nodes[0].b;
@@ -295,7 +297,13 @@ __global__ void k_wide_single(const Node* __restrict__ nodes, Wide4* __restrict_
     o.pad = 0;
     w4[0] = o;
     leafW[0] = make_int2(0, 0);
+    leafWf[nodes[0].b] = make_int2(0, 0);
     warrive[0] = 0;
+    *wcount = 1;
+}
+// Number of wide nodes: the scan's last entry plus the last flag.
+__global__ void k_wide_count(const i32* __restrict__ dep, const u32* __restrict__ widx, u32 nInner, u32* wcount) {
+    *wcount = widx[nInner - 1] + ((dep[nInner - 1] & 1) == 0 ? 1u : 0u);
 }
 
 size_t wide_build_scratch_bytes(u32 n) {
@@ -303,11 +311,11 @@ size_t wide_build_scratch_bytes(u32 n) {
     return 4 * m * sizeof(i32) + 256 + (size_t)n * sizeof(u32) + 256 + scan_scratch_bytes(n ? n : 1);
 }
 
-cudaError_t launch_wide_build(const Node* nodes, const i32* parent, u32 n, Wide4* w4, int2* leafW, u32* warrive,
-                              void* scratch, cudaStream_t s) {
+cudaError_t launch_wide_build(const Node* nodes, const i32* parent, u32 n, Wide4* w4, int2* leafW, int2* leafWf,
+                              u32* warrive, u32* wcount, void* scratch, cudaStream_t s) {
     if (n == 0) return cudaSuccess;
     if (n == 1) {
-        k_wide_single<<<1, 1, 0, s>>>(nodes, w4, leafW, warrive);
+        k_wide_single<<<1, 1, 0, s>>>(nodes, w4, leafW, leafWf, warrive, wcount);
         return cudaGetLastError();
     }
     const u32 m = 2 * n - 1;
@@ -332,7 +340,8 @@ cudaError_t launch_wide_build(const Node* nodes, const i32* parent, u32 n, Wide4
     k_wide_flag<<<ceil_div(n - 1, 256), 256, 0, s>>>(dep, n - 1, widx);
     cudaError_t e = exclusive_scan(widx, n - 1, scanScratch, s);
     if (e != cudaSuccess) return e;
-    k_wide_fill<<<ceil_div(n - 1, 256), 256, 0, s>>>(nodes, dep, widx, n, w4, leafW, warrive);
+    k_wide_fill<<<ceil_div(n - 1, 256), 256, 0, s>>>(nodes, dep, widx, n, w4, leafW, leafWf, warrive);
+    k_wide_count<<<1, 1, 0, s>>>(dep, widx, n - 1, wcount);
     return cudaGetLastError();
 }
 
@@ -407,27 +416,34 @@ __device__ __forceinline__ void climb_wide(const RefitJob& J, u32 i, f3 lo, f3 h
     atomicOr(status, ST_ITER_CAP);
 }
 
+__device__ __forceinline__ u32 job_of(const RefitJob* __restrict__ jobs, u32 numJobs, u32 g) {
+    u32 lo = 0, hi = numJobs;  // largest j with leafBase <= g
+    while (hi - lo > 1) {
+        const u32 mid = (lo + hi) >> 1;
+        if (jobs[mid].leafBase <= g) lo = mid; else hi = mid;
+    }
+    return lo;
+}
+
 __global__ void __launch_bounds__(256) k_refit(const RefitJob* __restrict__ jobs, u32 numJobs, u32 totalLeaves,
                                                u32* status) {
-    u32 g = blockIdx.x * blockDim.x + threadIdx.x;
-    if (g >= totalLeaves) return;
-    // find the job owning leaf g (few jobs; linear scan is fine up to a few
-    // hundred and stays uniform within a warp most of the time)
-    u32 j = 0;
-    {
-        u32 lo = 0, hi = numJobs;  // largest j with leafBase <= g
-        while (hi - lo > 1) {
-            u32 mid = (lo + hi) >> 1;
-            if (jobs[mid].leafBase <= g) lo = mid; else hi = mid;
-        }
-        j = lo;
-    }
+    __shared__ u32 sh_ext[8];
+    __shared__ u32 sh_j0;
+    // threads past the last leaf do the work of the last leaf and drop it:
+    // every thread reaches the block reduction below
+    const u32 g0 = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool valid = g0 < totalLeaves;
+    const u32 g = valid ? g0 : totalLeaves - 1;
+    const u32 j = job_of(jobs, numJobs, g);  // the job owning leaf g
+    if (threadIdx.x == 0) sh_j0 = j;
     const RefitJob J = jobs[j];
     const u32 n = J.n;
     const u32 i = g - J.leafBase;
     Node* nodes = J.nodes;
     const u32 leaf = n - 1 + i;
-    const u32 f = J.rootOnly ? i : (u32)__ldcg(&nodes[leaf].b);  // root only: the tree is not built
+    // root only: the tree is not built; levels: thread i is face i (its slot
+    // comes from leafWf)
+    const u32 f = (J.rootOnly || J.levels) ? i : (u32)__ldcg(&nodes[leaf].b);
     const u32 vid[3] = {J.facets[3 * f], J.facets[3 * f + 1], J.facets[3 * f + 2]};
     f3 lo, hi;
     float ext = 0.f;
@@ -469,11 +485,26 @@ __global__ void __launch_bounds__(256) k_refit(const RefitJob* __restrict__ jobs
         if (ok) ext = e;
     }
     {
-        // one atomic per warp and job: group lanes by their target slot
-        const unsigned act = __activemask();
-        const unsigned peers = __match_any_sync(act, (unsigned long long)J.maxExt);
-        const u32 e = __reduce_max_sync(peers, __float_as_uint(ext));
-        if (J.selfMargin > 0.f && (threadIdx.x & 31) == (unsigned)(__ffs(peers) - 1)) atomicMax(J.maxExt, e);
+        // H1 extent: one atomic per block for the block's first job (most
+        // blocks hold one job), per warp and job for the others
+        __syncthreads();
+        const u32 j0 = sh_j0;
+        const u32 eb = valid ? __float_as_uint(ext) : 0u;  // positive floats order as ints
+        const u32 e0 = __reduce_max_sync(0xFFFFFFFFu, j == j0 ? eb : 0u);
+        if ((threadIdx.x & 31) == 0) sh_ext[threadIdx.x >> 5] = e0;
+        if (valid && j != j0 && J.selfMargin > 0.f) {
+            const unsigned act = __activemask();
+            const unsigned peers = __match_any_sync(act, (unsigned long long)J.maxExt);
+            const u32 e = __reduce_max_sync(peers, eb);
+            if ((threadIdx.x & 31) == (unsigned)(__ffs(peers) - 1)) atomicMax(J.maxExt, e);
+        }
+        __syncthreads();
+        if (threadIdx.x == 0 && jobs[j0].selfMargin > 0.f) {
+            u32 e = 0;
+            for (u32 w = 0; w < (blockDim.x >> 5); ++w) e = max(e, sh_ext[w]);
+            atomicMax(jobs[j0].maxExt, e);
+        }
+        if (!valid) return;
     }
     if (J.rootOnly) {
         // union of the leaf boxes, one atomic per warp and job
@@ -493,6 +524,18 @@ __global__ void __launch_bounds__(256) k_refit(const RefitJob* __restrict__ jobs
                 atomicMax(&J.rootAcc[3 + k], r[3 + k]);
             }
         }
+        return;
+    }
+    if (J.w4 && J.levels) {
+        const int2 ws = J.leafWf[f];
+        if (ws.x < 0 || (u32)ws.x >= (n > 1 ? n - 1 : 1u) || ws.y < 0 || ws.y > 3) {
+            atomicOr(status, ST_ITER_CAP);
+            return;
+        }
+        Wide4* W = J.w4 + ws.x;
+        const int k = ws.y;
+        W->lox[k] = lo.x; W->loy[k] = lo.y; W->loz[k] = lo.z;
+        W->hix[k] = hi.x; W->hiy[k] = hi.y; W->hiz[k] = hi.z;
         return;
     }
     if (J.w4) {
@@ -620,6 +663,135 @@ void launch_root_boxes(const RefitJob* jobsDev, u32 numJobs, const uint2* chunks
     if (!numJobs || !numChunks) return;
     k_root_boxes<<<numChunks, 256, 0, s>>>(jobsDev, chunks);
     k_refit_roots<<<ceil_div(numJobs, 128), 128, 0, s>>>(jobsDev, numJobs);
+}
+
+// ---- level-synchronous 4-wide refit
+
+// Heights: every leaf climbs carrying the height of the node it leaves; the
+// last child to arrive at a wide node reads the node's height (the max over
+// its children + 1) and climbs on.
+__global__ void __launch_bounds__(256) k_wide_heights(const RefitJob* __restrict__ jobs, u32 numJobs,
+                                                      u32 totalLeaves, u32* status) {
+    const u32 g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= totalLeaves) return;
+    const RefitJob& J = jobs[job_of(jobs, numJobs, g)];
+    if (!J.w4 || !J.levels) return;
+    const u32 i = g - J.leafBase;
+    const u32 cap = J.n > 1 ? J.n - 1 : 1;
+    i32 w = J.leafW[i].x;
+    u32 h = 0;
+    for (u32 step = 0; step < 128; ++step) {
+        if (w < 0 || (u32)w >= cap) break;
+        const u32 nc = __ldcg(&J.w4[w].nchild);
+        if (nc == 0 || nc > 4) break;
+        atomicMax(&J.hacc[w], h + 1);
+        if (arrive_inc_acq_rel(&J.warrive[w], nc - 1) != nc - 1) return;
+        h = __ldcg(&J.hacc[w]);
+        w = __ldcg(&J.w4[w].parent);
+        if (w < 0) return;
+    }
+    atomicOr(status, ST_ITER_CAP);
+}
+
+__global__ void __launch_bounds__(256) k_level_count(const RefitJob* __restrict__ jobs, u32 numJobs,
+                                                     u32 totalLeaves, u32* __restrict__ hcount, u32* status) {
+    const u32 g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= totalLeaves) return;
+    const RefitJob& J = jobs[job_of(jobs, numJobs, g)];
+    if (!J.w4 || !J.levels) return;
+    const u32 local = g - J.leafBase;
+    if (local >= *J.wcount) return;
+    const u32 h = J.hacc[local];
+    if (h == 0 || h > MAX_LEVELS) {
+        atomicOr(status, ST_ITER_CAP);
+        atomicAdd(&hcount[0], 1u);  // marks the level lists unusable
+        return;
+    }
+    atomicAdd(&hcount[h], 1u);
+}
+
+__global__ void __launch_bounds__(256) k_level_fill(const RefitJob* __restrict__ jobs, u32 numJobs, u32 totalLeaves,
+                                                    const u32* __restrict__ hoff, u32* __restrict__ hcursor,
+                                                    uint2* __restrict__ list) {
+    const u32 g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= totalLeaves) return;
+    const u32 j = job_of(jobs, numJobs, g);
+    const RefitJob& J = jobs[j];
+    if (!J.w4 || !J.levels) return;
+    const u32 local = g - J.leafBase;
+    if (local >= *J.wcount) return;
+    const u32 h = J.hacc[local];
+    if (h == 0 || h > MAX_LEVELS) return;
+    list[hoff[h] + atomicAdd(&hcursor[h], 1u)] = make_uint2(local, j);
+}
+
+void launch_wide_heights(const RefitJob* jobsDev, u32 numJobs, u32 totalLeaves, u32* status, cudaStream_t s) {
+    if (totalLeaves) k_wide_heights<<<ceil_div(totalLeaves, 256), 256, 0, s>>>(jobsDev, numJobs, totalLeaves, status);
+}
+void launch_level_count(const RefitJob* jobsDev, u32 numJobs, u32 totalLeaves, u32* hcount, u32* status,
+                        cudaStream_t s) {
+    if (totalLeaves)
+        k_level_count<<<ceil_div(totalLeaves, 256), 256, 0, s>>>(jobsDev, numJobs, totalLeaves, hcount, status);
+}
+void launch_level_fill(const RefitJob* jobsDev, u32 numJobs, u32 totalLeaves, const u32* hoff, u32* hcursor,
+                       uint2* list, cudaStream_t s) {
+    if (totalLeaves)
+        k_level_fill<<<ceil_div(totalLeaves, 256), 256, 0, s>>>(jobsDev, numJobs, totalLeaves, hoff, hcursor, list);
+}
+
+// One wide node: the union of its slots (in slot order) into its parent's
+// slot, or into the binary root node at the top.
+__device__ __forceinline__ void refit_wide_node(const RefitJob& J, u32 local) {
+    Wide4* W = J.w4 + local;
+    const u32 nc = W->nchild;
+    const i32 par = W->parent;
+    const u32 ps = W->slot;
+    const float4* p = reinterpret_cast<const float4*>(W);
+    const float4 lx = p[0], ly = p[1], lz = p[2], hx = p[3], hy = p[4], hz = p[5];
+    f3 lo = mk(lx.x, ly.x, lz.x), hi = mk(hx.x, hy.x, hz.x);
+    if (nc > 1) { lo = vmin(lo, mk(lx.y, ly.y, lz.y)); hi = vmax(hi, mk(hx.y, hy.y, hz.y)); }
+    if (nc > 2) { lo = vmin(lo, mk(lx.z, ly.z, lz.z)); hi = vmax(hi, mk(hx.z, hy.z, hz.z)); }
+    if (nc > 3) { lo = vmin(lo, mk(lx.w, ly.w, lz.w)); hi = vmax(hi, mk(hx.w, hy.w, hz.w)); }
+    if (par < 0) {
+        store_box(J.nodes, lo, hi);
+        return;
+    }
+    Wide4* P = J.w4 + par;
+    P->lox[ps] = lo.x; P->loy[ps] = lo.y; P->loz[ps] = lo.z;
+    P->hix[ps] = hi.x; P->hiy[ps] = hi.y; P->hiz[ps] = hi.z;
+}
+
+__global__ void __launch_bounds__(256) k_refit_level(const RefitJob* __restrict__ jobs, const uint2* __restrict__ list,
+                                                     u32 count) {
+    const u32 t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= count) return;
+    const uint2 e = list[t];
+    refit_wide_node(jobs[e.y], e.x);
+}
+
+// Levels from..top in one block: the slots a level reads were written by the
+// same block before the preceding __syncthreads.
+__global__ void __launch_bounds__(1024) k_refit_top(const RefitJob* __restrict__ jobs, const uint2* __restrict__ list,
+                                                    const u32* __restrict__ hoff, u32 from, u32 top) {
+    for (u32 h = from; h <= top; ++h) {
+        const u32 b = hoff[h], e = hoff[h + 1];
+        for (u32 t = b + threadIdx.x; t < e; t += blockDim.x) {
+            const uint2 q = list[t];
+            refit_wide_node(jobs[q.y], q.x);
+        }
+        __syncthreads();
+    }
+}
+
+void launch_refit_levels(const RefitJob* jobsDev, const uint2* list, const u32* hoffDev, const u32* hostOff,
+                         u32 top, cudaStream_t s) {
+    u32 h = 1;
+    for (; h <= top; ++h) {
+        const u32 cnt = hostOff[h + 1] - hostOff[h];
+        if (cnt < 2048) break;
+        k_refit_level<<<ceil_div(cnt, 256), 256, 0, s>>>(jobsDev, list + hostOff[h], cnt);
+    }
+    if (h <= top) k_refit_top<<<1, 1024, 0, s>>>(jobsDev, list, hoffDev, h, top);
 }
 
 void launch_refit(const RefitJob* jobsDev, u32 numJobs, u32 totalLeaves, u32* status, cudaStream_t s) {

@@ -42,6 +42,13 @@ struct RefitJob {
     u32 rootOnly;
     u32* rootAcc;
     u32 nVert;              // vertices of the mesh (vertex form of the root box)
+    // level-synchronous 4-wide refit: the leaf kernel (face order) only
+    // writes each leaf box into its slot (leafWf); launch_refit_levels then
+    // combines the wide nodes height by height
+    u32 levels;
+    const int2* leafWf;     // per face: (wide node, slot)
+    const u32* wcount;      // number of wide nodes of this tree
+    u32* hacc;              // per wide node: height (1 = leaf children only)
 };
 
 // Scene box of a mesh (min/max over all its vertices) into box[6] (float
@@ -71,8 +78,24 @@ cudaError_t launch_karras(const u32* codes, const u32* idx, u32 n, Node* nodes, 
 // grandchildren their slots.  w4 and warrive need max(n - 1, 1) entries,
 // leafW n, scratch wide_build_scratch_bytes(n).  Boxes are filled by a refit.
 size_t wide_build_scratch_bytes(u32 n);
-cudaError_t launch_wide_build(const Node* nodes, const i32* parent, u32 n, Wide4* w4, int2* leafW, u32* warrive,
-                              void* scratch, cudaStream_t s);
+cudaError_t launch_wide_build(const Node* nodes, const i32* parent, u32 n, Wide4* w4, int2* leafW, int2* leafWf,
+                              u32* warrive, u32* wcount, void* scratch, cudaStream_t s);
+
+// Level lists of the 4-wide trees of a job table (jobs with w4 and levels):
+// heights by a climb, then every wide node into the list of its height as
+// (node, job).  hcount / hoff: MAX_LEVELS + 1 entries; the host reads hcount
+// to size the level launches.
+static constexpr u32 MAX_LEVELS = 64;
+void launch_wide_heights(const RefitJob* jobsDev, u32 numJobs, u32 totalLeaves, u32* status, cudaStream_t s);
+void launch_level_count(const RefitJob* jobsDev, u32 numJobs, u32 totalLeaves, u32* hcount, u32* status,
+                        cudaStream_t s);
+void launch_level_fill(const RefitJob* jobsDev, u32 numJobs, u32 totalLeaves, const u32* hoff, u32* hcursor,
+                       uint2* list, cudaStream_t s);
+// Per substep, after launch_refit wrote the leaf slots: levels 1 .. split-1
+// one launch each (hostOff[h] .. hostOff[h+1] of list), then levels split ..
+// top in one block, level by level.
+void launch_refit_levels(const RefitJob* jobsDev, const uint2* list, const u32* hoffDev, const u32* hostOff,
+                         u32 top, cudaStream_t s);
 // Leaves + bottom-up for every job (jobs in device memory, jobsHost mirrors
 // them for the launch size).
 void launch_refit(const RefitJob* jobsDev, u32 numJobs, u32 totalLeaves, u32* status, cudaStream_t s);

@@ -495,8 +495,20 @@ __global__ void __launch_bounds__(128, 8) k_fused(StepArgs A) {
             A.vcount[g] = (u32)nc;
         }
     }
-    warp_count(&A.counters[0], rows);
-    warp_count(&A.counters[1], (u32)nc);
+    // rows and contacts: one atomic per block and counter (every thread of
+    // the block gets here)
+    {
+        __shared__ u32 sh_cnt[2][FUSED_WARPS];
+        const u32 r = __reduce_add_sync(FULL_MASK, rows), c = __reduce_add_sync(FULL_MASK, (u32)nc);
+        if (lane == 0) { sh_cnt[0][threadIdx.x >> 5] = r; sh_cnt[1][threadIdx.x >> 5] = c; }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            unsigned long long R = 0, Cn = 0;
+            for (int w = 0; w < FUSED_WARPS; ++w) { R += sh_cnt[0][w]; Cn += sh_cnt[1][w]; }
+            if (R) { atomicAdd(&A.counters[0], R); atomicAdd(&A.counters[3], R); }
+            if (Cn) { atomicAdd(&A.counters[1], Cn); atomicAdd(&A.counters[4], Cn); }
+        }
+    }
     if (st) atomicOr(A.status, st);
 }
 
@@ -747,9 +759,15 @@ struct ys_scene {
     u32 nrjobs = 0, nrchunks = 0;
     DBuf<char> karrasScratch;
     DBuf<Wide4> w4;                  // cube layout: 4-wide trees used by every query and refit
-    DBuf<int2> leafW;
-    DBuf<u32> warrive;
+    DBuf<int2> leafW, leafWf;        // per leaf / per face: (wide node, slot)
+    DBuf<u32> warrive, wcount, hacc; // arrivals, wide nodes per mesh, heights
     DBuf<char> wideScratch;
+    // level-synchronous refit of the wide trees: nodes listed by height
+    DBuf<uint2> wlist;
+    DBuf<u32> hcount, hoff, hcursor;
+    std::vector<u32> lvl_off;        // host copy of hoff (MAX_LEVELS + 2)
+    u32 lvl_top = 0;
+    bool use_levels = false;
     DBuf<MeshDev> dmeshes;
     DBuf<RefitJob> jobs;            // 6 tables (cur x cv) of njobs, then one build slot
     std::vector<RefitJob> hjobs;
@@ -873,7 +891,8 @@ ys_status build_tree(ys_scene* s, HostMesh& H) {
                         s->claims.p + H.node_off, s->visits.p + H.foff, s->karrasScratch.p, st, cube));
     if (cube)
         YS_CK(launch_wide_build(s->nodes.p + H.node_off, s->parent.p + H.node_off, n, s->w4.p + H.w4_off,
-                                s->leafW.p + H.foff, s->warrive.p + H.w4_off, s->wideScratch.p, st));
+                                s->leafW.p + H.foff, s->leafWf.p + H.foff, s->warrive.p + H.w4_off,
+                                s->wcount.p + (&H - s->meshes.data()), s->wideScratch.p, st));
     RefitJob J;
     memset(&J, 0, sizeof(J));
     J.nodes = s->nodes.p + H.node_off;
@@ -905,13 +924,77 @@ ys_status build_tree(ys_scene* s, HostMesh& H) {
     return YS_OK;
 }
 
+void drop_graphs(ys_scene* s);
+
+// Upload the 6 job tables (cur x cv) with the level-mode flag of the 4-wide jobs.
+ys_status upload_jobs(ys_scene* s, bool levels) {
+    for (int c = 0; c < 3; ++c)
+        for (int w = 0; w < 2; ++w) {
+            std::vector<RefitJob> t = s->hjobs;
+            for (auto& J : t) {
+                J.x4 = s->X[c].p;
+                J.v4 = s->V[w].p;
+                J.levels = (levels && J.w4) ? 1u : 0u;
+            }
+            if (!t.empty())
+                YS_CK(cudaMemcpy(s->jobs.p + (size_t)(c * 2 + w) * s->njobs, t.data(), t.size() * sizeof(RefitJob),
+                                 cudaMemcpyHostToDevice));
+        }
+    return YS_OK;
+}
+
+// Level lists of the 4-wide trees after a build: heights, counts per height,
+// the lists.  Falls back to the climb refit when a tree is taller than
+// MAX_LEVELS.  Level sizes change with every build, so captured substeps
+// are dropped.
+ys_status build_levels(ys_scene* s) {
+    if (s->tree_layout != YS_TREE_CUBE || s->njobs == 0) return YS_OK;
+    bool any = false;
+    for (auto& J : s->hjobs) any = any || J.w4;
+    if (!any) return YS_OK;
+    cudaStream_t st = s->stream;
+    ys_status r = upload_jobs(s, true);
+    if (r) return r;
+    const RefitJob* table = s->jobs.p;
+    YS_CK(cudaMemsetAsync(s->hacc.p, 0, 4 * s->hacc.n, st));
+    launch_wide_heights(table, s->njobs, s->refitLeaves, s->status.p, st);
+    YS_CK(cudaMemsetAsync(s->hcount.p, 0, 4 * (MAX_LEVELS + 2), st));
+    launch_level_count(table, s->njobs, s->refitLeaves, s->hcount.p, s->status.p, st);
+    std::vector<u32> cnt(MAX_LEVELS + 2);
+    YS_CK(cudaMemcpyAsync(cnt.data(), s->hcount.p, 4 * cnt.size(), cudaMemcpyDeviceToHost, st));
+    YS_CK(cudaStreamSynchronize(st));
+    drop_graphs(s);
+    if (cnt[0] != 0) {  // a tree taller than MAX_LEVELS: climb instead
+        s->use_levels = false;
+        return upload_jobs(s, false);
+    }
+    s->lvl_off.assign(MAX_LEVELS + 2, 0);
+    s->lvl_top = 0;
+    for (u32 h = 1; h <= MAX_LEVELS; ++h) {
+        s->lvl_off[h + 1] = s->lvl_off[h] + cnt[h];
+        if (cnt[h]) s->lvl_top = h;
+    }
+    YS_CK(cudaMemcpyAsync(s->hoff.p, s->lvl_off.data(), 4 * s->lvl_off.size(), cudaMemcpyHostToDevice, st));
+    YS_CK(cudaMemsetAsync(s->hcursor.p, 0, 4 * (MAX_LEVELS + 2), st));
+    launch_level_fill(table, s->njobs, s->refitLeaves, s->hoff.p, s->hcursor.p, s->wlist.p, st);
+    YS_CK(cudaStreamSynchronize(st));  // the host copy of the offsets stays valid
+    s->use_levels = true;
+    return YS_OK;
+}
+
 ys_status preamble(ys_scene* s) {
     if (s->cursor != 0) return YS_OK;
     if (s->P.rebuild_frames && s->frame % s->P.rebuild_frames == 0) {
+        bool rebuilt = false;
         for (auto& H : s->meshes) {
             if (H.built && H.d.behavior == YS_FLOAT) continue;
             if (!H.needs_tree) continue;  // its root box comes from the root-only refit
             ys_status r = build_tree(s, H);
+            if (r) return r;
+            rebuilt = true;
+        }
+        if (rebuilt) {
+            ys_status r = build_levels(s);
             if (r) return r;
         }
     }
@@ -928,6 +1011,8 @@ ys_status refit(ys_scene* s) {
     const RefitJob* table = s->jobs.p + (size_t)(s->cur * 2 + s->cv) * s->njobs;
     YS_CK(cudaMemsetAsync(s->maxext.p, 0, s->maxext.n * 4, s->stream));
     launch_refit(table, s->njobs, s->refitLeaves, s->status.p, s->stream);
+    if (s->use_levels)
+        launch_refit_levels(table, s->wlist.p, s->hoff.p, s->lvl_off.data(), s->lvl_top, s->stream);
     if (s->nRootOnly) launch_refit_roots(table, s->njobs, s->stream);
     return YS_OK;
 }
@@ -1117,6 +1202,8 @@ ys_status ys_scene_destroy(ys_scene* s) {
     s->nodes.free(); s->parent.free(); s->claims.free(); s->claimOff.free(); s->karrasScratch.free(); s->rootAcc.free();
     s->rjobs.free(); s->rchunks.free(); s->dmeshes.free(); s->jobs.free(); s->counters.free(); s->sortScratch.free();
     s->w4.free(); s->leafW.free(); s->warrive.free(); s->wideScratch.free();
+    s->leafWf.free(); s->wcount.free(); s->hacc.free(); s->wlist.free(); s->hcount.free(); s->hoff.free();
+    s->hcursor.free();
     s->scanScratch.free(); s->rows.free(); s->contacts.free(); s->csr.free(); s->pool.free(); s->bucket.free();
     drop_graphs(s);
     s->csr_off.free(); s->vstart.free(); s->vcount.free(); s->ext.free();
@@ -1255,7 +1342,13 @@ ys_status ys_scene_pack(ys_scene* s) {
     YS_CK(s->dmeshes.alloc(md.size())); YS_CK(s->jobs.alloc(6 * s->meshes.size() + 2));
     if (s->tree_layout == YS_TREE_CUBE) {
         YS_CK(s->w4.alloc(std::max(nW4, 1u))); YS_CK(s->leafW.alloc(std::max(nF, 1u)));
+        YS_CK(s->leafWf.alloc(std::max(nF, 1u)));
         YS_CK(s->warrive.alloc(std::max(nW4, 1u))); YS_CK(s->wideScratch.alloc(wide_build_scratch_bytes(maxF)));
+        YS_CK(cudaMemset(s->warrive.p, 0, 4 * s->warrive.n));
+        YS_CK(s->wcount.alloc(s->meshes.size())); YS_CK(cudaMemset(s->wcount.p, 0, 4 * s->meshes.size()));
+        YS_CK(s->hacc.alloc(std::max(nW4, 1u))); YS_CK(s->wlist.alloc(std::max(nW4, 1u)));
+        YS_CK(s->hcount.alloc(MAX_LEVELS + 2)); YS_CK(s->hoff.alloc(MAX_LEVELS + 2));
+        YS_CK(s->hcursor.alloc(MAX_LEVELS + 2));
     }
     YS_CK(s->counters.alloc(8));
     YS_CK(s->sortScratch.alloc(sort_scratch_bytes(maxF)));
@@ -1354,6 +1447,9 @@ ys_status ys_scene_pack(ys_scene* s) {
             J.w4 = s->w4.p + H.w4_off;
             J.leafW = s->leafW.p + H.foff;
             J.warrive = s->warrive.p + H.w4_off;
+            J.leafWf = s->leafWf.p + H.foff;
+            J.wcount = s->wcount.p + m;
+            J.hacc = s->hacc.p + H.w4_off;
         }
         s->hjobs.push_back(J);
         leaves += J.n;
@@ -1385,20 +1481,20 @@ ys_status ys_scene_pack(ys_scene* s) {
                                  t.size() * sizeof(RefitJob), cudaMemcpyHostToDevice));
             }
     }
-    for (int c = 0; c < 3; ++c)
-        for (int w = 0; w < 2; ++w) {
-            std::vector<RefitJob> t = s->hjobs;
-            for (auto& J : t) { J.x4 = s->X[c].p; J.v4 = s->V[w].p; }
-            if (!t.empty())
-                YS_CK(cudaMemcpy(s->jobs.p + (size_t)(c * 2 + w) * s->njobs, t.data(), t.size() * sizeof(RefitJob),
-                                 cudaMemcpyHostToDevice));
-        }
+    {
+        ys_status r = upload_jobs(s, false);
+        if (r) return r;
+    }
     s->packed = true;
     s->cur = 0; s->prev = 1; s->cv = 0;
     // BroadPhase::build at initialize (Simulator::initialize -> build)
     for (auto& H : s->meshes) {
         if (!H.needs_tree) continue;
         ys_status r = build_tree(s, H);
+        if (r) return r;
+    }
+    {
+        ys_status r = build_levels(s);
         if (r) return r;
     }
     YS_CK(cudaStreamSynchronize(st));
