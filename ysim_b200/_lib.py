@@ -82,6 +82,8 @@ _PROTOS = {
     "ys_scene_set_record": (C.c_int, [C.c_void_p, C.c_int]),
     "ys_scene_set_graphs": (C.c_int, [C.c_void_p, C.c_int]),
     "ys_scene_set_tree_layout": (C.c_int, [C.c_void_p, C.c_int]),
+    "ys_scene_set_fused_variant": (C.c_int, [C.c_void_p, C.c_int]),
+    "ys_scene_autotune": (C.c_int, [C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p]),
     "ys_scene_sync": (C.c_int, [C.c_void_p]),
     "ys_scene_stream": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
     "ys_scene_get_state": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),

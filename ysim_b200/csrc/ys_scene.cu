@@ -263,8 +263,10 @@ __device__ __forceinline__ void insert_contact(VContact (&buf)[MAXC], int& nc, u
 }
 
 // WIDE: descend the 4-wide form of the trees (cube layout), else the binary one.
-template <bool WIDE>
-__global__ void __launch_bounds__(128, 8) k_fused(StepArgs A) {
+// MINB: CTAs per SM the registers are capped for (8: 64 registers, 6: 80,
+// 4: no cap); the results do not depend on it (ys_scene_autotune picks one).
+template <bool WIDE, int MINB>
+__global__ void __launch_bounds__(128, MINB) k_fused(StepArgs A) {
     __shared__ WarpWork wq[FUSED_WARPS];
     const u32 lane = threadIdx.x & 31u;
     WarpWork& Q = wq[threadIdx.x >> 5];
@@ -512,9 +514,18 @@ __global__ void __launch_bounds__(128, 8) k_fused(StepArgs A) {
     if (st) atomicOr(A.status, st);
 }
 
-void launch_fused(const StepArgs& A, u32 nV, cudaStream_t st) {
-    if (A.wide) k_fused<true><<<ceil_div(nV, 128), 128, 0, st>>>(A);
-    else k_fused<false><<<ceil_div(nV, 128), 128, 0, st>>>(A);
+static constexpr int FUSED_VARIANTS[3] = {8, 6, 4};  // register caps, as CTAs per SM
+
+void launch_fused(const StepArgs& A, u32 nV, cudaStream_t st, int minBlocks) {
+    const dim3 g(ceil_div(nV, 128)), b(128);
+    switch ((A.wide ? 0 : 10) + minBlocks) {
+        case 8: k_fused<true, 8><<<g, b, 0, st>>>(A); break;
+        case 6: k_fused<true, 6><<<g, b, 0, st>>>(A); break;
+        case 4: k_fused<true, 4><<<g, b, 0, st>>>(A); break;
+        case 18: k_fused<false, 8><<<g, b, 0, st>>>(A); break;
+        case 16: k_fused<false, 6><<<g, b, 0, st>>>(A); break;
+        default: k_fused<false, 4><<<g, b, 0, st>>>(A); break;
+    }
 }
 
 // ------------------------------------------------------------------ staged
@@ -787,6 +798,7 @@ struct ys_scene {
     // refit + fused substep replayed without host launch overhead
     bool use_graphs = true;
     cudaGraphExec_t graphs[18] = {};
+    int fused_min_blocks = 8;        // k_fused register cap (ys_scene_set_fused_variant / ys_scene_autotune)
     int tree_layout = YS_TREE_CUBE;  // Morton normalisation of the scene trees
     DBuf<char> sortScratch, scanScratch;
     // staged / record buffers
@@ -1102,7 +1114,7 @@ ys_status enqueue_fused(ys_scene* s) {
     if (r) return r;
     YS_CK(cudaMemsetAsync(s->counters.p, 0, s->record ? 24 : 16, s->stream));
     StepArgs A = make_args(s);
-    launch_fused(A, s->nV, s->stream);
+    launch_fused(A, s->nV, s->stream, s->fused_min_blocks);
     YS_CK(cudaGetLastError());
     return YS_OK;
 }
@@ -1159,7 +1171,7 @@ ys_status fused_substep(ys_scene* s) {
         s->evFused.push_back(s->evUsed);
         YS_CK(cudaEventRecord(next_event(s), s->stream));
     }
-    launch_fused(A, s->nV, s->stream);
+    launch_fused(A, s->nV, s->stream, s->fused_min_blocks);
     YS_CK(cudaGetLastError());
     if (s->timing) YS_CK(cudaEventRecord(next_event(s), s->stream));
     s->snapshot_pending = true;
@@ -1543,6 +1555,65 @@ ys_status ys_scene_set_tree_layout(ys_scene* s, int layout) {
     if (s->packed) return fail(YS_ERR_STATE, "ys_scene_set_tree_layout: call before ys_scene_pack");
     if (layout != YS_TREE_REFERENCE && layout != YS_TREE_CUBE) return fail(YS_ERR_BAD_ARG, "unknown tree layout");
     s->tree_layout = layout;
+    return YS_OK;
+}
+
+ys_status ys_scene_set_fused_variant(ys_scene* s, int min_blocks) {
+    if (!s) return fail(YS_ERR_BAD_ARG, "null scene");
+    if (min_blocks != 8 && min_blocks != 6 && min_blocks != 4)
+        return fail(YS_ERR_BAD_ARG, "fused variant: CTAs per SM must be 8, 6 or 4");
+    s->fused_min_blocks = min_blocks;
+    drop_graphs(s);
+    return YS_OK;
+}
+
+// Time every k_fused variant on the current state (the kernel only writes the
+// next-state buffers, which the next substep overwrites; the running totals
+// are restored) and keep the fastest.  The scene does not advance.
+ys_status ys_scene_autotune(ys_scene* s, uint32_t reps, int* chosen, float* ms_out) {
+    ys_status r = check_scene(s);
+    if (r) return r;
+    if (reps == 0) reps = 5;
+    cudaStream_t st = s->stream;
+    const bool rec = s->record;
+    s->record = false;
+    r = refit(s);  // trees of the current positions
+    if (r) { s->record = rec; return r; }
+    unsigned long long saved[8];
+    YS_CK(cudaMemcpyAsync(saved, s->counters.p, sizeof(saved), cudaMemcpyDeviceToHost, st));
+    YS_CK(cudaStreamSynchronize(st));
+    cudaEvent_t e0, e1;
+    YS_CK(cudaEventCreate(&e0));
+    YS_CK(cudaEventCreate(&e1));
+    const StepArgs A = make_args(s);
+    float best = 1e30f;
+    int bestV = s->fused_min_blocks;
+    for (int i = 0; i < 3; ++i) {
+        const int v = FUSED_VARIANTS[i];
+        launch_fused(A, s->nV, st, v);  // warm-up
+        float t = 0.f;
+        for (u32 k = 0; k < reps; ++k) {
+            cudaEventRecord(e0, st);
+            launch_fused(A, s->nV, st, v);
+            cudaEventRecord(e1, st);
+            cudaEventSynchronize(e1);
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, e0, e1);
+            t += ms;
+        }
+        t /= (float)reps;
+        if (ms_out) ms_out[i] = t;
+        if (t < best) { best = t; bestV = v; }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    YS_CK(cudaGetLastError());
+    YS_CK(cudaMemcpyAsync(s->counters.p, saved, sizeof(saved), cudaMemcpyHostToDevice, st));
+    YS_CK(cudaStreamSynchronize(st));
+    s->record = rec;
+    s->fused_min_blocks = bestV;
+    drop_graphs(s);
+    if (chosen) *chosen = bestV;
     return YS_OK;
 }
 

@@ -98,6 +98,17 @@ class Scene:
         if pack:
             self.pack()
 
+    def autotune(self, reps: int = 5):
+        """Pick the fused kernel's register cap by timing each variant on the
+        current state (the scene does not advance); returns (chosen, ms[3])."""
+        chosen = C.c_int()
+        ms = (C.c_float * 3)()
+        _lib.check(self.lib.ys_scene_autotune(self.h, reps, C.byref(chosen), ms), "ys_scene_autotune")
+        return chosen.value, list(ms)
+
+    def set_fused_variant(self, min_blocks: int):
+        _lib.check(self.lib.ys_scene_set_fused_variant(self.h, min_blocks), "ys_scene_set_fused_variant")
+
     def pack(self):
         _lib.check(self.lib.ys_scene_pack(self.h), "ys_scene_pack")
 
