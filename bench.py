@@ -221,7 +221,13 @@ def cpu_baseline(spec, state, nsub, threads=None):
     t0 = time.perf_counter()
     o.step(nsub)
     dt = time.perf_counter() - t0
-    return nsub / dt, cores, dt, kind
+    # one more substep on a single host thread (the reference's CPU style)
+    O.set_threads(1)
+    t1 = time.perf_counter()
+    o.step(1)
+    dt1 = time.perf_counter() - t1
+    O.set_threads(cores)
+    return nsub / dt, cores, dt, kind, 1.0 / dt1
 
 
 def reference_scene(spec):
@@ -379,12 +385,13 @@ def run_ours(args, rank, world, local):
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
         state = {"x": scene.get("x"), "v": scene.get("v"), "xprev": scene.get("xprev")}
-        v_cpu, cores, dt, kind = cpu_baseline(spec, state, args.cpu_substeps)
-        cpu = {"value": v_cpu, "unit": UNIT, "cores": cores, "kind": kind,
+        v_cpu, cores, dt, kind, v_one = cpu_baseline(spec, state, args.cpu_substeps)
+        cpu = {"value": v_cpu, "unit": UNIT, "cores": cores, "kind": kind, "single_thread_value": v_one,
                "sample": f"{args.cpu_substeps} substeps of the full workload from the GPU run's state "
                          f"({dt:.1f} s on {cores} threads; "
                          + ("reference Metal kernels compiled for the host + pinned CPU-hash restatement)"
-                            if kind == "reference" else "CPU restatement)")}
+                            if kind == "reference" else "CPU restatement)")
+                         + "; single_thread_value: one more substep on one host thread"}
 
     batched = None if args.no_batched else measure_batched(args, rank, world, local)
     adjoint = None if (args.no_adjoint or rank != 0) else measure_adjoint(args, local)
