@@ -428,8 +428,8 @@ def run_ours(args, rank, world, local):
 
 # ------------------------------------------------------------------ batched
 def measure_batched(args, rank, world, local, steps=100):
-    """Batched vs plain (C4): the instances of this rank's shard (instance i
-    on rank i mod N) as ONE scene -- one refit and one fused launch per
+    """Batched vs plain (C4): the instances of this rank's shard (balanced by
+    vertex count, generators.shard_instances) as ONE scene -- one refit and one fused launch per
     substep for all of them, replayed as a CUDA graph -- against the same
     instances as one scene each, stepped one after the other from the host.
     Batched is device-timed (CUDA events on its stream); plain is timed by the
@@ -441,8 +441,7 @@ def measure_batched(args, rank, world, local, steps=100):
     from ysim_b200 import generators as G
     from ysim_b200.scene import Scene
     full = G.config_c4(instances=args.instances)
-    mine = [m for m in full.meshes if m.group % world == rank]
-    spec = G.SceneSpec(full.name, full.params, mine, full.seed)
+    spec = G.shard_instances(full, rank, world)
     parts = G.split_instances(spec)
     scene = Scene(spec, device=local)
     stream = torch.cuda.ExternalStream(scene.stream(), device=local)
@@ -483,7 +482,8 @@ def measure_batched(args, rank, world, local, steps=100):
         q.close()
     nverts = sum(m.nV for m in full.meshes)
     return {"workload": f"{args.instances} FastGridCloth instances, side U{{16..256}} (seeded), each over its own "
-                        f"level-4 icosphere; subh 1/6000; instances sharded over {world} GPU(s)",
+                        f"level-4 icosphere; subh 1/6000; instances sharded over {world} GPU(s), balanced by "
+                        f"vertex count",
             "instances": args.instances, "vertices": nverts,
             "cloth_vertices": sum(m.nV for m in full.meshes if m.grid_n), "value": 1000.0 / b_ms,
             "unit": "batch substeps/s", "ms_per_substep": b_ms,

@@ -289,6 +289,25 @@ def split_instances(spec: SceneSpec) -> List[SceneSpec]:
     return [SceneSpec(f"{spec.name}_inst{g}", spec.params, ms, spec.seed) for g, ms in sorted(groups.items())]
 
 
+def shard_instances(spec: SceneSpec, rank: int, world: int) -> SceneSpec:
+    """The instances (groups) of a batched scene that rank `rank` of `world`
+    runs: largest first, each to the rank with the fewest vertices so far
+    (ties to the lower rank), so every rank gets a similar vertex count
+    whatever the mix of sizes.  Groups keep their ids; meshes keep their
+    order."""
+    sizes = {}
+    for m in spec.meshes:
+        sizes[m.group] = sizes.get(m.group, 0) + m.nV
+    load = [0] * world
+    owner = {}
+    for g in sorted(sizes, key=lambda g: (-sizes[g], g)):
+        r = min(range(world), key=lambda k: (load[k], k))
+        owner[g] = r
+        load[r] += sizes[g]
+    mine = [m for m in spec.meshes if owner[m.group] == rank]
+    return SceneSpec(f"{spec.name}_shard{rank}of{world}", spec.params, mine, spec.seed)
+
+
 # ---------------------------------------------------------------- adjoint
 def grid_spring_params(N: int, rest6, k3):
     """Per-spring stiffness and rest length of a FastGridCloth in the canonical
