@@ -48,6 +48,30 @@ typedef int ys_status;
 #define YS_MESH_COLLIDABLE 2u
 #define YS_MESH_SELF_COLLIDE 4u
 
+/* ColliderKind (include/sim/collision_pod.hpp; YSIM_COLLIDER_*,
+ * src/metal/common_types.metalh:80-84). */
+#define YS_COLLIDER_MESH 0u
+#define YS_COLLIDER_SPHERE 1u
+#define YS_COLLIDER_BOX 2u
+#define YS_COLLIDER_CYLINDER 3u
+#define YS_COLLIDER_PLANE 4u
+
+/* AnalyticShape (include/sim/collision_pod.hpp:295-309; mirror in
+ * src/metal/common_types.metalh:42-52), 96 bytes: world centre and radius
+ * (sphere radius, cylinder radius), half extents (box half extents, ellipsoid
+ * semi-axes) and cylinder half height, orientation (w, x, y, z) local to
+ * world, centre and orientation at the start of the step, collider kind,
+ * owning mesh index, behaviour, flags (bit 0: collidable).  Local frame: a
+ * plane is the half-space y <= 0, a cylinder's axis is +y. */
+typedef struct ys_analytic_shape {
+    float center_radius[4];
+    float half_ext_height[4];
+    float rot_quat[4];
+    float prev_center[4];
+    float prev_rot_quat[4];
+    uint32_t kind, obj_index, behavior, flags;
+} ys_analytic_shape;
+
 /* Self-collision row source: off, the reference default CPU-spatial-hash
  * semantics (Simulator::useCpuShSelf, simulator.hpp:93; CpuSpatialHash
  * spatial_hash.hpp:1946-1989) or BVH self queries (checkSelfCollisions,
@@ -160,6 +184,26 @@ ys_status ys_scene_set_fused_variant(ys_scene* s, int min_blocks);
  * reports it (*chosen) and the mean milliseconds per variant (ms_out[3], in
  * the order 8, 6, 4; may be null).  No counterpart in the reference. */
 ys_status ys_scene_autotune(ys_scene* s, uint32_t reps, int* chosen, float* ms_out);
+/* Analytic collider (GeneralMesh::colliderKind and transform): kind
+ * YS_COLLIDER_SPHERE / BOX / CYLINDER / PLANE (YS_COLLIDER_MESH: triangles,
+ * the default), centre, local half extents (sphere: semi-axes; box: half
+ * extents; cylinder: radius max(h[0], h[2]), half height h[1]; plane: unused,
+ * may be NULL) and orientation (w, x, y, z).  Before ys_scene_pack it makes
+ * the mesh an analytic collider: its triangles are neither queried nor refit,
+ * and the vertices of each cloth whose root box meets the collider's box at
+ * this substep's detect or the one before are tested against the shape
+ * (BroadPhase::detectCollisions markers, bvh.hpp:2886-2941;
+ * PackedCollisionData::endAnalyticPairs, scene.hpp:485-530;
+ * BruteForce::narrowAnalytic, bruteforce.hpp:245-309), contacts keyed
+ * (collider mesh, 0).  After pack it moves the collider: the pose is read at
+ * the next frame start, where the previous pose becomes the start of the
+ * swept test (Scene::refreshAnalyticShapes, scene.hpp:659-745).  The kind
+ * cannot change after pack; a cloth mesh cannot be an analytic collider. */
+ys_status ys_scene_set_collider(ys_scene* s, int mesh, uint32_t kind, const float center[3], const float half[3],
+                                const float rot_wxyz[4]);
+/* The scene's analytic shape table as of the last frame start (compact, in
+ * mesh order): *num_out entries, min(cap, *num_out) copied to out. */
+ys_status ys_scene_colliders(ys_scene* s, ys_analytic_shape* out, uint32_t cap, uint32_t* num_out);
 /* Tree layout (YS_TREE_REFERENCE / YS_TREE_CUBE) for every tree the scene
  * builds; call between ys_scene_create and ys_scene_pack.  Replaces the
  * Morton normalisation inside BVH<..>::build (include/sim/bvh.hpp:1194-1301). */
@@ -294,6 +338,27 @@ ys_status ys_shash_query(ys_shash* h, const float* d_qx, uint32_t num_queries, f
                          uint64_t cap, unsigned long long* d_count);
 /* Cell entries of the last build and triangles too large for the grid. */
 ys_status ys_shash_entries(ys_shash* h, uint32_t* n_entries, uint32_t* n_oversized);
+
+/* ---- Analytic narrow phase (BruteForce::narrowAnalytic,
+ * include/sim/bruteforce.hpp:245-309; narrow_pt_analytic,
+ * src/metal/bruteforce.metal:236-499): for each (cloth mesh, collider mesh)
+ * pair, every vertex of the cloth against the collider's shape, the segment
+ * x_prev -> x mapped into the shape's frame through its previous and current
+ * pose.  A contact is appended in NarrowCollision layout (48 B: (vertex, 0),
+ * (cloth, collider), normal and the signed distance of x, behaviours,
+ * (YS_COLLIDER_MESH, kind)) when the distance is below radius + thickness +
+ * the pair's rotation margin.  Host arrays: state_off (num_meshes + 1
+ * vertex offsets), behaviors (num_meshes), shapes (num_shapes), pairs
+ * (num_pairs x 2: cloth mesh index, collider mesh index, resolved to the
+ * shape whose obj_index matches; pairs without one, or whose shape is not
+ * collidable, are skipped).  Device arrays: d_x, d_xprev (packed xyz of all
+ * meshes), d_out, d_count.  *d_count is incremented, not reset (the triangle
+ * narrow phase fills the same buffer first); contacts beyond cap are counted,
+ * not written.  Asynchronous on stream; allocates nothing. */
+ys_status ys_narrow_analytic(const float* d_x, const float* d_xprev, const uint32_t* state_off,
+                             const uint32_t* behaviors, uint32_t num_meshes, const ys_analytic_shape* shapes,
+                             uint32_t num_shapes, const uint32_t* pairs, uint32_t num_pairs, float radius,
+                             float thickness, void* d_out, uint64_t cap, unsigned long long* d_count, void* stream);
 
 /* Standalone primitives used by the build. */
 ys_status ys_morton_codes(const float* d_x, uint32_t num_vertices, const uint32_t* d_facets, uint32_t num_facets,

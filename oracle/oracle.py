@@ -15,6 +15,8 @@ from .build_oracle import OUT, build
 NODE_DTYPE = np.dtype([("mn", "<f4", 3), ("a", "<i4"), ("mx", "<f4", 3), ("b", "<i4")])
 ROW_DTYPE = np.dtype([("point", "<u4"), ("tri", "<u4"), ("qobj", "<u4"), ("tobj", "<u4"), ("qbeh", "<u4"),
                       ("tbeh", "<u4"), ("qshape", "<u4"), ("tshape", "<u4")])
+SHAPE_DTYPE = np.dtype([("cr", "<f4", 4), ("he", "<f4", 4), ("rq", "<f4", 4), ("pc", "<f4", 4), ("prq", "<f4", 4),
+                        ("kind", "<u4"), ("obj", "<u4"), ("beh", "<u4"), ("flags", "<u4")])
 CONTACT_DTYPE = np.dtype([("point", "<u4"), ("tri", "<u4"), ("qobj", "<u4"), ("tobj", "<u4"), ("n", "<f4", 3),
                           ("d", "<f4"), ("qbeh", "<u4"), ("tbeh", "<u4"), ("qshape", "<u4"), ("tshape", "<u4")])
 
@@ -64,6 +66,13 @@ def lib():
             "yso_scene_contacts": (None, [vp, vp, vp]),
             "yso_scene_tree_nodes": (C.c_uint64, [vp, C.c_int]),
             "yso_scene_tree": (None, [vp, C.c_int, vp, vp, vp, vp]),
+            "yso_scene_set_collider": (C.c_int, [vp, C.c_int, C.c_uint32, vp, vp, vp]),
+            "yso_scene_shapes": (C.c_uint64, [vp, vp]),
+            "yso_analytic_one": (C.c_int, [vp, vp, vp, C.c_float, C.c_float, C.c_float, vp, vp]),
+            "yso_rot_margin": (C.c_float, [vp, C.c_float, C.c_float]),
+            "yso_broad_box": (C.c_int, [vp, C.c_float, vp]),
+            "yso_narrow_analytic": (C.c_uint64, [vp, vp, vp, vp, C.c_uint32, vp, C.c_uint32, vp, C.c_uint32,
+                                                 C.c_float, C.c_float, vp, C.c_uint64]),
             "yso_sh_face_face": (C.c_uint64, [vp, vp, vp, vp, vp, vp, C.c_uint32, C.c_float, C.c_int, vp,
                                               C.c_uint64, vp]),
         }
@@ -207,6 +216,44 @@ def adjacency(x, F):
     return out
 
 
+def analytic_one(shape, pcur, pprev, radius, thickness, rot_margin=0.0):
+    """narrow_pt_analytic for one vertex: (hit, normal, d)."""
+    sh = np.ascontiguousarray(shape, SHAPE_DTYPE).reshape(1)
+    n = np.zeros(3, np.float32)
+    d = np.zeros(1, np.float32)
+    hit = lib().yso_analytic_one(P(sh), P(np.asarray(pcur, np.float32)), P(np.asarray(pprev, np.float32)),
+                                 radius, thickness, rot_margin, P(n), P(d))
+    return bool(hit), n, float(d[0])
+
+
+def rot_margin(shape, radius, thickness) -> float:
+    sh = np.ascontiguousarray(shape, SHAPE_DTYPE).reshape(1)
+    return float(lib().yso_rot_margin(P(sh), radius, thickness))
+
+
+def broad_box(shape, inflate):
+    sh = np.ascontiguousarray(shape, SHAPE_DTYPE).reshape(1)
+    out = np.zeros(6, np.float32)
+    fin = lib().yso_broad_box(P(sh), inflate, P(out))
+    return bool(fin), out
+
+
+def narrow_analytic(x, xp, state_off, beh, shapes, pairs, radius, thickness, cap=None):
+    """narrowAnalytic over explicit (cloth, collider) pairs: contacts in
+    pair-then-vertex order and the total count."""
+    x = np.ascontiguousarray(x, np.float32)
+    xp = np.ascontiguousarray(xp, np.float32)
+    so = np.ascontiguousarray(state_off, np.uint32)
+    be = np.ascontiguousarray(beh, np.uint32)
+    sh = np.ascontiguousarray(shapes, SHAPE_DTYPE)
+    pr = np.ascontiguousarray(pairs, np.uint32).reshape(-1, 2)
+    cap = len(x) * max(len(pr), 1) if cap is None else cap
+    out = np.zeros(max(cap, 1), CONTACT_DTYPE)
+    n = lib().yso_narrow_analytic(P(x), P(xp), P(so), P(be), len(be), P(sh), len(sh), P(pr), len(pr), radius,
+                                  thickness, P(out), cap)
+    return out[: min(n, cap)], int(n)
+
+
 class OracleScene:
     """CPU restatement of the packed scene + Simulator::update substeps."""
 
@@ -225,8 +272,10 @@ class OracleScene:
             F = np.ascontiguousarray(m.facets, np.uint32)
             kp = np.array([m.kstretch, m.kshear, m.kbend, m.thickness], np.float32)
             rest = np.array(m.grid_rest, np.float32)
-            lib().yso_scene_add_mesh(self.h, m.behavior, m.flags, m.nV, P(x), P(v), P(mass), P(mask), m.nF, P(F),
-                                     P(kp), m.grid_n, P(rest))
+            idx = lib().yso_scene_add_mesh(self.h, m.behavior, m.flags, m.nV, P(x), P(v), P(mass), P(mask), m.nF,
+                                           P(F), P(kp), m.grid_n, P(rest))
+            if getattr(m, "collider", None) is not None:
+                self.set_collider(idx, *m.collider)
         lib().yso_scene_pack(self.h)
         self.nV = spec.nV
 
@@ -237,6 +286,19 @@ class OracleScene:
 
     def step(self, n=1):
         lib().yso_scene_step(self.h, n)
+
+    def set_collider(self, mesh, kind, center, half=(0.0, 0.0, 0.0), q=(1.0, 0.0, 0.0, 0.0)):
+        c = np.array(center, np.float32)
+        h = np.array(half, np.float32)
+        r = np.array(q, np.float32)
+        if lib().yso_scene_set_collider(self.h, mesh, kind, P(c), P(h), P(r)) != 0:
+            raise ValueError("yso_scene_set_collider rejected the collider")
+
+    def shapes(self):
+        n = lib().yso_scene_shapes(self.h, None)
+        out = np.zeros(n, SHAPE_DTYPE)
+        lib().yso_scene_shapes(self.h, P(out))
+        return out
 
     def stage(self, which: int):
         lib().yso_scene_stage(self.h, which)

@@ -133,6 +133,24 @@ uint32_t yref_narrow(const void* rows, uint32_t nrows, const float* x, const uin
     return count.v.load();
 }
 
+static_assert(sizeof(AnalyticShape) == 96, "AnalyticShape");
+
+// narrow_pt_analytic for every vertex of cloth mesh `oid` against
+// shapes[shape_index], one thread at a time (appends in vertex order).
+uint32_t yref_narrow_analytic(const float* x, const float* xprev, const uint32_t* voff, const void* shapes,
+                              uint32_t oid, uint32_t nverts, uint32_t shape_index, uint32_t cloth_beh, float radius,
+                              float thickness, float rot_margin, void* out, uint32_t cap) {
+    AnalyticNarrowParams p;
+    std::memset(&p, 0, sizeof(p));
+    p.oid = oid; p.numVerts = nverts; p.shapeIndex = shape_index; p.maxNumCollisions = cap;
+    p.clothBehavior = cloth_beh; p.radius = radius; p.thickness = thickness; p.rotMargin = rot_margin;
+    atomic_uint count; count.v.store(0);
+    for (uint i = 0; i < nverts; ++i)
+        narrow_pt_analytic(&count, (NarrowCollision*)out, (const packed_float3*)x, voff, (const AnalyticShape*)shapes,
+                           p, (const packed_float3*)xprev, i);
+    return count.v.load();
+}
+
 }  // extern "C"
 
 #elif defined(YS_REF_PHYSICS)

@@ -42,6 +42,7 @@ def lib():
             "yref_integrate_grid": (None, [vp, vp, vp, vp, vp, vp, vp, vp, u32, f32, vp, u32, vp]),
             "yref_bucket": (None, [vp, u32, vp, u32, vp, vp, vp]),
             "yref_sh_detect": (u32, [vp, vp, vp, vp, vp, vp, u32, f32, u32, vp, u32, vp]),
+            "yref_narrow_analytic": (u32, [vp, vp, vp, vp, u32, u32, u32, u32, f32, f32, f32, vp, u32]),
         }
         for k, (r, a) in sig.items():
             fn = getattr(L, k)
@@ -109,6 +110,18 @@ def narrow(rows, x, voff, F, foff, vaf, vaf_off, radius, thickness, xprev, cap=N
     n = lib().yref_narrow(P(np.ascontiguousarray(rows)), len(rows), P(c32(x)), P(c32(voff, np.uint32)),
                           P(c32(F, np.uint32)), P(c32(foff, np.uint32)), P(c32(vaf, np.uint32)),
                           P(c32(vaf_off, np.uint32)), radius, thickness, P(c32(xprev)), P(out), cap)
+    return out[: min(n, cap)]
+
+
+def narrow_analytic(x, xprev, voff, shapes, oid, shape_index, cloth_beh, radius, thickness, rot_margin, cap=None):
+    """narrow_pt_analytic over every vertex of cloth mesh oid against
+    shapes[shape_index] (SHAPE_DTYPE records)."""
+    voff = c32(voff, np.uint32)
+    nv = int(voff[oid + 1] - voff[oid])
+    cap = cap or max(64, nv)
+    out = np.zeros(cap, CONTACT_DTYPE)
+    n = lib().yref_narrow_analytic(P(c32(x)), P(c32(xprev)), P(voff), P(np.ascontiguousarray(shapes)), oid, nv,
+                                   shape_index, cloth_beh, radius, thickness, rot_margin, P(out), cap)
     return out[: min(n, cap)]
 
 

@@ -25,6 +25,7 @@
 //     triangle) order; the reference's GPU bucketing order is nondeterministic
 //     (physics.metal:596-599).
 #include <algorithm>
+#include <algorithm>
 #include <atomic>
 #include <cmath>
 #include <cstdint>
@@ -577,6 +578,247 @@ inline bool narrow_one(V3 qcur, V3 qprev, V3 t0, V3 t1, V3 t2, float band, float
     return true;
 }
 
+// ---------------------------------------------------------------- analytic
+// AnalyticShape (collision_pod.hpp:295-309): centerRadius, halfExtHeight,
+// rotQuat (w,x,y,z), prevCenterPad, prevRotQuat, kind, objIndex,
+// behaviorType, flags.  ColliderKind: 0 Mesh, 1 Sphere, 2 Box, 3 Cylinder,
+// 4 Plane.
+struct Shape {
+    float cr[4], he[4], rq[4], pc[4], prq[4];
+    u32 kind, obj, beh, flags;
+};
+static_assert(sizeof(Shape) == 96, "shape");
+enum Collider : u32 { CMesh = 0, CSphere = 1, CBox = 2, CCyl = 3, CPlane = 4 };
+
+inline float fmn(float a, float b) { return std::fmin(a, b); }
+inline float fmx(float a, float b) { return std::fmax(a, b); }
+inline float len(V3 a) { return std::sqrt(dot(a, a)); }
+inline V3 unit(V3 a) { return a * (1.0f / std::sqrt(dot(a, a))); }
+inline V3 hadamard(V3 a, V3 b) { return v3(a.x * b.x, a.y * b.y, a.z * b.z); }
+inline float axis_of(V3 a, int k) { return k == 0 ? a.x : (k == 1 ? a.y : a.z); }
+// quatRotate (bruteforce.metal:196-201): v + 2 * cross(qv, cross(qv, v) + qw * v).
+inline V3 qrot(float qw, V3 qv, V3 v) { return v + 2.0f * cross(qv, cross(qv, v) + qw * v); }
+// boxDominantAxis (bruteforce.metal:203-216).
+inline void dominant_axis(V3 q, V3 h, int& k, float& sg) {
+    V3 gap = v3(std::fabs(q.x) - h.x, std::fabs(q.y) - h.y, std::fabs(q.z) - h.z);
+    k = 0;
+    float best = gap.x;
+    if (gap.y > best) { best = gap.y; k = 1; }
+    if (gap.z > best) { best = gap.z; k = 2; }
+    sg = axis_of(q, k) >= 0.0f ? 1.0f : -1.0f;
+}
+
+// narrow_pt_analytic (bruteforce.metal:259-499) for one vertex; band =
+// radius + thickness + rotMargin.  Returns true with the world normal and
+// signed distance when the vertex is in contact.
+bool analytic_one(const Shape& sh, V3 pcur, V3 pprev, float radius, float thickness, float rot_margin,
+                  float n_out[3], float* d_out) {
+    if ((sh.flags & 1u) == 0u || sh.kind == CMesh) return false;
+    V3 a = qrot(sh.prq[0], -v3(sh.prq[1], sh.prq[2], sh.prq[3]), pprev - v3(sh.pc[0], sh.pc[1], sh.pc[2]));
+    V3 b = qrot(sh.rq[0], -v3(sh.rq[1], sh.rq[2], sh.rq[3]), pcur - v3(sh.cr[0], sh.cr[1], sh.cr[2]));
+    V3 seg = b - a;
+    const float band = radius + thickness + rot_margin;
+    V3 nl = v3(0.0f, 1.0f, 0.0f);
+    float d = 1e30f;
+    switch (sh.kind) {
+    case CPlane:
+        d = b.y;
+        break;
+    case CSphere: {
+        V3 e = v3(fmx(sh.he[0], 1e-8f), fmx(sh.he[1], 1e-8f), fmx(sh.he[2], 1e-8f));
+        float R = 1.0f + band / fmn(e.x, fmn(e.y, e.z));
+        V3 A = a / e, B = b / e;
+        float lenA = len(A);
+        V3 u;
+        bool got = false;
+        if (lenA < 1.0f) {
+            u = (lenA > 1e-6f) ? A : ((len(B) > 1e-6f) ? B : v3(0.0f, 1.0f, 0.0f));
+            got = true;
+        } else {
+            V3 D = B - A;
+            float qa = dot(D, D), qb = dot(A, D), qc = dot(A, A) - R * R, t = -1.0f;
+            if (qa > 1e-20f) {
+                float disc = qb * qb - qa * qc;
+                if (disc >= 0.0f) {
+                    float t0 = (-qb - std::sqrt(disc)) / qa;
+                    if (t0 >= 0.0f && t0 <= 1.0f) t = t0;
+                }
+            }
+            if (t >= 0.0f) { u = A + t * D; got = true; }
+            else if (len(B) > 1e-6f) { u = B; got = true; }
+        }
+        if (!got) return false;
+        V3 uh = unit(u);
+        V3 sp = hadamard(e, uh);
+        nl = unit(uh / e);
+        d = dot(nl, b - sp);
+        break;
+    }
+    case CBox: {
+        V3 h = v3(fmx(sh.he[0], 1e-8f), fmx(sh.he[1], 1e-8f), fmx(sh.he[2], 1e-8f));
+        V3 H = v3(h.x + band, h.y + band, h.z + band);
+        int k = 0;
+        float sg = 1.0f;
+        if (std::fabs(a.x) < h.x && std::fabs(a.y) < h.y && std::fabs(a.z) < h.z) {
+            dominant_axis(a, h, k, sg);
+        } else {
+            float tE = 0.0f, tX = 1.0f, esg = 1.0f;
+            int ek = -1;
+            bool miss = false;
+            for (int i = 0; i < 3 && !miss; ++i) {
+                float di = axis_of(seg, i), ai = axis_of(a, i), Hi = axis_of(H, i);
+                if (std::fabs(di) < 1e-12f) {
+                    if (std::fabs(ai) > Hi) miss = true;
+                    continue;
+                }
+                float inv = 1.0f / di;
+                float t1 = (-Hi - ai) * inv, t2 = (Hi - ai) * inv;
+                float tn = fmn(t1, t2), tf = fmx(t1, t2);
+                if (tn > tE) { tE = tn; ek = i; esg = (di > 0.0f) ? -1.0f : 1.0f; }
+                tX = fmn(tX, tf);
+            }
+            if (!miss && ek >= 0 && tE <= tX && tE <= 1.0f) { k = ek; sg = esg; }
+            else dominant_axis(b, h, k, sg);
+        }
+        nl = v3(k == 0 ? sg : 0.0f, k == 1 ? sg : 0.0f, k == 2 ? sg : 0.0f);
+        d = sg * axis_of(b, k) - axis_of(h, k);
+        break;
+    }
+    case CCyl: {
+        float r = fmx(sh.cr[3], 1e-8f), hh = fmx(sh.he[3], 1e-8f);
+        float R = r + band, HH = hh + band;
+        int feat = 0;
+        float capSg = 1.0f, nx = 1.0f, nz = 0.0f;
+        bool aIn = (std::sqrt(a.x * a.x + a.z * a.z) < r) && (std::fabs(a.y) < hh);
+        bool resolved = false;
+        if (!aIn) {
+            float tE = 0.0f, tX = 1.0f, ecap = 1.0f, ex = 1.0f, ez = 0.0f;
+            int ef = -1;
+            bool miss = false;
+            float qa = seg.x * seg.x + seg.z * seg.z;
+            float qb = a.x * seg.x + a.z * seg.z;
+            float qc = (a.x * a.x + a.z * a.z) - R * R;
+            if (qa > 1e-20f) {
+                float disc = qb * qb - qa * qc;
+                if (disc < 0.0f) miss = true;
+                else {
+                    float sq = std::sqrt(disc);
+                    float t1 = (-qb - sq) / qa, t2 = (-qb + sq) / qa;
+                    if (t1 > tE) { tE = t1; ef = 0; }
+                    tX = fmn(tX, t2);
+                }
+            } else if (qc > 0.0f) {
+                miss = true;
+            }
+            if (!miss) {
+                if (std::fabs(seg.y) < 1e-12f) {
+                    if (std::fabs(a.y) > HH) miss = true;
+                } else {
+                    float inv = 1.0f / seg.y;
+                    float t1 = (-HH - a.y) * inv, t2 = (HH - a.y) * inv;
+                    float tn = fmn(t1, t2), tf = fmx(t1, t2);
+                    if (tn > tE) { tE = tn; ef = 1; ecap = (seg.y > 0.0f) ? -1.0f : 1.0f; }
+                    tX = fmn(tX, tf);
+                }
+            }
+            if (!miss && ef >= 0 && tE <= tX && tE <= 1.0f) {
+                if (ef == 0) {
+                    float hx = a.x + tE * seg.x, hz = a.z + tE * seg.z;
+                    float l = std::sqrt(hx * hx + hz * hz);
+                    if (l > 1e-9f) { ex = hx / l; ez = hz / l; }
+                }
+                feat = ef; capSg = ecap; nx = ex; nz = ez; resolved = true;
+            }
+        }
+        if (!resolved) {
+            V3 q = aIn ? a : b;
+            float lxz = std::sqrt(q.x * q.x + q.z * q.z);
+            feat = ((r - lxz) <= (hh - std::fabs(q.y))) ? 0 : 1;
+            capSg = (q.y >= 0.0f) ? 1.0f : -1.0f;
+            if (lxz > 1e-9f) { nx = q.x / lxz; nz = q.z / lxz; } else { nx = 1.0f; nz = 0.0f; }
+        }
+        if (feat == 0) { nl = v3(nx, 0.0f, nz); d = dot(nl, b) - r; }
+        else { nl = v3(0.0f, capSg, 0.0f); d = capSg * b.y - hh; }
+        break;
+    }
+    default:
+        return false;
+    }
+    if (!(d < band)) return false;
+    V3 n = unit(qrot(sh.rq[0], v3(sh.rq[1], sh.rq[2], sh.rq[3]), nl));
+    n_out[0] = n.x; n_out[1] = n.y; n_out[2] = n.z;
+    *d_out = d;
+    return true;
+}
+
+// Quat operator* and rotateVector (material_quat.hpp:27-63).
+struct Q4 { float w, x, y, z; };
+inline Q4 qmul(const Q4& a, const Q4& b) {
+    return Q4{a.w * b.w - a.x * b.x - a.y * b.y - a.z * b.z, a.w * b.x + a.x * b.w + a.y * b.z - a.z * b.y,
+              a.w * b.y - a.x * b.z + a.y * b.w + a.z * b.x, a.w * b.z + a.x * b.y - a.y * b.x + a.z * b.w};
+}
+inline V3 qapply(const Q4& q, V3 v) {
+    Q4 r = qmul(qmul(q, Q4{0.0f, v.x, v.y, v.z}), Q4{q.w, -q.x, -q.y, -q.z});
+    return v3(r.x, r.y, r.z);
+}
+// analyticWorldHalf (bvh.hpp:2431-2462).
+V3 world_half(const Shape& s, const float* q) {
+    V3 h = v3(0.0f, 0.0f, 0.0f);
+    if (s.kind == CSphere) {
+        float r = std::max(std::max(s.he[0], s.he[1]), s.he[2]);
+        return v3(r, r, r);
+    }
+    if (s.kind == CBox) h = v3(s.he[0], s.he[1], s.he[2]);
+    else if (s.kind == CCyl) h = v3(s.cr[3], s.he[3], s.cr[3]);
+    else return h;
+    Q4 Q{q[0], q[1], q[2], q[3]};
+    V3 cx = qapply(Q, v3(1.0f, 0.0f, 0.0f)), cy = qapply(Q, v3(0.0f, 1.0f, 0.0f)), cz = qapply(Q, v3(0.0f, 0.0f, 1.0f));
+    return v3(std::fabs(cx.x) * h.x + std::fabs(cy.x) * h.y + std::fabs(cz.x) * h.z,
+              std::fabs(cx.y) * h.x + std::fabs(cy.y) * h.y + std::fabs(cz.y) * h.z,
+              std::fabs(cx.z) * h.x + std::fabs(cy.z) * h.y + std::fabs(cz.z) * h.z);
+}
+inline double quat_angle(const Shape& s) {
+    double dq = (double)s.rq[0] * s.prq[0] + (double)s.rq[1] * s.prq[1] + (double)s.rq[2] * s.prq[2] +
+                (double)s.rq[3] * s.prq[3];
+    dq = std::fabs(dq);
+    if (dq > 1.0) dq = 1.0;
+    return 2.0 * std::acos(dq);
+}
+// analyticRotBand (bvh.hpp:2465-2479).
+float rot_band(const Shape& s) {
+    double th = quat_angle(s);
+    if (th <= 0.0) return 0.0f;
+    double rmax = std::sqrt((double)s.he[0] * s.he[0] + (double)s.he[1] * s.he[1] + (double)s.he[2] * s.he[2]) +
+                  (double)s.cr[3];
+    return (float)(th * rmax);
+}
+// analyticRotMargin (bruteforce.hpp:201-240).
+float rot_margin(const Shape& s, float radius, float thickness) {
+    double th = quat_angle(s);
+    if (!(th > 1e-9)) return 0.0f;
+    double rmax = 0.0;
+    switch (s.kind) {
+    case CSphere: rmax = std::max({(double)s.he[0], (double)s.he[1], (double)s.he[2]}); break;
+    case CBox: rmax = std::sqrt((double)s.he[0] * s.he[0] + (double)s.he[1] * s.he[1] + (double)s.he[2] * s.he[2]); break;
+    case CCyl: rmax = std::sqrt((double)s.cr[3] * s.cr[3] + (double)s.he[3] * s.he[3]); break;
+    case CPlane: return 0.0f;
+    default: break;
+    }
+    return (float)(th * (rmax + (double)radius + (double)thickness));
+}
+// objectBroadAABB for an analytic collider (bvh.hpp:2494-2516); false = a
+// half-space, which overlaps everything.
+bool broad_box(const Shape& s, float inflate, Node& out) {
+    V3 c = v3(s.cr[0], s.cr[1], s.cr[2]);
+    if (s.kind == CPlane) { nset(out, c, c); return false; }
+    V3 p = v3(s.pc[0], s.pc[1], s.pc[2]);
+    V3 hc = world_half(s, s.rq), hp = world_half(s, s.prq);
+    float pad = inflate + rot_band(s);
+    V3 pv = v3(pad, pad, pad);
+    nset(out, vmin(c - hc, p - hp) - pv, vmax(c + hc, p + hp) + pv);
+    return true;
+}
+
 // ---------------------------------------------------------------- F / I
 // calc_spring (physics.metal:146-153).
 inline V3 spring(V3 p0, V3 v0, V3 p1, V3 v1, float rest, float ks, float kd) {
@@ -679,6 +921,10 @@ struct Mesh {
     bool built = false;
     std::vector<Node> tree; std::vector<i32> parent;
     std::vector<u32> codes, idx;
+    // colliderKind and the collider's pose (centre, local half extents,
+    // orientation w, x, y, z)
+    u32 collider = CMesh;
+    float pose[10] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 1.f, 0.f, 0.f, 0.f};
     bool cloth() const { return behavior == TriangularCloth || behavior == FastGridCloth; }
 };
 
@@ -703,7 +949,42 @@ struct Scene {
     std::vector<u32> csr_off;
     std::vector<Contact> csr;
     bool packed = false;
+    // analytic colliders: compact shape table (Scene::meshAnalytic) and its
+    // owners, the marker sets (PackedCollisionData::analyticPairs*)
+    std::vector<u32> shape_mesh;
+    std::vector<Shape> shapes;
+    bool primed = false;
+    std::vector<std::pair<u32, u32>> mk_fresh, mk_held, mk_pairs;
 };
+
+// Scene::refreshAnalyticShapes (scene.hpp:659-745).
+void refresh_shapes(Scene& S) {
+    for (size_t k = 0; k < S.shape_mesh.size(); ++k) {
+        const Mesh& M = S.meshes[S.shape_mesh[k]];
+        const float *c = M.pose, *h = M.pose + 3, *q = M.pose + 6;
+        Shape& dst = S.shapes[k];
+        Shape a;
+        std::memset(&a, 0, sizeof(a));
+        for (int i = 0; i < 4; ++i) a.rq[i] = q[i];
+        if (S.primed) {
+            a.pc[0] = dst.cr[0]; a.pc[1] = dst.cr[1]; a.pc[2] = dst.cr[2];
+            for (int i = 0; i < 4; ++i) a.prq[i] = dst.rq[i];
+        } else {
+            a.pc[0] = c[0]; a.pc[1] = c[1]; a.pc[2] = c[2];
+            for (int i = 0; i < 4; ++i) a.prq[i] = q[i];
+        }
+        a.kind = M.collider; a.obj = S.shape_mesh[k]; a.beh = M.behavior; a.flags = M.collidable ? 1u : 0u;
+        a.cr[0] = c[0]; a.cr[1] = c[1]; a.cr[2] = c[2];
+        switch (M.collider) {
+        case CSphere: a.cr[3] = h[0]; a.he[0] = h[0]; a.he[1] = h[1]; a.he[2] = h[2]; a.he[3] = h[1]; break;
+        case CBox: a.he[0] = h[0]; a.he[1] = h[1]; a.he[2] = h[2]; break;
+        case CCyl: a.cr[3] = std::max(h[0], h[2]); a.he[0] = h[0]; a.he[1] = h[1]; a.he[2] = h[2]; a.he[3] = h[1]; break;
+        default: break;
+        }
+        dst = a;
+    }
+    S.primed = true;
+}
 
 enum Status : u32 { ST_NONFINITE = 1u, ST_STACK_OVF = 2u, ST_PAIR_OVF = 4u, ST_ITER_CAP = 8u };
 
@@ -783,6 +1064,10 @@ void bvh_rows(Scene& S, u32 q, u32 t, u32 cap) {
 // self pass in front (simulator.hpp:3678-3701) when self_mode == SELF_HASH.
 void detect(Scene& S) {
     S.rows.clear(); S.nbroad = 0;
+    // beginAnalyticPairs (scene.hpp:511-515)
+    S.mk_held = S.mk_fresh;
+    S.mk_fresh.clear();
+    const float inflate = S.P.radius + S.P.margin;
     const u32 cap = S.P.cols_per_point * S.nV;
     const u32 nm = (u32)S.meshes.size();
     if (S.P.self_mode == SELF_HASH) {
@@ -802,15 +1087,37 @@ void detect(Scene& S) {
         for (u32 t = 0; t < nm; ++t) {
             Mesh& T = S.meshes[t];
             if (q == t) {
+                if (Q.collider != CMesh) continue;  // no live tree
                 if (S.P.self_mode != SELF_BVH || !Q.built) continue;
                 bvh_rows(S, q, q, cap);
                 continue;
             }
-            if (!T.collidable || !T.built || !Q.built) continue;
+            if (!T.collidable) continue;
+            if (T.collider != CMesh || Q.collider != CMesh) {
+                // one marker per overlapping (cloth query, analytic target)
+                // (bvh.hpp:2903-2937); the cloth's box is its tree root
+                if (T.collider == CMesh || !Q.cloth() || !Q.built) continue;
+                u32 slot = 0;
+                while (S.shape_mesh[slot] != t) ++slot;
+                Node tb;
+                const Node& qb = Q.tree[0];
+                bool hit = true;
+                if (broad_box(S.shapes[slot], inflate, tb))
+                    hit = !(tb.mx[0] < qb.mn[0] || tb.mn[0] > qb.mx[0] || tb.mx[1] < qb.mn[1] ||
+                            tb.mn[1] > qb.mx[1] || tb.mx[2] < qb.mn[2] || tb.mn[2] > qb.mx[2]);
+                if (hit) S.mk_fresh.push_back({q, t});
+                continue;
+            }
+            if (!T.built || !Q.built) continue;
             if (!root_overlap(Q, T)) continue;
             bvh_rows(S, q, t, cap);
         }
     }
+    // endAnalyticPairs (scene.hpp:519-531): this detect's markers, then the
+    // previous detect's that are not among them
+    S.mk_pairs = S.mk_fresh;
+    for (auto& h : S.mk_held)
+        if (std::find(S.mk_pairs.begin(), S.mk_pairs.end(), h) == S.mk_pairs.end()) S.mk_pairs.push_back(h);
 }
 
 // narrowAndSortByVertices (bruteforce.hpp:311-383): narrow every row, keep
@@ -847,6 +1154,27 @@ void narrow(Scene& S) {
         S.nnarrow++;
         if (S.contacts.size() >= cap) { S.status |= ST_PAIR_OVF; continue; }
         S.contacts.push_back(out[i]);
+    }
+    // narrowAnalytic (bruteforce.hpp:245-309): every vertex of the cloth of
+    // each live marker against the collider's shape, appended
+    for (auto& pr : S.mk_pairs) {
+        u32 slot = 0;
+        while (S.shape_mesh[slot] != pr.second) ++slot;
+        const Shape& sh = S.shapes[slot];
+        if (!(sh.flags & 1u)) continue;
+        const Mesh& Q = S.meshes[pr.first];
+        const float rm = rot_margin(sh, S.P.radius, S.P.margin);
+        for (u32 id = 0; id < Q.nV; ++id) {
+            Contact c;
+            const u32 g = Q.voff + id;
+            if (!analytic_one(sh, ld3(S.x.data(), g), ld3(S.xp.data(), g), S.P.radius, S.P.margin, rm, c.n, &c.d))
+                continue;
+            c.point = id; c.tri = 0; c.qobj = pr.first; c.tobj = pr.second;
+            c.qbeh = Q.behavior; c.tbeh = sh.beh; c.qshape = CMesh; c.tshape = sh.kind;
+            S.nnarrow++;
+            if (S.contacts.size() >= cap) { S.status |= ST_PAIR_OVF; continue; }
+            S.contacts.push_back(c);
+        }
     }
     // CPU CSR (bruteforce.hpp:358-383), then canonical order per vertex.
     S.csr_off.assign(S.nV + 1, 0);
@@ -976,6 +1304,7 @@ void env_forces(Scene& S) {
 // (periodic rebuild, environment forces) at cursor 0.
 void substep(Scene& S) {
     if (S.cursor == 0) {
+        refresh_shapes(S);
         if (S.P.rebuild_frames && S.frame % S.P.rebuild_frames == 0)
             for (auto& M : S.meshes) {
                 if (M.built && M.behavior == Float) continue;
@@ -1180,7 +1509,78 @@ void yso_scene_pack(void* h) {
     }
     S->voff.push_back(S->nV);
     for (u32 i = 0; i < S->nV; ++i) S->vaf_off[i + 1] += S->vaf_off[i];
+    // Scene::packAnalyticShapes (scene.hpp:762-781): seeded, not primed
+    S->shape_mesh.clear();
+    for (u32 m = 0; m < S->meshes.size(); ++m)
+        if (S->meshes[m].collider != CMesh) S->shape_mesh.push_back(m);
+    S->shapes.assign(S->shape_mesh.size(), Shape{});
+    S->primed = false;
+    refresh_shapes(*S);
+    S->primed = false;
+    S->mk_fresh.clear(); S->mk_held.clear(); S->mk_pairs.clear();
     S->packed = true;
+}
+// Analytic collider of a mesh: kind (0 = triangles), centre, half extents,
+// orientation (w, x, y, z); the kind is fixed once packed.  Returns 0 on success.
+int yso_scene_set_collider(void* h, int mesh, u32 kind, const float* c, const float* hx, const float* q) {
+    Scene* S = (Scene*)h;
+    if (mesh < 0 || (size_t)mesh >= S->meshes.size() || kind > CPlane) return -1;
+    Mesh& M = S->meshes[mesh];
+    if (kind != CMesh && M.cloth()) return -1;
+    if (S->packed && kind != M.collider) return -1;
+    M.collider = kind;
+    for (int i = 0; i < 3; ++i) { M.pose[i] = c[i]; M.pose[3 + i] = hx ? hx[i] : 0.f; }
+    for (int i = 0; i < 4; ++i) M.pose[6 + i] = q[i];
+    return 0;
+}
+uint64_t yso_scene_shapes(void* h, void* out) {
+    Scene* S = (Scene*)h;
+    if (out) std::memcpy(out, S->shapes.data(), sizeof(Shape) * S->shapes.size());
+    return S->shapes.size();
+}
+// One analytic narrow evaluation (returns 1 on contact).
+int yso_analytic_one(const void* shape, const float* pcur, const float* pprev, float radius, float thickness,
+                     float rot, float* n_out, float* d_out) {
+    return analytic_one(*(const Shape*)shape, ld3(pcur, 0), ld3(pprev, 0), radius, thickness, rot, n_out, d_out) ? 1
+                                                                                                                   : 0;
+}
+float yso_rot_margin(const void* shape, float radius, float thickness) {
+    return rot_margin(*(const Shape*)shape, radius, thickness);
+}
+// Broad box (6 floats lo, hi); returns 1 when finite.
+int yso_broad_box(const void* shape, float inflate, float* out6) {
+    Node n;
+    int f = broad_box(*(const Shape*)shape, inflate, n) ? 1 : 0;
+    for (int i = 0; i < 3; ++i) { out6[i] = n.mn[i]; out6[3 + i] = n.mx[i]; }
+    return f;
+}
+// narrowAnalytic over explicit pairs (2 u32 each: cloth mesh, collider mesh),
+// contacts (48 B) in pair-then-vertex order; returns the contact count
+// (contacts beyond cap are counted, not written).
+uint64_t yso_narrow_analytic(const float* x, const float* xp, const u32* state_off, const u32* beh, u32 nmesh,
+                             const void* shapes, u32 nshapes, const u32* pairs, u32 npairs, float radius,
+                             float thickness, void* out, uint64_t cap) {
+    const Shape* sh = (const Shape*)shapes;
+    Contact* o = (Contact*)out;
+    uint64_t n = 0;
+    for (u32 p = 0; p < npairs; ++p) {
+        u32 cloth = pairs[2 * p], obj = pairs[2 * p + 1];
+        if (cloth >= nmesh) continue;
+        int slot = -1;
+        for (u32 k = 0; k < nshapes; ++k) if (sh[k].obj == obj) { slot = (int)k; break; }
+        if (slot < 0 || !(sh[slot].flags & 1u)) continue;
+        const float rm = rot_margin(sh[slot], radius, thickness);
+        for (u32 id = 0; id < state_off[cloth + 1] - state_off[cloth]; ++id) {
+            const u32 g = state_off[cloth] + id;
+            Contact c;
+            if (!analytic_one(sh[slot], ld3(x, g), ld3(xp, g), radius, thickness, rm, c.n, &c.d)) continue;
+            c.point = id; c.tri = 0; c.qobj = cloth; c.tobj = obj;
+            c.qbeh = beh[cloth]; c.tbeh = sh[slot].beh; c.qshape = CMesh; c.tshape = sh[slot].kind;
+            if (n < cap) o[n] = c;
+            ++n;
+        }
+    }
+    return n;
 }
 void yso_scene_step(void* h, u32 nsub) {
     Scene* S = (Scene*)h;
@@ -1192,6 +1592,7 @@ void yso_scene_stage(void* h, int which) {
     switch (which) {
         case 0:  // frame preamble
             if (S.cursor == 0) {
+                refresh_shapes(S);
                 if (S.P.rebuild_frames && S.frame % S.P.rebuild_frames == 0)
                     for (auto& M : S.meshes) { if (M.built && M.behavior == Float) continue; build_tree(S, M); }
                 env_forces(S);

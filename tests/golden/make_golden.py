@@ -12,7 +12,11 @@ generators; outputs are the reference kernels' results:
                      pairs (inclusive AABB test, h = 1e-3 and a self query);
   substep_*.npz   -- one mid-drape substep of a small scene: broad rows (the
                      oracle's), narrow_pt_tri contacts, the cloth's spring
-                     forces and integrate_cloth(_grid) positions / velocities.
+                     forces and integrate_cloth(_grid) positions / velocities;
+  analytic.npz    -- narrow_pt_analytic contacts of vertex clouds around every
+                     collider kind (static, rotated, moving, ellipsoid,
+                     disabled; tests/analytic_cases.py), with the rotation
+                     margins passed to the kernel.
 """
 from __future__ import annotations
 
@@ -28,6 +32,9 @@ sys.path.insert(0, ROOT)
 from oracle import oracle as O  # noqa: E402
 from oracle import refkernels as R  # noqa: E402
 from ysim_b200 import generators as G  # noqa: E402
+
+sys.path.insert(0, os.path.dirname(HERE))
+import analytic_cases as AC  # noqa: E402
 
 
 def canon(p):
@@ -118,12 +125,29 @@ def substep(name):
                         c_d=rc["d"], csr_off=off, f=f, x_next=xn, v_next=vn, anomaly=np.int32(anomaly))
 
 
+def analytic():
+    shapes, x, xp, so, beh, pairs = AC.cases(seed=11, per_shape=600)
+    rms, out = [], []
+    for k, (cloth, obj) in enumerate(pairs):
+        rm = O.rot_margin(shapes[k], AC.RADIUS, AC.THICKNESS)
+        rms.append(rm)
+        if not shapes[k]["flags"] & 1:
+            continue  # narrowAnalytic skips a collider that is not collidable
+        out.append(R.narrow_analytic(x, xp, so, shapes, int(cloth), k, int(beh[cloth]), AC.RADIUS, AC.THICKNESS,
+                                     np.float32(rm)))
+    c = AC.canon_contacts(np.concatenate(out))
+    np.savez_compressed(os.path.join(HERE, "analytic.npz"), shapes=shapes.view(np.uint8), x=x, xprev=xp,
+                        state_off=so, beh=beh, pairs=pairs, radius=AC.RADIUS, thickness=AC.THICKNESS,
+                        rot_margin=np.array(rms, np.float32), contacts=c.view(np.uint8))
+
+
 if __name__ == "__main__":
     if not R.available():
         sys.exit("reference checkout absent: cannot regenerate golden vectors")
     morton_tree()
     for k in SPECS:
         substep(k)
+    analytic()
     for fn in sorted(os.listdir(HERE)):
         if fn.endswith(".npz"):
             print(fn, os.path.getsize(os.path.join(HERE, fn)))

@@ -188,3 +188,27 @@ def test_face_face_hash_matches_reference_kernels(oracle, self_rows):
         assert len(a) > 0, name
         assert np.array_equal(sa, sb), (name, sa, sb)
         assert np.array_equal(canon_rows_full(a), canon_rows_full(b)), name
+
+
+def test_analytic_narrow_matches_reference_kernel(oracle):
+    """narrow_pt_analytic (bruteforce.metal:236-499) restated: every contact
+    of every collider kind -- static, rotated, moving, ellipsoid, disabled --
+    bit for bit (normals and distances), none missing or extra."""
+    from analytic_cases import RADIUS, THICKNESS, canon_contacts, cases
+    shapes, x, xp, so, beh, pairs = cases(seed=23, per_shape=4000)
+    oc, n = oracle.narrow_analytic(x, xp, so, beh, shapes, pairs, RADIUS, THICKNESS)
+    ref = []
+    for k, (cloth, _) in enumerate(pairs):
+        if not shapes[k]["flags"] & 1:
+            continue
+        rm = np.float32(oracle.rot_margin(shapes[k], RADIUS, THICKNESS))
+        ref.append(refk.narrow_analytic(x, xp, so, shapes, int(cloth), k, int(beh[cloth]), RADIUS, THICKNESS, rm))
+    rc = canon_contacts(np.concatenate(ref))
+    oc = canon_contacts(oc)
+    assert n == len(oc) == len(rc)
+    assert np.array_equal(oc.view(np.uint8), rc.view(np.uint8))
+    for kind in (1, 2, 3, 4):
+        assert (rc["tshape"] == kind).sum() > 100, kind
+    # the disabled collider emits nothing
+    off = shapes["obj"][shapes["flags"] == 0]
+    assert not np.isin(rc["tobj"], off).any()

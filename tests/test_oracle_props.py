@@ -217,6 +217,93 @@ def test_oracle_matches_golden_substep(oracle, name):
         assert len(c) > 0
 
 
+def test_oracle_matches_golden_analytic(oracle):
+    """The oracle's analytic narrow phase reproduces the reference kernel's
+    contacts (tests/golden/analytic.npz) bit for bit."""
+    from analytic_cases import canon_contacts
+    g = np.load(os.path.join(GOLD, "analytic.npz"))
+    shapes = g["shapes"].view(oracle.SHAPE_DTYPE)
+    ref = g["contacts"].view(oracle.CONTACT_DTYPE)
+    for k in range(len(shapes)):
+        assert np.float32(oracle.rot_margin(shapes[k], g["radius"], g["thickness"])) == g["rot_margin"][k]
+    oc, n = oracle.narrow_analytic(g["x"], g["xprev"], g["state_off"], g["beh"], shapes, g["pairs"], g["radius"],
+                                   g["thickness"])
+    assert n == len(ref) > 1000
+    assert np.array_equal(canon_contacts(oc).view(np.uint8), ref.view(np.uint8))
+
+
+def test_analytic_margins_and_broad_box(oracle):
+    """Rotation margins follow theta = 2 acos|q . q_prev| (bruteforce.hpp:201-240,
+    bvh.hpp:2465-2479); the broad box of every shape holds the shape at both
+    poses, padded by the inflate band; a half-space has no finite box."""
+    from analytic_cases import cases
+    from ysim_b200 import generators as G
+    shapes, *_ = cases(seed=5, per_shape=10)
+    rad, th, inflate = np.float32(0.012), np.float32(0.015), np.float32(0.027)
+    rng = np.random.default_rng(0)
+    for s in shapes:
+        dq = min(abs(float(np.dot(s["rq"].astype(np.float64), s["prq"].astype(np.float64)))), 1.0)
+        theta = 2.0 * np.arccos(dq)
+        m = oracle.rot_margin(s, rad, th)
+        kind = int(s["kind"])
+        if theta <= 1e-9 or kind == 4:
+            assert m == 0.0
+        else:
+            he = s["he"].astype(np.float64)
+            rmax = {1: he[:3].max(), 2: np.sqrt((he[:3] ** 2).sum()),
+                    3: np.sqrt(float(s["cr"][3]) ** 2 + he[3] ** 2)}[kind]
+            assert m == np.float32(theta * (rmax + float(rad) + float(th)))
+        finite, box = oracle.broad_box(s, inflate)
+        assert finite == (kind != 4)
+        if not finite:
+            continue
+        # sample the shape's surface at both poses
+        u = rng.normal(size=(2000, 3))
+        u /= np.linalg.norm(u, axis=1, keepdims=True)
+        if kind == 1:
+            loc = u * s["he"][:3]
+        elif kind == 2:
+            loc = np.sign(u) * s["he"][:3] * rng.uniform(0, 1, (2000, 3)) ** 0.01
+        else:
+            r, hh = float(s["cr"][3]), float(s["he"][3])
+            ang = rng.uniform(0, 2 * np.pi, 2000)
+            loc = np.stack([r * np.cos(ang), rng.uniform(-hh, hh, 2000), r * np.sin(ang)], 1)
+        for c, q in ((s["cr"][:3], s["rq"]), (s["pc"][:3], s["prq"])):
+            w = G.quat_rotate(q.astype(np.float64), loc) + c
+            assert (w >= box[:3] + inflate - 1e-5).all() and (w <= box[3:] - inflate + 1e-5).all()
+
+
+def test_analytic_scene_markers_and_roll(oracle):
+    """Scene-level analytic path on the oracle: the pack seeds prev = cur, a
+    moved collider rolls its old pose into prev at the next frame, a cloth
+    under a half-space gets one contact per vertex within the band, and an
+    analytic collider emits no triangle rows."""
+    from ysim_b200 import generators as G
+    spec = G.config_c1(P=12, level=1, height=0.2)
+    cloth = spec.meshes[0]
+    plane = G.analytic_collider(4, (0.0, 0.19, 0.0))
+    sph = G.analytic_collider(1, (2.0, 0.0, 0.0), (0.1, 0.1, 0.1))
+    spec = G.SceneSpec("plane", spec.params, [cloth, plane, sph], 0)
+    o = oracle.OracleScene(spec)
+    sh = o.shapes()
+    assert len(sh) == 2 and list(sh["obj"]) == [1, 2]
+    assert np.array_equal(sh["pc"][:, :3], sh["cr"][:, :3]) and np.array_equal(sh["prq"], sh["rq"])
+    o.step(1)
+    assert o.stats()["broad_rows"] == 0
+    off, c = o.contacts()
+    assert len(c) == cloth.nV and (c["tobj"] == 1).all() and (c["tri"] == 0).all()
+    assert np.allclose(c["n"], [0.0, 1.0, 0.0])
+    o.set_collider(2, 1, (2.0, 0.05, 0.0), (0.1, 0.1, 0.1), G.quat_axis_angle((0, 1, 0), 0.1))
+    o.step(spec.params.substeps)  # through the next frame start
+    sh = o.shapes()
+    assert np.allclose(sh["pc"][1, :3], [2.0, 0.0, 0.0]) and np.allclose(sh["cr"][1, :3], [2.0, 0.05, 0.0])
+    assert sh["prq"][1, 0] == 1.0 and sh["rq"][1, 0] < 1.0
+    assert oracle.rot_margin(sh[1], 0.012, 0.015) > 0.0
+    o.step(spec.params.substeps)  # unchanged pose: prev catches up
+    sh = o.shapes()
+    assert np.array_equal(sh["pc"][1, :3], sh["cr"][1, :3]) and np.array_equal(sh["prq"][1], sh["rq"][1])
+
+
 # ---------------------------------------------------------------- host logic
 def test_generator_sizes_and_determinism():
     from ysim_b200 import generators as G

@@ -36,6 +36,13 @@ SELF_BVH = 2
 TREE_REFERENCE = 0  # Morton normalisation per axis, node for node the reference's tree
 TREE_CUBE = 1       # one scale for all axes (default)
 
+# ColliderKind (ys_analytic_shape.kind)
+COLLIDER_MESH = 0
+COLLIDER_SPHERE = 1
+COLLIDER_BOX = 2
+COLLIDER_CYLINDER = 3
+COLLIDER_PLANE = 4
+
 
 class SimParams(C.Structure):
     _fields_ = [
@@ -83,6 +90,11 @@ _PROTOS = {
     "ys_scene_set_graphs": (C.c_int, [C.c_void_p, C.c_int]),
     "ys_scene_set_tree_layout": (C.c_int, [C.c_void_p, C.c_int]),
     "ys_scene_set_fused_variant": (C.c_int, [C.c_void_p, C.c_int]),
+    "ys_scene_set_collider": (C.c_int, [C.c_void_p, C.c_int, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "ys_scene_colliders": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.POINTER(C.c_uint32)]),
+    "ys_narrow_analytic": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p,
+                                     C.c_uint32, C.c_void_p, C.c_uint32, C.c_float, C.c_float, C.c_void_p,
+                                     C.c_uint64, C.c_void_p, C.c_void_p]),
     "ys_scene_autotune": (C.c_int, [C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p]),
     "ys_scene_sync": (C.c_int, [C.c_void_p]),
     "ys_scene_stream": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),

@@ -17,7 +17,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 SRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "lib", "libysim_b200.so")
-SOURCES = ["ys_sort.cu", "ys_lbvh.cu", "ys_scan.cu", "ys_scene.cu", "ys_api.cu", "ys_shash.cu", "ys_shff.cu"]
+SOURCES = ["ys_sort.cu", "ys_lbvh.cu", "ys_scan.cu", "ys_scene.cu", "ys_api.cu", "ys_shash.cu", "ys_shff.cu", "ys_analytic.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-fmad=false", "-prec-div=true", "-prec-sqrt=true",
          "-Xcompiler", "-fPIC", "-Xcompiler", "-O3", "-diag-suppress", "549"]

@@ -19,6 +19,7 @@
 #include <string>
 #include <vector>
 
+#include "ys_analytic.cuh"
 #include "ys_collide.cuh"
 #include "ys_common.cuh"
 #include "ys_lbvh.cuh"
@@ -39,7 +40,10 @@ ys_status fail(ys_status code, const std::string& msg) {
         if (e_ != cudaSuccess) return fail(YS_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
     } while (0)
 
-enum : u32 { MF_STATIC = 1, MF_COLLIDABLE = 2, MF_SELF = 4, MF_QUERY = 8, MF_CLOTH = 16, MF_TREE = 32, MF_GRID = 64 };
+enum : u32 {
+    MF_STATIC = 1, MF_COLLIDABLE = 2, MF_SELF = 4, MF_QUERY = 8, MF_CLOTH = 16, MF_TREE = 32, MF_GRID = 64,
+    MF_ANALYTIC = 128,  // analytic collider: tested against its shape, its triangles unused
+};
 static constexpr int MAXC = 32;  // per-vertex contact buffer of the fused kernel
 
 struct MeshDev {
@@ -50,8 +54,11 @@ struct MeshDev {
     u32 tgt_begin, tgt_end;
     u32 gspr;  // FastGridCloth: offset of this mesh's per-spring k / L arrays, or NO_SPRINGS
     u32 w4_off, w4_cap;  // wide nodes of this mesh's tree (cube layout)
+    u32 shape;           // analytic collider: slot in the shape table
+    u32 pad[3];
 };
 static constexpr u32 NO_SPRINGS = 0xFFFFFFFFu;
+static constexpr u32 NO_PAIR = 0xFFFFFFFFu;
 
 struct StepArgs {
     const float4* x;
@@ -78,7 +85,15 @@ struct StepArgs {
     const float4* ext;  // external forces (applyEnvironmentForces) or null: g * m
     const float* gk;    // per-spring stiffness / rest length of grid cloths (MeshDev::gspr)
     const float* gL;
-    float subh, kair, kd, gx, gy, gz, margin, band;
+    // analytic colliders: shape table, marker pair of each target entry (or
+    // NO_PAIR), marker pairs (cloth, collider, slot, first thread) and this
+    // substep's active flag per pair
+    const DShape* shapes;
+    const u32* tpair;
+    const uint4* apairs;
+    const u32* mk_act;
+    u32 npairs, apair_total;
+    float subh, kair, kd, gx, gy, gz, margin, band, radius;
     u32 nV, self_mode, record, cap;
     u32* status;
     unsigned long long* counters;  // [0] broad rows, [1] contacts, [2] pool fill, [3] [4] running totals of 0, 1
@@ -262,6 +277,19 @@ __device__ __forceinline__ void insert_contact(VContact (&buf)[MAXC], int& nc, u
     ++nc;
 }
 
+// The analytic test out of line, so that the fused kernel's descent keeps its
+// register allocation (the call is taken only for live collider pairs).
+__device__ __noinline__ bool analytic_contact(const DShape* S, f3 pcur, f3 pprev, float radius, float thickness,
+                                              VContact* c) {
+    f3 n;
+    float d;
+    if (!analytic_narrow(S->s, pcur, pprev, radius, thickness, S->rot_margin, n, d)) return false;
+    c->tobj = S->s.obj;
+    c->tri = 0u;
+    c->nx = n.x; c->ny = n.y; c->nz = n.z; c->d = d;
+    return true;
+}
+
 // WIDE: descend the 4-wide form of the trees (cube layout), else the binary one.
 // MINB: CTAs per SM the registers are capped for (8: 64 registers, 6: 80,
 // 4: no cap); the results do not depend on it (ys_scene_autotune picks one).
@@ -321,11 +349,24 @@ __global__ void __launch_bounds__(128, MINB) k_fused(StepArgs A) {
         }
         if (selfOK) start(m, (m << 6) | KEY_SELF | lane);
     }
+    VContact buf[MAXC];
+    int nc = 0;
     const u32 te = query ? Mp->tgt_end : 0u;
     u32 tk = query ? Mp->tgt_begin : 0u;  // next target
     auto next_tree = [&]() -> bool {
         while (tk < te) {
-            const u32 t = A.targets[tk++];
+            const u32 k = tk++;
+            const u32 t = A.targets[k];
+            if (A.meshes[t].flags & MF_ANALYTIC) {
+                // narrowAnalytic for a marked (cloth, collider) pair: this
+                // vertex against the shape, no descent
+                const u32 p = A.tpair[k];
+                VContact c;
+                if (p != NO_PAIR && A.mk_act[p] &&
+                    analytic_contact(A.shapes + A.meshes[t].shape, xc, xpv, A.radius, mg, &c))
+                    insert_contact(buf, nc, st, c);
+                continue;
+            }
             const u32 tno = A.meshes[t].node_off, tnf = A.meshes[t].nF;
             if (tnf == 0 || !root_overlap(A.nodes + Mp->node_off, A.nodes + tno)) continue;
             qmn = xc - mk(mg, mg, mg);
@@ -336,8 +377,6 @@ __global__ void __launch_bounds__(128, MINB) k_fused(StepArgs A) {
         return false;
     };
 
-    VContact buf[MAXC];
-    int nc = 0;
     u32 qn = 0, cn = 0;  // warp-uniform fill of the queue and of the contact buffer
 
     auto flush = [&]() {
@@ -573,6 +612,57 @@ __global__ void __launch_bounds__(128) k_narrow_rows(StepArgs A, u32 nrows) {
     A.contacts[o] = c;
 }
 
+// narrow_pt_analytic over every vertex of every live (cloth, collider) marker
+// pair (BruteForce::narrowAnalytic, bruteforce.hpp:245-309), appended to the
+// contacts after the triangle rows: (vertex, 0), (cloth, collider).
+__global__ void __launch_bounds__(128) k_narrow_analytic_scene(StepArgs A) {
+    const u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= A.apair_total) return;
+    u32 lo = 0, hi = A.npairs;  // the pair whose thread range holds i
+    while (hi - lo > 1) {
+        const u32 mid = (lo + hi) >> 1;
+        if (A.apairs[mid].w <= i) lo = mid;
+        else hi = mid;
+    }
+    if (!A.mk_act[lo]) return;
+    const uint4 P = A.apairs[lo];
+    const MeshDev& Q = A.meshes[P.x];
+    const u32 id = i - P.w, g = Q.voff + id;
+    const DShape& S = A.shapes[P.z];
+    f3 n;
+    float d;
+    if (!analytic_narrow(S.s, ld(A.x, g), ld(A.xp, g), A.radius, A.margin, S.rot_margin, n, d)) return;
+    unsigned long long o = atomicAdd(&A.counters[1], 1ull);
+    if (o >= A.cap) { atomicOr(A.status, ST_PAIR_OVF); return; }
+    Contact c;
+    c.point = id; c.tri = 0u; c.qobj = P.x; c.tobj = P.y;
+    c.nx = n.x; c.ny = n.y; c.nz = n.z; c.d = d;
+    c.qbeh = Q.behavior; c.tbeh = S.s.beh; c.qshape = COL_MESH; c.tshape = S.s.kind;
+    A.contacts[o] = c;
+}
+
+// Analytic markers of one detect (BroadPhase::detectCollisions,
+// bvh.hpp:2886-2941): a (cloth, collider) pair is marked when the cloth's
+// root box overlaps the collider's broad box (AABB4::intersect; a half-space
+// always), and it is live when it was marked at this detect or at the one
+// before (PackedCollisionData::endAnalyticPairs, scene.hpp:485-530).
+__global__ void k_analytic_markers(const uint4* __restrict__ apairs, u32 np, const MeshDev* __restrict__ meshes,
+                                   const Node* __restrict__ nodes, const DShape* __restrict__ shapes,
+                                   u32* __restrict__ fresh, const u32* __restrict__ held, u32* __restrict__ act) {
+    const u32 p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= np) return;
+    const uint4 P = apairs[p];
+    const DShape& S = shapes[P.z];
+    u32 hit = 1u;
+    if (S.lo.w != 0.f) {
+        const Node r = nodes[meshes[P.x].node_off];
+        hit = (S.hi.x < r.mnx || S.lo.x > r.mxx || S.hi.y < r.mny || S.lo.y > r.mxy || S.hi.z < r.mnz ||
+               S.lo.z > r.mxz) ? 0u : 1u;
+    }
+    fresh[p] = hit;
+    act[p] = hit | held[p];
+}
+
 // Per-vertex CSR of the contacts (narrow_bucket_count/scan/scatter,
 // physics.metal:566-616), then canonical (tobj, tri) order per vertex.
 __global__ void k_bucket_count(StepArgs A, u32 nc) {
@@ -655,6 +745,10 @@ struct HostMesh {
     std::vector<u32> spr_off, spr_split, spr_nbr, vaf_off, vaf;
     std::vector<float> spr_rest;
     bool grid_springs_on = false;  // per-spring parameters set (ys_scene_set_grid_springs)
+    // analytic collider (GeneralMesh::colliderKind) and its pose: centre,
+    // local half extents, orientation (w, x, y, z)
+    u32 collider = COL_MESH;
+    float pose[10] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 1.f, 0.f, 0.f, 0.f};
 };
 
 template <class T>
@@ -788,6 +882,15 @@ struct ys_scene {
     DBuf<float4> ext;
     bool use_ext = false;
     DBuf<float> gk, gL;              // per-spring grid-cloth parameters
+    // analytic colliders: compact shape table (mesh of each slot), marker
+    // pairs, per-target pair ids, marker flags (fresh[2][np], live[np])
+    std::vector<int> shape_mesh;
+    std::vector<DShape> hshapes;
+    bool analytic_primed = false, shapes_uploaded = false;
+    DBuf<DShape> dshapes;
+    DBuf<uint4> apairs;
+    DBuf<u32> tpair, markers;
+    u32 npairs = 0, apair_total = 0;
     std::vector<MeshDev> hmeshes;    // host copy of the device mesh table
     // per-kernel CUDA-event timing of the fused path
     bool timing = false;
@@ -851,6 +954,13 @@ StepArgs make_args(ys_scene* s) {
     A.ext = s->use_ext ? s->ext.p : nullptr;
     A.gk = s->gk.p;
     A.gL = s->gL.p;
+    A.shapes = s->dshapes.p;
+    A.tpair = s->tpair.p;
+    A.apairs = s->apairs.p;
+    A.mk_act = s->markers.p ? s->markers.p + 2 * (size_t)s->npairs : nullptr;
+    A.npairs = s->npairs;
+    A.apair_total = s->apair_total;
+    A.radius = s->P.radius;
     A.subh = s->P.subh; A.kair = s->P.kair; A.kd = s->P.kd;
     A.gx = s->P.gravity[0]; A.gy = s->P.gravity[1]; A.gz = s->P.gravity[2];
     A.margin = s->P.margin;
@@ -994,8 +1104,73 @@ ys_status build_levels(ys_scene* s) {
     return YS_OK;
 }
 
+// Scene::refreshAnalyticShapes (scene.hpp:659-745): the shape of each
+// collider from its pose (sphere: semi-axes h, radius h.x; box: half extents
+// h; cylinder: radius max(h.x, h.z), half height h.y; plane: centre and
+// orientation only); after the first refresh the previous centre and
+// orientation roll into the prev slots.  Each entry also carries its broad
+// box (inflated by radius + margin, BVH::analyticInflate) and the narrow
+// rotation margin.  The device table is rewritten only when it changed.
+ys_status refresh_shapes(ys_scene* s) {
+    const size_t ns = s->shape_mesh.size();
+    if (ns == 0) return YS_OK;
+    std::vector<DShape> t(ns);
+    for (size_t k = 0; k < ns; ++k) {
+        const HostMesh& H = s->meshes[s->shape_mesh[k]];
+        const float *c = H.pose, *h = H.pose + 3, *q = H.pose + 6;
+        AShape a;
+        memset(&a, 0, sizeof(a));
+        a.rq = make_float4(q[0], q[1], q[2], q[3]);
+        if (s->analytic_primed) {
+            const AShape& o = s->hshapes[k].s;
+            a.pc = make_float4(o.cr.x, o.cr.y, o.cr.z, 0.f);
+            a.prq = o.rq;
+        } else {
+            a.pc = make_float4(c[0], c[1], c[2], 0.f);
+            a.prq = a.rq;
+        }
+        a.kind = H.collider;
+        a.obj = (u32)s->shape_mesh[k];
+        a.beh = H.d.behavior;
+        a.flags = (H.d.flags & YS_MESH_COLLIDABLE) ? 1u : 0u;
+        if (H.collider == COL_SPHERE) {
+            a.cr = make_float4(c[0], c[1], c[2], h[0]);
+            a.he = make_float4(h[0], h[1], h[2], h[1]);
+        } else if (H.collider == COL_BOX) {
+            a.cr = make_float4(c[0], c[1], c[2], 0.f);
+            a.he = make_float4(h[0], h[1], h[2], 0.f);
+        } else if (H.collider == COL_CYLINDER) {
+            a.cr = make_float4(c[0], c[1], c[2], std::max(h[0], h[2]));
+            a.he = make_float4(h[0], h[1], h[2], h[1]);
+        } else {  // plane
+            a.cr = make_float4(c[0], c[1], c[2], 0.f);
+            a.he = make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+        DShape& D = t[k];
+        memset(&D, 0, sizeof(D));
+        D.s = a;
+        f3 lo, hi;
+        const float inflate = s->P.radius + s->P.margin;
+        const bool finite = analytic_broad_box(a, inflate, lo, hi);
+        D.lo = make_float4(lo.x, lo.y, lo.z, finite ? 1.f : 0.f);
+        D.hi = make_float4(hi.x, hi.y, hi.z, 0.f);
+        D.rot_margin = analytic_rot_margin(a, s->P.radius, s->P.margin);
+    }
+    s->analytic_primed = true;
+    if (s->shapes_uploaded && memcmp(t.data(), s->hshapes.data(), ns * sizeof(DShape)) == 0) return YS_OK;
+    s->hshapes = t;
+    // pageable source: the call returns once the table is staged
+    YS_CK(cudaMemcpyAsync(s->dshapes.p, s->hshapes.data(), ns * sizeof(DShape), cudaMemcpyHostToDevice, s->stream));
+    s->shapes_uploaded = true;
+    return YS_OK;
+}
+
 ys_status preamble(ys_scene* s) {
     if (s->cursor != 0) return YS_OK;
+    {
+        ys_status r = refresh_shapes(s);
+        if (r) return r;
+    }
     if (s->P.rebuild_frames && s->frame % s->P.rebuild_frames == 0) {
         bool rebuilt = false;
         for (auto& H : s->meshes) {
@@ -1014,18 +1189,28 @@ ys_status preamble(ys_scene* s) {
     return YS_OK;
 }
 
+// Refit of every live tree, then the analytic markers from the new root
+// boxes (fresh flags in the slot of this substep's parity, held flags from
+// the other one).
 ys_status refit(ys_scene* s) {
     if (s->nrjobs)
         launch_root_boxes(s->rjobs.p + (size_t)(s->cur * 2 + s->cv) * s->nrjobs, s->nrjobs, s->rchunks.p,
                           s->nrchunks, s->stream);
-    if (s->njobs == 0) return YS_OK;
-    // the job table for the current (position, velocity) buffer pair
-    const RefitJob* table = s->jobs.p + (size_t)(s->cur * 2 + s->cv) * s->njobs;
-    YS_CK(cudaMemsetAsync(s->maxext.p, 0, s->maxext.n * 4, s->stream));
-    launch_refit(table, s->njobs, s->refitLeaves, s->status.p, s->stream);
-    if (s->use_levels)
-        launch_refit_levels(table, s->wlist.p, s->hoff.p, s->lvl_off.data(), s->lvl_top, s->stream);
-    if (s->nRootOnly) launch_refit_roots(table, s->njobs, s->stream);
+    if (s->njobs) {
+        // the job table for the current (position, velocity) buffer pair
+        const RefitJob* table = s->jobs.p + (size_t)(s->cur * 2 + s->cv) * s->njobs;
+        YS_CK(cudaMemsetAsync(s->maxext.p, 0, s->maxext.n * 4, s->stream));
+        launch_refit(table, s->njobs, s->refitLeaves, s->status.p, s->stream);
+        if (s->use_levels)
+            launch_refit_levels(table, s->wlist.p, s->hoff.p, s->lvl_off.data(), s->lvl_top, s->stream);
+        if (s->nRootOnly) launch_refit_roots(table, s->njobs, s->stream);
+    }
+    if (s->npairs) {
+        const size_t np = s->npairs;
+        k_analytic_markers<<<ceil_div(np, 128), 128, 0, s->stream>>>(
+            s->apairs.p, s->npairs, s->dmeshes.p, s->nodes.p, s->dshapes.p, s->markers.p + (size_t)s->cv * np,
+            s->markers.p + (size_t)(1 - s->cv) * np, s->markers.p + 2 * np);
+    }
     return YS_OK;
 }
 
@@ -1075,6 +1260,7 @@ ys_status narrow_and_sort(ys_scene* s) {
     YS_CK(cudaMemsetAsync(s->counters.p + 1, 0, 8, s->stream));
     StepArgs A = make_args(s);
     if (nrows) k_narrow_rows<<<ceil_div(nrows, 128), 128, 0, s->stream>>>(A, nrows);
+    if (s->apair_total) k_narrow_analytic_scene<<<ceil_div(s->apair_total, 128), 128, 0, s->stream>>>(A);
     YS_CK(cudaMemcpyAsync(cnt, s->counters.p, 16, cudaMemcpyDeviceToHost, s->stream));
     YS_CK(cudaStreamSynchronize(s->stream));
     u32 nc = (u32)std::min<unsigned long long>(cnt[1], s->cap);
@@ -1216,6 +1402,7 @@ ys_status ys_scene_destroy(ys_scene* s) {
     s->w4.free(); s->leafW.free(); s->warrive.free(); s->wideScratch.free();
     s->leafWf.free(); s->wcount.free(); s->hacc.free(); s->wlist.free(); s->hcount.free(); s->hoff.free();
     s->hcursor.free();
+    s->dshapes.free(); s->apairs.free(); s->tpair.free(); s->markers.free();
     s->scanScratch.free(); s->rows.free(); s->contacts.free(); s->csr.free(); s->pool.free(); s->bucket.free();
     drop_graphs(s);
     s->csr_off.free(); s->vstart.free(); s->vcount.free(); s->ext.free();
@@ -1275,6 +1462,9 @@ ys_status ys_scene_pack(ys_scene* s) {
         if (cloth) f |= MF_CLOTH;
         if (H.d.num_facets) f |= MF_TREE;
         if (H.d.behavior == YS_FAST_GRID_CLOTH) f |= MF_GRID;
+        // an analytic collider queries nothing (BroadPhase::detectCollisions
+        // marks only cloth -> collider pairs, bvh.hpp:2913-2937)
+        if (H.collider != COL_MESH) f = (f | MF_ANALYTIC) & ~MF_QUERY;
         H.flags = f;
         build_adjacency(H);
     }
@@ -1323,7 +1513,8 @@ ys_status ys_scene_pack(ys_scene* s) {
             for (size_t t = 0; t < s->meshes.size(); ++t) {
                 if (t == m) continue;
                 const HostMesh& T = s->meshes[t];
-                if (!(T.d.flags & YS_MESH_COLLIDABLE) || T.d.num_facets == 0) continue;
+                if (!(T.d.flags & YS_MESH_COLLIDABLE)) continue;
+                if (T.d.num_facets == 0 && T.collider == COL_MESH) continue;
                 if (T.d.group != H.d.group) continue;
                 targets.push_back((u32)t);
             }
@@ -1331,6 +1522,11 @@ ys_status ys_scene_pack(ys_scene* s) {
         D.gspr = NO_SPRINGS;
         D.w4_off = H.w4_off;
         D.w4_cap = H.w4_cap;
+        D.shape = NO_PAIR;
+        if (H.collider != COL_MESH) {
+            D.shape = (u32)s->shape_mesh.size();
+            s->shape_mesh.push_back((int)m);
+        }
         md[m] = D;
     }
     spr_off[nV] = (u32)spr_nbr.size();
@@ -1392,6 +1588,49 @@ ys_status ys_scene_pack(ys_scene* s) {
     }
     YS_CK(cudaMemcpy(s->dmeshes.p, md.data(), sizeof(MeshDev) * md.size(), cudaMemcpyHostToDevice));
     s->hmeshes = md;
+    // Analytic marker pairs: every (cloth query mesh with a tree, analytic
+    // target), in target order; pair p owns threads [w, w + nV) of the staged
+    // analytic kernel.
+    {
+        std::vector<uint4> ap;
+        std::vector<u32> tp(std::max<size_t>(targets.size(), 1), NO_PAIR);
+        u32 vb = 0;
+        for (size_t m = 0; m < md.size(); ++m) {
+            const u32 f = md[m].flags;
+            if (!(f & MF_QUERY) || !(f & MF_CLOTH) || !(f & MF_TREE) || md[m].nV == 0) continue;
+            for (u32 k = md[m].tgt_begin; k < md[m].tgt_end; ++k) {
+                const u32 t = targets[k];
+                if (!(md[t].flags & MF_ANALYTIC)) continue;
+                tp[k] = (u32)ap.size();
+                ap.push_back(make_uint4((u32)m, t, md[t].shape, vb));
+                vb += md[m].nV;
+            }
+        }
+        s->npairs = (u32)ap.size();
+        s->apair_total = vb;
+        YS_CK(s->tpair.alloc(tp.size()));
+        YS_CK(cudaMemcpy(s->tpair.p, tp.data(), 4 * tp.size(), cudaMemcpyHostToDevice));
+        if (!ap.empty()) {
+            YS_CK(s->apairs.alloc(ap.size()));
+            YS_CK(cudaMemcpy(s->apairs.p, ap.data(), sizeof(uint4) * ap.size(), cudaMemcpyHostToDevice));
+            YS_CK(s->markers.alloc(3 * ap.size()));
+            YS_CK(cudaMemset(s->markers.p, 0, 4 * 3 * ap.size()));
+        }
+        if (!s->shape_mesh.empty()) {
+            // seeded at pack (Scene::packAnalyticShapes, scene.hpp:762-781):
+            // the first frame's refresh still takes prev = cur
+            YS_CK(s->dshapes.alloc(s->shape_mesh.size()));
+            DShape z;
+            memset(&z, 0, sizeof(z));
+            s->hshapes.assign(s->shape_mesh.size(), z);
+            s->analytic_primed = false;
+            s->shapes_uploaded = false;
+            ys_status r = refresh_shapes(s);
+            if (r) return r;
+            s->analytic_primed = false;
+            YS_CK(cudaStreamSynchronize(s->stream));
+        }
+    }
     YS_CK(cudaMemset(s->status.p, 0, 4));
     YS_CK(cudaMemset(s->maxext.p, 0, 4 * s->meshes.size()));
     YS_CK(cudaMemset(s->counters.p, 0, 8 * s->counters.n));
@@ -1406,7 +1645,8 @@ ys_status ys_scene_pack(ys_scene* s) {
         const bool selfQ = s->P.self_mode == YS_SELF_BVH ||
                            (s->P.self_mode == YS_SELF_HASH && (H.flags & MF_CLOTH) && (H.flags & MF_SELF));
         if (selfQ) descended[m] = 1;
-        for (u32 k = md[m].tgt_begin; k < md[m].tgt_end; ++k) descended[targets[k]] = 1;
+        for (u32 k = md[m].tgt_begin; k < md[m].tgt_end; ++k)
+            if (!(md[targets[k]].flags & MF_ANALYTIC)) descended[targets[k]] = 1;
         if (md[m].tgt_end > md[m].tgt_begin) rootUsed[m] = 1;
     }
     for (size_t m = 0; m < s->meshes.size(); ++m) {
@@ -1555,6 +1795,36 @@ ys_status ys_scene_set_tree_layout(ys_scene* s, int layout) {
     if (s->packed) return fail(YS_ERR_STATE, "ys_scene_set_tree_layout: call before ys_scene_pack");
     if (layout != YS_TREE_REFERENCE && layout != YS_TREE_CUBE) return fail(YS_ERR_BAD_ARG, "unknown tree layout");
     s->tree_layout = layout;
+    return YS_OK;
+}
+
+ys_status ys_scene_set_collider(ys_scene* s, int mesh, uint32_t kind, const float center[3], const float half[3],
+                                const float rot_wxyz[4]) {
+    if (!s) return fail(YS_ERR_BAD_ARG, "null scene");
+    if (mesh < 0 || (size_t)mesh >= s->meshes.size()) return fail(YS_ERR_BAD_ARG, "ys_scene_set_collider: bad mesh");
+    if (kind > COL_PLANE) return fail(YS_ERR_BAD_ARG, "ys_scene_set_collider: unknown collider kind");
+    if (!center || !rot_wxyz || (!half && kind != COL_PLANE && kind != COL_MESH))
+        return fail(YS_ERR_BAD_ARG, "ys_scene_set_collider: null pose");
+    HostMesh& H = s->meshes[mesh];
+    if (kind != COL_MESH && (H.d.behavior == YS_TRIANGULAR_CLOTH || H.d.behavior == YS_FAST_GRID_CLOTH))
+        return fail(YS_ERR_BAD_ARG, "ys_scene_set_collider: a cloth mesh cannot be an analytic collider");
+    if (s->packed && kind != H.collider)
+        return fail(YS_ERR_STATE, "ys_scene_set_collider: the collider kind is fixed at ys_scene_pack");
+    H.collider = kind;
+    for (int k = 0; k < 3; ++k) H.pose[k] = center[k];
+    for (int k = 0; k < 3; ++k) H.pose[3 + k] = half ? half[k] : 0.f;
+    for (int k = 0; k < 4; ++k) H.pose[6 + k] = rot_wxyz[k];
+    return YS_OK;
+}
+
+ys_status ys_scene_colliders(ys_scene* s, ys_analytic_shape* out, uint32_t cap, uint32_t* num_out) {
+    if (!s) return fail(YS_ERR_BAD_ARG, "null scene");
+    const u32 n = (u32)s->hshapes.size();
+    if (num_out) *num_out = n;
+    if (out) {
+        static_assert(sizeof(ys_analytic_shape) == sizeof(AShape), "ys_analytic_shape layout");
+        for (u32 k = 0; k < n && k < cap; ++k) memcpy(&out[k], &s->hshapes[k].s, sizeof(AShape));
+    }
     return YS_OK;
 }
 
@@ -2094,6 +2364,8 @@ ys_status ys_adjoint_create(ys_adjoint** out, ys_scene* s, int mesh, uint32_t st
         if ((int)m != mesh && (s->meshes[m].flags & MF_CLOTH))
             return fail(YS_ERR_BAD_ARG, "the adjoint scene holds one cloth (obstacles are static)");
     if (s->P.self_mode != YS_SELF_OFF) return fail(YS_ERR_BAD_ARG, "the adjoint needs self-collision off");
+    if (!s->shape_mesh.empty())
+        return fail(YS_ERR_BAD_ARG, "the adjoint differentiates triangle obstacles, not analytic colliders");
     ys_adjoint* a = new ys_adjoint();
     a->s = s; a->mesh = mesh; a->T = steps; a->K = checkpoint_every;
     a->nseg = (steps + checkpoint_every - 1) / checkpoint_every;

@@ -35,6 +35,9 @@ class Mesh:
     grid_n: int = 0
     grid_rest: tuple = (0.0,) * 6
     group: int = 0
+    # analytic collider: (kind, centre (3), local half extents (3), orientation
+    # (w, x, y, z)) or None for a triangle collider
+    collider: Optional[tuple] = None
 
     @property
     def nV(self) -> int:
@@ -189,6 +192,60 @@ def obstacle_sphere(level: int, radius: float, center=(0.0, 0.0, 0.0), amplitude
                 v=np.zeros_like(x), mass=np.zeros(len(x), F32), mask=np.ones(len(x), F32))
 
 
+# ---------------------------------------------------------------- analytic colliders
+# AnalyticShape record (collision_pod.hpp:295-309), the layout of
+# ys_analytic_shape.
+SHAPE_DTYPE = np.dtype([("cr", "<f4", 4), ("he", "<f4", 4), ("rq", "<f4", 4), ("pc", "<f4", 4), ("prq", "<f4", 4),
+                        ("kind", "<u4"), ("obj", "<u4"), ("beh", "<u4"), ("flags", "<u4")])
+assert SHAPE_DTYPE.itemsize == 96
+
+
+def quat_axis_angle(axis, angle: float):
+    """(w, x, y, z) of a rotation by angle (radians) about axis."""
+    a = np.asarray(axis, np.float64)
+    a = a / np.linalg.norm(a)
+    h = 0.5 * angle
+    return (float(np.cos(h)), *(float(c) for c in a * np.sin(h)))
+
+
+def quat_rotate(q, v: np.ndarray) -> np.ndarray:
+    """Rotate rows of v by the unit quaternion q = (w, x, y, z) (float64)."""
+    w, qv = q[0], np.asarray(q[1:], np.float64)
+    v = np.asarray(v, np.float64)
+    t = 2.0 * np.cross(qv, v)
+    return v + w * t + np.cross(qv, t)
+
+
+def fit_local_half(x: np.ndarray, center, q) -> tuple:
+    """Scene::fitAnalyticLocalHalf's geometry fit (scene.hpp:622-640): the
+    vertices in the collider's frame (inverse rotation about the centre),
+    per-axis max |coordinate| -- the smallest origin-centred box holding the
+    mesh."""
+    qi = (q[0], -q[1], -q[2], -q[3])
+    loc = quat_rotate(qi, np.asarray(x, np.float64) - np.asarray(center, np.float64))
+    return tuple(float(h) for h in np.abs(loc).max(axis=0))
+
+
+def analytic_collider(kind: int, center, half=(0.0, 0.0, 0.0), q=(1.0, 0.0, 0.0, 0.0), level: int = 2) -> Mesh:
+    """A static analytic collider (behavior Float, collidable) with a coarse
+    triangle surface of its shape for display: an ellipsoid from an
+    icosphere, a box or cylinder from a scaled icosphere, a plane from a
+    2 x 2 quad.  Only the shape (kind, centre, half extents, orientation)
+    takes part in the collision path."""
+    from ._lib import COLLIDER_PLANE, FLOAT, MESH_COLLIDABLE, MESH_STATIC
+    if kind == COLLIDER_PLANE:
+        v = np.array([[-1, 0, -1], [1, 0, -1], [1, 0, 1], [-1, 0, 1]], np.float64)
+        f = np.array([[0, 2, 1], [0, 3, 2]], np.uint32)
+    else:
+        v, f = icosphere(level)
+        v = v * np.asarray(half, np.float64)
+    x = (quat_rotate(q, v) + np.asarray(center, np.float64)).astype(F32)
+    return Mesh(behavior=FLOAT, flags=MESH_STATIC | MESH_COLLIDABLE, x=x, facets=np.asarray(f, np.uint32),
+                v=np.zeros_like(x), mass=np.zeros(len(x), F32), mask=np.ones(len(x), F32),
+                collider=(int(kind), tuple(float(c) for c in center), tuple(float(h) for h in half),
+                          tuple(float(c) for c in q)))
+
+
 # ---------------------------------------------------------------- configs
 def config_c1(seed: int = 1, P: int = 64, level: int = 4, height: float = 1.0) -> SceneSpec:
     """Plain FastGridCloth 64x64 over a static level-4 icosphere (r 0.3);
@@ -205,6 +262,24 @@ def config_c1(seed: int = 1, P: int = 64, level: int = 4, height: float = 1.0) -
                  thickness=1e-3, grid_n=P, grid_rest=fast_grid_rest(x, P))
     obst = obstacle_sphere(level, 0.3)
     return SceneSpec("c1_fastgrid64_ico4", Params(subh=1.0 / 6000.0, substeps=10), [cloth, obst], seed)
+
+
+def config_c1_analytic(seed: int = 1, P: int = 64, height: float = 1.0) -> SceneSpec:
+    """C1's FastGridCloth falling on analytic colliders instead of a triangle
+    obstacle: a sphere (r 0.3) at the origin, a box tilted 30 degrees, a
+    cylinder on its side and a floor plane at y = -0.35 (the analytic
+    collider path: BroadPhase markers + narrow_pt_analytic)."""
+    from ._lib import COLLIDER_BOX, COLLIDER_CYLINDER, COLLIDER_PLANE, COLLIDER_SPHERE
+    spec = config_c1(seed=seed, P=P, height=height)
+    cloth = spec.meshes[0]
+    shapes = [
+        analytic_collider(COLLIDER_SPHERE, (0.0, 0.0, 0.0), (0.3, 0.3, 0.3)),
+        analytic_collider(COLLIDER_BOX, (0.32, -0.1, 0.2), (0.12, 0.08, 0.1), quat_axis_angle((0, 0, 1), np.pi / 6)),
+        analytic_collider(COLLIDER_CYLINDER, (-0.3, -0.15, -0.25), (0.1, 0.15, 0.1),
+                          quat_axis_angle((1, 0, 0), np.pi / 2)),
+        analytic_collider(COLLIDER_PLANE, (0.0, -0.35, 0.0)),
+    ]
+    return SceneSpec(f"c1_fastgrid{P}_analytic", spec.params, [cloth] + shapes, seed)
 
 
 def config_c2(seed: int = 2, P: int = 512, level: int = 7, height: float = 0.37, self_mode: int = 1,

@@ -89,6 +89,8 @@ class Scene:
                               (C.c_float * 6)(*m.grid_rest), m.group)
             idx = C.c_int()
             _lib.check(self.lib.ys_scene_add_mesh(self.h, C.byref(d), C.byref(idx)), "ys_scene_add_mesh")
+            if m.collider is not None:
+                self.set_collider(idx.value, *m.collider)
         if tree_layout is not None:
             _lib.check(self.lib.ys_scene_set_tree_layout(self.h, int(tree_layout)), "ys_scene_set_tree_layout")
         self.nV = spec.nV
@@ -105,6 +107,23 @@ class Scene:
         ms = (C.c_float * 3)()
         _lib.check(self.lib.ys_scene_autotune(self.h, reps, C.byref(chosen), ms), "ys_scene_autotune")
         return chosen.value, list(ms)
+
+    def set_collider(self, mesh: int, kind: int, center, half=(0.0, 0.0, 0.0), q=(1.0, 0.0, 0.0, 0.0)):
+        """Analytic collider kind and pose of a mesh (before pack: declares
+        it; after: moves it from the next frame on)."""
+        c = (C.c_float * 3)(*center)
+        h = (C.c_float * 3)(*half)
+        r = (C.c_float * 4)(*q)
+        _lib.check(self.lib.ys_scene_set_collider(self.h, mesh, kind, c, h, r), "ys_scene_set_collider")
+
+    def colliders(self) -> np.ndarray:
+        """The analytic shape table as of the last frame start."""
+        from .generators import SHAPE_DTYPE
+        n = C.c_uint32()
+        _lib.check(self.lib.ys_scene_colliders(self.h, None, 0, C.byref(n)), "ys_scene_colliders")
+        out = np.zeros(n.value, SHAPE_DTYPE)
+        _lib.check(self.lib.ys_scene_colliders(self.h, _ptr(out), n.value, C.byref(n)), "ys_scene_colliders")
+        return out
 
     def set_fused_variant(self, min_blocks: int):
         _lib.check(self.lib.ys_scene_set_fused_variant(self.h, min_blocks), "ys_scene_set_fused_variant")
