@@ -93,6 +93,7 @@ struct StepArgs {
     const uint4* apairs;
     const u32* mk_act;
     u32 npairs, apair_total;
+    u32 analytic;  // the scene has analytic colliders
     float subh, kair, kd, gx, gy, gz, margin, band, radius;
     u32 nV, self_mode, record, cap;
     u32* status;
@@ -152,6 +153,8 @@ __device__ __forceinline__ u32 query_vertex(const StepArgs& A, u32 g, u32 m, con
     for (u32 k = M.tgt_begin; k < M.tgt_end; ++k) {
         const u32 t = A.targets[k];
         const MeshDev T = A.meshes[t];
+        // an analytic collider has no live tree (its pairs are markers)
+        if ((T.flags & MF_ANALYTIC) || T.nF == 0) continue;
         if (!root_overlap(A.nodes + M.node_off, A.nodes + T.node_off)) continue;
         f3 qmn = xc - mk(mg, mg, mg), qmx = xc + mk(mg, mg, mg);
         st |= descend(A, T, qmn, qmx, [&](u32 f) {
@@ -293,7 +296,9 @@ __device__ __noinline__ bool analytic_contact(const DShape* S, f3 pcur, f3 pprev
 // WIDE: descend the 4-wide form of the trees (cube layout), else the binary one.
 // MINB: CTAs per SM the registers are capped for (8: 64 registers, 6: 80,
 // 4: no cap); the results do not depend on it (ys_scene_autotune picks one).
-template <bool WIDE, int MINB>
+// ANA: the scene has analytic colliders (without them the kernel carries no
+// analytic branch).
+template <bool WIDE, int MINB, bool ANA>
 __global__ void __launch_bounds__(128, MINB) k_fused(StepArgs A) {
     __shared__ WarpWork wq[FUSED_WARPS];
     const u32 lane = threadIdx.x & 31u;
@@ -357,7 +362,7 @@ __global__ void __launch_bounds__(128, MINB) k_fused(StepArgs A) {
         while (tk < te) {
             const u32 k = tk++;
             const u32 t = A.targets[k];
-            if (A.meshes[t].flags & MF_ANALYTIC) {
+            if (ANA && (A.meshes[t].flags & MF_ANALYTIC)) {
                 // narrowAnalytic for a marked (cloth, collider) pair: this
                 // vertex against the shape, no descent
                 const u32 p = A.tpair[k];
@@ -555,16 +560,22 @@ __global__ void __launch_bounds__(128, MINB) k_fused(StepArgs A) {
 
 static constexpr int FUSED_VARIANTS[3] = {8, 6, 4};  // register caps, as CTAs per SM
 
+template <bool ANA>
+void launch_fused_t(const StepArgs& A, dim3 g, dim3 b, cudaStream_t st, int minBlocks) {
+    switch ((A.wide ? 0 : 10) + minBlocks) {
+        case 8: k_fused<true, 8, ANA><<<g, b, 0, st>>>(A); break;
+        case 6: k_fused<true, 6, ANA><<<g, b, 0, st>>>(A); break;
+        case 4: k_fused<true, 4, ANA><<<g, b, 0, st>>>(A); break;
+        case 18: k_fused<false, 8, ANA><<<g, b, 0, st>>>(A); break;
+        case 16: k_fused<false, 6, ANA><<<g, b, 0, st>>>(A); break;
+        default: k_fused<false, 4, ANA><<<g, b, 0, st>>>(A); break;
+    }
+}
+
 void launch_fused(const StepArgs& A, u32 nV, cudaStream_t st, int minBlocks) {
     const dim3 g(ceil_div(nV, 128)), b(128);
-    switch ((A.wide ? 0 : 10) + minBlocks) {
-        case 8: k_fused<true, 8><<<g, b, 0, st>>>(A); break;
-        case 6: k_fused<true, 6><<<g, b, 0, st>>>(A); break;
-        case 4: k_fused<true, 4><<<g, b, 0, st>>>(A); break;
-        case 18: k_fused<false, 8><<<g, b, 0, st>>>(A); break;
-        case 16: k_fused<false, 6><<<g, b, 0, st>>>(A); break;
-        default: k_fused<false, 4><<<g, b, 0, st>>>(A); break;
-    }
+    if (A.analytic) launch_fused_t<true>(A, g, b, st, minBlocks);
+    else launch_fused_t<false>(A, g, b, st, minBlocks);
 }
 
 // ------------------------------------------------------------------ staged
@@ -960,6 +971,7 @@ StepArgs make_args(ys_scene* s) {
     A.mk_act = s->markers.p ? s->markers.p + 2 * (size_t)s->npairs : nullptr;
     A.npairs = s->npairs;
     A.apair_total = s->apair_total;
+    A.analytic = s->shape_mesh.empty() ? 0u : 1u;
     A.radius = s->P.radius;
     A.subh = s->P.subh; A.kair = s->P.kair; A.kd = s->P.kd;
     A.gx = s->P.gravity[0]; A.gy = s->P.gravity[1]; A.gz = s->P.gravity[2];
