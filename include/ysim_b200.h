@@ -92,6 +92,16 @@ typedef struct ys_analytic_shape {
 #define YS_TREE_REFERENCE 0
 #define YS_TREE_CUBE 1
 
+/* Tree builder.  KARRAS: buildTree_Tri (src/metal/bvh.metal:352-393), then
+ * the boxes bottom-up (the reference default).  APETREI: agglomerativeBuild_Tri
+ * + agglomerativeSwapRoot (bvh.metal:884-1199; BVH::useAgglomerative,
+ * bvh.hpp:292-295): topology and boxes in one pass, one thread per leaf
+ * climbing to the root, the root moved to slot 0.  Its tree is the
+ * reference's Apetrei tree node for node; runs of equal Morton codes split by
+ * primitive index, so every node has one parent. */
+#define YS_BUILD_KARRAS 0
+#define YS_BUILD_APETREI 1
+
 /* Simulator / SymplecticSystem parameters: subh, kair, kd
  * (symplectic_system.hpp:191-198), gravity (Scene::environment), margin and
  * radius (simulator.hpp:180-181), substeps per frame, BVH rebuild period in
@@ -208,6 +218,10 @@ ys_status ys_scene_colliders(ys_scene* s, ys_analytic_shape* out, uint32_t cap, 
  * builds; call between ys_scene_create and ys_scene_pack.  Replaces the
  * Morton normalisation inside BVH<..>::build (include/sim/bvh.hpp:1194-1301). */
 ys_status ys_scene_set_tree_layout(ys_scene* s, int layout);
+/* Builder (YS_BUILD_KARRAS / YS_BUILD_APETREI) of every tree the scene builds
+ * (BroadPhase::build with Simulator::useAgglomerativeBVH, bvh.hpp:2322-2325);
+ * call before ys_scene_pack. */
+ys_status ys_scene_set_tree_builder(ys_scene* s, int builder);
 ys_status ys_scene_sync(ys_scene* s);
 /* CUDA stream of the scene (cudaStream_t) as void*. */
 ys_status ys_scene_stream(ys_scene* s, void** stream_out);
@@ -284,6 +298,9 @@ ys_status ys_lbvh_destroy(ys_lbvh* t);
  * index) key determineRange already orders by, so every node has one parent
  * and a query reports every overlapping leaf exactly once. */
 ys_status ys_lbvh_set_split(ys_lbvh* t, int consistent);
+/* Builder of the next builds (YS_BUILD_KARRAS, the default, or
+ * YS_BUILD_APETREI; the Karras split option does not apply to Apetrei). */
+ys_status ys_lbvh_set_builder(ys_lbvh* t, int builder);
 /* build(): scene box, Morton, radix sort, Karras, leaves, bottom-up
  * (bvh.hpp:1194-1301). */
 ys_status ys_lbvh_build(ys_lbvh* t, const float* d_x, uint32_t num_vertices, const uint32_t* d_facets,

@@ -39,6 +39,8 @@ def lib():
             "yso_leaves": (None, [vp, vp, C.c_float, C.c_int, vp, C.c_uint32, vp]),
             "yso_bottom_up": (None, [vp, C.c_uint32]),
             "yso_build_tree": (None, [vp, C.c_uint32, vp, C.c_uint32, vp, vp, vp, vp]),
+            "yso_build_tree_apetrei": (C.c_int, [vp, C.c_uint32, vp, C.c_uint32, vp, vp, vp, vp]),
+            "yso_scene_set_builder": (None, [vp, C.c_int]),
             "yso_query_points": (C.c_uint64, [vp, C.c_uint32, vp, vp, C.c_uint32, C.c_float, C.c_int, vp,
                                               C.c_uint64]),
             "yso_self_hash": (C.c_uint64, [vp, vp, C.c_uint32, vp, C.c_uint32, C.c_float, vp, C.c_uint64]),
@@ -96,15 +98,19 @@ def max_threads() -> int:
     return lib().yso_max_threads()
 
 
-def build_tree(x: np.ndarray, F: np.ndarray):
+def build_tree(x: np.ndarray, F: np.ndarray, builder: int = 0):
+    """Box, Morton, sort and the Karras (builder 0) or Apetrei (1) build."""
     x = np.ascontiguousarray(x, np.float32)
     F = np.ascontiguousarray(F, np.uint32)
     n = len(F)
     nodes = np.zeros(2 * n - 1, NODE_DTYPE)
-    parent = np.zeros(2 * n - 1, np.int32)
+    parent = np.full(2 * n - 1, -1, np.int32)
     codes = np.zeros(n, np.uint32)
     idx = np.zeros(n, np.uint32)
-    lib().yso_build_tree(P(x), len(x), P(F), n, P(nodes), P(parent), P(codes), P(idx))
+    if builder == 1:
+        lib().yso_build_tree_apetrei(P(x), len(x), P(F), n, P(nodes), P(parent), P(codes), P(idx))
+    else:
+        lib().yso_build_tree(P(x), len(x), P(F), n, P(nodes), P(parent), P(codes), P(idx))
     return nodes, parent, codes, idx
 
 
@@ -257,11 +263,12 @@ def narrow_analytic(x, xp, state_off, beh, shapes, pairs, radius, thickness, cap
 class OracleScene:
     """CPU restatement of the packed scene + Simulator::update substeps."""
 
-    def __init__(self, spec):
+    def __init__(self, spec, builder: int = 0):
         p = spec.params
         fp = np.array([p.subh, p.kair, p.kd, *p.gravity, p.margin, p.radius], np.float32)
         ip = np.array([p.substeps, p.rebuild_frames, p.self_mode, p.cols_per_point], np.uint32)
         self.h = lib().yso_scene_new(P(fp), P(ip))
+        lib().yso_scene_set_builder(self.h, builder)
         self.spec = spec
         self._keep = []
         for m in spec.meshes:

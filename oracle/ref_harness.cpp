@@ -14,6 +14,7 @@
 // designed (its arrival counters and fences are real).
 #include <cstdint>
 #include <cstring>
+#include <vector>
 
 #include "metal_shim.h"
 using namespace metal;
@@ -74,6 +75,27 @@ void yref_swept_leaves(const float* x, const float* v, const uint32_t* F, uint32
     for (long long i = 0; i < (long long)n; ++i)
         buildSweptLeaf_Tri((const packed_float3*)x, (const packed_float3*)v, (const packed_uint3*)F, np, dt,
                            (const MortonNode*)mortons, (BVHNode*)nodes, (uint)i);
+}
+
+// zeroVisitCounts over the N-1 flags + agglomerativeBuild_Tri (one thread per
+// leaf, run one after another: a node's second arrival always comes from a
+// later thread) + agglomerativeSwapRoot (BVH::agglomerativeBuildGPU /
+// agglomerativeSwapRootGPU, bvh.hpp:649-694).  Returns the pre-swap root slot.
+int32_t yref_agglomerative(const float* x, const uint32_t* F, uint32_t n, const uint32_t* mortons, void* nodes,
+                           int32_t* parent) {
+    const int np = (int)n;
+    const uint ni = n > 1 ? n - 1 : 1;
+    std::vector<uint32_t> flags(ni, 0u);
+    std::vector<int> rl(ni, 0), rr(ni, 0);
+    atomic_int root;
+    root.v.store(-1);
+    for (uint i = 0; i < n; ++i)
+        agglomerativeBuild_Tri((const packed_float3*)x, (const packed_uint3*)F, np, (const MortonNode*)mortons,
+                               (BVHNode*)nodes, (int*)parent, (atomic_uint*)flags.data(), rl.data(), rr.data(), &root,
+                               i);
+    const int k = root.v.load();
+    agglomerativeSwapRoot((BVHNode*)nodes, (int*)parent, &k, np, 0u);
+    return k;
 }
 
 // zeroVisitCounts + bottomUpBoxes, leaf threads concurrent.

@@ -33,6 +33,7 @@ def lib():
             "yref_leaves": (None, [vp, vp, u32, vp, vp]),
             "yref_swept_leaves": (None, [vp, vp, vp, u32, f32, vp, vp]),
             "yref_bottom_up": (None, [vp, vp, u32, vp]),
+            "yref_agglomerative": (C.c_int32, [vp, vp, u32, vp, vp, vp]),
             "yref_query_points": (u32, [vp, u32, vp, vp, u32, f32, u32, u32, vp, u32, vp]),
             "yref_narrow": (u32, [vp, u32, vp, vp, vp, vp, vp, vp, f32, f32, vp, vp, u32]),
             "yref_tri_forces": (None, [vp, vp, vp, vp, vp, vp, f32, f32, f32, vp, vp, vp, vp, vp, vp, vp, vp, vp,
@@ -111,6 +112,17 @@ def narrow(rows, x, voff, F, foff, vaf, vaf_off, radius, thickness, xprev, cap=N
                           P(c32(F, np.uint32)), P(c32(foff, np.uint32)), P(c32(vaf, np.uint32)),
                           P(c32(vaf_off, np.uint32)), radius, thickness, P(c32(xprev)), P(out), cap)
     return out[: min(n, cap)]
+
+
+def agglomerative(x, F, codes, idx):
+    """agglomerativeBuild_Tri + agglomerativeSwapRoot over sorted (code, index)
+    pairs: (nodes, parent, pre-swap root slot)."""
+    n = len(codes)
+    mortons = np.ascontiguousarray(np.stack([codes, idx], 1), np.uint32)
+    nodes = np.zeros(2 * n - 1, NODE_DTYPE)
+    parent = np.full(2 * n - 1, -1, np.int32)
+    k = lib().yref_agglomerative(P(c32(x)), P(c32(F, np.uint32)), n, P(mortons), P(nodes), P(parent))
+    return nodes, parent, int(k)
 
 
 def narrow_analytic(x, xprev, voff, shapes, oid, shape_index, cloth_beh, radius, thickness, rot_margin, cap=None):

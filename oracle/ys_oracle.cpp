@@ -212,6 +212,66 @@ void leaves(const float* x, const float* v, float dt, int swept, const u32* F, u
         nset(L, lo, hi);
     }
 }
+// ---------------------------------------------------------------- K2 Apetrei
+// agglomerativeBuild_Tri + agglomerativeSwapRoot (bvh.metal:884-1199).  Leaf i
+// of the sorted order sits at slot N-1+i with its triangle's box.  Each leaf
+// climbs: at range [L, R] it joins the side whose neighbouring key differs
+// less (code XOR, ties by index XOR; a range touching an end can only grow the
+// other way), so its parent is slot R (it is R's left child) or slot L-1 (the
+// right child).  The first arrival at a node stops; the second combines the
+// two boxes and climbs on with the node's full range.  The root, wherever it
+// lands, is then moved to slot 0 and every link to either slot patched.
+// Leaves run in order: a node's second arrival always comes from a later
+// leaf, so this is the concurrent build's result.  Returns the slot the root
+// was built in.
+int apetrei_topology(const float* x, const u32* F, const u32* codes, const u32* idx, u32 n, Node* tree, i32* parent) {
+    for (u32 i = 0; i < n; ++i) { tree[n - 1 + i].a = -1; tree[n - 1 + i].b = (i32)idx[i]; }
+    leaves(x, nullptr, 0.f, 0, F, n, tree);
+    if (n <= 1) return 0;
+    const int N = (int)n;
+    std::vector<u32> arrivals(n - 1, 0);
+    std::vector<int> lo(n - 1, 0), hi(n - 1, 0);
+    int root = -1;
+    for (int id = 0; id < N; ++id) {
+        int node = N - 1 + id, L = id, R = id;
+        for (int step = 0; step < 2 * N; ++step) {
+            if (L == 0 && R == N - 1) { root = node; break; }
+            bool right;
+            if (L == 0) right = true;
+            else if (R == N - 1) right = false;
+            else {
+                const u32 dr = codes[R] ^ codes[R + 1], dl = codes[L - 1] ^ codes[L];
+                right = (dr != dl) ? dr < dl : (idx[R] ^ idx[R + 1]) < (idx[L - 1] ^ idx[L]);
+            }
+            const int p = right ? R : L - 1;
+            if (right) { tree[p].a = node; lo[p] = L; }
+            else { tree[p].b = node; hi[p] = R; }
+            parent[node] = p;
+            if (arrivals[p]++ == 0) break;
+            const Node& A = tree[tree[p].a];
+            const Node& B = tree[tree[p].b];
+            nset(tree[p], vmin(nmin(A), nmin(B)), vmax(nmax(A), nmax(B)));
+            node = p; L = lo[p]; R = hi[p];
+        }
+    }
+    const int k = root;
+    if (k > 0) {
+        const Node Rn = tree[k], O = tree[0];
+        const int p0 = parent[0];
+        const int ra = Rn.a == 0 ? k : Rn.a, rb = Rn.b == 0 ? k : Rn.b;
+        tree[0] = Rn; tree[0].a = ra; tree[0].b = rb;
+        tree[k] = O;
+        parent[O.a] = k; parent[O.b] = k;
+        parent[ra] = 0; parent[rb] = 0;
+        if (p0 != k) {
+            if (tree[p0].a == 0) tree[p0].a = k; else tree[p0].b = k;
+            parent[k] = p0;
+        }
+        parent[0] = -1;
+    }
+    return root;
+}
+
 // bottomUpCombine (bvh.hpp:1534-1553): parent = min/max of children, exact.
 void bottom_up(Node* tree, u32 nNodes) {
     if (nNodes == 0) return;
@@ -955,6 +1015,7 @@ struct Scene {
     std::vector<Shape> shapes;
     bool primed = false;
     std::vector<std::pair<u32, u32>> mk_fresh, mk_held, mk_pairs;
+    int builder = 0;  // 0 Karras (buildTree_Tri + bottomUpBoxes), 1 Apetrei (agglomerativeBuild_Tri)
 };
 
 // Scene::refreshAnalyticShapes (scene.hpp:659-745).
@@ -1000,9 +1061,13 @@ void build_tree(Scene& S, Mesh& M) {
     radix_sort(M.codes.data(), M.idx.data(), n);
     M.tree.assign(2 * (size_t)n - 1, Node{});
     M.parent.assign(2 * (size_t)n - 1, -1);
-    karras_topology(M.codes.data(), M.idx.data(), n, M.tree.data(), M.parent.data());
-    leaves(x, nullptr, 0.f, 0, M.F.data(), n, M.tree.data());
-    bottom_up(M.tree.data(), 2 * n - 1);
+    if (S.builder == 1) {
+        apetrei_topology(x, M.F.data(), M.codes.data(), M.idx.data(), n, M.tree.data(), M.parent.data());
+    } else {
+        karras_topology(M.codes.data(), M.idx.data(), n, M.tree.data(), M.parent.data());
+        leaves(x, nullptr, 0.f, 0, M.F.data(), n, M.tree.data());
+        bottom_up(M.tree.data(), 2 * n - 1);
+    }
     M.built = true;
 }
 
@@ -1367,6 +1432,18 @@ void yso_build_tree(const float* x, u32 nV, const u32* F, u32 nF, void* tree, in
     leaves(x, nullptr, 0.f, 0, F, nF, (Node*)tree);
     bottom_up((Node*)tree, 2 * nF - 1);
 }
+
+// The same with the Apetrei build; returns the slot the root was built in.
+int yso_build_tree_apetrei(const float* x, u32 nV, const u32* F, u32 nF, void* tree, int32_t* parent, u32* codes,
+                           u32* idx) {
+    if (nF == 0) return -1;
+    float box[6]; scene_box(x, nV, box);
+    fill_mortons(x, F, nF, box, codes, idx);
+    radix_sort(codes, idx, nF);
+    return apetrei_topology(x, F, codes, idx, nF, (Node*)tree, parent);
+}
+// Tree builder of a scene's meshes: 0 Karras, 1 Apetrei.
+void yso_scene_set_builder(void* h, int builder) { ((Scene*)h)->builder = builder; }
 
 // Point query: writes (point, tri) pairs in vertex-major DFS order; returns the
 // number of candidates (pairs beyond cap are counted, not written).

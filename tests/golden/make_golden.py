@@ -9,7 +9,9 @@ without the reference.  Inputs are seeded synthetic data of this repository's
 generators; outputs are the reference kernels' results:
   morton_tree.npz -- fillMortons_Tri codes, stable sort, buildTree_Tri topology,
                      bottomUpBoxes boxes, buildSweptLeaf_Tri refit, queryPoints
-                     pairs (inclusive AABB test, h = 1e-3 and a self query);
+                     pairs (inclusive AABB test, h = 1e-3 and a self query),
+                     and the agglomerativeBuild_Tri + agglomerativeSwapRoot
+                     tree (agg_*);
   substep_*.npz   -- one mid-drape substep of a small scene: broad rows (the
                      oracle's), narrow_pt_tri contacts, the cloth's spring
                      forces and integrate_cloth(_grid) positions / velocities;
@@ -61,6 +63,9 @@ def morton_tree():
         self_q = name == "grid"
         margin = np.float32(0.03 if self_q else 0.02)
         rows, n, _ = R.query_points(q, f, swept, margin, 0, 0 if self_q else 1)
+        an, ap, _ = R.agglomerative(x, f, codes, idx)
+        out.update({f"{name}_agg_a": an["a"], f"{name}_agg_b": an["b"], f"{name}_agg_mn": an["mn"],
+                    f"{name}_agg_mx": an["mx"], f"{name}_agg_parent": ap})
         out.update({f"{name}_x": x, f"{name}_f": f, f"{name}_q": q, f"{name}_v": v, f"{name}_box": box,
                     f"{name}_codes": codes, f"{name}_idx": idx, f"{name}_a": nodes["a"], f"{name}_b": nodes["b"],
                     f"{name}_mn": nodes["mn"], f"{name}_mx": nodes["mx"], f"{name}_parent": parent,

@@ -57,6 +57,30 @@ def test_gpu_lbvh_matches_golden(cuda_lib):
             _lib.check(cuda_lib.ys_lbvh_destroy(h))
 
 
+def test_gpu_apetrei_build_matches_golden(cuda_lib):
+    """ys_lbvh_set_builder(YS_BUILD_APETREI): the reference's
+    agglomerativeBuild_Tri + agglomerativeSwapRoot tree, node for node."""
+    from ysim_b200 import _lib
+    from test_gpu_parity import tree_arrays
+    g = np.load(os.path.join(GOLD, "morton_tree.npz"))
+    for name in ("soup", "grid"):
+        x, f = g[f"{name}_x"], g[f"{name}_f"]
+        h = C.c_void_p()
+        _lib.check(cuda_lib.ys_lbvh_create(C.byref(h), len(f), 0, None))
+        try:
+            _lib.check(cuda_lib.ys_lbvh_set_builder(h, _lib.BUILD_APETREI))
+            dx, df = _dev(x.reshape(-1)), _dev(f.reshape(-1).astype(np.int32))
+            _lib.check(cuda_lib.ys_lbvh_build(h, _p(dx), len(x), _p(df), len(f)))
+            nodes, parent, codes, idx = tree_arrays(cuda_lib, h)
+            assert np.array_equal(codes, g[f"{name}_codes"]) and np.array_equal(idx, g[f"{name}_idx"])
+            assert np.array_equal(nodes["a"], g[f"{name}_agg_a"]) and np.array_equal(nodes["b"], g[f"{name}_agg_b"])
+            assert np.array_equal(parent, g[f"{name}_agg_parent"])
+            assert np.array_equal(nodes["mn"], g[f"{name}_agg_mn"])
+            assert np.array_equal(nodes["mx"], g[f"{name}_agg_mx"])
+        finally:
+            _lib.check(cuda_lib.ys_lbvh_destroy(h))
+
+
 @pytest.mark.parametrize("name", ["c1", "c2hash"])
 @pytest.mark.parametrize("fused", [False, True])
 def test_gpu_substep_matches_golden(cuda_lib, name, fused):

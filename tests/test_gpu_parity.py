@@ -59,12 +59,14 @@ def test_radix_sort_bit_exact(cuda_lib, oracle, n):
     assert np.array_equal(rk, keys[o]) and np.array_equal(rv, vals[o])
 
 
-def _lbvh(cuda_lib, x, f, consistent=False):
+def _lbvh(cuda_lib, x, f, consistent=False, builder=0):
     from ysim_b200 import _lib
     h = C.c_void_p()
     _lib.check(cuda_lib.ys_lbvh_create(C.byref(h), len(f), 0, None))
     if consistent:
         _lib.check(cuda_lib.ys_lbvh_set_split(h, 1))
+    if builder:
+        _lib.check(cuda_lib.ys_lbvh_set_builder(h, builder))
     dx, df = _dev(x.reshape(-1)), _dev(f.reshape(-1).astype(np.int32))
     _lib.check(cuda_lib.ys_lbvh_build(h, _p(dx), len(x), _p(df), len(f)))
     return h, dx, df
@@ -104,8 +106,12 @@ def _tree_equal(a_nodes, b_nodes):
     assert np.array_equal(a_nodes["mx"][r].view(np.uint32), b_nodes["mx"][r].view(np.uint32))
 
 
+@pytest.mark.parametrize("builder", [0, 1], ids=["karras", "apetrei"])
 @pytest.mark.parametrize("case", ["soup", "grid", "tiny1", "tiny2", "dups"])
-def test_lbvh_build_refit_query(cuda_lib, oracle, case):
+def test_lbvh_build_refit_query(cuda_lib, oracle, case, builder):
+    """Karras (buildTree_Tri + bottomUpBoxes) or Apetrei (agglomerativeBuild_Tri
+    + agglomerativeSwapRoot) build, swept refit and queries, node for node
+    against the oracle."""
     from ysim_b200 import _lib, generators as G
     import torch
     if case == "soup":
@@ -120,12 +126,16 @@ def test_lbvh_build_refit_query(cuda_lib, oracle, case):
     else:  # identical centroids -> identical Morton codes, index tie-breaks
         x, f, q = G.soup(3000, seed=8)
         x = np.tile(x[:3], (3000, 1)).astype(np.float32)
-    h, dx, df = _lbvh(cuda_lib, x, f)
+    h, dx, df = _lbvh(cuda_lib, x, f, builder=builder)
     try:
         nodes, parent, codes, idx = tree_arrays(cuda_lib, h)
-        rn, rp, rc, ri = oracle.build_tree(x, f)
+        rn, rp, rc, ri = oracle.build_tree(x, f, builder=builder)
         assert np.array_equal(codes, rc) and np.array_equal(idx, ri)
-        assert np.array_equal(parent[1:], rp[1:])
+        if builder:
+            assert np.array_equal(parent, rp)
+            assert reachable(rn).all()  # consistent: every node reached once
+        else:
+            assert np.array_equal(parent[1:], rp[1:])
         _tree_equal(nodes, rn)
         # swept refit
         rng = np.random.default_rng(1)
@@ -177,16 +187,28 @@ def test_scene_staged_and_fused_match_oracle(cuda_lib, oracle, name, layout):
     """Rows, contacts and states equal the oracle's (which builds the
     reference's trees) under both tree layouts: the layout changes the descent
     order, never a candidate set."""
+    _scene_parity(oracle, name, layout, 0)
+
+
+@pytest.mark.parametrize("layout", [0, 1], ids=["reference_tree", "cube_tree"])
+@pytest.mark.parametrize("name", ["c1", "c2hash"])
+def test_scene_apetrei_build_matches_oracle(cuda_lib, oracle, name, layout):
+    """The same with every tree built by the Apetrei path (the oracle builds
+    the reference's Apetrei trees)."""
+    _scene_parity(oracle, name, layout, 1)
+
+
+def _scene_parity(oracle, name, layout, builder):
     from ysim_b200.scene import Scene
     spec = _small_specs()[name]
     o = _advance_to_contact(spec, 3)
     x0, v0, xp0 = o.get("x"), o.get("v"), o.get("xprev")
-    s = Scene(spec, tree_layout=layout)
+    s = Scene(spec, tree_layout=layout, tree_builder=builder)
     try:
         # both sides start at frame 0 from the same mid-drape state, so the
         # frame-0 preamble rebuilds every non-Float tree from x0 on both
         s.set("x", x0); s.set("v", v0); s.set("xprev", xp0)
-        o2 = oracle.OracleScene(spec)
+        o2 = oracle.OracleScene(spec, builder=builder)
         o2.set("x", x0); o2.set("v", v0); o2.set("xprev", xp0)
         for sub in range(spec.params.substeps + 2):
             # ---- oracle stages
@@ -217,11 +239,11 @@ def test_scene_staged_and_fused_match_oracle(cuda_lib, oracle, name, layout):
     finally:
         s.close()
     # fused path from the same state
-    s = Scene(spec, tree_layout=layout)
+    s = Scene(spec, tree_layout=layout, tree_builder=builder)
     try:
         s.set("x", x0); s.set("v", v0); s.set("xprev", xp0)
         s.set_record(True)
-        o3 = oracle.OracleScene(spec)
+        o3 = oracle.OracleScene(spec, builder=builder)
         o3.set("x", x0); o3.set("v", v0); o3.set("xprev", xp0)
         for sub in range(2 * spec.params.substeps + 3):
             o3.step(1)
@@ -238,14 +260,15 @@ def test_scene_staged_and_fused_match_oracle(cuda_lib, oracle, name, layout):
         s.close()
 
 
-def test_scene_tree_matches_oracle(cuda_lib, oracle):
+@pytest.mark.parametrize("builder", [0, 1], ids=["karras", "apetrei"])
+def test_scene_tree_matches_oracle(cuda_lib, oracle, builder):
     """With the reference layout the scene's trees are the reference's, node
-    for node (codes, order, parents, boxes)."""
+    for node (codes, order, parents, boxes), from either builder."""
     from ysim_b200 import _lib
     from ysim_b200.scene import Scene
     spec = _small_specs()["c2hash"]
-    s = Scene(spec, tree_layout=_lib.TREE_REFERENCE)
-    o = oracle.OracleScene(spec)
+    s = Scene(spec, tree_layout=_lib.TREE_REFERENCE, tree_builder=builder)
+    o = oracle.OracleScene(spec, builder=builder)
     o.stage(0)
     try:
         for m in range(len(spec.meshes)):

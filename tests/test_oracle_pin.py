@@ -212,3 +212,28 @@ def test_analytic_narrow_matches_reference_kernel(oracle):
     # the disabled collider emits nothing
     off = shapes["obj"][shapes["flags"] == 0]
     assert not np.isin(rc["tobj"], off).any()
+
+
+def _dup_soup(seed=7):
+    """Triangles clustered on 40 points: runs of equal Morton codes."""
+    rng = np.random.default_rng(seed)
+    c = rng.uniform(0, 1, (40, 3))[rng.integers(0, 40, 600)]
+    x = (c[:, None, :] + rng.normal(0, 1e-4, (600, 3, 3))).reshape(-1, 3).astype(np.float32)
+    return x, np.arange(len(x), dtype=np.uint32).reshape(-1, 3)
+
+
+def test_apetrei_build_matches_reference_kernel(oracle):
+    """agglomerativeBuild_Tri + agglomerativeSwapRoot (bvh.metal:884-1199)
+    restated: children, parents and boxes node for node, the root in slot 0,
+    one parent per node even over runs of equal codes."""
+    cases = [(x, f) for x, f, _ in _inputs()] + [_dup_soup()]
+    for x, f in cases:
+        nodes, parent, codes, idx = oracle.build_tree(x, f, builder=1)
+        rn, rp, k = refk.agglomerative(x, f, codes, idx)
+        assert np.array_equal(nodes["a"], rn["a"]) and np.array_equal(nodes["b"], rn["b"])
+        assert np.array_equal(parent, rp) and parent[0] == -1
+        _boxes_equal(nodes, rn)
+        n = len(f)
+        claims = np.bincount(np.concatenate([nodes["a"][: n - 1], nodes["b"][: n - 1]]), minlength=2 * n - 1)
+        assert claims[0] == 0 and (claims[1:] == 1).all()
+    assert len(codes) - len(np.unique(codes)) > 100  # the last case has runs of equal codes

@@ -186,6 +186,10 @@ def test_oracle_matches_golden_morton_tree(oracle):
         assert np.array_equal(sw["mn"], g[f"{name}_swept_mn"]) and np.array_equal(sw["mx"], g[f"{name}_swept_mx"])
         pairs = canon_pairs(oracle.query_points(sw, f, q, float(g[f"{name}_margin"]), bool(g[f"{name}_self"])))
         assert np.array_equal(pairs, g[f"{name}_pairs"]) and len(pairs) > 0
+        an, ap, _, _ = oracle.build_tree(x, f, builder=1)
+        assert np.array_equal(an["a"], g[f"{name}_agg_a"]) and np.array_equal(an["b"], g[f"{name}_agg_b"])
+        assert np.array_equal(ap, g[f"{name}_agg_parent"])
+        assert np.array_equal(an["mn"], g[f"{name}_agg_mn"]) and np.array_equal(an["mx"], g[f"{name}_agg_mx"])
 
 
 @pytest.mark.parametrize("name", ["c1", "c2hash"])

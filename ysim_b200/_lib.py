@@ -36,6 +36,9 @@ SELF_BVH = 2
 TREE_REFERENCE = 0  # Morton normalisation per axis, node for node the reference's tree
 TREE_CUBE = 1       # one scale for all axes (default)
 
+BUILD_KARRAS = 0    # buildTree_Tri + bottom-up boxes (reference default)
+BUILD_APETREI = 1   # agglomerativeBuild_Tri: topology and boxes in one pass
+
 # ColliderKind (ys_analytic_shape.kind)
 COLLIDER_MESH = 0
 COLLIDER_SPHERE = 1
@@ -90,6 +93,8 @@ _PROTOS = {
     "ys_scene_set_graphs": (C.c_int, [C.c_void_p, C.c_int]),
     "ys_scene_set_tree_layout": (C.c_int, [C.c_void_p, C.c_int]),
     "ys_scene_set_fused_variant": (C.c_int, [C.c_void_p, C.c_int]),
+    "ys_scene_set_tree_builder": (C.c_int, [C.c_void_p, C.c_int]),
+    "ys_lbvh_set_builder": (C.c_int, [C.c_void_p, C.c_int]),
     "ys_scene_set_collider": (C.c_int, [C.c_void_p, C.c_int, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p]),
     "ys_scene_colliders": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.POINTER(C.c_uint32)]),
     "ys_narrow_analytic": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p,

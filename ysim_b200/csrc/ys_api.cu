@@ -49,6 +49,8 @@ struct ys_lbvh {
     RefitJob* job = nullptr;
     const u32* facets = nullptr;
     bool consistent = false;  // Karras split of runs of equal codes (ys_lbvh_set_split)
+    int builder = YS_BUILD_KARRAS;  // ys_lbvh_set_builder
+    void* aggScratch = nullptr;     // Apetrei range ends and root slot
 };
 
 #define YS_CK2(call)                                                                                   \
@@ -73,6 +75,7 @@ ys_status ys_lbvh_create(ys_lbvh** out, uint32_t maxPrims, int device, void* str
     if (e == cudaSuccess) e = cudaMalloc((void**)&t->claimOff, (nn + 2) * 4);
     if (e == cudaSuccess) e = cudaMalloc((void**)&t->claims, (nn + 1) * 4);
     if (e == cudaSuccess) e = cudaMalloc(&t->karrasScratch, karras_scratch_bytes(maxPrims));
+    if (e == cudaSuccess) e = cudaMalloc(&t->aggScratch, apetrei_scratch_bytes(maxPrims));
     if (e == cudaSuccess) e = cudaMalloc((void**)&t->codes, (size_t)maxPrims * 4);
     if (e == cudaSuccess) e = cudaMalloc((void**)&t->idx, (size_t)maxPrims * 4);
     if (e == cudaSuccess) e = cudaMalloc((void**)&t->visits, (size_t)maxPrims * 4);
@@ -93,7 +96,7 @@ ys_status ys_lbvh_destroy(ys_lbvh* t) {
     if (!t) return YS_OK;
     cudaSetDevice(t->device);
     cudaStreamSynchronize(t->stream);
-    cudaFree(t->nodes); cudaFree(t->parent); cudaFree(t->claimOff); cudaFree(t->claims); cudaFree(t->karrasScratch); cudaFree(t->codes); cudaFree(t->idx); cudaFree(t->visits);
+    cudaFree(t->nodes); cudaFree(t->parent); cudaFree(t->claimOff); cudaFree(t->claims); cudaFree(t->karrasScratch); cudaFree(t->aggScratch); cudaFree(t->codes); cudaFree(t->idx); cudaFree(t->visits);
     cudaFree(t->box); cudaFree(t->status); cudaFree(t->scratch); cudaFree(t->job);
     delete t;
     return YS_OK;
@@ -118,6 +121,13 @@ ys_status ys_lbvh_set_split(ys_lbvh* t, int consistent) {
     return YS_OK;
 }
 
+ys_status ys_lbvh_set_builder(ys_lbvh* t, int builder) {
+    if (!t) return fail(YS_ERR_BAD_ARG, "null tree");
+    if (builder != YS_BUILD_KARRAS && builder != YS_BUILD_APETREI) return fail(YS_ERR_BAD_ARG, "unknown tree builder");
+    t->builder = builder;
+    return YS_OK;
+}
+
 ys_status ys_lbvh_build(ys_lbvh* t, const float* x, uint32_t nV, const uint32_t* F, uint32_t nF) {
     if (!t || !x || !F || nF == 0 || nV == 0) return fail(YS_ERR_BAD_ARG, "bad argument");
     if (nF > t->maxPrims) return fail(YS_ERR_CAPACITY, "more primitives than the tree was created for");
@@ -127,6 +137,13 @@ ys_status ys_lbvh_build(ys_lbvh* t, const float* x, uint32_t nV, const uint32_t*
     launch_box(nullptr, x, 0, nV, t->box, t->stream);
     launch_morton(nullptr, x, 0, F, nF, t->box, t->codes, t->idx, t->stream);
     YS_CK2(radix_sort_pairs(t->codes, t->idx, nF, t->scratch, 0, 32, t->stream));
+    if (t->builder == YS_BUILD_APETREI) {
+        // topology and boxes in one pass: no refit afterwards
+        YS_CK2(launch_apetrei(nullptr, x, 0, F, t->codes, t->idx, nF, t->nodes, t->parent, t->claimOff, t->claims,
+                              t->visits, t->karrasScratch, t->aggScratch, t->status, t->stream));
+        YS_CK2(cudaStreamSynchronize(t->stream));
+        return YS_OK;
+    }
     YS_CK2(launch_karras(t->codes, t->idx, nF, t->nodes, t->parent, t->claimOff, t->claims, t->visits,
                          t->karrasScratch, t->stream, t->consistent));
     YS_CK2(cudaGetLastError());

@@ -130,8 +130,9 @@ __global__ void k_claim_fill(const Node* __restrict__ nodes, u32 nInner, u32* __
                              i32* __restrict__ claims) {
     const u32 i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= nInner) return;
-    claims[atomicAdd(&claimOff[nodes[i].a], 1u)] = (i32)i;
-    claims[atomicAdd(&claimOff[nodes[i].b], 1u)] = (i32)i;
+    const i32 a = nodes[i].a, b = nodes[i].b, nn = 2 * (i32)nInner + 1;
+    if (a >= 0 && a < nn) claims[atomicAdd(&claimOff[a], 1u)] = (i32)i;
+    if (b >= 0 && b < nn) claims[atomicAdd(&claimOff[b], 1u)] = (i32)i;
 }
 
 __global__ void __launch_bounds__(256) k_karras(const u32* __restrict__ codes, const u32* __restrict__ idx, u32 n,
@@ -797,6 +798,163 @@ void launch_refit_levels(const RefitJob* jobsDev, const uint2* list, const u32* 
 void launch_refit(const RefitJob* jobsDev, u32 numJobs, u32 totalLeaves, u32* status, cudaStream_t s) {
     if (totalLeaves == 0) return;
     k_refit<<<ceil_div(totalLeaves, 256), 256, 0, s>>>(jobsDev, numJobs, totalLeaves, status);
+}
+
+// ------------------------------------------------------------------ Apetrei
+// agglomerativeBuild_Tri + agglomerativeSwapRoot (bvh.metal:884-1199): the
+// topology and every box in one pass, one thread per leaf.
+__global__ void k_apetrei_init(Node* __restrict__ nodes, u32* __restrict__ flags, u32 nInner) {
+    const u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nInner) return;
+    nodes[i].a = -1;
+    nodes[i].b = -1;
+    flags[i] = 0u;
+}
+
+// Leaf i (sorted order) at slot n-1+i with its triangle's box; then the climb:
+// at range [L, R] join the side whose neighbouring key differs less (code XOR,
+// ties by index XOR; an end forces the other side).  Going right the parent is
+// slot R and this node its left child; going left, slot L-1 and the right
+// child.  The arrival (acq_rel) releases the child link, the range end and
+// the box; the first arrival stops, the second combines and climbs on with
+// the node's range.  A valid climb widens the range every step, so 2n steps
+// bound it; indices are checked before use.
+__global__ void __launch_bounds__(256) k_apetrei(const float4* x4, const float* x3, u32 voff, const u32* __restrict__ F,
+                                                 const u32* __restrict__ codes, const u32* __restrict__ idx, u32 n,
+                                                 Node* __restrict__ nodes, i32* __restrict__ parent,
+                                                 u32* __restrict__ flags, i32* __restrict__ rangeL,
+                                                 i32* __restrict__ rangeR, i32* __restrict__ root, u32* status) {
+    const int N = (int)n;
+    const int id = (int)(blockIdx.x * blockDim.x + threadIdx.x);
+    if (id >= N) return;
+    const u32 f = idx[id];
+    const f3 p0 = load_pos(x4, x3, voff + F[3 * f]), p1 = load_pos(x4, x3, voff + F[3 * f + 1]),
+             p2 = load_pos(x4, x3, voff + F[3 * f + 2]);
+    f3 lo = vmin(vmin(p0, p1), p2), hi = vmax(vmax(p0, p1), p2);
+    const int leaf = N - 1 + id;
+    nodes[leaf].a = -1;
+    nodes[leaf].b = (i32)f;
+    store_box(&nodes[leaf], lo, hi);
+    if (N == 1) {
+        *root = leaf;
+        return;
+    }
+    int node = leaf, L = id, R = id;
+    for (int step = 0; step < 2 * N; ++step) {
+        if (L == 0 && R == N - 1) {
+            *root = node;
+            return;
+        }
+        bool right;
+        if (L == 0) right = true;
+        else if (R == N - 1) right = false;
+        else {
+            const u32 dr = codes[R] ^ codes[R + 1], dl = codes[L - 1] ^ codes[L];
+            right = dr != dl ? dr < dl : (idx[R] ^ idx[R + 1]) < (idx[L - 1] ^ idx[L]);
+        }
+        const int p = right ? R : L - 1;
+        if (right) {
+            __stcg(&nodes[p].a, node);
+            __stcg(&rangeL[p], L);
+        } else {
+            __stcg(&nodes[p].b, node);
+            __stcg(&rangeR[p], R);
+        }
+        __stcg(&parent[node], p);
+        if (arrive_acq_rel(&flags[p]) == 0u) return;
+        const i32 ca = __ldcg(&nodes[p].a), cb = __ldcg(&nodes[p].b);
+        if (ca < 0 || ca >= 2 * N - 1 || cb < 0 || cb >= 2 * N - 1) {
+            atomicOr(status, ST_ITER_CAP);
+            return;
+        }
+        const float4* A = reinterpret_cast<const float4*>(&nodes[ca]);
+        const float4* B = reinterpret_cast<const float4*>(&nodes[cb]);
+        const float4 a0 = __ldcg(A), a1 = __ldcg(A + 1), b0 = __ldcg(B), b1 = __ldcg(B + 1);
+        lo = vmin(mk(a0.x, a0.y, a0.z), mk(b0.x, b0.y, b0.z));
+        hi = vmax(mk(a1.x, a1.y, a1.z), mk(b1.x, b1.y, b1.z));
+        store_box(&nodes[p], lo, hi);
+        node = p;
+        L = __ldcg(&rangeL[p]);
+        R = __ldcg(&rangeR[p]);
+        if (L < 0 || R >= N || L > R) {
+            atomicOr(status, ST_ITER_CAP);
+            return;
+        }
+    }
+    atomicOr(status, ST_ITER_CAP);
+}
+
+// agglomerativeSwapRoot (bvh.metal:1131-1199): the root (built in slot k)
+// moves to slot 0 and the node that was there to slot k, with the children's
+// parent links, the displaced node's parent's child link and the root's own
+// links to slot 0 patched.  One thread.
+__global__ void k_apetrei_swap(Node* __restrict__ nodes, i32* __restrict__ parent, const i32* __restrict__ root,
+                               u32 n, u32* status) {
+    if (blockIdx.x || threadIdx.x || n <= 1) return;
+    const i32 k = *root;
+    if (k == 0) return;
+    const i32 nInner = (i32)n - 1, nn = 2 * (i32)n - 1;
+    if (k < 0 || k >= nInner) {  // the root must be an internal slot
+        atomicOr(status, ST_ITER_CAP);
+        return;
+    }
+    const Node Rn = nodes[k], O = nodes[0];
+    const i32 p0 = parent[0];
+    const i32 ra = Rn.a == 0 ? k : Rn.a, rb = Rn.b == 0 ? k : Rn.b;
+    if (O.a < 0 || O.a >= nn || O.b < 0 || O.b >= nn || ra < 0 || ra >= nn || rb < 0 || rb >= nn ||
+        (p0 != k && (p0 < 0 || p0 >= nInner))) {
+        atomicOr(status, ST_ITER_CAP);
+        return;
+    }
+    Node r0 = Rn;
+    r0.a = ra;
+    r0.b = rb;
+    nodes[0] = r0;
+    nodes[k] = O;
+    parent[O.a] = k;
+    parent[O.b] = k;
+    parent[ra] = 0;
+    parent[rb] = 0;
+    if (p0 != k) {
+        if (nodes[p0].a == 0) nodes[p0].a = k;
+        else nodes[p0].b = k;
+        parent[k] = p0;
+    }
+    parent[0] = -1;
+}
+
+// Claimant counts of a built tree (one per child link; leaves and the root's
+// absent parent included by their zero).
+__global__ void k_claim_count(const Node* __restrict__ nodes, u32 nInner, u32* __restrict__ claimCount) {
+    const u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nInner) return;
+    const i32 a = nodes[i].a, b = nodes[i].b, nn = 2 * (i32)nInner + 1;
+    if (a >= 0 && a < nn) atomicAdd(&claimCount[a], 1u);
+    if (b >= 0 && b < nn) atomicAdd(&claimCount[b], 1u);
+}
+
+size_t apetrei_scratch_bytes(u32 n) { return 8 * (size_t)(n ? n : 1) + 256; }
+
+cudaError_t launch_apetrei(const float4* x4, const float* x3, u32 voff, const u32* facets, const u32* codes,
+                           const u32* idx, u32 n, Node* nodes, i32* parent, u32* claimOff, i32* claims, u32* visits,
+                           void* scanScratch, void* aggScratch, u32* status, cudaStream_t s) {
+    if (n == 0) return cudaSuccess;
+    const u32 nInner = n > 1 ? n - 1 : 0;
+    i32* rangeL = reinterpret_cast<i32*>(aggScratch);
+    i32* rangeR = rangeL + (n ? n : 1);
+    i32* root = reinterpret_cast<i32*>(reinterpret_cast<char*>(aggScratch) + 8 * (size_t)(n ? n : 1));
+    k_parent_init<<<ceil_div(2 * n, 256), 256, 0, s>>>(parent, claimOff, 2 * n - 1);
+    if (nInner) k_apetrei_init<<<ceil_div(nInner, 256), 256, 0, s>>>(nodes, visits, nInner);
+    k_apetrei<<<ceil_div(n, 256), 256, 0, s>>>(x4, x3, voff, facets, codes, idx, n, nodes, parent, visits, rangeL,
+                                                rangeR, root, status);
+    if (n > 1) {
+        k_apetrei_swap<<<1, 32, 0, s>>>(nodes, parent, root, n, status);
+        k_claim_count<<<ceil_div(nInner, 256), 256, 0, s>>>(nodes, nInner, claimOff);
+    }
+    cudaError_t e = exclusive_scan(claimOff, 2 * n, scanScratch, s);
+    if (e != cudaSuccess) return e;
+    if (n > 1) k_claim_fill<<<ceil_div(nInner, 256), 256, 0, s>>>(nodes, nInner, claimOff, claims);
+    return cudaGetLastError();
 }
 
 }  // namespace ys

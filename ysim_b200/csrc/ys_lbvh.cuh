@@ -73,6 +73,16 @@ void launch_morton(const float4* x4, const float* x3, u32 voff, const u32* facet
 size_t karras_scratch_bytes(u32 n);
 cudaError_t launch_karras(const u32* codes, const u32* idx, u32 n, Node* nodes, i32* parent, u32* claimOff,
                           i32* claims, u32* visits, void* scratch, cudaStream_t s, bool consistent = false);
+// Apetrei build (agglomerativeBuild_Tri + agglomerativeSwapRoot,
+// bvh.metal:884-1199) of sorted (code, index) pairs: topology, leaf boxes
+// from the current positions and every internal box in one pass, the root
+// moved to slot 0, claimant lists filled as launch_karras does, visit
+// counters left even.  Its tree is consistent for any input (runs of equal
+// codes split by index).  aggScratch holds apetrei_scratch_bytes(n).
+size_t apetrei_scratch_bytes(u32 n);
+cudaError_t launch_apetrei(const float4* x4, const float* x3, u32 voff, const u32* facets, const u32* codes,
+                           const u32* idx, u32 n, Node* nodes, i32* parent, u32* claimOff, i32* claims, u32* visits,
+                           void* scanScratch, void* aggScratch, u32* status, cudaStream_t s);
 // 4-wide form of a consistent binary tree of n leaves: internal nodes at even
 // depth become wide nodes (numbered by an exclusive scan), their children and
 // grandchildren their slots.  w4 and warrive need max(n - 1, 1) entries,

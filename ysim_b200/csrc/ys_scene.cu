@@ -914,6 +914,8 @@ struct ys_scene {
     cudaGraphExec_t graphs[18] = {};
     int fused_min_blocks = 8;        // k_fused register cap (ys_scene_set_fused_variant / ys_scene_autotune)
     int tree_layout = YS_TREE_CUBE;  // Morton normalisation of the scene trees
+    int tree_builder = YS_BUILD_KARRAS;
+    DBuf<char> aggScratch;           // Apetrei range ends and root slot
     DBuf<char> sortScratch, scanScratch;
     // staged / record buffers
     u32 cap = 0;
@@ -1021,8 +1023,15 @@ ys_status build_tree(ys_scene* s, HostMesh& H) {
                   s->tree_layout == YS_TREE_CUBE);
     YS_CK(radix_sort_pairs(codes, idx, n, s->sortScratch.p, 0, 32, st));
     const bool cube = s->tree_layout == YS_TREE_CUBE;
-    YS_CK(launch_karras(codes, idx, n, s->nodes.p + H.node_off, s->parent.p + H.node_off, claim_off(s, H),
-                        s->claims.p + H.node_off, s->visits.p + H.foff, s->karrasScratch.p, st, cube));
+    const bool agg = s->tree_builder == YS_BUILD_APETREI;
+    if (agg)
+        YS_CK(launch_apetrei(s->X[s->cur].p, nullptr, H.voff, s->F3.p + 3 * (size_t)H.foff, codes, idx, n,
+                             s->nodes.p + H.node_off, s->parent.p + H.node_off, claim_off(s, H),
+                             s->claims.p + H.node_off, s->visits.p + H.foff, s->karrasScratch.p, s->aggScratch.p,
+                             s->status.p, st));
+    else
+        YS_CK(launch_karras(codes, idx, n, s->nodes.p + H.node_off, s->parent.p + H.node_off, claim_off(s, H),
+                            s->claims.p + H.node_off, s->visits.p + H.foff, s->karrasScratch.p, st, cube));
     if (cube)
         YS_CK(launch_wide_build(s->nodes.p + H.node_off, s->parent.p + H.node_off, n, s->w4.p + H.w4_off,
                                 s->leafW.p + H.foff, s->leafWf.p + H.foff, s->warrive.p + H.w4_off,
@@ -1043,8 +1052,10 @@ ys_status build_tree(ys_scene* s, HostMesh& H) {
     J.selfMargin = 0.f;
     J.maxExt = s->maxext.p;  // unused (selfMargin == 0)
     RefitJob* slot = s->jobs.p + 6 * (size_t)s->njobs;
-    YS_CK(cudaMemcpyAsync(slot, &J, sizeof(J), cudaMemcpyHostToDevice, st));
-    launch_refit(slot, 1, n, s->status.p, st);
+    if (!agg) {  // the Apetrei build wrote every box already
+        YS_CK(cudaMemcpyAsync(slot, &J, sizeof(J), cudaMemcpyHostToDevice, st));
+        launch_refit(slot, 1, n, s->status.p, st);
+    }
     RefitJob JW = J;  // the wide boxes (and the root box) from the same positions
     if (cube) {
         JW.w4 = s->w4.p + H.w4_off;
@@ -1409,7 +1420,7 @@ ys_status ys_scene_destroy(ys_scene* s) {
     s->Fbuf.free(); s->mass.free(); s->mask.free(); s->vobj.free(); s->targets.free(); s->spr_off.free();
     s->spr_split.free(); s->spr_nbr.free(); s->vaf_off.free(); s->vaf.free(); s->maxext.free(); s->status.free();
     s->codes.free(); s->idx.free(); s->visits.free(); s->box.free(); s->spr_rest.free(); s->scratch3.free(); s->gk.free(); s->gL.free(); s->F4.free(); s->F3.free();
-    s->nodes.free(); s->parent.free(); s->claims.free(); s->claimOff.free(); s->karrasScratch.free(); s->rootAcc.free();
+    s->nodes.free(); s->parent.free(); s->claims.free(); s->claimOff.free(); s->karrasScratch.free(); s->aggScratch.free(); s->rootAcc.free();
     s->rjobs.free(); s->rchunks.free(); s->dmeshes.free(); s->jobs.free(); s->counters.free(); s->sortScratch.free();
     s->w4.free(); s->leafW.free(); s->warrive.free(); s->wideScratch.free();
     s->leafWf.free(); s->wcount.free(); s->hacc.free(); s->wlist.free(); s->hcount.free(); s->hoff.free();
@@ -1559,6 +1570,7 @@ ys_status ys_scene_pack(ys_scene* s) {
     YS_CK(s->claims.alloc(std::max(nNodes, 1u)));
     YS_CK(s->claimOff.alloc((size_t)nNodes + s->meshes.size() + 1));
     YS_CK(s->karrasScratch.alloc(karras_scratch_bytes(maxF)));
+    if (s->tree_builder == YS_BUILD_APETREI) YS_CK(s->aggScratch.alloc(apetrei_scratch_bytes(maxF)));
     YS_CK(s->dmeshes.alloc(md.size())); YS_CK(s->jobs.alloc(6 * s->meshes.size() + 2));
     if (s->tree_layout == YS_TREE_CUBE) {
         YS_CK(s->w4.alloc(std::max(nW4, 1u))); YS_CK(s->leafW.alloc(std::max(nF, 1u)));
@@ -1837,6 +1849,14 @@ ys_status ys_scene_colliders(ys_scene* s, ys_analytic_shape* out, uint32_t cap, 
         static_assert(sizeof(ys_analytic_shape) == sizeof(AShape), "ys_analytic_shape layout");
         for (u32 k = 0; k < n && k < cap; ++k) memcpy(&out[k], &s->hshapes[k].s, sizeof(AShape));
     }
+    return YS_OK;
+}
+
+ys_status ys_scene_set_tree_builder(ys_scene* s, int builder) {
+    if (!s) return fail(YS_ERR_BAD_ARG, "null scene");
+    if (s->packed) return fail(YS_ERR_STATE, "ys_scene_set_tree_builder: call before ys_scene_pack");
+    if (builder != YS_BUILD_KARRAS && builder != YS_BUILD_APETREI) return fail(YS_ERR_BAD_ARG, "unknown tree builder");
+    s->tree_builder = builder;
     return YS_OK;
 }
 

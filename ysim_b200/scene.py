@@ -68,7 +68,8 @@ class _System:
 class Scene:
     """A packed scene on one GPU (one CUDA stream)."""
 
-    def __init__(self, spec: SceneSpec, device: int = 0, pack: bool = True, tree_layout: Optional[int] = None):
+    def __init__(self, spec: SceneSpec, device: int = 0, pack: bool = True, tree_layout: Optional[int] = None,
+                 tree_builder: Optional[int] = None):
         self.lib = _lib.load()
         self.spec = spec
         p = spec.params
@@ -93,6 +94,8 @@ class Scene:
                 self.set_collider(idx.value, *m.collider)
         if tree_layout is not None:
             _lib.check(self.lib.ys_scene_set_tree_layout(self.h, int(tree_layout)), "ys_scene_set_tree_layout")
+        if tree_builder is not None:
+            _lib.check(self.lib.ys_scene_set_tree_builder(self.h, int(tree_builder)), "ys_scene_set_tree_builder")
         self.nV = spec.nV
         self.broad_phase = _BroadPhase(self)
         self.narrow_phase = _NarrowPhase(self)
