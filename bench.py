@@ -393,6 +393,11 @@ def run_ours(args, rank, world, local):
                             if kind == "reference" else "CPU restatement)")
                          + "; single_thread_value: one more substep on one host thread"}
 
+    build = analytic = None
+    if rank == 0:
+        m0 = spec.meshes[0]
+        build = measure_build(scene.get("x")[: m0.nV], m0.facets, local)
+        analytic = measure_analytic(local)
     batched = None if args.no_batched else measure_batched(args, rank, world, local)
     adjoint = None if (args.no_adjoint or rank != 0) else measure_adjoint(args, local)
 
@@ -418,12 +423,83 @@ def run_ours(args, rank, world, local):
             "clocks": clocks,
             "batched": batched,
             "adjoint": adjoint,
+            "tree_build": build,
+            "analytic_colliders": analytic,
         }
         print(json.dumps(line), flush=True)
     scene.close()
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
+
+
+# ------------------------------------------------------------------ tree build
+def measure_build(x, F, local, reps=10):
+    """One full rebuild of a tree (scene box, Morton codes, radix sort, then
+    Karras topology + bottom-up boxes, or the Apetrei one-pass build) through
+    the standalone LBVH, on the cloth's positions at the end of the run;
+    median of `reps` CUDA-event-timed builds after 3 warm-up builds."""
+    import ctypes as C
+    import torch
+    from ysim_b200 import _lib
+    lib = _lib.load()
+    dx = torch.from_numpy(np.ascontiguousarray(x, np.float32).reshape(-1)).to(f"cuda:{local}")
+    df = torch.from_numpy(np.ascontiguousarray(F, np.uint32).view(np.int32).reshape(-1)).to(f"cuda:{local}")
+    out = {"mesh": f"C2 cloth, {len(F):,} triangles", "reps": reps}
+    for name, builder in (("karras", _lib.BUILD_KARRAS), ("apetrei", _lib.BUILD_APETREI)):
+        h = C.c_void_p()
+        _lib.check(lib.ys_lbvh_create(C.byref(h), len(F), local, None), "ys_lbvh_create")
+        try:
+            _lib.check(lib.ys_lbvh_set_builder(h, builder), "ys_lbvh_set_builder")
+            times = []
+            for i in range(3 + reps):
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                torch.cuda.synchronize()
+                e0.record()
+                _lib.check(lib.ys_lbvh_build(h, C.c_void_p(dx.data_ptr()), len(x), C.c_void_p(df.data_ptr()),
+                                             len(F)), "ys_lbvh_build")
+                e1.record()
+                torch.cuda.synchronize()
+                if i >= 3:
+                    times.append(e0.elapsed_time(e1))
+            out[f"{name}_ms"] = float(np.median(times))
+        finally:
+            lib.ys_lbvh_destroy(h)
+    out["apetrei_over_karras"] = out["apetrei_ms"] / out["karras_ms"]
+    return out
+
+
+def measure_analytic(local, steps=200):
+    """C1's FastGridCloth 64 x 64 draped over obstacles, fused substeps per
+    second: over the triangle icosphere (level 4, BVH queries), and over
+    analytic colliders (sphere, box, cylinder, floor plane; markers + shape
+    tests, no obstacle tree).  Pre-rolled to contact, device-timed."""
+    import torch
+    from ysim_b200 import generators as G
+    from ysim_b200.scene import Scene
+    out = {"workload": "C1 cloth 64x64 (4,096 v), 200 fused substeps after a 2-frame pre-roll from height 0.32"}
+    for name, spec in (("triangle_icosphere", G.config_c1(height=0.32)),
+                       ("analytic_shapes", G.config_c1_analytic(height=0.32))):
+        sc = Scene(spec, device=local)
+        try:
+            sc.step(2 * spec.params.substeps)
+            stream = torch.cuda.ExternalStream(sc.stream(), device=local)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            sc.sync()
+            e0.record(stream)
+            sc.step(steps)
+            e1.record(stream)
+            sc.sync()
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1)
+            st = sc.stats()
+            out[name] = {"substeps_per_s": steps / (ms / 1000.0), "ms_per_substep": ms / steps,
+                         "contacts_last_substep": st["contacts"], "flags": st["flags"]}
+        finally:
+            sc.close()
+    return out
 
 
 # ------------------------------------------------------------------ batched
