@@ -86,12 +86,13 @@ struct StepArgs {
     const float* gk;    // per-spring stiffness / rest length of grid cloths (MeshDev::gspr)
     const float* gL;
     // analytic colliders: shape table, marker pair of each target entry (or
-    // NO_PAIR), marker pairs (cloth, collider, slot, first thread) and this
-    // substep's active flag per pair
+    // NO_PAIR), marker pairs (cloth, collider, slot, first thread), and the
+    // marker flags of this detect (written) and of the previous one (read)
     const DShape* shapes;
     const u32* tpair;
     const uint4* apairs;
-    const u32* mk_act;
+    u32* mk_fresh;
+    const u32* mk_held;
     u32 npairs, apair_total;
     u32 analytic;  // the scene has analytic colliders
     float subh, kair, kd, gx, gy, gz, margin, band, radius;
@@ -280,6 +281,24 @@ __device__ __forceinline__ void insert_contact(VContact (&buf)[MAXC], int& nc, u
     ++nc;
 }
 
+// Analytic marker of one detect (BroadPhase::detectCollisions,
+// bvh.hpp:2886-2941): the cloth's root box against the collider's broad box
+// (AABB4::intersect; a half-space always overlaps).  A pair is live when it
+// is marked at this detect or was at the previous one
+// (PackedCollisionData::endAnalyticPairs, scene.hpp:485-530).  The cloth's
+// first vertex records this detect's mark for the next; the flags of the two
+// detects alternate between two slots by substep parity.
+__device__ __forceinline__ bool analytic_live(const StepArgs& A, const DShape& S, const Node* root, u32 p, bool writer) {
+    bool fresh = true;
+    if (S.lo.w != 0.f) {
+        const Node r = *root;
+        fresh = !(S.hi.x < r.mnx || S.lo.x > r.mxx || S.hi.y < r.mny || S.lo.y > r.mxy || S.hi.z < r.mnz ||
+                  S.lo.z > r.mxz);
+    }
+    if (writer) A.mk_fresh[p] = fresh ? 1u : 0u;
+    return fresh || A.mk_held[p] != 0u;
+}
+
 // The analytic test out of line, so that the fused kernel's descent keeps its
 // register allocation (the call is taken only for live collider pairs).
 __device__ __noinline__ bool analytic_contact(const DShape* S, f3 pcur, f3 pprev, float radius, float thickness,
@@ -366,9 +385,11 @@ __global__ void __launch_bounds__(128, MINB) k_fused(StepArgs A) {
                 // narrowAnalytic for a marked (cloth, collider) pair: this
                 // vertex against the shape, no descent
                 const u32 p = A.tpair[k];
+                if (p == NO_PAIR) continue;
+                const DShape* S = A.shapes + A.meshes[t].shape;
                 VContact c;
-                if (p != NO_PAIR && A.mk_act[p] &&
-                    analytic_contact(A.shapes + A.meshes[t].shape, xc, xpv, A.radius, mg, &c))
+                if (analytic_live(A, *S, A.nodes + Mp->node_off, p, g == Mp->voff) &&
+                    analytic_contact(S, xc, xpv, A.radius, mg, &c))
                     insert_contact(buf, nc, st, c);
                 continue;
             }
@@ -635,11 +656,11 @@ __global__ void __launch_bounds__(128) k_narrow_analytic_scene(StepArgs A) {
         if (A.apairs[mid].w <= i) lo = mid;
         else hi = mid;
     }
-    if (!A.mk_act[lo]) return;
     const uint4 P = A.apairs[lo];
     const MeshDev& Q = A.meshes[P.x];
     const u32 id = i - P.w, g = Q.voff + id;
     const DShape& S = A.shapes[P.z];
+    if (!analytic_live(A, S, A.nodes + Q.node_off, lo, id == 0)) return;
     f3 n;
     float d;
     if (!analytic_narrow(S.s, ld(A.x, g), ld(A.xp, g), A.radius, A.margin, S.rot_margin, n, d)) return;
@@ -650,28 +671,6 @@ __global__ void __launch_bounds__(128) k_narrow_analytic_scene(StepArgs A) {
     c.nx = n.x; c.ny = n.y; c.nz = n.z; c.d = d;
     c.qbeh = Q.behavior; c.tbeh = S.s.beh; c.qshape = COL_MESH; c.tshape = S.s.kind;
     A.contacts[o] = c;
-}
-
-// Analytic markers of one detect (BroadPhase::detectCollisions,
-// bvh.hpp:2886-2941): a (cloth, collider) pair is marked when the cloth's
-// root box overlaps the collider's broad box (AABB4::intersect; a half-space
-// always), and it is live when it was marked at this detect or at the one
-// before (PackedCollisionData::endAnalyticPairs, scene.hpp:485-530).
-__global__ void k_analytic_markers(const uint4* __restrict__ apairs, u32 np, const MeshDev* __restrict__ meshes,
-                                   const Node* __restrict__ nodes, const DShape* __restrict__ shapes,
-                                   u32* __restrict__ fresh, const u32* __restrict__ held, u32* __restrict__ act) {
-    const u32 p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= np) return;
-    const uint4 P = apairs[p];
-    const DShape& S = shapes[P.z];
-    u32 hit = 1u;
-    if (S.lo.w != 0.f) {
-        const Node r = nodes[meshes[P.x].node_off];
-        hit = (S.hi.x < r.mnx || S.lo.x > r.mxx || S.hi.y < r.mny || S.lo.y > r.mxy || S.hi.z < r.mnz ||
-               S.lo.z > r.mxz) ? 0u : 1u;
-    }
-    fresh[p] = hit;
-    act[p] = hit | held[p];
 }
 
 // Per-vertex CSR of the contacts (narrow_bucket_count/scan/scatter,
@@ -894,7 +893,8 @@ struct ys_scene {
     bool use_ext = false;
     DBuf<float> gk, gL;              // per-spring grid-cloth parameters
     // analytic colliders: compact shape table (mesh of each slot), marker
-    // pairs, per-target pair ids, marker flags (fresh[2][np], live[np])
+    // pairs, per-target pair ids, marker flags of two detects (2 x np, by
+    // substep parity)
     std::vector<int> shape_mesh;
     std::vector<DShape> hshapes;
     bool analytic_primed = false, shapes_uploaded = false;
@@ -970,7 +970,8 @@ StepArgs make_args(ys_scene* s) {
     A.shapes = s->dshapes.p;
     A.tpair = s->tpair.p;
     A.apairs = s->apairs.p;
-    A.mk_act = s->markers.p ? s->markers.p + 2 * (size_t)s->npairs : nullptr;
+    A.mk_fresh = s->markers.p ? s->markers.p + (size_t)s->cv * s->npairs : nullptr;
+    A.mk_held = s->markers.p ? s->markers.p + (size_t)(1 - s->cv) * s->npairs : nullptr;
     A.npairs = s->npairs;
     A.apair_total = s->apair_total;
     A.analytic = s->shape_mesh.empty() ? 0u : 1u;
@@ -1212,9 +1213,8 @@ ys_status preamble(ys_scene* s) {
     return YS_OK;
 }
 
-// Refit of every live tree, then the analytic markers from the new root
-// boxes (fresh flags in the slot of this substep's parity, held flags from
-// the other one).
+// Refit of every live tree (the analytic markers are taken from the new root
+// boxes by the kernels that consume them).
 ys_status refit(ys_scene* s) {
     if (s->nrjobs)
         launch_root_boxes(s->rjobs.p + (size_t)(s->cur * 2 + s->cv) * s->nrjobs, s->nrjobs, s->rchunks.p,
@@ -1227,12 +1227,6 @@ ys_status refit(ys_scene* s) {
         if (s->use_levels)
             launch_refit_levels(table, s->wlist.p, s->hoff.p, s->lvl_off.data(), s->lvl_top, s->stream);
         if (s->nRootOnly) launch_refit_roots(table, s->njobs, s->stream);
-    }
-    if (s->npairs) {
-        const size_t np = s->npairs;
-        k_analytic_markers<<<ceil_div(np, 128), 128, 0, s->stream>>>(
-            s->apairs.p, s->npairs, s->dmeshes.p, s->nodes.p, s->dshapes.p, s->markers.p + (size_t)s->cv * np,
-            s->markers.p + (size_t)(1 - s->cv) * np, s->markers.p + 2 * np);
     }
     return YS_OK;
 }
@@ -1637,8 +1631,8 @@ ys_status ys_scene_pack(ys_scene* s) {
         if (!ap.empty()) {
             YS_CK(s->apairs.alloc(ap.size()));
             YS_CK(cudaMemcpy(s->apairs.p, ap.data(), sizeof(uint4) * ap.size(), cudaMemcpyHostToDevice));
-            YS_CK(s->markers.alloc(3 * ap.size()));
-            YS_CK(cudaMemset(s->markers.p, 0, 4 * 3 * ap.size()));
+            YS_CK(s->markers.alloc(2 * ap.size()));
+            YS_CK(cudaMemset(s->markers.p, 0, 4 * 2 * ap.size()));
         }
         if (!s->shape_mesh.empty()) {
             // seeded at pack (Scene::packAnalyticShapes, scene.hpp:762-781):
