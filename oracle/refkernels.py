@@ -34,6 +34,12 @@ def lib():
             "yref_swept_leaves": (None, [vp, vp, vp, u32, f32, vp, vp]),
             "yref_bottom_up": (None, [vp, vp, u32, vp]),
             "yref_agglomerative": (C.c_int32, [vp, vp, u32, vp, vp, vp]),
+            "yref_scene_roundtrip": (C.c_int, [C.c_char_p, vp, C.c_size_t, vp]),
+            "yref_runconfig_roundtrip": (C.c_int, [C.c_char_p, vp, C.c_size_t]),
+            "yref_primitive": (C.c_int, [C.c_int, f32, C.c_int, vp, vp, C.c_size_t, C.c_size_t, vp, vp]),
+            "yref_uniform_float": (None, [u32, f32, f32, u32, vp]),
+            "yref_profile_paths": (C.c_int, [C.c_char_p, C.c_char_p, C.c_int, vp, C.c_size_t]),
+            "yref_profiler_csv": (C.c_int, [C.c_char_p, C.c_int, vp, vp, vp, vp, vp, C.c_int, vp, vp, C.c_int]),
             "yref_query_points": (u32, [vp, u32, vp, vp, u32, f32, u32, u32, vp, u32, vp]),
             "yref_narrow": (u32, [vp, u32, vp, vp, vp, vp, vp, vp, f32, f32, vp, vp, u32]),
             "yref_tri_forces": (None, [vp, vp, vp, vp, vp, vp, f32, f32, f32, vp, vp, vp, vp, vp, vp, vp, vp, vp,
@@ -123,6 +129,53 @@ def agglomerative(x, F, codes, idx):
     parent = np.full(2 * n - 1, -1, np.int32)
     k = lib().yref_agglomerative(P(c32(x)), P(c32(F, np.uint32)), n, P(mortons), P(nodes), P(parent))
     return nodes, parent, int(k)
+
+
+def scene_roundtrip(text: str, runconfig: bool = False):
+    """scene_format (or sim_config) parseString + toString: (ok, text or error, warnings)."""
+    buf = C.create_string_buffer(1 << 22)
+    w = np.zeros(1, np.int32)
+    if runconfig:
+        rc = lib().yref_runconfig_roundtrip(text.encode(), buf, len(buf))
+    else:
+        rc = lib().yref_scene_roundtrip(text.encode(), buf, len(buf), P(w))
+    return rc == 0, buf.value.decode(), int(w[0])
+
+
+def primitive(kind: str, size: float, tess: int):
+    """primitive::sphere / cube / cylinder at the origin: (positions, facets)."""
+    k = {"sphere": 0, "cube": 1, "cylinder": 2}[kind]
+    nv, nf = np.zeros(1, np.uint32), np.zeros(1, np.uint32)
+    lib().yref_primitive(k, size, tess, None, None, 0, 0, P(nv), P(nf))
+    pos = np.zeros((int(nv[0]), 3), np.float32)
+    fac = np.zeros((int(nf[0]), 3), np.uint32)
+    lib().yref_primitive(k, size, tess, P(pos), P(fac), len(pos), len(fac), P(nv), P(nf))
+    return pos, fac
+
+
+def uniform_float(seed: int, lo: float, hi: float, n: int):
+    """std::uniform_real_distribution<float>(lo, hi) over std::mt19937(seed)."""
+    out = np.zeros(n, np.float32)
+    lib().yref_uniform_float(seed, lo, hi, n, P(out))
+    return out
+
+
+def profile_paths(root: str, scene_path: str, frames: int):
+    buf = C.create_string_buffer(4096)
+    lib().yref_profile_paths(root.encode(), scene_path.encode(), frames, buf, len(buf))
+    return tuple(buf.value.decode().split("\n"))
+
+
+def profiler_csv(path: str, seq, wall, frame_ms, broad, narrow, names, sec_ms, max_frames=240) -> str:
+    """FrameProfilerHistory::exportCsv of the given frames; returns the file's text."""
+    n = len(seq)
+    arr = (C.c_char_p * max(len(names), 1))(*[s.encode() for s in names])
+    sec = np.ascontiguousarray(np.asarray(sec_ms, np.float64).reshape(n, len(names)))
+    lib().yref_profiler_csv(path.encode(), n, P(np.asarray(seq, np.uint64)), P(np.asarray(wall, np.float64)),
+                            P(np.asarray(frame_ms, np.float64)), P(np.asarray(broad, np.uint64)),
+                            P(np.asarray(narrow, np.uint64)), len(names), arr, P(sec), max_frames)
+    with open(path) as f:
+        return f.read()
 
 
 def narrow_analytic(x, xprev, voff, shapes, oid, shape_index, cloth_beh, radius, thickness, rot_margin, cap=None):

@@ -1603,7 +1603,6 @@ int yso_scene_set_collider(void* h, int mesh, u32 kind, const float* c, const fl
     Scene* S = (Scene*)h;
     if (mesh < 0 || (size_t)mesh >= S->meshes.size() || kind > CPlane) return -1;
     Mesh& M = S->meshes[mesh];
-    if (kind != CMesh && M.cloth()) return -1;
     if (S->packed && kind != M.collider) return -1;
     M.collider = kind;
     for (int i = 0; i < 3; ++i) { M.pose[i] = c[i]; M.pose[3 + i] = hx ? hx[i] : 0.f; }

@@ -15,6 +15,12 @@ generators; outputs are the reference kernels' results:
   substep_*.npz   -- one mid-drape substep of a small scene: broad rows (the
                      oracle's), narrow_pt_tri contacts, the cloth's spring
                      forces and integrate_cloth(_grid) positions / velocities;
+  scene_io.json   -- the scene-file / run-config round trips and load errors
+                     (scene_format.hpp, sim_config.hpp) of tests/golden/scenes
+                     and tests/scene_cases.py, libstdc++'s mt19937 +
+                     uniform_real_distribution<float> draws, and a
+                     FrameProfiler CSV export;
+  scene_io_geom.npz -- primitive::sphere / cube / cylinder meshes;
   analytic.npz    -- narrow_pt_analytic contacts of vertex clouds around every
                      collider kind (static, rotated, moving, ellipsoid,
                      disabled; tests/analytic_cases.py), with the rotation
@@ -37,6 +43,7 @@ from ysim_b200 import generators as G  # noqa: E402
 
 sys.path.insert(0, os.path.dirname(HERE))
 import analytic_cases as AC  # noqa: E402
+import scene_cases as SCN  # noqa: E402
 
 
 def canon(p):
@@ -146,6 +153,51 @@ def analytic():
                         rot_margin=np.array(rms, np.float32), contacts=c.view(np.uint8))
 
 
+def profiler_frames():
+    """A fixed set of frames for the FrameProfiler CSV check."""
+    rng = np.random.default_rng(9)
+    n = 250
+    fms = rng.uniform(0.0, 40.0, n)
+    fms[3], fms[7], fms[9] = 0.0, 1e-7, 123456789.0
+    sec = rng.uniform(0, 5, (n, 4))
+    sec[0, 0], sec[1, 1] = 1e300, -2.5e-20
+    return dict(seq=(np.arange(n) + 5).tolist(), wall=np.cumsum(rng.uniform(0.001, 0.05, n)).tolist(),
+                frame_ms=fms.tolist(), broad=rng.integers(0, 10**9, n).tolist(),
+                narrow=rng.integers(0, 10**6, n).tolist(), names=["physics total", "refit", "substep-kernel", "x.y"],
+                sec_ms=sec.tolist(), max_frames=240)
+
+
+def scene_io():
+    import json
+    import tempfile
+    out = {"roundtrip": {}, "runconfig": {}, "errors": [], "jiggle": {}}
+    for name in SCN.fixture_names():
+        t = SCN.fixture_text(name)
+        out["roundtrip"][name] = R.scene_roundtrip(t)[1]
+        out["runconfig"][name] = R.scene_roundtrip(t, runconfig=True)[1]
+    for name, t in SCN.error_cases():
+        ok1, m1, _ = R.scene_roundtrip(t)
+        ok2, m2, _ = R.scene_roundtrip(t, runconfig=True)
+        out["errors"].append({"name": name, "scene": [ok1, m1], "runconfig": [ok2, m2]})
+    for seed in SCN.JIGGLE_SEEDS:
+        out["jiggle"][str(seed)] = R.uniform_float(seed, 0.0, 1.0 / 10000.0, 700).view(np.uint32).tolist()
+    pf = profiler_frames()
+    with tempfile.TemporaryDirectory() as d:
+        out["profiler_csv"] = R.profiler_csv(os.path.join(d, "p.csv"), pf["seq"], pf["wall"], pf["frame_ms"],
+                                             pf["broad"], pf["narrow"], pf["names"], pf["sec_ms"], pf["max_frames"])
+    out["profiler_frames"] = pf
+    out["paths"] = [list(R.profile_paths(r, sp, f)) + [r, sp, f]
+                    for r, sp, f in (("", "/a/b/flag.ysim.json", 30), ("/x/y", "scene", 5), ("", "noext", 1))]
+    with open(os.path.join(HERE, "scene_io.json"), "w") as f:
+        json.dump(out, f)
+    geom = {}
+    for k, s, t in SCN.PRIMITIVE_CASES:
+        p, fc = R.primitive(k, s, t)
+        geom[f"{k}_{s}_{t}_x"] = p
+        geom[f"{k}_{s}_{t}_f"] = fc
+    np.savez_compressed(os.path.join(HERE, "scene_io_geom.npz"), **geom)
+
+
 if __name__ == "__main__":
     if not R.available():
         sys.exit("reference checkout absent: cannot regenerate golden vectors")
@@ -153,6 +205,7 @@ if __name__ == "__main__":
     for k in SPECS:
         substep(k)
     analytic()
+    scene_io()
     for fn in sorted(os.listdir(HERE)):
         if fn.endswith(".npz"):
             print(fn, os.path.getsize(os.path.join(HERE, fn)))

@@ -143,7 +143,7 @@ __device__ __forceinline__ u32 query_vertex(const StepArgs& A, u32 g, u32 m, con
                 if (h1_face(A.x, M.voff, tri, lid, mg, inv, h)) sink(m, f, tri, M.voff);
             });
         }
-    } else if (A.self_mode == YS_SELF_BVH) {
+    } else if (A.self_mode == YS_SELF_BVH && !(M.flags & MF_ANALYTIC)) {
         f3 qmn = xc - mk(mg, mg, mg), qmx = xc + mk(mg, mg, mg);
         st |= descend(A, M, qmn, qmx, [&](u32 f) {
             uint4 tri = A.F[M.foff + f];
@@ -154,8 +154,9 @@ __device__ __forceinline__ u32 query_vertex(const StepArgs& A, u32 g, u32 m, con
     for (u32 k = M.tgt_begin; k < M.tgt_end; ++k) {
         const u32 t = A.targets[k];
         const MeshDev T = A.meshes[t];
-        // an analytic collider has no live tree (its pairs are markers)
-        if ((T.flags & MF_ANALYTIC) || T.nF == 0) continue;
+        // an analytic collider has no live tree and queries none (its pairs
+        // are markers)
+        if ((T.flags & MF_ANALYTIC) || (M.flags & MF_ANALYTIC) || T.nF == 0) continue;
         if (!root_overlap(A.nodes + M.node_off, A.nodes + T.node_off)) continue;
         f3 qmn = xc - mk(mg, mg, mg), qmx = xc + mk(mg, mg, mg);
         st |= descend(A, T, qmn, qmx, [&](u32 f) {
@@ -366,7 +367,7 @@ __global__ void __launch_bounds__(128, MINB) k_fused(StepArgs A) {
             inv = 1.f / cs;
             H1Vertex h;
             if (h1_vertex(xc, xpv, inv, h)) { selfOK = true; h1_query_box(h, mg, qmn, qmx); }
-        } else if (A.self_mode == YS_SELF_BVH) {
+        } else if (A.self_mode == YS_SELF_BVH && !(mflags & MF_ANALYTIC)) {
             selfOK = true;
             qmn = xc - mk(mg, mg, mg);
             qmx = xc + mk(mg, mg, mg);
@@ -393,6 +394,7 @@ __global__ void __launch_bounds__(128, MINB) k_fused(StepArgs A) {
                     insert_contact(buf, nc, st, c);
                 continue;
             }
+            if (ANA && (mflags & MF_ANALYTIC)) continue;  // no queries from an analytic collider
             const u32 tno = A.meshes[t].node_off, tnf = A.meshes[t].nF;
             if (tnf == 0 || !root_overlap(A.nodes + Mp->node_off, A.nodes + tno)) continue;
             qmn = xc - mk(mg, mg, mg);
@@ -1479,9 +1481,11 @@ ys_status ys_scene_pack(ys_scene* s) {
         if (cloth) f |= MF_CLOTH;
         if (H.d.num_facets) f |= MF_TREE;
         if (H.d.behavior == YS_FAST_GRID_CLOTH) f |= MF_GRID;
-        // an analytic collider queries nothing (BroadPhase::detectCollisions
-        // marks only cloth -> collider pairs, bvh.hpp:2913-2937)
-        if (H.collider != COL_MESH) f = (f | MF_ANALYTIC) & ~MF_QUERY;
+        // an analytic collider descends no tree: as a query it only marks
+        // pairs with analytic targets (when it is cloth) and keeps the CPU-hash
+        // self rows (BroadPhase::detectCollisions, bvh.hpp:2886-2937;
+        // simulator.hpp:3678-3701)
+        if (H.collider != COL_MESH) f |= MF_ANALYTIC;
         H.flags = f;
         build_adjacency(H);
     }
@@ -1664,7 +1668,7 @@ ys_status ys_scene_pack(ys_scene* s) {
                            (s->P.self_mode == YS_SELF_HASH && (H.flags & MF_CLOTH) && (H.flags & MF_SELF));
         if (selfQ) descended[m] = 1;
         for (u32 k = md[m].tgt_begin; k < md[m].tgt_end; ++k)
-            if (!(md[targets[k]].flags & MF_ANALYTIC)) descended[targets[k]] = 1;
+            if (!(md[targets[k]].flags & MF_ANALYTIC) && !(H.flags & MF_ANALYTIC)) descended[targets[k]] = 1;
         if (md[m].tgt_end > md[m].tgt_begin) rootUsed[m] = 1;
     }
     for (size_t m = 0; m < s->meshes.size(); ++m) {
@@ -1824,8 +1828,6 @@ ys_status ys_scene_set_collider(ys_scene* s, int mesh, uint32_t kind, const floa
     if (!center || !rot_wxyz || (!half && kind != COL_PLANE && kind != COL_MESH))
         return fail(YS_ERR_BAD_ARG, "ys_scene_set_collider: null pose");
     HostMesh& H = s->meshes[mesh];
-    if (kind != COL_MESH && (H.d.behavior == YS_TRIANGULAR_CLOTH || H.d.behavior == YS_FAST_GRID_CLOTH))
-        return fail(YS_ERR_BAD_ARG, "ys_scene_set_collider: a cloth mesh cannot be an analytic collider");
     if (s->packed && kind != H.collider)
         return fail(YS_ERR_STATE, "ys_scene_set_collider: the collider kind is fixed at ys_scene_pack");
     H.collider = kind;
