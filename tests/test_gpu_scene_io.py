@@ -66,11 +66,27 @@ def test_headless_run_writes_the_profile(cuda_lib, tmp_path, level):
     assert len(side.scene.objects) == 6 and side.profile.frames == 4
 
 
-def test_all_fields_scene_runs(cuda_lib, tmp_path):
+def test_all_fields_scene_matches_the_oracle(cuda_lib, oracle, tmp_path):
     """Pins, a Rigid body, a plane collider, wind gates and the unsupported
-    motion constraints (reported, not applied) on the staged path."""
+    motion constraints (reported, not applied), staged: the same states and
+    flags as the oracle.  The fixture's cloth (k / m = 1.5e6 at subh = 1/1200)
+    is beyond the explicit integrator's stability limit, so both sides
+    sanitise vertices and raise the non-finite flag alike."""
+    from ysim_b200 import loader as L
     from ysim_b200 import run as RUN
+    from ysim_b200.scene import Scene
+    ls = L.load(os.path.join(SCENES, "all_fields.json"))
+    s = Scene(ls.spec)
+    o = oracle.OracleScene(ls.spec)
+    try:
+        for _ in range(2):
+            s.step_staged(ls.spec.params.substeps)
+            o.step(ls.spec.params.substeps)
+            assert rel_err(s.get("x"), o.get("x")) <= TOL
+            assert rel_err(s.get("v"), o.get("v")) <= TOL
+        assert s.stats()["flags"] == o.stats()["flags"]
+    finally:
+        s.close()
     summary = RUN.run(os.path.join(SCENES, "all_fields.json"), frames=2, csv_path=str(tmp_path / "a.csv"),
-                      staged=True, quiet=True)
-    assert summary["finite"] and summary["flags"] == 0
-    assert any("spline" in w for w in summary["warnings"])
+                      quiet=True)
+    assert summary["finite"] and any("spline" in w for w in summary["warnings"])
