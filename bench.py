@@ -192,6 +192,8 @@ def measured_traffic(args):
     with open(path) as fh:
         d = json.load(fh)
     return {"k_fused": d.get("k_fused"), "refit": d.get("refit"),
+            "k_fused_warp_instructions": d.get("k_fused_warp_instructions"),
+            "k_fused_threads_per_instruction": d.get("k_fused_threads_per_instruction"),
             "source": "ncu capture, profiles/traffic_c2_tricloth512.json (" + d.get("command", "") + ")"}
 
 
@@ -381,6 +383,18 @@ def run_ours(args, rank, world, local):
                              "avg_launch_ms": refit_ms, "traffic": traffic.get("refit"),
                              "launches_per_substep": "leaf kernel + one per low level + one top-level block"},
             "traffic_source": traffic.get("source")}
+    # The kernel is issue- and latency-bound, not bandwidth-bound: the same
+    # launch against the SMs' instruction-issue peak (148 SMs x 4 schedulers x
+    # 1 warp instruction per cycle at the sampled SM clock), with the warp
+    # instructions of the committed ncu capture of this workload.
+    ninst = traffic.get("k_fused_warp_instructions")
+    if ninst and clocks.get("sm_mhz"):
+        peak_ginst = 148 * 4 * clocks["sm_mhz"] / 1000.0
+        got = ninst / (fused_ms / 1000.0) / 1e9
+        roof["issue"] = {"bound": "instruction issue", "warp_instructions": ninst, "achieved": got,
+                         "peak": peak_ginst, "unit": "G warp inst/s", "frac": got / peak_ginst,
+                         "threads_per_instruction": traffic.get("k_fused_threads_per_instruction"),
+                         "source": "warp instructions per launch from the ncu capture; duration and clock live"}
 
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:

@@ -208,7 +208,10 @@ ys_status ys_scene_autotune(ys_scene* s, uint32_t reps, int* chosen, float* ms_o
  * (collider mesh, 0).  After pack it moves the collider: the pose is read at
  * the next frame start, where the previous pose becomes the start of the
  * swept test (Scene::refreshAnalyticShapes, scene.hpp:659-745).  The kind
- * cannot change after pack; a cloth mesh cannot be an analytic collider. */
+ * cannot change after pack.  A cloth may be an analytic collider too (the
+ * reference's default for a cloth sphere, cube or cylinder primitive): it
+ * then descends no tree, is tested against other analytic colliders, keeps
+ * its CPU-hash self rows, and is a shape target for other cloths. */
 ys_status ys_scene_set_collider(ys_scene* s, int mesh, uint32_t kind, const float center[3], const float half[3],
                                 const float rot_wxyz[4]);
 /* The scene's analytic shape table as of the last frame start (compact, in
