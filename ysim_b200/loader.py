@@ -31,7 +31,6 @@ reported in `warnings`, and do not act.
 from __future__ import annotations
 
 import dataclasses
-import os
 from typing import List, Optional
 
 import numpy as np
@@ -111,7 +110,7 @@ def _geometry(o: SF.Object, scene_dir: str, seed: int):
     return x, f, pos, F32(p.size), float(p.mass)
 
 
-def load(source, scene_path: str = "", cuda_backend_only: bool = True) -> LoadedScene:
+def load(source, scene_path: str = "") -> LoadedScene:
     """A RunConfig, SceneSnapshot or the path of a scene / run-config file."""
     if isinstance(source, str):
         scene_path = source
