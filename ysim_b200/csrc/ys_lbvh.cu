@@ -31,8 +31,12 @@ __device__ __forceinline__ f3 load_pos(const float4* x4, const float* x3, u32 i)
     return x4 ? ld(x4, i) : ldp(x3, i);
 }
 
-// bvh.hpp:1229-1231: box over every vertex of the mesh.
+// bvh.hpp:1229-1231: box over every vertex of the mesh.  Grid-stride
+// threads, a warp reduction, a block reduction through shared memory, and
+// one atomic per block and slot (min / max on the order-preserving integer
+// form of the floats, exact).
 __global__ void __launch_bounds__(256) k_box(const float4* x4, const float* x3, u32 voff, u32 nV, u32* box) {
+    __shared__ u32 sh[6][8];
     u32 mn[3] = {0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu}, mx[3] = {0u, 0u, 0u};
     for (u32 i = blockIdx.x * blockDim.x + threadIdx.x; i < nV; i += gridDim.x * blockDim.x) {
         f3 p = load_pos(x4, x3, voff + i);
@@ -45,9 +49,18 @@ __global__ void __launch_bounds__(256) k_box(const float4* x4, const float* x3, 
         mn[k] = __reduce_min_sync(0xffffffffu, mn[k]);
         mx[k] = __reduce_max_sync(0xffffffffu, mx[k]);
     }
+    const u32 w = threadIdx.x >> 5, nw = blockDim.x >> 5;
     if ((threadIdx.x & 31) == 0) {
 #pragma unroll
-        for (int k = 0; k < 3; ++k) { atomicMin(&box[k], mn[k]); atomicMax(&box[3 + k], mx[k]); }
+        for (int k = 0; k < 3; ++k) { sh[k][w] = mn[k]; sh[3 + k][w] = mx[k]; }
+    }
+    __syncthreads();
+    if (threadIdx.x < 6) {
+        const u32 k = threadIdx.x;
+        u32 v = sh[k][0];
+        for (u32 j = 1; j < nw; ++j) v = k < 3 ? min(v, sh[k][j]) : max(v, sh[k][j]);
+        if (k < 3) atomicMin(&box[k], v);
+        else atomicMax(&box[k], v);
     }
 }
 
@@ -55,7 +68,7 @@ void launch_box_init(u32* box, cudaStream_t s) { k_box_init<<<1, 32, 0, s>>>(box
 void launch_box(const float4* x4, const float* x3, u32 voff, u32 nV, u32* box, cudaStream_t s) {
     if (nV == 0) return;
     int blocks = ceil_div(nV, 256);
-    if (blocks > 148 * 8) blocks = 148 * 8;
+    if (blocks > 148 * 2) blocks = 148 * 2;
     k_box<<<blocks, 256, 0, s>>>(x4, x3, voff, nV, box);
 }
 
