@@ -636,11 +636,82 @@ def measure_adjoint(args, local, steps=200, every=20, reps=4):
     s.close()
     f = float(np.median(fw)) / steps
     g = float(np.median(bw)) / steps
+    f64 = measure_adjoint_fp64(spec, k, L, target, local, steps, every, reps)
     return {"workload": "FastGridCloth 128x128 over a level-4 icosphere, 200 steps, checkpoint every 20",
             "forward_ms_per_step": f, "backward_ms_per_step": g, "backward_over_forward": g / f,
             "plain_forward_ms_per_step": plain, "unit": "ms/step",
             "gradients": "w.r.t. per-spring k, L and v0; checked against FP64 finite differences and an FP64 "
-                         "reference adjoint in the GPU tests"}
+                         "reference adjoint in the GPU tests",
+            "fp64": f64}
+
+
+def measure_adjoint_fp64(spec, k, L, target, local, steps, every, reps, window=40):
+    """The adjoint's 64-bit mode on the same workload: forward and backward
+    ms/step (same loss), and the gradient against FP64 central differences of
+    the same rollout on the workload's first `window` steps, a branch-stable
+    window (contacts detected, none pushing: the contact response makes the
+    rollout piecewise once vertices are pushed to the thickness and re-tested
+    there, and differences across those branches measure no derivative).
+    The check problem takes a random initial velocity and the linear loss
+    sum(w x_T); per parameter group the three largest and three random
+    components, each step balancing truncation against round-off (k: 1e-3
+    relative, L: 1e-6, v0: 1e-5); relative error = |g - fd| / max(|fd|, 1% of
+    the group's largest gradient)."""
+    import torch
+    from ysim_b200.adjoint import ClothRollout
+    c = spec.meshes[0]
+    dev = torch.device("cuda", local)
+    roll = ClothRollout(spec, steps=steps, checkpoint_every=every, device=local, precision=64)
+    stream = torch.cuda.ExternalStream(roll.scene.stream(), device=local)
+    kt = torch.tensor(k, dtype=torch.float64, device=dev, requires_grad=True)
+    Lt = torch.tensor(L, dtype=torch.float64, device=dev, requires_grad=True)
+    vt = torch.zeros((c.nV, 3), dtype=torch.float64, device=dev, requires_grad=True)
+    tgt = target.double()
+    fw, bw = [], []
+    for it in range(reps + 1):
+        kt.grad = Lt.grad = vt.grad = None
+        a, b, d = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+        torch.cuda.synchronize()
+        a.record(stream)
+        xT = roll(kt, Lt, vt)
+        b.record(stream)
+        ((xT - tgt) ** 2).sum(1).mean().backward()
+        d.record(stream)
+        torch.cuda.synchronize()
+        if it:
+            fw.append(a.elapsed_time(b) / steps)
+            bw.append(b.elapsed_time(d) / steps)
+    roll.close()
+    # finite-difference check on the branch-stable window
+    rng = np.random.default_rng(11)
+    v0 = torch.tensor(rng.normal(0, 0.02, (c.nV, 3)), device=dev)
+    w = torch.tensor(rng.normal(0, 1, (c.nV, 3)) / c.nV, device=dev)
+    roll = ClothRollout(spec, steps=window, checkpoint_every=every, device=local, precision=64)
+    params = [t.detach().clone().requires_grad_(True) for t in (kt, Lt, v0)]
+    (roll(*params) * w).sum().backward()
+    grads = [p.grad.cpu().numpy().reshape(-1) for p in params]
+    base = [p.detach().clone().reshape(-1) for p in params]
+
+    def loss(group, i, delta):
+        p = [b_.clone() for b_ in base]
+        p[group][i] += delta
+        with torch.no_grad():
+            return float((roll(p[0], p[1], p[2].reshape(-1, 3)) * w).sum())
+
+    worst, n = 0.0, 0
+    for group, g in enumerate(grads):
+        for i in list(np.argsort(-np.abs(g))[:3]) + list(rng.integers(len(g), size=3)):
+            i = int(i)
+            eps = 1e-3 * abs(float(base[0][i])) if group == 0 else (1e-6 if group == 1 else 1e-5)
+            fd = (loss(group, i, eps) - loss(group, i, -eps)) / (2 * eps)
+            worst = max(worst, abs(g[i] - fd) / max(abs(fd), 1e-2 * float(np.abs(g).max())))
+            n += 1
+    roll.close()
+    f, b = float(np.median(fw)), float(np.median(bw))
+    return {"forward_ms_per_step": f, "backward_ms_per_step": b, "backward_over_forward": b / f,
+            "fd_check": {"window_steps": window, "components": n, "worst_rel_err": worst,
+                         "loss": "sum(w x_T), random v0"},
+            "arithmetic": "binary64 throughout; bit-identical to the FP64 reference rollout in the GPU tests"}
 
 
 def run_batched(args, rank, world, local):

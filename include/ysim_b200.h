@@ -287,6 +287,18 @@ ys_status ys_adjoint_set_params(ys_adjoint* a, const float* d_k, const float* d_
 ys_status ys_adjoint_forward(ys_adjoint* a, float* d_xT);
 /* dL/dx_T in; dL/dk, dL/dL (per spring) and dL/dv0 (3 floats per vertex) out. */
 ys_status ys_adjoint_backward(ys_adjoint* a, const float* d_dLdx, float* d_gk, float* d_gL, float* d_gv0);
+/* Arithmetic of the rollout and its reverse pass: 32 (default; the fused
+ * substep's binary32 arithmetic, bit-identical to the scene's own steps) or
+ * 64 (binary64 throughout, for gradients that must agree with FP64 finite
+ * differences; needs static obstacles, keeps at most 16 contacts per vertex
+ * and step, YS_ERR_CAPACITY beyond; the scene's own state is not advanced).
+ * The float entry points above then widen their inputs and round their
+ * outputs; the _f64 ones below take and give binary64 (device pointers,
+ * same layouts). */
+ys_status ys_adjoint_set_precision(ys_adjoint* a, int bits);
+ys_status ys_adjoint_set_params_f64(ys_adjoint* a, const double* d_k, const double* d_L, const double* d_v0);
+ys_status ys_adjoint_forward_f64(ys_adjoint* a, double* d_xT);
+ys_status ys_adjoint_backward_f64(ys_adjoint* a, const double* d_dLdx, double* d_gk, double* d_gL, double* d_gv0);
 
 /* ---- Standalone LBVH over one triangle soup (BVH<CUDA,PR,LINEAR,TRIANGLE>,
  * bvh.hpp:141-2308).  Device pointers; x / v packed xyz floats. ---------- */

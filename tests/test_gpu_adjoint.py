@@ -162,3 +162,122 @@ def test_checkpoint_interval_does_not_change_gradients(cuda_lib):
     for o in out[1:]:
         for a, b in zip(out[0], o):
             assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
+
+
+# ---------------------------------------------------------------- 64-bit mode
+def _f32_spec(spec):
+    """The scene keeps its parameters in binary32; the FP64 reference is given
+    the same values, so that both FP64 rollouts solve one problem."""
+    import dataclasses
+    r = lambda v: float(np.float32(v))
+    p = spec.params
+    spec.params = dataclasses.replace(p, subh=r(p.subh), kd=r(p.kd), kair=r(p.kair), margin=r(p.margin),
+                                      radius=r(p.radius), gravity=tuple(r(g) for g in p.gravity))
+    spec.meshes[0].thickness = r(spec.meshes[0].thickness)
+    return spec
+
+
+def _roll64(spec, k, L, v0, T, K=5):
+    import torch
+    from ysim_b200.adjoint import ClothRollout
+    roll = ClothRollout(spec, steps=T, checkpoint_every=K, precision=64)
+    t = [torch.tensor(np.asarray(a, np.float64), device="cuda", requires_grad=True) for a in (k, L, v0)]
+    return roll, t
+
+
+# Bit-for-bit agreement holds on any window, pushes and releases included:
+# both FP64 rollouts take the same branch at every test because they compute
+# the same binary64 values.
+@pytest.mark.parametrize("height,T", [(0.5, 40), (0.2995, 60), (0.2995, 25)],
+                         ids=["contact_free_40", "contacts_60_pushes", "contacts_25"])
+def test_fp64_adjoint_matches_fp64_reference_bit_for_bit(cuda_lib, height, T):
+    import torch
+    spec = _f32_spec(_small(height=height))
+    k, L, v0, w, R = _problem(spec)
+    w64 = w.astype(np.float64)
+    x64, ncontacts = R.forward(T, keep=True)
+    assert (ncontacts > 0) == (height < 0.4)
+    gk64, gL64, gv64 = R.backward(T, w64)
+    roll, (kt, Lt, vt) = _roll64(spec, k, L, v0, T, K=7)
+    try:
+        xT = roll(kt, Lt, vt)
+        assert xT.dtype == torch.float64
+        assert np.array_equal(xT.detach().cpu().numpy(), x64)
+        (xT * torch.tensor(w64, device="cuda")).sum().backward()
+        assert np.array_equal(kt.grad.cpu().numpy(), gk64)
+        assert np.array_equal(Lt.grad.cpu().numpy(), gL64)
+        assert np.array_equal(vt.grad.cpu().numpy(), gv64)
+    finally:
+        roll.close()
+
+
+@pytest.mark.parametrize("height,contacts", WINDOWS)
+def test_fp64_adjoint_within_1e4_of_fp64_finite_differences(cuda_lib, height, contacts):
+    """Central differences of the GPU's own FP64 rollout, per parameter group
+    at the step that balances truncation against round-off (k: 1e-3
+    relative; L: 1e-6; v0: 1e-5), on the largest and on random components;
+    each must agree with the adjoint to 1e-4 of the larger of |fd| and 1% of
+    the group's largest gradient."""
+    import torch
+    spec = _f32_spec(_small(height=height))
+    k, L, v0, w, _ = _problem(spec)
+    T = _window(spec, v0, contacts)
+    w64 = torch.tensor(w.astype(np.float64), device="cuda")
+    roll, (kt, Lt, vt) = _roll64(spec, k, L, v0, T)
+    try:
+        (roll(kt, Lt, vt) * w64).sum().backward()
+        grads = [kt.grad.cpu().numpy().reshape(-1), Lt.grad.cpu().numpy().reshape(-1), vt.grad.cpu().numpy().reshape(-1)]
+        base = [t.detach().clone().reshape(-1) for t in (kt, Lt, vt)]
+
+        def loss(group, i, delta):
+            p = [b.clone() for b in base]
+            p[group][i] += delta
+            with torch.no_grad():
+                return float((roll(p[0], p[1], p[2].reshape(-1, 3)) * w64).sum())
+
+        rng = np.random.default_rng(7)
+        worst = 0.0
+        for group, g in enumerate(grads):
+            idx = list(np.argsort(-np.abs(g))[:3]) + list(rng.integers(len(g), size=3))
+            for i in idx:
+                eps = 1e-3 * abs(float(base[0][i])) if group == 0 else (1e-6 if group == 1 else 1e-5)
+                fd = (loss(group, int(i), eps) - loss(group, int(i), -eps)) / (2 * eps)
+                err = abs(g[i] - fd) / max(abs(fd), 1e-2 * np.abs(g).max())
+                worst = max(worst, err)
+                assert err <= 1e-4, (group, int(i), g[i], fd, err)
+        print("fp64 adjoint vs fp64 fd, worst relative error", worst)
+    finally:
+        roll.close()
+
+
+def test_fp64_mode_float_entry_points_and_checkpoints(cuda_lib):
+    """Float tensors through the 64-bit mode give the binary64 results
+    rounded; checkpoint intervals leave the binary64 gradients unchanged."""
+    import torch
+    spec = _f32_spec(_small())
+    T = 24
+    k, L, v0, w, R = _problem(spec, seed=1)
+    x64, _ = R.forward(T, keep=True)
+    g64 = R.backward(T, w.astype(np.float64))
+    from ysim_b200.adjoint import ClothRollout
+    roll = ClothRollout(spec, steps=T, checkpoint_every=5, precision=64)
+    try:
+        kt, Lt, vt = (torch.tensor(a, device="cuda", requires_grad=True) for a in (k, L, v0))
+        xT = roll(kt, Lt, vt)
+        assert xT.dtype == torch.float32
+        assert np.array_equal(xT.detach().cpu().numpy(), x64.astype(np.float32))
+        (xT * torch.tensor(w, device="cuda")).sum().backward()
+        for got, want in zip((kt.grad, Lt.grad, vt.grad), g64):
+            assert np.array_equal(got.cpu().numpy(), want.astype(np.float32))
+    finally:
+        roll.close()
+    out = []
+    for K in (1, 24):
+        roll, (kt, Lt, vt) = _roll64(spec, k, L, v0, T, K=K)
+        try:
+            (roll(kt, Lt, vt) * torch.tensor(w.astype(np.float64), device="cuda")).sum().backward()
+            out.append([t.grad.cpu().numpy() for t in (kt, Lt, vt)])
+        finally:
+            roll.close()
+    for a, b, c in zip(out[0], out[1], g64):
+        assert np.array_equal(a, b) and np.array_equal(a, c)

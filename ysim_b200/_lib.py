@@ -144,6 +144,10 @@ _PROTOS = {
     "ys_adjoint_set_params": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "ys_adjoint_forward": (C.c_int, [C.c_void_p, C.c_void_p]),
     "ys_adjoint_backward": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "ys_adjoint_set_precision": (C.c_int, [C.c_void_p, C.c_int]),
+    "ys_adjoint_set_params_f64": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "ys_adjoint_forward_f64": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "ys_adjoint_backward_f64": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "ys_morton_codes": (C.c_int, [C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p,
                                   C.c_void_p]),
     "ys_radix_sort_scratch_bytes": (C.c_size_t, [C.c_uint32]),

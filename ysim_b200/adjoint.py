@@ -13,6 +13,13 @@ reverse kernels (springs, semi-implicit integration, contact projection with
 the forward's active set).  Gradients are w.r.t. per-spring stiffness, rest
 length (canonical spring order, see generators.grid_spring_params) and the
 cloth's initial velocity.
+
+    roll = ClothRollout(spec, steps=200, precision=64)
+    xT = roll(k64, L64, v064)      # float64 tensors: binary64 in and out
+
+precision=64 runs the rollout and its reverse pass in binary64 (the FP64
+reference rollout's operations; the gradients then agree with FP64 finite
+differences), float32 tensors are widened and the results rounded.
 """
 from __future__ import annotations
 
@@ -39,7 +46,8 @@ class _Fn(torch.autograd.Function):
 
 
 class ClothRollout:
-    def __init__(self, spec: SceneSpec, steps: int, checkpoint_every: int = 20, device: int = 0):
+    def __init__(self, spec: SceneSpec, steps: int, checkpoint_every: int = 20, device: int = 0,
+                 precision: int = 32):
         self.scene = Scene(spec, device=device)
         self.lib = self.scene.lib
         self.device = torch.device("cuda", device)
@@ -50,6 +58,10 @@ class ClothRollout:
         self.h = h
         self.S = int(self.lib.ys_adjoint_num_springs(self.h))
         self.steps = steps
+        self.precision = precision
+        self._f64 = False  # the last forward took binary64 tensors
+        if precision != 32:
+            _lib.check(self.lib.ys_adjoint_set_precision(self.h, precision), "ys_adjoint_set_precision")
 
     def close(self):
         if getattr(self, "h", None):
@@ -71,6 +83,16 @@ class ClothRollout:
         torch.cuda.current_stream(self.device).synchronize()
 
     def _forward(self, k, L, v0):
+        self._f64 = self.precision == 64 and k.dtype == torch.float64
+        if self._f64:
+            k, L, v0 = (t.detach().contiguous().double() for t in (k, L, v0))
+            assert k.numel() == self.S and L.numel() == self.S and v0.numel() == 3 * self.nV
+            self._sync_torch()
+            _lib.check(self.lib.ys_adjoint_set_params_f64(self.h, self._p(k), self._p(L), self._p(v0)),
+                       "set_params_f64")
+            xT = torch.empty((self.nV, 3), dtype=torch.float64, device=self.device)
+            _lib.check(self.lib.ys_adjoint_forward_f64(self.h, self._p(xT)), "ys_adjoint_forward_f64")
+            return xT
         k = k.detach().contiguous().float()
         L = L.detach().contiguous().float()
         v0 = v0.detach().contiguous().float()
@@ -83,6 +105,15 @@ class ClothRollout:
         return xT
 
     def _backward(self, gx):
+        if self._f64:
+            gx = gx.contiguous().double()
+            gk = torch.empty(self.S, dtype=torch.float64, device=self.device)
+            gL = torch.empty(self.S, dtype=torch.float64, device=self.device)
+            gv = torch.empty((self.nV, 3), dtype=torch.float64, device=self.device)
+            self._sync_torch()
+            _lib.check(self.lib.ys_adjoint_backward_f64(self.h, self._p(gx), self._p(gk), self._p(gL), self._p(gv)),
+                       "ys_adjoint_backward_f64")
+            return gk, gL, gv
         gx = gx.contiguous().float()
         gk = torch.empty(self.S, dtype=torch.float32, device=self.device)
         gL = torch.empty(self.S, dtype=torch.float32, device=self.device)

@@ -2305,6 +2305,8 @@ __global__ void k_mesh_unpack4(const float4* __restrict__ in, float* __restrict_
 
 }  // namespace ys
 
+#include "ys_adj64.cuh"
+
 struct ys_adjoint {
     ys_scene* s = nullptr;
     int mesh = 0;
@@ -2320,6 +2322,22 @@ struct ys_adjoint {
     std::vector<DBuf<VContact>> st_pool;
     DBuf<float4> ax, av, ax2, av2, xbar, vbar, fbar;
     bool forward_done = false;
+    // 64-bit mode (ys_adjoint_set_precision): the cloth's state in binary64
+    // (local vertex index), the parameters, checkpoints, one segment of
+    // recorded steps (states and sorted contacts), the reverse-pass buffers
+    int bits = 32;
+    DBuf<D4> d_x0, d_v0;
+    DBuf<double> d_k, d_L;
+    std::vector<DBuf<D4>> dck_x, dck_xp, dck_v, dst_x, dst_v;
+    std::vector<DBuf<DContact>> dst_c;
+    std::vector<DBuf<u32>> dst_f, dst_n;
+    DBuf<D4> dX[3], dV[2];
+    DBuf<DContact> dsc_c;  // contacts of steps that are not recorded
+    DBuf<u32> dsc_f, dsc_n;
+    DBuf<D4> dax, dav, dax2, dav2, dxbar, dvbar, dfbar;
+    DBuf<double> dgk, dgL;
+    DBuf<unsigned long long> dbox;
+    DBuf<u32> dstatus;
 };
 
 namespace {
@@ -2336,6 +2354,217 @@ void restore_state(ys_scene* s, const float4* x, const float4* xp, const float4*
     s->frame = frame;
     s->cursor = cursor;
     s->snapshot_pending = false;
+}
+
+// ---- 64-bit mode
+void d64_free(ys_adjoint* a) {
+    for (auto* v : {&a->dck_x, &a->dck_xp, &a->dck_v, &a->dst_x, &a->dst_v}) {
+        for (auto& b : *v) b.free();
+        v->clear();
+    }
+    for (auto& b : a->dst_c) b.free();
+    for (auto& b : a->dst_f) b.free();
+    for (auto& b : a->dst_n) b.free();
+    a->dst_c.clear(); a->dst_f.clear(); a->dst_n.clear();
+    for (auto* b : {&a->d_x0, &a->d_v0, &a->dX[0], &a->dX[1], &a->dX[2], &a->dV[0], &a->dV[1], &a->dax, &a->dav,
+                    &a->dax2, &a->dav2, &a->dxbar, &a->dvbar, &a->dfbar})
+        b->free();
+    a->d_k.free(); a->d_L.free(); a->dgk.free(); a->dgL.free();
+    a->dsc_c.free(); a->dsc_f.free(); a->dsc_n.free(); a->dbox.free(); a->dstatus.free();
+}
+
+cudaError_t d64_alloc(ys_adjoint* a) {
+    const size_t n = a->nV, c = (size_t)a->nV * D64_CAP;
+    cudaError_t e;
+    for (auto* b : {&a->d_x0, &a->d_v0, &a->dX[0], &a->dX[1], &a->dX[2], &a->dV[0], &a->dV[1], &a->dax, &a->dav,
+                    &a->dax2, &a->dav2, &a->dxbar, &a->dvbar, &a->dfbar})
+        if ((e = b->alloc(n))) return e;
+    if ((e = a->d_k.alloc(a->S)) || (e = a->d_L.alloc(a->S)) || (e = a->dgk.alloc(a->S)) || (e = a->dgL.alloc(a->S)))
+        return e;
+    if ((e = a->dsc_c.alloc(c)) || (e = a->dsc_f.alloc(c)) || (e = a->dsc_n.alloc(n)) || (e = a->dbox.alloc(6)) ||
+        (e = a->dstatus.alloc(1)))
+        return e;
+    a->dck_x.resize(a->nseg); a->dck_xp.resize(a->nseg); a->dck_v.resize(a->nseg);
+    for (u32 i = 0; i < a->nseg; ++i)
+        if ((e = a->dck_x[i].alloc(n)) || (e = a->dck_xp[i].alloc(n)) || (e = a->dck_v[i].alloc(n))) return e;
+    a->dst_x.resize(a->K); a->dst_v.resize(a->K); a->dst_c.resize(a->K); a->dst_f.resize(a->K); a->dst_n.resize(a->K);
+    for (u32 i = 0; i < a->K; ++i)
+        if ((e = a->dst_x[i].alloc(n)) || (e = a->dst_v[i].alloc(n)) || (e = a->dst_c[i].alloc(c)) ||
+            (e = a->dst_f[i].alloc(c)) || (e = a->dst_n[i].alloc(n)))
+            return e;
+    return cudaSuccess;
+}
+
+// The per-spring parameters the float path would use, widened: the mesh's
+// per-spring arrays once set, else FastGridClothBehaviorParams' per-family
+// stiffness and rest length.
+ys_status d64_params_from_scene(ys_adjoint* a) {
+    ys_scene* s = a->s;
+    const HostMesh& H = s->meshes[a->mesh];
+    const MeshDev& M = s->hmeshes[a->mesh];
+    cudaStream_t st = s->stream;
+    if (H.grid_springs_on) {
+        k_d64_widen<<<ceil_div(a->S, 256), 256, 0, st>>>(s->gk.p + M.gspr, a->d_k.p, a->S);
+        k_d64_widen<<<ceil_div(a->S, 256), 256, 0, st>>>(s->gL.p + M.gspr, a->d_L.p, a->S);
+        YS_CK(cudaGetLastError());
+        return YS_OK;
+    }
+    const size_t n = a->N;
+    const size_t cnt[6] = {n * (n - 1), (n - 1) * n, (n - 1) * (n - 1), (n - 1) * (n - 1), n * (n - 2), (n - 2) * n};
+    const float kf[6] = {M.kstretch, M.kstretch, M.kshear, M.kshear, M.kbend, M.kbend};
+    std::vector<double> k, L;
+    k.reserve(a->S); L.reserve(a->S);
+    for (int f = 0; f < 6; ++f) {
+        k.insert(k.end(), cnt[f], (double)kf[f]);
+        L.insert(L.end(), cnt[f], (double)M.rest[f]);
+    }
+    YS_CK(cudaMemcpyAsync(a->d_k.p, k.data(), 8 * (size_t)a->S, cudaMemcpyHostToDevice, st));
+    YS_CK(cudaMemcpyAsync(a->d_L.p, L.data(), 8 * (size_t)a->S, cudaMemcpyHostToDevice, st));
+    YS_CK(cudaStreamSynchronize(st));  // k, L live on the host stack
+    return YS_OK;
+}
+
+// Trees of the obstacles the cloth queries (built on first use).
+ys_status d64_trees(ys_adjoint* a) {
+    ys_scene* s = a->s;
+    bool any = false;
+    for (size_t m = 0; m < s->meshes.size(); ++m) {
+        HostMesh& H = s->meshes[m];
+        if ((int)m == a->mesh || H.built || !H.needs_tree || H.d.num_facets == 0) continue;
+        ys_status r = build_tree(s, H);
+        if (r) return r;
+        any = true;
+    }
+    return any ? build_levels(s) : YS_OK;
+}
+
+A64 d64_args(ys_adjoint* a) {
+    ys_scene* s = a->s;
+    const MeshDev& M = s->hmeshes[a->mesh];
+    A64 A;
+    memset(&A, 0, sizeof(A));
+    A.sx = s->X[s->cur].p;
+    A.F = s->F4.p;
+    A.nodes = s->nodes.p;
+    A.meshes = s->dmeshes.p;
+    A.targets = s->targets.p;
+    A.ext = s->use_ext ? s->ext.p : nullptr;
+    A.mass = s->mass.p;
+    A.mask = s->mask.p;
+    A.tgt_begin = M.tgt_begin;
+    A.tgt_end = M.tgt_end;
+    A.cloth = (u32)a->mesh;
+    A.voff = a->voff;
+    A.nV = a->nV;
+    A.N = a->N;
+    A.gx = s->P.gravity[0]; A.gy = s->P.gravity[1]; A.gz = s->P.gravity[2];
+    A.kair = s->P.kair; A.kd = s->P.kd; A.subh = s->P.subh;
+    A.thickness = M.thickness;
+    A.margin = s->P.margin;
+    A.radius = s->P.radius;
+    A.k = a->d_k.p;
+    A.L = a->d_L.p;
+    A.box = a->dbox.p;
+    A.status = a->dstatus.p;
+    return A;
+}
+
+void d64_step(ys_adjoint* a, A64 A, cudaStream_t st) {
+    cudaMemsetAsync(a->dbox.p, 0, 6 * sizeof(unsigned long long), st);
+    const u32 gb = std::min<u32>(ceil_div(a->nV, 256), 148 * 4);
+    k_d64_box<<<gb, 256, 0, st>>>(A);
+    k_d64_step<<<ceil_div(a->nV, 128), 128, 0, st>>>(A);
+}
+
+ys_status d64_status(ys_adjoint* a) {
+    u32 f = 0;
+    YS_CK(cudaMemcpyAsync(&f, a->dstatus.p, 4, cudaMemcpyDeviceToHost, a->s->stream));
+    YS_CK(cudaStreamSynchronize(a->s->stream));
+    if (f & YS_FLAG_CONTACT_OVF) return fail(YS_ERR_CAPACITY, "FP64 rollout: more than 16 contacts at a vertex");
+    if (f & YS_FLAG_STACK_OVF) return fail(YS_ERR_CAPACITY, "FP64 rollout: tree descent stack exceeded");
+    return YS_OK;
+}
+
+// Forward rollout in binary64 from (d_x0, d_v0); x_T stays in the returned
+// buffer.  Checkpoints every K steps.
+ys_status d64_forward(ys_adjoint* a, const D4** xT) {
+    ys_scene* s = a->s;
+    cudaStream_t st = s->stream;
+    ys_status r = d64_trees(a);
+    if (r) return r;
+    const size_t bytes = sizeof(D4) * a->nV;
+    D4 *x = a->dX[0].p, *xp = a->dX[1].p, *xn = a->dX[2].p, *v = a->dV[0].p, *vn = a->dV[1].p;
+    YS_CK(cudaMemcpyAsync(x, a->d_x0.p, bytes, cudaMemcpyDeviceToDevice, st));
+    YS_CK(cudaMemcpyAsync(xp, a->d_x0.p, bytes, cudaMemcpyDeviceToDevice, st));
+    YS_CK(cudaMemcpyAsync(v, a->d_v0.p, bytes, cudaMemcpyDeviceToDevice, st));
+    YS_CK(cudaMemsetAsync(a->dstatus.p, 0, 4, st));
+    A64 A = d64_args(a);
+    A.cs = a->dsc_c.p; A.cf = a->dsc_f.p; A.cn = a->dsc_n.p;
+    for (u32 t = 0; t < a->T; ++t) {
+        if (t % a->K == 0) {
+            const u32 i = t / a->K;
+            YS_CK(cudaMemcpyAsync(a->dck_x[i].p, x, bytes, cudaMemcpyDeviceToDevice, st));
+            YS_CK(cudaMemcpyAsync(a->dck_xp[i].p, xp, bytes, cudaMemcpyDeviceToDevice, st));
+            YS_CK(cudaMemcpyAsync(a->dck_v[i].p, v, bytes, cudaMemcpyDeviceToDevice, st));
+        }
+        A.x = x; A.xp = xp; A.v = v; A.xn = xn; A.vn = vn;
+        d64_step(a, A, st);
+        D4* old_xp = xp;
+        xp = x; x = xn; xn = old_xp;
+        std::swap(v, vn);
+    }
+    YS_CK(cudaGetLastError());
+    r = d64_status(a);
+    if (r) return r;
+    *xT = x;
+    a->forward_done = true;
+    return YS_OK;
+}
+
+// Reverse pass in binary64; the seed dL/dx_T is in dax on entry.  Each
+// segment is replayed from its checkpoint with its states and contacts
+// recorded, then reversed step by step.
+ys_status d64_backward(ys_adjoint* a) {
+    ys_scene* s = a->s;
+    cudaStream_t st = s->stream;
+    const size_t bytes = sizeof(D4) * a->nV;
+    YS_CK(cudaMemsetAsync(a->dav.p, 0, bytes, st));
+    YS_CK(cudaMemsetAsync(a->dgk.p, 0, 8 * (size_t)a->S, st));
+    YS_CK(cudaMemsetAsync(a->dgL.p, 0, 8 * (size_t)a->S, st));
+    YS_CK(cudaMemsetAsync(a->dstatus.p, 0, 4, st));
+    A64 A = d64_args(a);
+    for (int seg = (int)a->nseg - 1; seg >= 0; --seg) {
+        const u32 t0 = (u32)seg * a->K, t1 = std::min(a->T, t0 + a->K);
+        D4 *xp = a->dX[1].p, *xn = a->dX[2].p, *vn = a->dV[1].p;
+        YS_CK(cudaMemcpyAsync(xp, a->dck_xp[seg].p, bytes, cudaMemcpyDeviceToDevice, st));
+        YS_CK(cudaMemcpyAsync(a->dst_x[0].p, a->dck_x[seg].p, bytes, cudaMemcpyDeviceToDevice, st));
+        YS_CK(cudaMemcpyAsync(a->dst_v[0].p, a->dck_v[seg].p, bytes, cudaMemcpyDeviceToDevice, st));
+        for (u32 t = t0; t < t1; ++t) {
+            const u32 k = t - t0;
+            A.x = a->dst_x[k].p; A.xp = xp; A.v = a->dst_v[k].p;
+            // the step's outputs go straight into the next step's record
+            const bool last = k + 1 == t1 - t0;
+            A.xn = last ? xn : a->dst_x[k + 1].p;
+            A.vn = last ? vn : a->dst_v[k + 1].p;
+            A.cs = a->dst_c[k].p; A.cf = a->dst_f[k].p; A.cn = a->dst_n[k].p;
+            d64_step(a, A, st);
+            xp = a->dst_x[k].p;
+        }
+        for (int t = (int)t1 - 1; t >= (int)t0; --t) {
+            const u32 k = (u32)t - t0;
+            A.x = a->dst_x[k].p; A.v = a->dst_v[k].p;
+            A.cs = a->dst_c[k].p; A.cf = a->dst_f[k].p; A.cn = a->dst_n[k].p;
+            J64 J;
+            J.ax = a->dax.p; J.av = a->dav.p; J.xbar = a->dxbar.p; J.vbar = a->dvbar.p; J.fbar = a->dfbar.p;
+            J.ax_out = a->dax2.p; J.av_out = a->dav2.p; J.gk = a->dgk.p; J.gL = a->dgL.p;
+            k_d64_adj_vertex<<<ceil_div(a->nV, 128), 128, 0, st>>>(A, J);
+            k_d64_adj_springs<<<ceil_div(a->nV, 128), 128, 0, st>>>(A, J);
+            std::swap(a->dax.p, a->dax2.p);
+            std::swap(a->dav.p, a->dav2.p);
+        }
+    }
+    YS_CK(cudaGetLastError());
+    return d64_status(a);
 }
 
 }  // namespace
@@ -2434,6 +2663,7 @@ ys_status ys_adjoint_destroy(ys_adjoint* a) {
     for (auto& b : a->st_pool) b.free();
     a->x0.free(); a->v0.free(); a->ax.free(); a->av.free(); a->ax2.free(); a->av2.free();
     a->xbar.free(); a->vbar.free(); a->fbar.free();
+    d64_free(a);
     delete a;
     return YS_OK;
 }
@@ -2451,8 +2681,93 @@ ys_status ys_adjoint_set_params(ys_adjoint* a, const float* d_k, const float* d_
         if (r) return r;
     }
     if (d_v0) k_mesh_pack4<<<ceil_div(a->nV, 256), 256, 0, s->stream>>>(d_v0, a->v0.p, a->voff, a->nV);
+    if (a->bits == 64) {  // the same values, widened
+        if (d_k) k_d64_widen<<<ceil_div(a->S, 256), 256, 0, s->stream>>>(d_k, a->d_k.p, a->S);
+        if (d_L) k_d64_widen<<<ceil_div(a->S, 256), 256, 0, s->stream>>>(d_L, a->d_L.p, a->S);
+        if (d_v0) k_d64_from_f3<<<ceil_div(a->nV, 256), 256, 0, s->stream>>>(d_v0, a->d_v0.p, a->nV);
+    }
     YS_CK(cudaGetLastError());
     a->forward_done = false;
+    return YS_OK;
+}
+
+// Arithmetic of the rollout and its reverse pass: 32 (the fused substep's
+// own binary32 arithmetic, the default) or 64 (binary64 throughout, the
+// operations of the FP64 reference rollout; the scene's state is left as it
+// is).  Switching to 64 widens the current parameters and initial state.
+ys_status ys_adjoint_set_precision(ys_adjoint* a, int bits) {
+    if (!a) return fail(YS_ERR_BAD_ARG, "null adjoint");
+    if (bits != 32 && bits != 64) return fail(YS_ERR_BAD_ARG, "precision is 32 or 64 bits");
+    if (bits == a->bits) return YS_OK;
+    ys_scene* s = a->s;
+    a->forward_done = false;
+    if (bits == 32) {
+        YS_CK(cudaStreamSynchronize(s->stream));
+        d64_free(a);
+        a->bits = 32;
+        return YS_OK;
+    }
+    for (size_t m = 0; m < s->meshes.size(); ++m)
+        if ((int)m != a->mesh && s->meshes[m].d.num_facets && !(s->meshes[m].flags & MF_STATIC))
+            return fail(YS_ERR_BAD_ARG, "the FP64 rollout needs static obstacles");
+    cudaError_t e = d64_alloc(a);
+    if (e) {
+        d64_free(a);
+        return fail(YS_ERR_CUDA, cudaGetErrorString(e));
+    }
+    k_d64_from_f4<<<ceil_div(a->nV, 256), 256, 0, s->stream>>>(a->x0.p, a->d_x0.p, a->voff, a->nV);
+    k_d64_from_f4<<<ceil_div(a->nV, 256), 256, 0, s->stream>>>(a->v0.p, a->d_v0.p, a->voff, a->nV);
+    YS_CK(cudaGetLastError());
+    ys_status r = d64_params_from_scene(a);
+    if (r) {
+        d64_free(a);
+        return r;
+    }
+    a->bits = 64;
+    return YS_OK;
+}
+
+// 64-bit mode: parameters in binary64 (device pointers, NULL keeps).
+ys_status ys_adjoint_set_params_f64(ys_adjoint* a, const double* d_k, const double* d_L, const double* d_v0) {
+    if (!a) return fail(YS_ERR_BAD_ARG, "null adjoint");
+    if (a->bits != 64) return fail(YS_ERR_STATE, "set the adjoint's precision to 64 first");
+    cudaStream_t st = a->s->stream;
+    if (d_k) YS_CK(cudaMemcpyAsync(a->d_k.p, d_k, 8 * (size_t)a->S, cudaMemcpyDeviceToDevice, st));
+    if (d_L) YS_CK(cudaMemcpyAsync(a->d_L.p, d_L, 8 * (size_t)a->S, cudaMemcpyDeviceToDevice, st));
+    if (d_v0) k_d64_from_d3<<<ceil_div(a->nV, 256), 256, 0, st>>>(d_v0, a->d_v0.p, a->nV);
+    YS_CK(cudaGetLastError());
+    a->forward_done = false;
+    return YS_OK;
+}
+
+// 64-bit mode: forward rollout; x_T (3 doubles per vertex) into d_xT.
+ys_status ys_adjoint_forward_f64(ys_adjoint* a, double* d_xT) {
+    if (!a) return fail(YS_ERR_BAD_ARG, "null adjoint");
+    if (a->bits != 64) return fail(YS_ERR_STATE, "set the adjoint's precision to 64 first");
+    const D4* x = nullptr;
+    ys_status r = d64_forward(a, &x);
+    if (r) return r;
+    if (d_xT) k_d64_to_d3<<<ceil_div(a->nV, 256), 256, 0, a->s->stream>>>(x, d_xT, a->nV);
+    YS_CK(cudaGetLastError());
+    YS_CK(cudaStreamSynchronize(a->s->stream));
+    return YS_OK;
+}
+
+// 64-bit mode: reverse pass with binary64 seed and gradients.
+ys_status ys_adjoint_backward_f64(ys_adjoint* a, const double* d_dLdx, double* d_gk, double* d_gL, double* d_gv0) {
+    if (!a || !d_dLdx || !d_gk || !d_gL || !d_gv0) return fail(YS_ERR_BAD_ARG, "null argument");
+    if (a->bits != 64) return fail(YS_ERR_STATE, "set the adjoint's precision to 64 first");
+    if (!a->forward_done) return fail(YS_ERR_STATE, "run ys_adjoint_forward first");
+    cudaStream_t st = a->s->stream;
+    k_d64_from_d3<<<ceil_div(a->nV, 256), 256, 0, st>>>(d_dLdx, a->dax.p, a->nV);
+    YS_CK(cudaGetLastError());
+    ys_status r = d64_backward(a);
+    if (r) return r;
+    YS_CK(cudaMemcpyAsync(d_gk, a->dgk.p, 8 * (size_t)a->S, cudaMemcpyDeviceToDevice, st));
+    YS_CK(cudaMemcpyAsync(d_gL, a->dgL.p, 8 * (size_t)a->S, cudaMemcpyDeviceToDevice, st));
+    k_d64_to_d3<<<ceil_div(a->nV, 256), 256, 0, st>>>(a->dav.p, d_gv0, a->nV);
+    YS_CK(cudaGetLastError());
+    YS_CK(cudaStreamSynchronize(st));
     return YS_OK;
 }
 
@@ -2461,6 +2776,14 @@ ys_status ys_adjoint_set_params(ys_adjoint* a, const float* d_k, const float* d_
 ys_status ys_adjoint_forward(ys_adjoint* a, float* d_xT) {
     if (!a) return fail(YS_ERR_BAD_ARG, "null adjoint");
     ys_scene* s = a->s;
+    if (a->bits == 64) {
+        const D4* x = nullptr;
+        ys_status r = d64_forward(a, &x);
+        if (r) return r;
+        if (d_xT) k_d64_to_f3<<<ceil_div(a->nV, 256), 256, 0, s->stream>>>(x, d_xT, a->nV);
+        YS_CK(cudaGetLastError());
+        return YS_OK;
+    }
     restore_state(s, a->x0.p, a->x0.p, a->v0.p, 0, 0);
     const bool rec = s->record;
     s->record = false;
@@ -2493,6 +2816,18 @@ ys_status ys_adjoint_backward(ys_adjoint* a, const float* d_dLdx, float* d_gk, f
     if (!a->forward_done) return fail(YS_ERR_STATE, "run ys_adjoint_forward first");
     ys_scene* s = a->s;
     cudaStream_t st = s->stream;
+    if (a->bits == 64) {
+        k_d64_from_f3<<<ceil_div(a->nV, 256), 256, 0, st>>>(d_dLdx, a->dax.p, a->nV);
+        YS_CK(cudaGetLastError());
+        ys_status r = d64_backward(a);
+        if (r) return r;
+        k_d64_narrow<<<ceil_div(a->S, 256), 256, 0, st>>>(a->dgk.p, d_gk, a->S);
+        k_d64_narrow<<<ceil_div(a->S, 256), 256, 0, st>>>(a->dgL.p, d_gL, a->S);
+        k_d64_to_f3<<<ceil_div(a->nV, 256), 256, 0, st>>>(a->dav.p, d_gv0, a->nV);
+        YS_CK(cudaGetLastError());
+        YS_CK(cudaStreamSynchronize(st));
+        return YS_OK;
+    }
     const size_t bytes = sizeof(float4) * s->nV;
     YS_CK(cudaMemsetAsync(a->ax.p, 0, bytes, st));
     YS_CK(cudaMemsetAsync(a->av.p, 0, bytes, st));
