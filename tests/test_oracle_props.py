@@ -339,3 +339,16 @@ def test_c_abi_exports_every_declared_symbol():
     assert not missing, missing
     assert names <= set(_lib.EXPORTED) | {"ys_last_error", "ys_version"}, sorted(names - set(_lib.EXPORTED))
     assert lib.ys_version
+
+
+def test_scene_uploads_are_ordered_on_the_scene_stream():
+    """A scene runs on a non-blocking stream, which does not wait for work on
+    the legacy default stream: a plain cudaMemset, or a cudaMemcpy from
+    pageable host memory (which may return before its DMA lands), could
+    still be in flight when the scene's kernels read the buffer.  Every
+    upload and clear in the scene code therefore goes on the scene's stream
+    (read-backs after a stream synchronisation may stay synchronous)."""
+    import re
+    src = open(os.path.join(os.path.dirname(GOLD), "..", "ysim_b200", "csrc", "ys_scene.cu")).read()
+    assert not re.search(r"cudaMemset\(", src)
+    assert not re.search(r"cudaMemcpy\([^;]*cudaMemcpyHostToDevice\)", src)

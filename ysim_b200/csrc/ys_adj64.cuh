@@ -60,6 +60,9 @@ struct __align__(32) DContact { double nx, ny, nz, d; };
 static constexpr u32 D64_CAP = 16;    // contacts kept per vertex and step
 static constexpr int D64_STACK = 64;  // tree descent stack
 static constexpr u32 D64_VISIT_CAP = 1u << 20;
+// Block size of the per-vertex kernels (32 measured the same on the
+// 128x128 rollout: the step kernel is bound by its divergent descents).
+static constexpr u32 D64_BLOCK = 128;
 
 // Order-preserving map of binary64 onto u64 (larger double, larger key), so
 // that min / max are integer atomics; NaN is left out by the callers.
@@ -188,7 +191,7 @@ __global__ void __launch_bounds__(256) k_d64_box(A64 A) {
 
 // One step of the FP64 rollout: contacts (recorded sorted in cs / cf / cn),
 // forces, integration and the contact response.
-__global__ void __launch_bounds__(128) k_d64_step(A64 A) {
+__global__ void __launch_bounds__(D64_BLOCK) k_d64_step(A64 A) {
     const u32 i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= A.nV) return;
     const u32 g = A.voff + i;
@@ -288,7 +291,7 @@ struct J64 {
 
 // Reverse of the integration and the contact response of step t (the
 // forward's active set replayed from the recorded contacts).
-__global__ void __launch_bounds__(128) k_d64_adj_vertex(A64 A, J64 J) {
+__global__ void __launch_bounds__(D64_BLOCK) k_d64_adj_vertex(A64 A, J64 J) {
     const u32 i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= A.nV) return;
     const u32 g = A.voff + i;
@@ -333,7 +336,7 @@ __global__ void __launch_bounds__(128) k_d64_adj_vertex(A64 A, J64 J) {
 
 // Reverse of the spring and drag forces of step t: gathered per vertex, the
 // spring parameters' gradients accumulated by the lower-index end.
-__global__ void __launch_bounds__(128) k_d64_adj_springs(A64 A, J64 J) {
+__global__ void __launch_bounds__(D64_BLOCK) k_d64_adj_springs(A64 A, J64 J) {
     const u32 i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= A.nV) return;
     const int N = (int)A.N, row = (int)(i / A.N), col = (int)(i % A.N);

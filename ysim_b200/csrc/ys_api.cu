@@ -83,7 +83,10 @@ ys_status ys_lbvh_create(ys_lbvh** out, uint32_t maxPrims, int device, void* str
     if (e == cudaSuccess) e = cudaMalloc((void**)&t->status, 4);
     if (e == cudaSuccess) e = cudaMalloc(&t->scratch, sort_scratch_bytes(maxPrims));
     if (e == cudaSuccess) e = cudaMalloc((void**)&t->job, sizeof(RefitJob));
-    if (e == cudaSuccess) e = cudaMemset(t->status, 0, 4);
+    // completed before this returns: later launches may go to any stream,
+    // including non-blocking ones that do not wait for the legacy stream
+    if (e == cudaSuccess) e = cudaMemsetAsync(t->status, 0, 4, 0);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(0);
     if (e != cudaSuccess) {
         ys_lbvh_destroy(t);
         return fail(YS_ERR_CUDA, cudaGetErrorString(e));

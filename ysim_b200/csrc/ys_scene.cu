@@ -1085,8 +1085,7 @@ ys_status upload_jobs(ys_scene* s, bool levels) {
                 J.levels = (levels && J.w4) ? 1u : 0u;
             }
             if (!t.empty())
-                YS_CK(cudaMemcpy(s->jobs.p + (size_t)(c * 2 + w) * s->njobs, t.data(), t.size() * sizeof(RefitJob),
-                                 cudaMemcpyHostToDevice));
+                YS_CK(cudaMemcpyAsync(s->jobs.p + (size_t)(c * 2 + w) * s->njobs, t.data(), t.size() * sizeof(RefitJob), cudaMemcpyHostToDevice, s->stream)); YS_CK(cudaStreamSynchronize(s->stream));
         }
     return YS_OK;
 }
@@ -1241,7 +1240,7 @@ ys_status ensure_staged(ys_scene* s) {
     YS_CK(s->bucket.alloc(s->nV + 1));
     YS_CK(s->csr_off.alloc(s->nV + 1));
     YS_CK(s->Fbuf.alloc(s->nV));
-    YS_CK(cudaMemset(s->Fbuf.p, 0, s->nV * sizeof(float4)));
+    YS_CK(cudaMemsetAsync(s->Fbuf.p, 0, s->nV * sizeof(float4), s->stream));
     YS_CK(s->scanScratch.alloc(scan_scratch_bytes(s->nV + 1)));
     s->staged_ready = true;
     return YS_OK;
@@ -1252,8 +1251,8 @@ ys_status ensure_record(ys_scene* s) {
     YS_CK(s->pool.alloc(s->cap));
     YS_CK(s->vstart.alloc(s->nV));
     YS_CK(s->vcount.alloc(s->nV));
-    YS_CK(cudaMemset(s->vcount.p, 0, s->nV * 4));
-    YS_CK(cudaMemset(s->vstart.p, 0, s->nV * 4));
+    YS_CK(cudaMemsetAsync(s->vcount.p, 0, s->nV * 4, s->stream));
+    YS_CK(cudaMemsetAsync(s->vstart.p, 0, s->nV * 4, s->stream));
     s->record_ready = true;
     return YS_OK;
 }
@@ -1574,8 +1573,8 @@ ys_status ys_scene_pack(ys_scene* s) {
         YS_CK(s->w4.alloc(std::max(nW4, 1u))); YS_CK(s->leafW.alloc(std::max(nF, 1u)));
         YS_CK(s->leafWf.alloc(std::max(nF, 1u)));
         YS_CK(s->warrive.alloc(std::max(nW4, 1u))); YS_CK(s->wideScratch.alloc(wide_build_scratch_bytes(maxF)));
-        YS_CK(cudaMemset(s->warrive.p, 0, 4 * s->warrive.n));
-        YS_CK(s->wcount.alloc(s->meshes.size())); YS_CK(cudaMemset(s->wcount.p, 0, 4 * s->meshes.size()));
+        YS_CK(cudaMemsetAsync(s->warrive.p, 0, 4 * s->warrive.n, s->stream));
+        YS_CK(s->wcount.alloc(s->meshes.size())); YS_CK(cudaMemsetAsync(s->wcount.p, 0, 4 * s->meshes.size(), s->stream));
         YS_CK(s->hacc.alloc(std::max(nW4, 1u))); YS_CK(s->wlist.alloc(std::max(nW4, 1u)));
         YS_CK(s->hcount.alloc(MAX_LEVELS + 2)); YS_CK(s->hoff.alloc(MAX_LEVELS + 2));
         YS_CK(s->hcursor.alloc(MAX_LEVELS + 2));
@@ -1585,30 +1584,30 @@ ys_status ys_scene_pack(ys_scene* s) {
     // uploads
     DBuf<float> tmp3;
     YS_CK(tmp3.alloc(3 * (size_t)nV));
-    YS_CK(cudaMemcpy(tmp3.p, x3.data(), 12 * (size_t)nV, cudaMemcpyHostToDevice));
+    YS_CK(cudaMemcpyAsync(tmp3.p, x3.data(), 12 * (size_t)nV, cudaMemcpyHostToDevice, s->stream)); YS_CK(cudaStreamSynchronize(s->stream));
     for (auto& b : s->X) k_pack4<<<ceil_div(nV, 256), 256, 0, st>>>(tmp3.p, b.p, nV);
     YS_CK(cudaStreamSynchronize(st));
-    YS_CK(cudaMemcpy(tmp3.p, v3.data(), 12 * (size_t)nV, cudaMemcpyHostToDevice));
+    YS_CK(cudaMemcpyAsync(tmp3.p, v3.data(), 12 * (size_t)nV, cudaMemcpyHostToDevice, s->stream)); YS_CK(cudaStreamSynchronize(s->stream));
     for (auto& b : s->V) k_pack4<<<ceil_div(nV, 256), 256, 0, st>>>(tmp3.p, b.p, nV);
     YS_CK(cudaStreamSynchronize(st));
     tmp3.free();
-    YS_CK(cudaMemcpy(s->mass.p, mass.data(), 4 * (size_t)nV, cudaMemcpyHostToDevice));
-    YS_CK(cudaMemcpy(s->mask.p, mask.data(), 4 * (size_t)nV, cudaMemcpyHostToDevice));
-    YS_CK(cudaMemcpy(s->vobj.p, vobj.data(), 4 * (size_t)nV, cudaMemcpyHostToDevice));
-    if (!targets.empty()) YS_CK(cudaMemcpy(s->targets.p, targets.data(), 4 * targets.size(), cudaMemcpyHostToDevice));
-    YS_CK(cudaMemcpy(s->spr_off.p, spr_off.data(), 4 * (size_t)(nV + 1), cudaMemcpyHostToDevice));
-    YS_CK(cudaMemcpy(s->spr_split.p, spr_split.data(), 4 * (size_t)nV, cudaMemcpyHostToDevice));
+    YS_CK(cudaMemcpyAsync(s->mass.p, mass.data(), 4 * (size_t)nV, cudaMemcpyHostToDevice, s->stream)); YS_CK(cudaStreamSynchronize(s->stream));
+    YS_CK(cudaMemcpyAsync(s->mask.p, mask.data(), 4 * (size_t)nV, cudaMemcpyHostToDevice, s->stream)); YS_CK(cudaStreamSynchronize(s->stream));
+    YS_CK(cudaMemcpyAsync(s->vobj.p, vobj.data(), 4 * (size_t)nV, cudaMemcpyHostToDevice, s->stream)); YS_CK(cudaStreamSynchronize(s->stream));
+    if (!targets.empty()) YS_CK(cudaMemcpyAsync(s->targets.p, targets.data(), 4 * targets.size(), cudaMemcpyHostToDevice, s->stream)); YS_CK(cudaStreamSynchronize(s->stream));
+    YS_CK(cudaMemcpyAsync(s->spr_off.p, spr_off.data(), 4 * (size_t)(nV + 1), cudaMemcpyHostToDevice, s->stream)); YS_CK(cudaStreamSynchronize(s->stream));
+    YS_CK(cudaMemcpyAsync(s->spr_split.p, spr_split.data(), 4 * (size_t)nV, cudaMemcpyHostToDevice, s->stream)); YS_CK(cudaStreamSynchronize(s->stream));
     if (!spr_nbr.empty()) {
-        YS_CK(cudaMemcpy(s->spr_nbr.p, spr_nbr.data(), 4 * spr_nbr.size(), cudaMemcpyHostToDevice));
-        YS_CK(cudaMemcpy(s->spr_rest.p, spr_rest.data(), 4 * spr_rest.size(), cudaMemcpyHostToDevice));
+        YS_CK(cudaMemcpyAsync(s->spr_nbr.p, spr_nbr.data(), 4 * spr_nbr.size(), cudaMemcpyHostToDevice, s->stream)); YS_CK(cudaStreamSynchronize(s->stream));
+        YS_CK(cudaMemcpyAsync(s->spr_rest.p, spr_rest.data(), 4 * spr_rest.size(), cudaMemcpyHostToDevice, s->stream)); YS_CK(cudaStreamSynchronize(s->stream));
     }
-    YS_CK(cudaMemcpy(s->vaf_off.p, vaf_off.data(), 4 * (size_t)(nV + 1), cudaMemcpyHostToDevice));
-    if (!vaf.empty()) YS_CK(cudaMemcpy(s->vaf.p, vaf.data(), 4 * vaf.size(), cudaMemcpyHostToDevice));
+    YS_CK(cudaMemcpyAsync(s->vaf_off.p, vaf_off.data(), 4 * (size_t)(nV + 1), cudaMemcpyHostToDevice, s->stream)); YS_CK(cudaStreamSynchronize(s->stream));
+    if (!vaf.empty()) YS_CK(cudaMemcpyAsync(s->vaf.p, vaf.data(), 4 * vaf.size(), cudaMemcpyHostToDevice, s->stream)); YS_CK(cudaStreamSynchronize(s->stream));
     if (nF) {
-        YS_CK(cudaMemcpy(s->F4.p, F4.data(), 16 * (size_t)nF, cudaMemcpyHostToDevice));
-        YS_CK(cudaMemcpy(s->F3.p, F3.data(), 12 * (size_t)nF, cudaMemcpyHostToDevice));
+        YS_CK(cudaMemcpyAsync(s->F4.p, F4.data(), 16 * (size_t)nF, cudaMemcpyHostToDevice, s->stream)); YS_CK(cudaStreamSynchronize(s->stream));
+        YS_CK(cudaMemcpyAsync(s->F3.p, F3.data(), 12 * (size_t)nF, cudaMemcpyHostToDevice, s->stream)); YS_CK(cudaStreamSynchronize(s->stream));
     }
-    YS_CK(cudaMemcpy(s->dmeshes.p, md.data(), sizeof(MeshDev) * md.size(), cudaMemcpyHostToDevice));
+    YS_CK(cudaMemcpyAsync(s->dmeshes.p, md.data(), sizeof(MeshDev) * md.size(), cudaMemcpyHostToDevice, s->stream)); YS_CK(cudaStreamSynchronize(s->stream));
     s->hmeshes = md;
     // Analytic marker pairs: every (cloth query mesh with a tree, analytic
     // target), in target order; pair p owns threads [w, w + nV) of the staged
@@ -1631,12 +1630,12 @@ ys_status ys_scene_pack(ys_scene* s) {
         s->npairs = (u32)ap.size();
         s->apair_total = vb;
         YS_CK(s->tpair.alloc(tp.size()));
-        YS_CK(cudaMemcpy(s->tpair.p, tp.data(), 4 * tp.size(), cudaMemcpyHostToDevice));
+        YS_CK(cudaMemcpyAsync(s->tpair.p, tp.data(), 4 * tp.size(), cudaMemcpyHostToDevice, s->stream)); YS_CK(cudaStreamSynchronize(s->stream));
         if (!ap.empty()) {
             YS_CK(s->apairs.alloc(ap.size()));
-            YS_CK(cudaMemcpy(s->apairs.p, ap.data(), sizeof(uint4) * ap.size(), cudaMemcpyHostToDevice));
+            YS_CK(cudaMemcpyAsync(s->apairs.p, ap.data(), sizeof(uint4) * ap.size(), cudaMemcpyHostToDevice, s->stream)); YS_CK(cudaStreamSynchronize(s->stream));
             YS_CK(s->markers.alloc(2 * ap.size()));
-            YS_CK(cudaMemset(s->markers.p, 0, 4 * 2 * ap.size()));
+            YS_CK(cudaMemsetAsync(s->markers.p, 0, 4 * 2 * ap.size(), s->stream));
         }
         if (!s->shape_mesh.empty()) {
             // seeded at pack (Scene::packAnalyticShapes, scene.hpp:762-781):
@@ -1653,9 +1652,9 @@ ys_status ys_scene_pack(ys_scene* s) {
             YS_CK(cudaStreamSynchronize(s->stream));
         }
     }
-    YS_CK(cudaMemset(s->status.p, 0, 4));
-    YS_CK(cudaMemset(s->maxext.p, 0, 4 * s->meshes.size()));
-    YS_CK(cudaMemset(s->counters.p, 0, 8 * s->counters.n));
+    YS_CK(cudaMemsetAsync(s->status.p, 0, 4, s->stream));
+    YS_CK(cudaMemsetAsync(s->maxext.p, 0, 4 * s->meshes.size(), s->stream));
+    YS_CK(cudaMemsetAsync(s->counters.p, 0, 8 * s->counters.n, s->stream));
     // Which trees a query descends: the targets of every query mesh, and the
     // self-queried meshes.  A query mesh whose own tree nothing descends
     // still needs that tree's root box (the inter-object cull): a root-only
@@ -1738,7 +1737,7 @@ ys_status ys_scene_pack(ys_scene* s) {
         for (size_t j = 0; j < nacc; ++j)
             for (int k = 0; k < 3; ++k) acc[32 * j + k] = 0xFFFFFFFFu;
         YS_CK(s->rootAcc.alloc(acc.size()));
-        YS_CK(cudaMemcpy(s->rootAcc.p, acc.data(), 4 * acc.size(), cudaMemcpyHostToDevice));
+        YS_CK(cudaMemcpyAsync(s->rootAcc.p, acc.data(), 4 * acc.size(), cudaMemcpyHostToDevice, s->stream)); YS_CK(cudaStreamSynchronize(s->stream));
         for (size_t j = 0; j < s->hjobs.size(); ++j)
             if (s->hjobs[j].rootOnly) s->hjobs[j].rootAcc = s->rootAcc.p + 32 * j;
         for (size_t j = 0; j < hr.size(); ++j) hr[j].rootAcc = s->rootAcc.p + 32 * (s->njobs + j);
@@ -1746,13 +1745,13 @@ ys_status ys_scene_pack(ys_scene* s) {
     if (s->nrjobs) {
         YS_CK(s->rjobs.alloc(6 * (size_t)s->nrjobs));
         YS_CK(s->rchunks.alloc(chunks.size()));
-        YS_CK(cudaMemcpy(s->rchunks.p, chunks.data(), chunks.size() * sizeof(uint2), cudaMemcpyHostToDevice));
+        YS_CK(cudaMemcpyAsync(s->rchunks.p, chunks.data(), chunks.size() * sizeof(uint2), cudaMemcpyHostToDevice, s->stream)); YS_CK(cudaStreamSynchronize(s->stream));
         for (int c = 0; c < 3; ++c)
             for (int w = 0; w < 2; ++w) {
                 std::vector<RefitJob> t = hr;
                 for (auto& J : t) { J.x4 = s->X[c].p; J.v4 = s->V[w].p; }
-                YS_CK(cudaMemcpy(s->rjobs.p + (size_t)(c * 2 + w) * s->nrjobs, t.data(),
-                                 t.size() * sizeof(RefitJob), cudaMemcpyHostToDevice));
+                YS_CK(cudaMemcpyAsync(s->rjobs.p + (size_t)(c * 2 + w) * s->nrjobs, t.data(),
+                                 t.size() * sizeof(RefitJob), cudaMemcpyHostToDevice, s->stream)); YS_CK(cudaStreamSynchronize(s->stream));
             }
     }
     {
@@ -2338,6 +2337,10 @@ struct ys_adjoint {
     DBuf<double> dgk, dgL;
     DBuf<unsigned long long> dbox;
     DBuf<u32> dstatus;
+    cudaGraphExec_t g_fwd = nullptr, g_bwd = nullptr;  // the two passes, captured on first use
+    const D4* g_fwd_xT = nullptr;                      // buffer holding x_T after the forward graph
+    const D4* g_bwd_av = nullptr;                      // buffer holding dL/dv0 after the backward graph
+    A64 g_args;                                        // the scene-derived arguments the graphs hold
 };
 
 namespace {
@@ -2357,7 +2360,10 @@ void restore_state(ys_scene* s, const float4* x, const float4* xp, const float4*
 }
 
 // ---- 64-bit mode
+void d64_drop_graphs(ys_adjoint* a);
+
 void d64_free(ys_adjoint* a) {
+    d64_drop_graphs(a);
     for (auto* v : {&a->dck_x, &a->dck_xp, &a->dck_v, &a->dst_x, &a->dst_v}) {
         for (auto& b : *v) b.free();
         v->clear();
@@ -2473,7 +2479,7 @@ void d64_step(ys_adjoint* a, A64 A, cudaStream_t st) {
     cudaMemsetAsync(a->dbox.p, 0, 6 * sizeof(unsigned long long), st);
     const u32 gb = std::min<u32>(ceil_div(a->nV, 256), 148 * 4);
     k_d64_box<<<gb, 256, 0, st>>>(A);
-    k_d64_step<<<ceil_div(a->nV, 128), 128, 0, st>>>(A);
+    k_d64_step<<<ceil_div(a->nV, D64_BLOCK), D64_BLOCK, 0, st>>>(A);
 }
 
 ys_status d64_status(ys_adjoint* a) {
@@ -2485,13 +2491,10 @@ ys_status d64_status(ys_adjoint* a) {
     return YS_OK;
 }
 
-// Forward rollout in binary64 from (d_x0, d_v0); x_T stays in the returned
-// buffer.  Checkpoints every K steps.
-ys_status d64_forward(ys_adjoint* a, const D4** xT) {
-    ys_scene* s = a->s;
-    cudaStream_t st = s->stream;
-    ys_status r = d64_trees(a);
-    if (r) return r;
+// Enqueue the forward rollout in binary64 from (d_x0, d_v0), checkpoints
+// every K steps; *xT receives the buffer that will hold x_T.
+ys_status d64_enqueue_forward(ys_adjoint* a, const D4** xT) {
+    cudaStream_t st = a->s->stream;
     const size_t bytes = sizeof(D4) * a->nV;
     D4 *x = a->dX[0].p, *xp = a->dX[1].p, *xn = a->dX[2].p, *v = a->dV[0].p, *vn = a->dV[1].p;
     YS_CK(cudaMemcpyAsync(x, a->d_x0.p, bytes, cudaMemcpyDeviceToDevice, st));
@@ -2514,21 +2517,20 @@ ys_status d64_forward(ys_adjoint* a, const D4** xT) {
         std::swap(v, vn);
     }
     YS_CK(cudaGetLastError());
-    r = d64_status(a);
-    if (r) return r;
     *xT = x;
-    a->forward_done = true;
     return YS_OK;
 }
 
-// Reverse pass in binary64; the seed dL/dx_T is in dax on entry.  Each
+// Enqueue the reverse pass in binary64; the seed dL/dx_T is in dax.  Each
 // segment is replayed from its checkpoint with its states and contacts
-// recorded, then reversed step by step.
-ys_status d64_backward(ys_adjoint* a) {
-    ys_scene* s = a->s;
-    cudaStream_t st = s->stream;
+// recorded, then reversed step by step.  The adjoints ping-pong between
+// dax / dax2 and dav / dav2; the buffer holding dL/dv0 at the end (fixed by
+// T) goes to g_bwd_av, the spring gradients to dgk, dgL.
+ys_status d64_enqueue_backward(ys_adjoint* a) {
+    cudaStream_t st = a->s->stream;
     const size_t bytes = sizeof(D4) * a->nV;
-    YS_CK(cudaMemsetAsync(a->dav.p, 0, bytes, st));
+    D4 *ax = a->dax.p, *ax2 = a->dax2.p, *av = a->dav.p, *av2 = a->dav2.p;
+    YS_CK(cudaMemsetAsync(av, 0, bytes, st));
     YS_CK(cudaMemsetAsync(a->dgk.p, 0, 8 * (size_t)a->S, st));
     YS_CK(cudaMemsetAsync(a->dgL.p, 0, 8 * (size_t)a->S, st));
     YS_CK(cudaMemsetAsync(a->dstatus.p, 0, 4, st));
@@ -2555,15 +2557,70 @@ ys_status d64_backward(ys_adjoint* a) {
             A.x = a->dst_x[k].p; A.v = a->dst_v[k].p;
             A.cs = a->dst_c[k].p; A.cf = a->dst_f[k].p; A.cn = a->dst_n[k].p;
             J64 J;
-            J.ax = a->dax.p; J.av = a->dav.p; J.xbar = a->dxbar.p; J.vbar = a->dvbar.p; J.fbar = a->dfbar.p;
-            J.ax_out = a->dax2.p; J.av_out = a->dav2.p; J.gk = a->dgk.p; J.gL = a->dgL.p;
-            k_d64_adj_vertex<<<ceil_div(a->nV, 128), 128, 0, st>>>(A, J);
-            k_d64_adj_springs<<<ceil_div(a->nV, 128), 128, 0, st>>>(A, J);
-            std::swap(a->dax.p, a->dax2.p);
-            std::swap(a->dav.p, a->dav2.p);
+            J.ax = ax; J.av = av; J.xbar = a->dxbar.p; J.vbar = a->dvbar.p; J.fbar = a->dfbar.p;
+            J.ax_out = ax2; J.av_out = av2; J.gk = a->dgk.p; J.gL = a->dgL.p;
+            k_d64_adj_vertex<<<ceil_div(a->nV, D64_BLOCK), D64_BLOCK, 0, st>>>(A, J);
+            k_d64_adj_springs<<<ceil_div(a->nV, D64_BLOCK), D64_BLOCK, 0, st>>>(A, J);
+            std::swap(ax, ax2);
+            std::swap(av, av2);
         }
     }
     YS_CK(cudaGetLastError());
+    a->g_bwd_av = av;
+    return YS_OK;
+}
+
+// One executable graph per direction, captured on first use: the whole
+// T-step sequence is fixed by (T, K) and the adjoint's own buffers, so later
+// calls replay it without host launch overhead.
+template <class Fn>
+ys_status d64_graph(ys_adjoint* a, cudaGraphExec_t& exec, Fn&& enqueue) {
+    cudaStream_t st = a->s->stream;
+    // scene-side arguments (external forces, parameters, buffers) changed
+    // since the capture: capture again
+    const A64 now = d64_args(a);
+    if ((a->g_fwd || a->g_bwd) && memcmp(&now, &a->g_args, sizeof(A64)) != 0) d64_drop_graphs(a);
+    a->g_args = now;
+    if (!exec) {
+        cudaGraph_t g = nullptr;
+        YS_CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+        ys_status er = enqueue();
+        cudaError_t ce = cudaStreamEndCapture(st, &g);
+        if (er) { if (g) cudaGraphDestroy(g); return er; }
+        if (ce != cudaSuccess) return fail(YS_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(ce));
+        ce = cudaGraphInstantiate(&exec, g, 0);
+        cudaGraphDestroy(g);
+        if (ce != cudaSuccess) { exec = nullptr; return fail(YS_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ce)); }
+    }
+    YS_CK(cudaGraphLaunch(exec, st));
+    return YS_OK;
+}
+
+void d64_drop_graphs(ys_adjoint* a) {
+    if (a->g_fwd || a->g_bwd) cudaStreamSynchronize(a->s->stream);
+    if (a->g_fwd) cudaGraphExecDestroy(a->g_fwd);
+    if (a->g_bwd) cudaGraphExecDestroy(a->g_bwd);
+    a->g_fwd = a->g_bwd = nullptr;
+}
+
+// Forward rollout in binary64; x_T stays in the returned buffer.
+ys_status d64_forward(ys_adjoint* a, const D4** xT) {
+    ys_status r = d64_trees(a);
+    if (r) return r;
+    r = d64_graph(a, a->g_fwd, [&]() { return d64_enqueue_forward(a, &a->g_fwd_xT); });
+    if (r) return r;
+    r = d64_status(a);
+    if (r) return r;
+    *xT = a->g_fwd_xT;
+    a->forward_done = true;
+    return YS_OK;
+}
+
+// Reverse pass in binary64; the seed dL/dx_T is in dax on entry, dL/dv0
+// in g_bwd_av on return.
+ys_status d64_backward(ys_adjoint* a) {
+    ys_status r = d64_graph(a, a->g_bwd, [&]() { return d64_enqueue_backward(a); });
+    if (r) return r;
     return d64_status(a);
 }
 
@@ -2765,7 +2822,7 @@ ys_status ys_adjoint_backward_f64(ys_adjoint* a, const double* d_dLdx, double* d
     if (r) return r;
     YS_CK(cudaMemcpyAsync(d_gk, a->dgk.p, 8 * (size_t)a->S, cudaMemcpyDeviceToDevice, st));
     YS_CK(cudaMemcpyAsync(d_gL, a->dgL.p, 8 * (size_t)a->S, cudaMemcpyDeviceToDevice, st));
-    k_d64_to_d3<<<ceil_div(a->nV, 256), 256, 0, st>>>(a->dav.p, d_gv0, a->nV);
+    k_d64_to_d3<<<ceil_div(a->nV, 256), 256, 0, st>>>(a->g_bwd_av, d_gv0, a->nV);
     YS_CK(cudaGetLastError());
     YS_CK(cudaStreamSynchronize(st));
     return YS_OK;
@@ -2823,7 +2880,7 @@ ys_status ys_adjoint_backward(ys_adjoint* a, const float* d_dLdx, float* d_gk, f
         if (r) return r;
         k_d64_narrow<<<ceil_div(a->S, 256), 256, 0, st>>>(a->dgk.p, d_gk, a->S);
         k_d64_narrow<<<ceil_div(a->S, 256), 256, 0, st>>>(a->dgL.p, d_gL, a->S);
-        k_d64_to_f3<<<ceil_div(a->nV, 256), 256, 0, st>>>(a->dav.p, d_gv0, a->nV);
+        k_d64_to_f3<<<ceil_div(a->nV, 256), 256, 0, st>>>(a->g_bwd_av, d_gv0, a->nV);
         YS_CK(cudaGetLastError());
         YS_CK(cudaStreamSynchronize(st));
         return YS_OK;
