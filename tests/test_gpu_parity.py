@@ -170,7 +170,49 @@ def _small_specs():
         "c1": G.config_c1(P=24, level=2, height=0.2999),
         "c2hash": G.config_c2(P=40, level=3, height=0.33, gravity=-9.81),
         "c2bvh": G.config_c2(P=40, level=3, height=0.33, self_mode=2, gravity=-9.81),
+        "edge": _edge_spec(),
     }
+
+
+def _edge_spec():
+    """A FastGridCloth 16x16 (size 0.5) resting 5e-4 above a level-2
+    icosphere (r 0.2) and an obstacle mesh built to hit the contact edge
+    cases of narrow_pt_tri and integrate_cloth_grid:
+      * a flat quad exactly in the cloth's plane (previous and current
+        distance both 0: the orientation falls back to d_cur, the contact
+        has d = 0 and pushes by the full thickness);
+      * a strip 5e-4 below the pinned first row (mask 0: the push is applied
+        all the same, physics.metal:291-296), one of its triangles listed
+        twice (two contacts with equal n and d push twice);
+      * a degenerate (collinear) triangle under the cloth (normal below
+        1e-12: no contact);
+    and two coincident cloth vertices (spring length below 1e-7: skipped)."""
+    from ysim_b200 import _lib, generators as G
+    F32 = np.float32
+    P, H = 16, F32(0.2005)
+    x, f = G.grid_cloth(P, 0.5, (0.0, float(H), 0.0))
+    rest = G.fast_grid_rest(x, P)
+    x[8 * P + 5] = x[8 * P + 4]
+    mask = np.ones(P * P, F32)
+    mask[:P] = 0.0
+    cloth = G.Mesh(behavior=_lib.FAST_GRID_CLOTH, flags=_lib.MESH_COLLIDABLE, x=x, facets=f, v=np.zeros_like(x),
+                   mass=np.full(P * P, 1e-3, F32), mask=mask, kstretch=1e3, kshear=5e2, kbend=1e1,
+                   thickness=1e-3, grid_n=P, grid_rest=rest)
+    sph = G.obstacle_sphere(2, 0.2)
+    zrow = float(x[0, 2])
+    low = F32(H - F32(5e-4))
+    extra = np.array([[0.1, H, 0.1], [0.3, H, 0.1], [0.3, H, 0.3], [0.1, H, 0.3],          # in-plane quad
+                      [-0.3, low, zrow - 0.01], [0.3, low, zrow - 0.01], [0.3, low, zrow + 0.01],
+                      [-0.3, low, zrow + 0.01],                                              # strip under row 0
+                      [0.0, H - 0.001, 0.0], [0.01, H - 0.001, 0.0], [0.02, H - 0.001, 0.0]],  # collinear
+                     F32)
+    b = sph.nV
+    tris = np.array([[b, b + 1, b + 2], [b, b + 2, b + 3], [b + 4, b + 5, b + 6], [b + 4, b + 6, b + 7],
+                     [b + 4, b + 5, b + 6], [b + 8, b + 9, b + 10]], np.uint32)
+    ox = np.concatenate([sph.x, extra]).astype(F32)
+    ob = G.Mesh(behavior=sph.behavior, flags=sph.flags, x=ox, facets=np.concatenate([sph.facets, tris]),
+                v=np.zeros_like(ox), mass=np.zeros(len(ox), F32), mask=np.ones(len(ox), F32))
+    return G.SceneSpec("edge_cases", G.Params(subh=1.0 / 6000.0, substeps=10), [cloth, ob], 0)
 
 
 def _advance_to_contact(spec, frames):
@@ -198,10 +240,18 @@ def test_scene_apetrei_build_matches_oracle(cuda_lib, oracle, name, layout):
     _scene_parity(oracle, name, layout, 1)
 
 
-def _scene_parity(oracle, name, layout, builder):
+@pytest.mark.parametrize("layout", [0, 1], ids=["reference_tree", "cube_tree"])
+def test_scene_edge_cases_match_oracle(cuda_lib, oracle, layout):
+    """The edge-case scene from its first substep (where the in-plane
+    contacts, the pinned pushes and the double push all fire), staged and
+    fused, against the oracle."""
+    _scene_parity(oracle, "edge", layout, 0, advance=0)
+
+
+def _scene_parity(oracle, name, layout, builder, advance=3):
     from ysim_b200.scene import Scene
     spec = _small_specs()[name]
-    o = _advance_to_contact(spec, 3)
+    o = _advance_to_contact(spec, advance)
     x0, v0, xp0 = o.get("x"), o.get("v"), o.get("xprev")
     s = Scene(spec, tree_layout=layout, tree_builder=builder)
     try:

@@ -242,6 +242,11 @@ __global__ void __launch_bounds__(D64_BLOCK) k_d64_step(A64 A) {
             dd3 cn;
             double cd;
             if (!narrow64(p, pp, t0, t1, t2, A.radius, A.margin, cn, cd)) continue;
+            // a face reported twice (the reference tree layout over runs of
+            // equal codes) is one candidate, as in a search over all faces
+            bool seen = false;
+            for (u32 c = base; c < n && !seen; ++c) seen = cf[c] == f;
+            if (seen) continue;
             if (n >= D64_CAP) { st |= YS_FLAG_CONTACT_OVF; continue; }
             // insert sorted by face among this object's contacts
             u32 s = n++;
