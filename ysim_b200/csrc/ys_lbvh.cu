@@ -755,12 +755,10 @@ void launch_level_fill(const RefitJob* jobsDev, u32 numJobs, u32 totalLeaves, co
 
 // One wide node: the union of its slots (in slot order) into its parent's
 // slot, or into the binary root node at the top.
-__device__ __forceinline__ void refit_wide_node(const RefitJob& J, u32 local) {
-    Wide4* W = J.w4 + local;
-    const u32 nc = W->nchild;
-    const i32 par = W->parent;
-    const u32 ps = W->slot;
-    const float4* p = reinterpret_cast<const float4*>(W);
+// Box of wide node `local` (the union of its nc child slots) into its slot
+// `ps` of parent `par`, or into the binary root node when par < 0.
+__device__ __forceinline__ void refit_wide_box(const RefitJob& J, u32 local, i32 par, u32 ps, u32 nc) {
+    const float4* p = reinterpret_cast<const float4*>(J.w4 + local);
     const float4 lx = p[0], ly = p[1], lz = p[2], hx = p[3], hy = p[4], hz = p[5];
     f3 lo = mk(lx.x, ly.x, lz.x), hi = mk(hx.x, hy.x, hz.x);
     if (nc > 1) { lo = vmin(lo, mk(lx.y, ly.y, lz.y)); hi = vmax(hi, mk(hx.y, hy.y, hz.y)); }
@@ -775,6 +773,11 @@ __device__ __forceinline__ void refit_wide_node(const RefitJob& J, u32 local) {
     P->hix[ps] = hi.x; P->hiy[ps] = hi.y; P->hiz[ps] = hi.z;
 }
 
+__device__ __forceinline__ void refit_wide_node(const RefitJob& J, u32 local) {
+    const Wide4* W = J.w4 + local;
+    refit_wide_box(J, local, W->parent, W->slot, W->nchild);
+}
+
 __global__ void __launch_bounds__(256) k_refit_level(const RefitJob* __restrict__ jobs, const uint2* __restrict__ list,
                                                      u32 count) {
     const u32 t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -783,29 +786,55 @@ __global__ void __launch_bounds__(256) k_refit_level(const RefitJob* __restrict_
     refit_wide_node(jobs[e.y], e.x);
 }
 
-// Levels from..top in one block: the slots a level reads were written by the
-// same block before the preceding __syncthreads.
-__global__ void __launch_bounds__(1024) k_refit_top(const RefitJob* __restrict__ jobs, const uint2* __restrict__ list,
-                                                    const u32* __restrict__ hoff, u32 from, u32 top) {
+// Levels from..top in one block.  A node's list entry, parent link, slot and
+// child count do not change between refits; they are staged in shared memory
+// first, so that a level costs one dependent round trip (its children's
+// boxes, written by this block before the preceding __syncthreads) instead of
+// three.  Up to REFIT_TOP_NODES nodes (16 B of shared memory each).
+static constexpr u32 REFIT_TOP_NODES = 8192;
+static constexpr u32 REFIT_TOP_THREADS = 1024;
+
+__global__ void __launch_bounds__(REFIT_TOP_THREADS) k_refit_top(const RefitJob* __restrict__ jobs,
+                                                                const uint2* __restrict__ list,
+                                                                const u32* __restrict__ hoff, u32 from, u32 top) {
+    extern __shared__ uint4 sh_top[];  // (node, job, parent, slot << 8 | nchild)
+    const u32 b0 = hoff[from], e0 = hoff[top + 1];
+    for (u32 t = b0 + threadIdx.x; t < e0 && t - b0 < REFIT_TOP_NODES; t += blockDim.x) {
+        const uint2 q = list[t];
+        const Wide4* W = jobs[q.y].w4 + q.x;
+        sh_top[t - b0] = make_uint4(q.x, q.y, (u32)W->parent, (W->slot << 8) | (W->nchild & 0xFFu));
+    }
+    __syncthreads();
     for (u32 h = from; h <= top; ++h) {
         const u32 b = hoff[h], e = hoff[h + 1];
-        for (u32 t = b + threadIdx.x; t < e; t += blockDim.x) {
-            const uint2 q = list[t];
-            refit_wide_node(jobs[q.y], q.x);
+        for (u32 t = b + threadIdx.x; t < e && t - b0 < REFIT_TOP_NODES; t += blockDim.x) {
+            const uint4 it = sh_top[t - b0];
+            refit_wide_box(jobs[it.y], it.x, (i32)it.z, it.w >> 8, it.w & 0xFFu);
         }
         __syncthreads();
     }
 }
 
+cudaError_t refit_levels_prepare() {
+    return cudaFuncSetAttribute(k_refit_top, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)(REFIT_TOP_NODES * sizeof(uint4)));
+}
+
 void launch_refit_levels(const RefitJob* jobsDev, const uint2* list, const u32* hoffDev, const u32* hostOff,
                          u32 top, cudaStream_t s) {
+    // one launch per level down to the first level of fewer than 2048 nodes
+    // (or until the rest no longer fits the top kernel's staging), then the
+    // top kernel: one block is the faster form only for small levels
     u32 h = 1;
     for (; h <= top; ++h) {
         const u32 cnt = hostOff[h + 1] - hostOff[h];
-        if (cnt < 2048) break;
-        k_refit_level<<<ceil_div(cnt, 256), 256, 0, s>>>(jobsDev, list + hostOff[h], cnt);
+        if (cnt < 2048 && hostOff[top + 1] - hostOff[h] <= REFIT_TOP_NODES) break;
+        if (cnt) k_refit_level<<<ceil_div(cnt, 256), 256, 0, s>>>(jobsDev, list + hostOff[h], cnt);
     }
-    if (h <= top) k_refit_top<<<1, 1024, 0, s>>>(jobsDev, list, hoffDev, h, top);
+    if (h <= top) {
+        const u32 nodes = hostOff[top + 1] - hostOff[h];
+        k_refit_top<<<1, REFIT_TOP_THREADS, nodes * sizeof(uint4), s>>>(jobsDev, list, hoffDev, h, top);
+    }
 }
 
 void launch_refit(const RefitJob* jobsDev, u32 numJobs, u32 totalLeaves, u32* status, cudaStream_t s) {

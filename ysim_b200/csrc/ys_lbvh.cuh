@@ -104,6 +104,9 @@ void launch_level_fill(const RefitJob* jobsDev, u32 numJobs, u32 totalLeaves, co
 // Per substep, after launch_refit wrote the leaf slots: levels 1 .. split-1
 // one launch each (hostOff[h] .. hostOff[h+1] of list), then levels split ..
 // top in one block, level by level.
+// Allow the top-levels refit kernel its staging shared memory (once, before
+// the first launch_refit_levels; not during a stream capture).
+cudaError_t refit_levels_prepare();
 void launch_refit_levels(const RefitJob* jobsDev, const uint2* list, const u32* hoffDev, const u32* hostOff,
                          u32 top, cudaStream_t s);
 // Leaves + bottom-up for every job (jobs in device memory, jobsHost mirrors

@@ -1100,6 +1100,7 @@ ys_status build_levels(ys_scene* s) {
     for (auto& J : s->hjobs) any = any || J.w4;
     if (!any) return YS_OK;
     cudaStream_t st = s->stream;
+    YS_CK(refit_levels_prepare());
     ys_status r = upload_jobs(s, true);
     if (r) return r;
     const RefitJob* table = s->jobs.p;
