@@ -387,6 +387,52 @@ def test_spatial_hash_equals_lbvh_query(cuda_lib, oracle, case):
     assert np.array_equal(got, canon_pairs(oracle.brute_q1(x, f, q, float(h_margin), False)))
 
 
+def test_large_query_sets_in_morton_order(cuda_lib, oracle):
+    """Large query sets run their threads in the points' Morton order (pairs
+    still name the input points): from 2^21 points the LBVH query, which then
+    equals the oracle's queryPoints over the oracle's own tree, and from 2^23
+    the spatial hash, which then equals the LBVH, as sets."""
+    import torch
+    from ysim_b200 import _lib, generators as G
+    x, f, _ = G.soup(60_000, seed=41, nq=1)
+    rng = np.random.default_rng(42)
+    margin = np.float32(1e-3)
+    dx, df = _dev(x.reshape(-1)), _dev(f.reshape(-1).astype(np.int32))
+    cap = 1 << 22
+    pairs = torch.empty(2 * cap, dtype=torch.int32, device="cuda")
+    cnt = torch.zeros(1, dtype=torch.int64, device="cuda")
+
+    def lbvh_pairs(h, dq, nq):
+        _lib.check(cuda_lib.ys_lbvh_query(h, _p(dq), nq, margin, 0, _p(pairs), cap, _p(cnt)))
+        n = int(cnt.item())
+        assert n <= cap
+        return canon_pairs(pairs[: 2 * n].cpu().numpy().view(np.uint32))
+
+    q2 = rng.uniform(0, 1, ((1 << 21) + 1000, 3)).astype(np.float32)
+    q8 = rng.uniform(0, 1, ((1 << 23) + 1000, 3)).astype(np.float32)
+    dq2, dq8 = _dev(q2.reshape(-1)), _dev(q8.reshape(-1))
+    h, _, _ = _lbvh(cuda_lib, x, f)
+    try:
+        rn, _, _, _ = oracle.build_tree(x, f)
+        want = canon_pairs(oracle.query_points(rn, f, q2, float(margin)))
+        assert len(want) > 5000
+        for _ in range(2):  # the second call reuses the order buffers
+            assert np.array_equal(lbvh_pairs(h, dq2, len(q2)), want)
+        bvh8 = lbvh_pairs(h, dq8, len(q8))
+    finally:
+        _lib.check(cuda_lib.ys_lbvh_destroy(h))
+    sh = C.c_void_p()
+    _lib.check(cuda_lib.ys_shash_create(C.byref(sh), len(f), 64 * len(f), 0, None))
+    try:
+        _lib.check(cuda_lib.ys_shash_build(sh, _p(dx), _p(df), len(f), np.float32(2 * margin)))
+        _lib.check(cuda_lib.ys_shash_query(sh, _p(dq8), len(q8), margin, _p(pairs), cap, _p(cnt)))
+        n = int(cnt.item())
+        assert len(bvh8) > 20000
+        assert np.array_equal(canon_pairs(pairs[: 2 * n].cpu().numpy().view(np.uint32)), bvh8)
+    finally:
+        _lib.check(cuda_lib.ys_shash_destroy(sh))
+
+
 def _dup_code_soup(seed=7):
     """Triangles in clusters of 20 around 300 centres, each cluster far inside
     one Morton cell (1/1024 of the box): long runs of equal codes."""

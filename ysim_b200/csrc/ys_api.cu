@@ -17,10 +17,12 @@ ys_status fail(ys_status code, const std::string& msg);
 // (point, triangle), appended with one atomic per lane-batch.
 __global__ void __launch_bounds__(128) k_query_points(const Node* __restrict__ nodes, u32 numNodes,
                                                       const u32* __restrict__ F, const float* __restrict__ qx, u32 nQ,
-                                                      float m, int self, u32* __restrict__ pairs, u64 cap,
-                                                      unsigned long long* count, u32* status) {
-    const u32 p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= nQ) return;
+                                                      const u32* __restrict__ order, float m, int self,
+                                                      u32* __restrict__ pairs, u64 cap, unsigned long long* count,
+                                                      u32* status) {
+    const u32 k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= nQ) return;
+    const u32 p = order ? order[k] : k;  // the point of this thread (Morton order for large query sets)
     const f3 q = ldp(qx, p);
     const f3 qmn = q - mk(m, m, m), qmx = q + mk(m, m, m);
     u32 st = traverse(nodes, numNodes, qmn, qmx, [&](u32 f) {
@@ -49,6 +51,7 @@ struct ys_lbvh {
     RefitJob* job = nullptr;
     const u32* facets = nullptr;
     bool consistent = false;  // Karras split of runs of equal codes (ys_lbvh_set_split)
+    QueryOrder qorder;        // Morton order of large query sets
     int builder = YS_BUILD_KARRAS;  // ys_lbvh_set_builder
     void* aggScratch = nullptr;     // Apetrei range ends and root slot
 };
@@ -101,6 +104,7 @@ ys_status ys_lbvh_destroy(ys_lbvh* t) {
     cudaStreamSynchronize(t->stream);
     cudaFree(t->nodes); cudaFree(t->parent); cudaFree(t->claimOff); cudaFree(t->claims); cudaFree(t->karrasScratch); cudaFree(t->aggScratch); cudaFree(t->codes); cudaFree(t->idx); cudaFree(t->visits);
     cudaFree(t->box); cudaFree(t->status); cudaFree(t->scratch); cudaFree(t->job);
+    query_order_free(t->qorder);
     delete t;
     return YS_OK;
 }
@@ -163,8 +167,13 @@ ys_status ys_lbvh_query(ys_lbvh* t, const float* qx, uint32_t nQ, float margin, 
                         unsigned long long* count) {
     if (!t || !qx || !count || t->n == 0) return fail(YS_ERR_BAD_ARG, "bad argument / tree not built");
     YS_CK2(cudaMemsetAsync(count, 0, 8, t->stream));
-    if (nQ) k_query_points<<<ceil_div(nQ, 128), 128, 0, t->stream>>>(t->nodes, 2 * t->n - 1, t->facets, qx, nQ, margin,
-                                                                      self, pairs, cap, count, t->status);
+    const u32* order = nullptr;
+    if (nQ >= QUERY_ORDER_MIN_LBVH) {
+        YS_CK2(query_order(t->qorder, qx, nQ, t->stream));
+        order = t->qorder.idx;
+    }
+    if (nQ) k_query_points<<<ceil_div(nQ, 128), 128, 0, t->stream>>>(t->nodes, 2 * t->n - 1, t->facets, qx, nQ, order,
+                                                                      margin, self, pairs, cap, count, t->status);
     YS_CK2(cudaGetLastError());
     YS_CK2(cudaStreamSynchronize(t->stream));
     return YS_OK;

@@ -2,6 +2,7 @@
 #include <utility>
 
 #include "ys_lbvh.cuh"
+#include "ys_sort.cuh"
 
 namespace ys {
 
@@ -114,6 +115,50 @@ void launch_morton(const float4* x4, const float* x3, u32 voff, const u32* facet
                    u32* idx, cudaStream_t s, bool cube) {
     if (nF == 0) return;
     k_morton<<<ceil_div(nF, 256), 256, 0, s>>>(x4, x3, voff, facets, nF, box, codes, idx, cube ? 1 : 0);
+}
+
+// ------------------------------------------------------------------ query order
+// Morton code of each query point over the points' own box (10 bits per
+// axis), paired with its index for the sort.
+__global__ void k_point_codes(const float* __restrict__ qx, u32 n, const u32* __restrict__ box, u32* __restrict__ codes,
+                              u32* __restrict__ idx) {
+    const u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const f3 p = ldp(qx, i);
+    const float c[3] = {p.x, p.y, p.z};
+    u32 q[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        const float lo = funord(box[a]), w = funord(box[3 + a]) - lo;
+        const float t = w > 0.f ? (c[a] - lo) / w : 0.f;
+        const int v = (int)(t * 1024.f);  // NaN converts to 0
+        q[a] = (u32)min(max(v, 0), 1023);
+    }
+    codes[i] = (expand_bits(q[0]) << 2) | (expand_bits(q[1]) << 1) | expand_bits(q[2]);
+    idx[i] = i;
+}
+
+void query_order_free(QueryOrder& o) {
+    cudaFree(o.codes); cudaFree(o.idx); cudaFree(o.scratch); cudaFree(o.box);
+    o = QueryOrder();
+}
+
+cudaError_t query_order(QueryOrder& o, const float* qx, u32 n, cudaStream_t s) {
+    if (n > o.cap) {
+        cudaStreamSynchronize(s);
+        query_order_free(o);
+        cudaError_t e;
+        if ((e = cudaMalloc((void**)&o.codes, 4 * (size_t)n)) || (e = cudaMalloc((void**)&o.idx, 4 * (size_t)n)) ||
+            (e = cudaMalloc(&o.scratch, sort_scratch_bytes(n))) || (e = cudaMalloc((void**)&o.box, 32))) {
+            query_order_free(o);
+            return e;
+        }
+        o.cap = n;
+    }
+    launch_box_init(o.box, s);
+    launch_box(nullptr, qx, 0, n, o.box, s);
+    k_point_codes<<<ceil_div(n, 256), 256, 0, s>>>(qx, n, o.box, o.codes, o.idx);
+    return radix_sort_pairs(o.codes, o.idx, n, o.scratch, 0, 32, s);
 }
 
 // ------------------------------------------------------------------ Karras

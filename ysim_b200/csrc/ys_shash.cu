@@ -23,6 +23,7 @@
 #include <string>
 
 #include "ys_common.cuh"
+#include "ys_lbvh.cuh"
 #include "ys_scan.cuh"
 #include "ysim_b200.h"
 
@@ -106,10 +107,11 @@ __global__ void __launch_bounds__(128) k_sh_query(const float* __restrict__ qx, 
                                                   const ShTri* __restrict__ tris, const u32* __restrict__ bstart,
                                                   const u32* __restrict__ sorted,
                                                   const unsigned short* __restrict__ sord, const u32* __restrict__ big,
-                                                  const u32* __restrict__ nbig, u32* __restrict__ pairs, u64 cap,
-                                                  unsigned long long* count) {
-    const u32 p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= nQ) return;
+                                                  const u32* __restrict__ nbig, const u32* __restrict__ order,
+                                                  u32* __restrict__ pairs, u64 cap, unsigned long long* count) {
+    const u32 k0 = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k0 >= nQ) return;
+    const u32 p = order ? order[k0] : k0;  // the point of this thread (Morton order for large query sets)
     const f3 q = ldp(qx, p);
     const f3 qmn = q - mk(m, m, m), qmx = q + mk(m, m, m);  // queryPoints box
     const float a3[3] = {qmn.x, qmn.y, qmn.z}, b3[3] = {qmx.x, qmx.y, qmx.z};
@@ -162,6 +164,7 @@ struct ys_shash {
         *big = nullptr, *nbig = nullptr;
     unsigned short *eord = nullptr, *sord = nullptr;  // cell ordinal of each entry within its triangle's range
     void* scan = nullptr;
+    QueryOrder qorder;  // Morton order of large query sets
 };
 
 #define YS_CK3(call)                                                                                   \
@@ -211,6 +214,7 @@ ys_status ys_shash_destroy(ys_shash* h) {
     cudaStreamSynchronize(h->stream);
     cudaFree(h->tris); cudaFree(h->counts); cudaFree(h->ebucket); cudaFree(h->etri); cudaFree(h->sorted); cudaFree(h->eord); cudaFree(h->sord);
     cudaFree(h->bstart); cudaFree(h->bfill); cudaFree(h->big); cudaFree(h->nbig); cudaFree(h->scan);
+    query_order_free(h->qorder);
     delete h;
     return YS_OK;
 }
@@ -251,8 +255,13 @@ ys_status ys_shash_query(ys_shash* h, const float* d_qx, uint32_t nQ, float marg
     if (!(2.0f * margin <= h->cell)) return fail(YS_ERR_BAD_ARG, "cell must be at least 2 * margin");
     cudaStream_t s = h->stream;
     YS_CK3(cudaMemsetAsync(d_count, 0, 8, s));
+    const u32* order = nullptr;
+    if (nQ >= QUERY_ORDER_MIN_HASH) {
+        YS_CK3(query_order(h->qorder, d_qx, nQ, s));
+        order = h->qorder.idx;
+    }
     if (nQ) k_sh_query<<<ceil_div(nQ, 128), 128, 0, s>>>(d_qx, nQ, margin, h->inv, h->mask, h->tris, h->bstart,
-                                                          h->sorted, h->sord, h->big, h->nbig, d_pairs, cap,
+                                                          h->sorted, h->sord, h->big, h->nbig, order, d_pairs, cap,
                                                           d_count);
     YS_CK3(cudaGetLastError());
     YS_CK3(cudaStreamSynchronize(s));
