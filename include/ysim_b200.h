@@ -325,7 +325,9 @@ ys_status ys_lbvh_refit(ys_lbvh* t, const float* d_x, const float* d_v, float dt
 /* queryPoints (bvh.hpp:1803-1841): (point, triangle) pairs for every query
  * point whose box [p - margin, p + margin] overlaps a leaf; self = skip
  * triangles containing the point.  *d_count receives the candidate count
- * (pairs beyond cap are counted, not written). */
+ * (pairs beyond cap are counted, not written).  Pair order is unspecified:
+ * from 2^21 query points the points are visited in their Morton order, with
+ * order buffers (12 B per point plus sort scratch) kept by the tree. */
 ys_status ys_lbvh_query(ys_lbvh* t, const float* d_qx, uint32_t num_queries, float margin, int self,
                         uint32_t* d_pairs, uint64_t cap, unsigned long long* d_count);
 /* Device pointers of the tree arrays (nodes, parents, codes, indices). */
@@ -365,7 +367,8 @@ ys_status ys_shash_destroy(ys_shash* h);
 /* Bin every triangle's AABB into the grid cells (edge `cell`) it overlaps. */
 ys_status ys_shash_build(ys_shash* h, const float* d_x, const uint32_t* d_facets, uint32_t num_facets, float cell);
 /* (point, triangle) pairs whose boxes [p - margin, p + margin] and triangle
- * AABB overlap; requires cell >= 2 * margin. */
+ * AABB overlap; requires cell >= 2 * margin.  Pair order is unspecified:
+ * from 2^23 query points the points are visited in their Morton order. */
 ys_status ys_shash_query(ys_shash* h, const float* d_qx, uint32_t num_queries, float margin, uint32_t* d_pairs,
                          uint64_t cap, unsigned long long* d_count);
 /* Cell entries of the last build and triangles too large for the grid. */
