@@ -68,8 +68,11 @@ __global__ void __launch_bounds__(256) k_box(const float4* x4, const float* x3, 
 void launch_box_init(u32* box, cudaStream_t s) { k_box_init<<<1, 32, 0, s>>>(box); }
 void launch_box(const float4* x4, const float* x3, u32 voff, u32 nV, u32* box, cudaStream_t s) {
     if (nV == 0) return;
+    // up to full occupancy (8 blocks of 256 per SM): the reduction is a
+    // stream over the vertices, and with fewer threads in flight a 48M-vertex
+    // box ran at a quarter of the bandwidth
     int blocks = ceil_div(nV, 256);
-    if (blocks > 148 * 2) blocks = 148 * 2;
+    if (blocks > 148 * 8) blocks = 148 * 8;
     k_box<<<blocks, 256, 0, s>>>(x4, x3, voff, nV, box);
 }
 
