@@ -20,6 +20,7 @@
 // scan -> k_sh_emit (bucket ids) -> bucket histogram -> scan -> scatter.
 // Triangles spanning more than MAX_CELLS cells go to a short overflow list
 // that every query tests directly.
+#include <algorithm>
 #include <string>
 
 #include "ys_common.cuh"
@@ -158,6 +159,7 @@ struct ys_shash {
     int device = 0;
     cudaStream_t stream = nullptr;
     u32 maxTris = 0, maxEntries = 0, nF = 0, mask = 0, nE = 0;
+    u32 tableCap = 0;  // buckets allocated (power of two); each build uses 2 nE rounded up, at most this
     float cell = 0.f, inv = 0.f;
     ShTri* tris = nullptr;
     u32 *counts = nullptr, *ebucket = nullptr, *etri = nullptr, *bstart = nullptr, *bfill = nullptr, *sorted = nullptr,
@@ -186,6 +188,7 @@ ys_status ys_shash_create(ys_shash** out, uint32_t max_tris, uint32_t max_entrie
     u32 T = 1;
     while (T < 2u * max_entries && T < (1u << 31)) T <<= 1;
     h->mask = T - 1;
+    h->tableCap = T;
     cudaError_t e = cudaSuccess;
     if (e == cudaSuccess) e = cudaMalloc((void**)&h->tris, sizeof(ShTri) * (size_t)max_tris);
     if (e == cudaSuccess) e = cudaMalloc((void**)&h->counts, 4 * ((size_t)max_tris + 1));
@@ -234,7 +237,11 @@ ys_status ys_shash_build(ys_shash* h, const float* d_x, const uint32_t* d_facets
     YS_CK3(cudaStreamSynchronize(s));
     if (nE > h->maxEntries) return fail(YS_ERR_CAPACITY, "cell entries exceed the hash capacity");
     h->nE = nE;
-    const u32 T = h->mask + 1;
+    // buckets for this build's entries (load factor at most 1/2): clearing
+    // and scanning a table sized for the capacity cost more than the build
+    u32 T = 1;
+    while (T < 2u * std::max(nE, 1u) && T < h->tableCap) T <<= 1;
+    h->mask = T - 1;
     YS_CK3(cudaMemsetAsync(h->bstart, 0, 4 * ((size_t)T + 1), s));
     YS_CK3(cudaMemsetAsync(h->nbig, 0, 4, s));
     k_sh_emit<<<ceil_div(nF, 256), 256, 0, s>>>(h->tris, h->counts, nF, h->mask, h->ebucket, h->etri, h->eord,
