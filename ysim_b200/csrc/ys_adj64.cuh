@@ -58,6 +58,9 @@ __device__ __forceinline__ dd3 ldf(const float4* p, u32 i) {
 struct __align__(32) DContact { double nx, ny, nz, d; };
 
 static constexpr u32 D64_CAP = 16;    // contacts kept per vertex and step
+static constexpr int D64_SPLIT = 4;   // the contact search splits a vertex's descent at this depth
+static constexpr u32 D64_LANES = 1u << D64_SPLIT;  // into this many threads, one per subtree
+static constexpr u32 D64_LCAP = 8;    // contacts one of those threads may find
 static constexpr int D64_STACK = 64;  // tree descent stack
 static constexpr u32 D64_VISIT_CAP = 1u << 20;
 // Block size of the per-vertex kernels (32 measured the same on the
@@ -99,6 +102,12 @@ struct A64 {
     DContact* cs;  // D64_CAP slots per vertex, sorted by (object, face)
     u32* cf;       // their face ids
     u32* cn;       // contacts per vertex
+    // the contact search's output, per (vertex, subtree): D64_LCAP contacts
+    // in search order, their face ids and target ordinals, the count
+    DContact* ls;
+    u32* lf;
+    u32* lk;
+    u32* ln;
     unsigned long long* box;  // cloth swept box: ~dord(min) x3 then dord(max) x3, all by atomicMax
     u32* status;
 };
@@ -189,15 +198,21 @@ __global__ void __launch_bounds__(256) k_d64_box(A64 A) {
     }
 }
 
-// One step of the FP64 rollout: contacts (recorded sorted in cs / cf / cn),
-// forces, integration and the contact response.
-__global__ void __launch_bounds__(D64_BLOCK) k_d64_step(A64 A) {
-    const u32 i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= A.nV) return;
-    const u32 g = A.voff + i;
+// Contact search of one step, D64_LANES threads per vertex: thread j of a
+// vertex descends the subtree reached from the root by the bits of j (high
+// bit first) over D64_SPLIT levels; a leaf met above that depth belongs to
+// the thread whose remaining bits are zero.  Together the threads visit
+// every root-to-leaf path the one-thread descent visits, with D64_LANES
+// times the threads in flight (a 128x128 cloth is otherwise 512 warps, and
+// the descents' dependent loads are the step's time).
+__global__ void __launch_bounds__(D64_BLOCK) k_d64_cand(A64 A) {
+    const u32 tid = blockIdx.x * blockDim.x + threadIdx.x;
+    if (tid >= A.nV * D64_LANES) return;
+    const u32 i = tid / D64_LANES, j = tid % D64_LANES;
     const dd3 p = ldd(A.x, i), pp = ldd(A.xp, i);
-    DContact* cs = A.cs + (size_t)i * D64_CAP;
-    u32* cf = A.cf + (size_t)i * D64_CAP;
+    DContact* ls = A.ls + (size_t)tid * D64_LCAP;
+    u32* lf = A.lf + (size_t)tid * D64_LCAP;
+    u32* lk = A.lk + (size_t)tid * D64_LCAP;
     u32 n = 0, st = 0;
     const dd3 blo = dm(dunord(~A.box[0]), dunord(~A.box[1]), dunord(~A.box[2]));
     const dd3 bhi = dm(dunord(A.box[3]), dunord(A.box[4]), dunord(A.box[5]));
@@ -213,16 +228,33 @@ __global__ void __launch_bounds__(D64_BLOCK) k_d64_step(A64 A) {
         if (bhi.x < (double)root.mnx || blo.x > (double)root.mxx || bhi.y < (double)root.mny ||
             blo.y > (double)root.mxy || bhi.z < (double)root.mnz || blo.z > (double)root.mxz)
             continue;
-        const u32 base = n, nn = 2 * T.nF - 1;
+        const u32 nn = 2 * T.nF - 1;
+        // this thread's subtree
+        int id = 0;
+        bool mine = true;
+        for (int L = 0; L < D64_SPLIT; ++L) {
+            const Node q = nodes[id];
+            if (fhi.x < q.mnx || flo.x > q.mxx || fhi.y < q.mny || flo.y > q.mxy || fhi.z < q.mnz || flo.z > q.mxz) {
+                mine = false;
+                break;
+            }
+            if (q.a < 0) {  // a leaf above the split depth
+                mine = (j & ((1u << (D64_SPLIT - L)) - 1u)) == 0u;
+                break;
+            }
+            id = ((j >> (D64_SPLIT - 1 - L)) & 1u) ? q.b : q.a;
+            if (id < 0 || (u32)id >= nn) { mine = false; break; }
+        }
+        if (!mine) continue;
         int stack[D64_STACK];
         int sp = 1;
-        stack[0] = 0;
+        stack[0] = id;
         u32 visited = 0;
         while (sp > 0) {
             if (++visited > D64_VISIT_CAP) { st |= YS_FLAG_STACK_OVF; break; }
-            const int id = stack[--sp];
-            if (id < 0 || (u32)id >= nn) continue;
-            const Node q = nodes[id];
+            const int nid = stack[--sp];
+            if (nid < 0 || (u32)nid >= nn) continue;
+            const Node q = nodes[nid];
             if (fhi.x < q.mnx || flo.x > q.mxx || fhi.y < q.mny || flo.y > q.mxy || fhi.z < q.mnz || flo.z > q.mxz)
                 continue;
             if (q.a >= 0) {
@@ -242,21 +274,51 @@ __global__ void __launch_bounds__(D64_BLOCK) k_d64_step(A64 A) {
             dd3 cn;
             double cd;
             if (!narrow64(p, pp, t0, t1, t2, A.radius, A.margin, cn, cd)) continue;
-            // a face reported twice (the reference tree layout over runs of
-            // equal codes) is one candidate, as in a search over all faces
+            if (n >= D64_LCAP) { st |= YS_FLAG_CONTACT_OVF; continue; }
+            ls[n] = DContact{cn.x, cn.y, cn.z, cd};
+            lf[n] = f;
+            lk[n] = k - A.tgt_begin;
+            ++n;
+        }
+    }
+    A.ln[tid] = n;
+    if (st) atomicOr(A.status, st);
+}
+
+// One step of the FP64 rollout for each vertex: its contacts from the
+// search threads merged into one list sorted by (object, face) (a face
+// reported twice -- the reference tree layout over runs of equal codes -- is
+// one candidate, as in a search over all faces; recorded in cs / cf / cn),
+// then forces, integration and the contact response.
+__global__ void __launch_bounds__(D64_BLOCK) k_d64_step(A64 A) {
+    const u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= A.nV) return;
+    const u32 g = A.voff + i;
+    const dd3 p = ldd(A.x, i);
+    DContact* cs = A.cs + (size_t)i * D64_CAP;
+    u32* cf = A.cf + (size_t)i * D64_CAP;
+    unsigned long long key[D64_CAP];
+    u32 n = 0, st = 0;
+    for (u32 j = 0; j < D64_LANES; ++j) {
+        const u32 tid = i * D64_LANES + j;
+        const u32 m = min(A.ln[tid], D64_LCAP);
+        for (u32 c = 0; c < m; ++c) {
+            const size_t o = (size_t)tid * D64_LCAP + c;
+            const unsigned long long kc = ((unsigned long long)A.lk[o] << 32) | A.lf[o];
             bool seen = false;
-            for (u32 c = base; c < n && !seen; ++c) seen = cf[c] == f;
+            for (u32 e = 0; e < n && !seen; ++e) seen = key[e] == kc;
             if (seen) continue;
             if (n >= D64_CAP) { st |= YS_FLAG_CONTACT_OVF; continue; }
-            // insert sorted by face among this object's contacts
-            u32 s = n++;
-            while (s > base && cf[s - 1] > f) {
-                cs[s] = cs[s - 1];
-                cf[s] = cf[s - 1];
-                --s;
+            u32 s2 = n++;
+            while (s2 > 0 && key[s2 - 1] > kc) {
+                key[s2] = key[s2 - 1];
+                cs[s2] = cs[s2 - 1];
+                cf[s2] = cf[s2 - 1];
+                --s2;
             }
-            cs[s] = DContact{cn.x, cn.y, cn.z, cd};
-            cf[s] = f;
+            key[s2] = kc;
+            cs[s2] = A.ls[o];
+            cf[s2] = A.lf[o];
         }
     }
     A.cn[i] = n;

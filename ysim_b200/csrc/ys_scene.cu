@@ -2333,6 +2333,8 @@ struct ys_adjoint {
     std::vector<DBuf<u32>> dst_f, dst_n;
     DBuf<D4> dX[3], dV[2];
     DBuf<DContact> dsc_c;  // contacts of steps that are not recorded
+    DBuf<DContact> dls;    // contact search output per (vertex, search thread)
+    DBuf<u32> dlf, dlk, dln;
     DBuf<u32> dsc_f, dsc_n;
     DBuf<D4> dax, dav, dax2, dav2, dxbar, dvbar, dfbar;
     DBuf<double> dgk, dgL;
@@ -2378,6 +2380,7 @@ void d64_free(ys_adjoint* a) {
         b->free();
     a->d_k.free(); a->d_L.free(); a->dgk.free(); a->dgL.free();
     a->dsc_c.free(); a->dsc_f.free(); a->dsc_n.free(); a->dbox.free(); a->dstatus.free();
+    a->dls.free(); a->dlf.free(); a->dlk.free(); a->dln.free();
 }
 
 cudaError_t d64_alloc(ys_adjoint* a) {
@@ -2388,6 +2391,8 @@ cudaError_t d64_alloc(ys_adjoint* a) {
         if ((e = b->alloc(n))) return e;
     if ((e = a->d_k.alloc(a->S)) || (e = a->d_L.alloc(a->S)) || (e = a->dgk.alloc(a->S)) || (e = a->dgL.alloc(a->S)))
         return e;
+    const size_t nl = n * D64_LANES, cl = nl * D64_LCAP;
+    if ((e = a->dls.alloc(cl)) || (e = a->dlf.alloc(cl)) || (e = a->dlk.alloc(cl)) || (e = a->dln.alloc(nl))) return e;
     if ((e = a->dsc_c.alloc(c)) || (e = a->dsc_f.alloc(c)) || (e = a->dsc_n.alloc(n)) || (e = a->dbox.alloc(6)) ||
         (e = a->dstatus.alloc(1)))
         return e;
@@ -2473,6 +2478,10 @@ A64 d64_args(ys_adjoint* a) {
     A.L = a->d_L.p;
     A.box = a->dbox.p;
     A.status = a->dstatus.p;
+    A.ls = a->dls.p;
+    A.lf = a->dlf.p;
+    A.lk = a->dlk.p;
+    A.ln = a->dln.p;
     return A;
 }
 
@@ -2480,6 +2489,7 @@ void d64_step(ys_adjoint* a, A64 A, cudaStream_t st) {
     cudaMemsetAsync(a->dbox.p, 0, 6 * sizeof(unsigned long long), st);
     const u32 gb = std::min<u32>(ceil_div(a->nV, 256), 148 * 4);
     k_d64_box<<<gb, 256, 0, st>>>(A);
+    k_d64_cand<<<ceil_div(a->nV * D64_LANES, D64_BLOCK), D64_BLOCK, 0, st>>>(A);
     k_d64_step<<<ceil_div(a->nV, D64_BLOCK), D64_BLOCK, 0, st>>>(A);
 }
 
