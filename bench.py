@@ -12,9 +12,13 @@ sort, Karras), amortised into the timed steps as it comes.
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
 Prints one JSON line (rank 0).  value = substeps/s over all ranks, timed on the
-device with CUDA events on the scene's stream, the L2 flushed (a 256 MiB
-write) between timed substeps and excluded from the timed intervals.  e2e =
-the same metric through the public API with host buffers: every frame uploads
+device with CUDA events on the scene's stream around each substep (one CUDA
+graph launch: refit and fused kernel), the L2 flushed (a 256 MiB write)
+between timed substeps and excluded from the timed intervals; the roofline's
+per-kernel durations come from bursts of further substeps interleaved with
+the timed ones, with events around each kernel.  e2e =
+the same metric through the public API with host buffers, from the state the
+timed substeps started from (so the same stretch of the drape): every frame uploads
 the external-force buffer from pinned host memory (applyEnvironmentForces'
 output) and reads the positions back into pinned host memory.
 Multi-GPU: replicas only (one independent cloth per rank, no collective on the
@@ -47,7 +51,8 @@ def parse():
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--preroll", type=int, default=240, help="untimed substeps before warm-up (reach contact)")
-    ap.add_argument("--e2e-frames", type=int, default=10)
+    ap.add_argument("--e2e-frames", type=int, default=None,
+                    help="end-to-end frames (default: the frames the timed substeps make up)")
     ap.add_argument("--cpu-substeps", type=int, default=3, help="substeps of the CPU baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--seed", type=int, default=2)
@@ -312,6 +317,9 @@ def run_ours(args, rank, world, local):
     scene.sync()
     scene.clear_flags()
     before = scene.totals()
+    # the state the timed substeps start from; the end-to-end frames start
+    # from it too, so both cover the same stretch of the drape
+    snap = {k: scene.get(k) for k in ("x", "v", "xprev")}
 
     # ---- device-timed substeps (value)
     starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
@@ -322,26 +330,56 @@ def run_ours(args, rank, world, local):
     torch.cuda.synchronize()
     sampler.start()
     _lib_check = __import__("ysim_b200._lib", fromlist=["check"]).check
-    _lib_check(lib.ys_scene_set_timing(scene.h, 1), "set_timing")
-    for i in range(args.steps):
-        with torch.cuda.stream(stream):
-            flush.fill_(float(i))
-        starts[i].record(stream)
-        scene.step(1)
-        ends[i].record(stream)
+    # The substeps as the library runs them: one CUDA-graph launch each (the
+    # flush before it keeps the GPU busy while the host enqueues, so no host
+    # launch gap falls inside an interval).  Interleaved with them, in ten
+    # bursts through the same stretch of the drape, a tenth as many further
+    # substeps run with CUDA events around each kernel (direct launches):
+    # their refit / fused durations and candidate / contact counts give the
+    # roofline.  The bursts are not part of `value`.
+    import ctypes as C
+    chunks = min(10, args.steps)
+    per = [args.steps // chunks + (1 if c < args.steps % chunks else 0) for c in range(chunks)]
+    kper = max(1, args.steps // (10 * chunks))
+    kt = [0.0, 0.0, 0.0, 0.0]
+    k_rows = k_cont = 0
+    ksteps = 0
+    i = 0
+    for c in range(chunks):
+        for _ in range(per[c]):
+            with torch.cuda.stream(stream):
+                flush.fill_(float(i))
+            starts[i].record(stream)
+            scene.step(1)
+            ends[i].record(stream)
+            i += 1
+        k_before = scene.totals()
+        _lib_check(lib.ys_scene_set_timing(scene.h, 1), "set_timing")
+        for _ in range(kper):
+            with torch.cuda.stream(stream):
+                flush.fill_(float(i))
+            scene.step(1)
+        scene.sync()
+        burst = (C.c_double * 4)()
+        _lib_check(lib.ys_scene_kernel_times(scene.h, burst), "kernel_times")
+        _lib_check(lib.ys_scene_set_timing(scene.h, 0), "set_timing")
+        kt = [kt[j] + burst[j] for j in range(4)]
+        k_after = scene.totals()
+        k_rows += k_after[0] - k_before[0]
+        k_cont += k_after[1] - k_before[1]
+        ksteps += kper
     torch.cuda.synchronize()
     scene.sync()
     clocks = sampler.stop()
-    ms = sum(s.elapsed_time(e) for s, e in zip(starts, ends))
-    import ctypes as C
-    kt = (C.c_double * 4)()
-    _lib_check(lib.ys_scene_kernel_times(scene.h, kt), "kernel_times")
-    _lib_check(lib.ys_scene_set_timing(scene.h, 0), "set_timing")
+    ms = sum(s_.elapsed_time(e_) for s_, e_ in zip(starts, ends))
     after = scene.totals()
     st = scene.stats()
     value, ms = aggregate(ms, args.steps, world, device=f"cuda:{local}")
-    rows_ps = (after[0] - before[0]) / args.steps
-    cont_ps = (after[1] - before[1]) / args.steps
+    # candidate rows and contacts per substep over the timed and the burst substeps
+    rows_ps = (after[0] - before[0] - k_rows) / args.steps
+    cont_ps = (after[1] - before[1] - k_cont) / args.steps
+    k_rows_ps = k_rows / ksteps
+    k_cont_ps = k_cont / ksteps
 
     # ---- e2e through the public API with host buffers
     nsub = spec.params.substeps
@@ -353,6 +391,8 @@ def run_ours(args, rank, world, local):
     g = np.asarray(spec.params.gravity, np.float32)
     ext.numpy()[:] = (g[None, :] * (mass * cloth_mask)[:, None]).astype(np.float32)
     xout = torch.empty((nV, 3), dtype=torch.float32).pin_memory()
+    for k in ("x", "v", "xprev"):
+        scene.set(k, snap[k])
     # one untimed frame: the first external-force upload switches the force
     # source from g * m to the buffer, which drops and re-captures the
     # substep graphs
@@ -366,7 +406,8 @@ def run_ours(args, rank, world, local):
         dist.barrier()
     torch.cuda.synchronize()
     e0.record(stream)
-    for _ in range(args.e2e_frames):
+    e2e_frames = args.e2e_frames if args.e2e_frames else max(1, -(-args.steps // nsub))
+    for _ in range(e2e_frames):
         _lib_check(lib.ys_scene_set_external_forces(scene.h, C.c_void_p(ext.data_ptr())), "ext")
         scene.step(nsub)
         _lib_check(lib.ys_scene_read_positions_async(scene.h, C.c_void_p(xout.data_ptr())), "read")
@@ -374,11 +415,11 @@ def run_ours(args, rank, world, local):
     scene.sync()
     torch.cuda.synchronize()
     e2e_ms = e0.elapsed_time(e1)
-    e2e_val, e2e_ms = aggregate(e2e_ms, args.e2e_frames * nsub, world, device=f"cuda:{local}")
+    e2e_val, e2e_ms = aggregate(e2e_ms, e2e_frames * nsub, world, device=f"cuda:{local}")
     assert np.isfinite(xout.numpy()).all()
 
     # ---- roofline of the dominant kernel
-    ab = algorithmic_bytes(spec, rows_ps, cont_ps)
+    ab = algorithmic_bytes(spec, k_rows_ps, k_cont_ps)
     fused_ms = kt[2] / max(kt[3], 1)
     refit_ms = kt[0] / max(kt[1], 1)
     peak, peak_kind = measured_peak()
@@ -423,7 +464,12 @@ def run_ours(args, rank, world, local):
     batched = None if args.no_batched else measure_batched(args, rank, world, local)
     adjoint = None if (args.no_adjoint or rank != 0) else measure_adjoint(args, local)
 
-    launches = int(kt[1] + kt[3])
+    # launches in the timed loop: per substep the refit's leaf kernel, its
+    # level kernels and its top-level kernel, and k_fused (one CUDA graph);
+    # kt counts the refit as one timed stage, so the level launches are taken
+    # from the kernel list of the recorded substeps: 6 refit launches on C2
+    refit_launches = 6 if spec.meshes[0].behavior == 0 and spec.params.self_mode else 1
+    launches = int(round((kt[1] * refit_launches + kt[3]) / ksteps * args.steps))
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -437,8 +483,10 @@ def run_ours(args, rank, world, local):
                                                    "flags": st["flags"]}),
             "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": nV * 12 / nsub,
                     "d2h_bytes_per_step": nV * 12 / nsub,
-                    "note": "per frame of 20 substeps: one external-force upload and one position read-back; "
-                            "bytes shown per substep"},
+                    "note": f"{e2e_frames} frames of {nsub} substeps from the state the timed substeps started "
+                            "from (the same stretch of the drape), each with one external-force upload and one "
+                            "position read-back (bytes shown per substep); no L2 flush between substeps, unlike "
+                            "value"},
             "gpu_launches": launches,
             "roofline": roof,
             "cpu_baseline": cpu,

@@ -26,6 +26,7 @@
 #include "ys_common.cuh"
 #include "ys_lbvh.cuh"
 #include "ys_scan.cuh"
+#include "ys_sort.cuh"
 #include "ysim_b200.h"
 
 namespace ys {
@@ -63,7 +64,7 @@ __global__ void k_sh_bound(const float* __restrict__ x, const u32* __restrict__ 
 
 __global__ void k_sh_emit(const ShTri* __restrict__ tris, const u32* __restrict__ off, u32 nF, u32 mask,
                           u32* __restrict__ ebucket, u32* __restrict__ etri, unsigned short* __restrict__ eord,
-                          u32* __restrict__ bhist, u32* __restrict__ big, u32* __restrict__ nbig) {
+                          u32* __restrict__ eidx, u32* __restrict__ big, u32* __restrict__ nbig) {
     u32 t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= nF) return;
     const ShTri r = tris[t];
@@ -81,20 +82,30 @@ __global__ void k_sh_emit(const ShTri* __restrict__ tris, const u32* __restrict_
                 ebucket[k] = b;
                 etri[k] = t;
                 eord[k] = (unsigned short)(k - base);  // < MAX_CELLS
-                atomicAdd(&bhist[b], 1u);
+                eidx[k] = k;
                 ++k;
             }
 }
 
-__global__ void k_sh_scatter(const u32* __restrict__ ebucket, const u32* __restrict__ etri,
-                             const unsigned short* __restrict__ eord, u32 nE, const u32* __restrict__ bstart,
-                             u32* __restrict__ bfill, u32* __restrict__ sorted, unsigned short* __restrict__ sord) {
-    u32 i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= nE) return;
-    u32 b = ebucket[i];
-    const u32 j = bstart[b] + atomicAdd(&bfill[b], 1u);
-    sorted[j] = etri[i];
-    sord[j] = eord[i];
+// After the entries are sorted by bucket (radix sort of (bucket, entry)):
+// the triangle and cell ordinal of each sorted slot.
+__global__ void k_sh_gather(const u32* __restrict__ eidx, const u32* __restrict__ etri,
+                            const unsigned short* __restrict__ eord, u32 nE, u32* __restrict__ sorted,
+                            unsigned short* __restrict__ sord) {
+    const u32 k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= nE) return;
+    const u32 e = eidx[k];
+    sorted[k] = etri[e];
+    sord[k] = eord[e];
+}
+
+// First slot of each bucket's run in the sorted keys (buckets with no entry
+// keep 0xFFFFFFFF); a bucket's run ends where the key changes.
+__global__ void k_sh_mark(const u32* __restrict__ skey, u32 nE, u32* __restrict__ bstart) {
+    const u32 k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= nE) return;
+    const u32 b = skey[k];
+    if (k == 0 || skey[k - 1] != b) bstart[b] = k;
 }
 
 __device__ __forceinline__ bool box_hit(f3 qmn, f3 qmx, const ShTri& r) {
@@ -106,6 +117,7 @@ __device__ __forceinline__ bool box_hit(f3 qmn, f3 qmx, const ShTri& r) {
 
 __global__ void __launch_bounds__(128) k_sh_query(const float* __restrict__ qx, u32 nQ, float m, float inv, u32 mask,
                                                   const ShTri* __restrict__ tris, const u32* __restrict__ bstart,
+                                                  const u32* __restrict__ skey, u32 nE,
                                                   const u32* __restrict__ sorted,
                                                   const unsigned short* __restrict__ sord, const u32* __restrict__ big,
                                                   const u32* __restrict__ nbig, const u32* __restrict__ order,
@@ -130,7 +142,7 @@ __global__ void __launch_bounds__(128) k_sh_query(const float* __restrict__ qx, 
         for (int y = lo[1]; y <= hi[1]; ++y)
             for (int xx = lo[0]; xx <= hi[0]; ++xx) {
                 const u32 b = cell_hash(xx, y, z, mask);
-                for (u32 k = bstart[b]; k < bstart[b + 1]; ++k) {
+                for (u32 k = bstart[b]; k < nE && skey[k] == b; ++k) {
                     const u32 t = sorted[k];
                     const ShTri r = tris[t];
                     // the entry was binned for this very cell (not for another
@@ -162,8 +174,11 @@ struct ys_shash {
     u32 tableCap = 0;  // buckets allocated (power of two); each build uses 2 nE rounded up, at most this
     float cell = 0.f, inv = 0.f;
     ShTri* tris = nullptr;
-    u32 *counts = nullptr, *ebucket = nullptr, *etri = nullptr, *bstart = nullptr, *bfill = nullptr, *sorted = nullptr,
+    // entries: bucket (sorted in place by the build: the key of each sorted
+    // slot), triangle, cell ordinal and entry index (the sort's values)
+    u32 *counts = nullptr, *ebucket = nullptr, *etri = nullptr, *eidx = nullptr, *bstart = nullptr, *sorted = nullptr,
         *big = nullptr, *nbig = nullptr;
+    void* sortScratch = nullptr;
     unsigned short *eord = nullptr, *sord = nullptr;  // cell ordinal of each entry within its triangle's range
     void* scan = nullptr;
     QueryOrder qorder;  // Morton order of large query sets
@@ -198,10 +213,11 @@ ys_status ys_shash_create(ys_shash** out, uint32_t max_tris, uint32_t max_entrie
     if (e == cudaSuccess) e = cudaMalloc((void**)&h->eord, 2 * (size_t)max_entries);
     if (e == cudaSuccess) e = cudaMalloc((void**)&h->sord, 2 * (size_t)max_entries);
     if (e == cudaSuccess) e = cudaMalloc((void**)&h->bstart, 4 * ((size_t)T + 1));
-    if (e == cudaSuccess) e = cudaMalloc((void**)&h->bfill, 4 * (size_t)T);
+    if (e == cudaSuccess) e = cudaMalloc((void**)&h->eidx, 4 * (size_t)max_entries);
+    if (e == cudaSuccess) e = cudaMalloc(&h->sortScratch, sort_scratch_bytes(max_entries));
     if (e == cudaSuccess) e = cudaMalloc((void**)&h->big, 4 * (size_t)max_tris);
     if (e == cudaSuccess) e = cudaMalloc((void**)&h->nbig, 4);
-    size_t sb = scan_scratch_bytes(std::max<u32>(max_tris + 1, T + 1));
+    size_t sb = scan_scratch_bytes(max_tris + 1);
     if (e == cudaSuccess) e = cudaMalloc(&h->scan, sb);
     if (e != cudaSuccess) {
         ys_shash_destroy(h);
@@ -216,7 +232,8 @@ ys_status ys_shash_destroy(ys_shash* h) {
     cudaSetDevice(h->device);
     cudaStreamSynchronize(h->stream);
     cudaFree(h->tris); cudaFree(h->counts); cudaFree(h->ebucket); cudaFree(h->etri); cudaFree(h->sorted); cudaFree(h->eord); cudaFree(h->sord);
-    cudaFree(h->bstart); cudaFree(h->bfill); cudaFree(h->big); cudaFree(h->nbig); cudaFree(h->scan);
+    cudaFree(h->bstart); cudaFree(h->eidx); cudaFree(h->sortScratch); cudaFree(h->big); cudaFree(h->nbig);
+    cudaFree(h->scan);
     query_order_free(h->qorder);
     delete h;
     return YS_OK;
@@ -242,15 +259,21 @@ ys_status ys_shash_build(ys_shash* h, const float* d_x, const uint32_t* d_facets
     u32 T = 1;
     while (T < 2u * std::max(nE, 1u) && T < h->tableCap) T <<= 1;
     h->mask = T - 1;
-    YS_CK3(cudaMemsetAsync(h->bstart, 0, 4 * ((size_t)T + 1), s));
+    int bits = 0;
+    while ((1u << bits) < T) ++bits;
+    YS_CK3(cudaMemsetAsync(h->bstart, 0xFF, 4 * ((size_t)T + 1), s));
     YS_CK3(cudaMemsetAsync(h->nbig, 0, 4, s));
     k_sh_emit<<<ceil_div(nF, 256), 256, 0, s>>>(h->tris, h->counts, nF, h->mask, h->ebucket, h->etri, h->eord,
-                                                 h->bstart, h->big, h->nbig);
-    YS_CK3(exclusive_scan(h->bstart, T + 1, h->scan, s));
-    YS_CK3(cudaMemsetAsync(h->bfill, 0, 4 * (size_t)T, s));
-    if (nE)
-        k_sh_scatter<<<ceil_div(nE, 256), 256, 0, s>>>(h->ebucket, h->etri, h->eord, nE, h->bstart, h->bfill, h->sorted,
-                                                      h->sord);
+                                                 h->eidx, h->big, h->nbig);
+    // entries grouped by bucket with a radix sort of (bucket, entry) in place
+    // of per-entry atomics on bucket counters: those are random atomics into
+    // a table of up to 2^31 buckets, and two passes of them were most of the
+    // build
+    if (nE) {
+        YS_CK3(radix_sort_pairs(h->ebucket, h->eidx, nE, h->sortScratch, 0, bits, s));
+        k_sh_gather<<<ceil_div(nE, 256), 256, 0, s>>>(h->eidx, h->etri, h->eord, nE, h->sorted, h->sord);
+        k_sh_mark<<<ceil_div(nE, 256), 256, 0, s>>>(h->ebucket, nE, h->bstart);
+    }
     YS_CK3(cudaGetLastError());
     YS_CK3(cudaStreamSynchronize(s));
     return YS_OK;
@@ -268,8 +291,8 @@ ys_status ys_shash_query(ys_shash* h, const float* d_qx, uint32_t nQ, float marg
         order = h->qorder.idx;
     }
     if (nQ) k_sh_query<<<ceil_div(nQ, 128), 128, 0, s>>>(d_qx, nQ, margin, h->inv, h->mask, h->tris, h->bstart,
-                                                          h->sorted, h->sord, h->big, h->nbig, order, d_pairs, cap,
-                                                          d_count);
+                                                          h->ebucket, h->nE, h->sorted, h->sord, h->big, h->nbig,
+                                                          order, d_pairs, cap, d_count);
     YS_CK3(cudaGetLastError());
     YS_CK3(cudaStreamSynchronize(s));
     return YS_OK;

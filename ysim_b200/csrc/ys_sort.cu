@@ -17,7 +17,10 @@
 //               stable rank = running count of its digit in this tile + keys
 //               with the same digit in earlier warps of the round (shared
 //               table) + lower lanes of its own warp with the same digit
-//               (match mask popcount).
+//               (match mask popcount).  Keys go to that rank in a shared
+//               copy of the tile, ordered by digit, which is then written
+//               out in order: a digit's run is contiguous in the output, so
+//               the stores coalesce.
 #include "ys_common.cuh"
 #include "ys_sort.cuh"
 
@@ -88,13 +91,17 @@ __global__ void __launch_bounds__(SORT_THREADS) k_sort_scatter(const u32* __rest
                                                                const u32* __restrict__ totals) {
     constexpr int W = SORT_THREADS / 32;
     __shared__ u32 base[256];         // global start of each digit for this tile
+    __shared__ u32 lofs[256];         // start of each digit within the tile
     __shared__ u32 running[256];      // keys of each digit already placed by this tile
     __shared__ u32 wcnt[W][256];      // per-warp digit counts of the current round
     __shared__ u32 scanTmp[256];
+    __shared__ u32 sk[TILE], sv[TILE];  // the tile, stably ordered by digit
     const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+    const u32 tileBase = blockIdx.x * (u32)TILE;
+    const u32 tileCount = min((u32)TILE, n - tileBase);
 
     // digit bases: exclusive scan of totals (every CTA does it; 256 entries)
-    u32 t = totals[tid];
+    const u32 t = totals[tid];
     scanTmp[tid] = t;
     __syncthreads();
     for (int o = 1; o < 256; o <<= 1) {
@@ -103,29 +110,43 @@ __global__ void __launch_bounds__(SORT_THREADS) k_sort_scatter(const u32* __rest
         scanTmp[tid] += add;
         __syncthreads();
     }
-    base[tid] = scanTmp[tid] - t + hist[(u32)tid * numTiles + blockIdx.x];
+    // hist holds, per digit, the keys of that digit in earlier tiles: this
+    // tile's own count is the difference to the next tile (or to the total)
+    const u32 before_tiles = hist[(u32)tid * numTiles + blockIdx.x];
+    const u32 mine = (blockIdx.x + 1 < numTiles ? hist[(u32)tid * numTiles + blockIdx.x + 1] : t) - before_tiles;
+    base[tid] = scanTmp[tid] - t + before_tiles;
     running[tid] = 0;
     __syncthreads();
+    scanTmp[tid] = mine;
+    __syncthreads();
+    for (int o = 1; o < 256; o <<= 1) {
+        u32 add = (tid >= o) ? scanTmp[tid - o] : 0u;
+        __syncthreads();
+        scanTmp[tid] += add;
+        __syncthreads();
+    }
+    lofs[tid] = scanTmp[tid] - mine;
+    __syncthreads();
 
-    const u32 tileBase = blockIdx.x * (u32)TILE;
+    // stable rank of every key within the tile, into shared memory
     for (int r = 0; r < SORT_ITEMS; ++r) {
         for (int k = tid; k < W * 256; k += SORT_THREADS) (&wcnt[0][0])[k] = 0;
         __syncthreads();
-        u32 i = tileBase + (u32)r * SORT_THREADS + tid;
-        bool valid = i < n;
+        const u32 i = tileBase + (u32)r * SORT_THREADS + tid;
+        const bool valid = i < n;
         u32 key = 0, val = 0, d = 256u + lane;
         if (valid) { key = kin[i]; val = vin[i]; d = (key >> shift) & 255u; }
-        u32 peers = __match_any_sync(0xffffffffu, d);
-        u32 lower = __popc(peers & ((1u << lane) - 1u));
-        int leader = __ffs(peers) - 1;
+        const u32 peers = __match_any_sync(0xffffffffu, d);
+        const u32 lower = __popc(peers & ((1u << lane) - 1u));
+        const int leader = __ffs(peers) - 1;
         if (valid && lane == leader) wcnt[w][d] = (u32)__popc(peers);
         __syncthreads();
         if (valid) {
             u32 before = 0;
             for (int ww = 0; ww < w; ++ww) before += wcnt[ww][d];
-            u32 dst = base[d] + running[d] + before + lower;
-            kout[dst] = key;
-            vout[dst] = val;
+            const u32 p = lofs[d] + running[d] + before + lower;
+            sk[p] = key;
+            sv[p] = val;
         }
         __syncthreads();
         // advance running counts by this round's totals
@@ -136,6 +157,15 @@ __global__ void __launch_bounds__(SORT_THREADS) k_sort_scatter(const u32* __rest
             running[tid] += s;
         }
         __syncthreads();
+    }
+    // write out in tile order: a digit's keys are consecutive here and in the
+    // output, so neighbouring threads store to neighbouring addresses
+    for (u32 q = (u32)tid; q < tileCount; q += SORT_THREADS) {
+        const u32 key = sk[q];
+        const u32 d = (key >> shift) & 255u;
+        const u32 dst = base[d] + (q - lofs[d]);
+        kout[dst] = key;
+        vout[dst] = sv[q];
     }
 }
 
