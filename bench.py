@@ -639,7 +639,7 @@ def measure_batched(args, rank, world, local, steps=100):
             "batched_over_plain": p_ms / b_ms, "steps": steps, "flags": flags,
             "fused_variant": {"ctas_per_sm": tuned, "note": "chosen by ys_scene_autotune on the batched scene, "
                                                              "used for the plain scenes too"},
-            "note": "BASELINE's ~4.3M vertices for this config differs from the drawn total (vertices above)"}
+            "note": "the ~4.3M vertices quoted for this config differ from the drawn total (vertices above)"}
 
 
 def measure_adjoint(args, local, steps=200, every=20, reps=4):

@@ -1,6 +1,6 @@
 """One substep of the reference implementation on the host cores.
 
-TEST / BASELINE INFRASTRUCTURE ONLY (bench.py --impl reference).  The stages
+TEST AND CPU-BASELINE INFRASTRUCTURE ONLY (bench.py --impl reference).  The stages
 are the reference's own kernels compiled for the host (oracle/_ref, OpenMP
 over thread ids, the way dispatchThreads spreads them over the GPU):
 buildSweptLeaf_Tri + bottomUpBoxes (refit), queryPoints (inter-object rows),

@@ -15,7 +15,7 @@
 // when the reference sources are present) and against brute-force
 // enumerations for the candidate sets (tests/test_oracle_*.py).
 //
-// Documented deviations from the Metal build (all listed in DESIGN.md):
+// Documented deviations from the Metal build:
 //   * rsqrt(x) (fast, bruteforce.metal:118, physics.metal:276) is written as
 //     1.0f / sqrtf(x) (IEEE) on both sides.
 //   * integrate reads the per-vertex mass m[v] where physics.metal:250 reads
