@@ -177,10 +177,10 @@ def _f32_spec(spec):
     return spec
 
 
-def _roll64(spec, k, L, v0, T, K=5):
+def _roll64(spec, k, L, v0, T, K=5, tree_layout=None):
     import torch
     from ysim_b200.adjoint import ClothRollout
-    roll = ClothRollout(spec, steps=T, checkpoint_every=K, precision=64)
+    roll = ClothRollout(spec, steps=T, checkpoint_every=K, precision=64, tree_layout=tree_layout)
     t = [torch.tensor(np.asarray(a, np.float64), device="cuda", requires_grad=True) for a in (k, L, v0)]
     return roll, t
 
@@ -188,9 +188,12 @@ def _roll64(spec, k, L, v0, T, K=5):
 # Bit-for-bit agreement holds on any window, pushes and releases included:
 # both FP64 rollouts take the same branch at every test because they compute
 # the same binary64 values.
-@pytest.mark.parametrize("height,T", [(0.5, 40), (0.2995, 60), (0.2995, 25)],
-                         ids=["contact_free_40", "contacts_60_pushes", "contacts_25"])
-def test_fp64_adjoint_matches_fp64_reference_bit_for_bit(cuda_lib, height, T):
+@pytest.mark.parametrize("height,T,layout", [(0.5, 40, None), (0.2995, 60, None), (0.2995, 25, None),
+                                              (0.2995, 60, 0)],
+                         ids=["contact_free_40", "contacts_60_pushes", "contacts_25", "contacts_60_reference_tree"])
+def test_fp64_adjoint_matches_fp64_reference_bit_for_bit(cuda_lib, height, T, layout):
+    """The contact search descends the scene's float tree of the obstacle, in
+    the cube layout (default) or the reference's layout."""
     import torch
     spec = _f32_spec(_small(height=height))
     k, L, v0, w, R = _problem(spec)
@@ -198,7 +201,7 @@ def test_fp64_adjoint_matches_fp64_reference_bit_for_bit(cuda_lib, height, T):
     x64, ncontacts = R.forward(T, keep=True)
     assert (ncontacts > 0) == (height < 0.4)
     gk64, gL64, gv64 = R.backward(T, w64)
-    roll, (kt, Lt, vt) = _roll64(spec, k, L, v0, T, K=7)
+    roll, (kt, Lt, vt) = _roll64(spec, k, L, v0, T, K=7, tree_layout=layout)
     try:
         xT = roll(kt, Lt, vt)
         assert xT.dtype == torch.float64

@@ -47,8 +47,8 @@ class _Fn(torch.autograd.Function):
 
 class ClothRollout:
     def __init__(self, spec: SceneSpec, steps: int, checkpoint_every: int = 20, device: int = 0,
-                 precision: int = 32):
-        self.scene = Scene(spec, device=device)
+                 precision: int = 32, tree_layout=None):
+        self.scene = Scene(spec, device=device, tree_layout=tree_layout)
         self.lib = self.scene.lib
         self.device = torch.device("cuda", device)
         self.nV = spec.meshes[0].nV
