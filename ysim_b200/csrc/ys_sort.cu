@@ -8,8 +8,7 @@
 //
 // B200 design, per pass (3 launches):
 //   upsweep  -- each 256-thread CTA owns a tile of TILE keys and builds a
-//               256-bin digit histogram with warp-aggregated shared atomics
-//               (__match_any_sync: one atomic per distinct digit per warp);
+//               256-bin digit histogram from per-warp shared histograms;
 //   scan     -- one CTA per digit scans that digit's column of tile counts;
 //               digit bases come from a 256-entry scan done redundantly by
 //               every scatter CTA (256 loads, no extra launch);
@@ -31,25 +30,39 @@ static constexpr int SORT_ITEMS = 16;
 static constexpr int TILE = SORT_THREADS * SORT_ITEMS;  // 4096 keys per CTA
 
 // hist layout: digit-major, hist[d * numTiles + tile].
+// Per-warp histograms in shared memory (plain shared atomics; a warp's lanes
+// with the same digit serialise on one address, which is cheaper here than a
+// match per key), summed per digit at the end.  Keys are read four at a time.
 __global__ void __launch_bounds__(SORT_THREADS) k_sort_upsweep(const u32* __restrict__ keys, u32 n, int shift,
                                                                u32* __restrict__ hist, u32 numTiles) {
-    __shared__ u32 h[256];
-    const int tid = threadIdx.x;
-    h[tid] = 0;
+    constexpr int W = SORT_THREADS / 32;
+    __shared__ u32 h[W][256];
+    const int tid = threadIdx.x, w = tid >> 5;
+    for (int k = tid; k < W * 256; k += SORT_THREADS) (&h[0][0])[k] = 0;
     __syncthreads();
     const u32 base = blockIdx.x * (u32)TILE;
-    const int lane = tid & 31;
-#pragma unroll 4
-    for (int r = 0; r < SORT_ITEMS; ++r) {
-        u32 i = base + (u32)r * SORT_THREADS + tid;
-        bool valid = i < n;
-        u32 d = valid ? (keys[i] >> shift) & 255u : 256u + lane;  // invalid lanes get unique digits
-        u32 peers = __match_any_sync(0xffffffffu, d);
-        int leader = __ffs(peers) - 1;
-        if (valid && lane == leader) atomicAdd(&h[d], (u32)__popc(peers));
+    u32* hw = h[w];
+    if (base + TILE <= n && (reinterpret_cast<uintptr_t>(keys) & 15u) == 0) {
+        const uint4* k4 = reinterpret_cast<const uint4*>(keys + base);
+#pragma unroll
+        for (int r = 0; r < SORT_ITEMS / 4; ++r) {
+            const uint4 q = k4[r * SORT_THREADS + tid];
+            atomicAdd(&hw[(q.x >> shift) & 255u], 1u);
+            atomicAdd(&hw[(q.y >> shift) & 255u], 1u);
+            atomicAdd(&hw[(q.z >> shift) & 255u], 1u);
+            atomicAdd(&hw[(q.w >> shift) & 255u], 1u);
+        }
+    } else {
+        for (int r = 0; r < SORT_ITEMS; ++r) {
+            const u32 i = base + (u32)r * SORT_THREADS + tid;
+            if (i < n) atomicAdd(&hw[(keys[i] >> shift) & 255u], 1u);
+        }
     }
     __syncthreads();
-    hist[(u32)tid * numTiles + blockIdx.x] = h[tid];
+    u32 sum = 0;
+#pragma unroll
+    for (int ww = 0; ww < W; ++ww) sum += h[ww][tid];
+    hist[(u32)tid * numTiles + blockIdx.x] = sum;
 }
 
 // One CTA per digit: exclusive scan of hist[d, 0..numTiles) in place; total
