@@ -137,7 +137,7 @@ void launch_refit_roots(const RefitJob* jobsDev, u32 numJobs, cudaStream_t s);
 // (then the union of the swept leaf boxes is the union of {x, x + v dt} over
 // the vertices): one block per chunk (job, first vertex) of ROOT_CHUNK
 // vertices, then launch_refit_roots on the same jobs.
-static constexpr u32 ROOT_CHUNK = 2048;
+static constexpr u32 ROOT_CHUNK = 512;
 void launch_root_boxes(const RefitJob* jobsDev, u32 numJobs, const uint2* chunks, u32 numChunks, cudaStream_t s);
 
 }  // namespace ys
