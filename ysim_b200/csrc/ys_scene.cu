@@ -552,9 +552,23 @@ __global__ void __launch_bounds__(128, MINB) k_fused(StepArgs A) {
         A.xn[g] = A.x[g];
         A.vn[g] = A.v[g];
     }
-    if (valid && A.record) {
-        u32 base = (u32)atomicAdd(&A.counters[2], (unsigned long long)nc);
-        if (base + (u32)nc > A.cap) {
+    if (A.record) {
+        // pool slots: one atomic per warp (every lane of the block reaches
+        // this point), the lanes' runs in lane order after the warp's base
+        const u32 mine = valid ? (u32)nc : 0u;
+        u32 incl = mine;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const u32 y = __shfl_up_sync(FULL_MASK, incl, o);
+            if ((int)lane >= o) incl += y;
+        }
+        const u32 total = __shfl_sync(FULL_MASK, incl, 31);
+        u32 wbase = 0;
+        if (lane == 31 && total) wbase = (u32)atomicAdd(&A.counters[2], (unsigned long long)total);
+        wbase = __shfl_sync(FULL_MASK, wbase, 31);
+        const u32 base = wbase + (incl - mine);
+        if (!valid) {
+        } else if (base + (u32)nc > A.cap) {
             st |= ST_PAIR_OVF;
             A.vstart[g] = 0;
             A.vcount[g] = 0;
