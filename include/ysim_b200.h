@@ -183,7 +183,7 @@ ys_status ys_scene_set_record(ys_scene* s, int record);
  * that rebuild trees, record contacts or time kernels run eagerly). */
 ys_status ys_scene_set_graphs(ys_scene* s, int on);
 /* Register cap of the fused substep kernel, as CTAs per SM (8: 64 registers,
- * 6: 80, 4: uncapped).  The results are the same for every value; the speed
+ * 7: 72, 4: uncapped).  The results are the same for every value; the speed
  * depends on the scene (self-colliding scenes favour 8, spring-bound ones
  * fewer spills).  No counterpart in the reference (its Metal pipelines have
  * fixed threadgroup sizes). */
@@ -192,7 +192,7 @@ ys_status ys_scene_set_fused_variant(ys_scene* s, int min_blocks);
  * each; the kernel only writes the next-state buffers and the running totals
  * are restored, so the scene does not advance), keeps the fastest, and
  * reports it (*chosen) and the mean milliseconds per variant (ms_out[3], in
- * the order 8, 6, 4; may be null).  No counterpart in the reference. */
+ * the order 8, 7, 4; may be null).  No counterpart in the reference. */
 ys_status ys_scene_autotune(ys_scene* s, uint32_t reps, int* chosen, float* ms_out);
 /* Analytic collider (GeneralMesh::colliderKind and transform): kind
  * YS_COLLIDER_SPHERE / BOX / CYLINDER / PLANE (YS_COLLIDER_MESH: triangles,

@@ -16,7 +16,7 @@ def test_fused_variants_agree_and_autotune_keeps_state(cuda_lib):
     from ysim_b200.scene import Scene
     spec = _spec()
     outs = []
-    for v in (8, 6, 4):
+    for v in (8, 7, 4):
         s = Scene(spec)
         try:
             s.set_fused_variant(v)
@@ -34,7 +34,7 @@ def test_fused_variants_agree_and_autotune_keeps_state(cuda_lib):
         s.step(20)
         x0, t0 = s.get("x"), s.totals()
         chosen, ms = s.autotune(reps=3)
-        assert chosen in (8, 6, 4) and all(m > 0 for m in ms)
+        assert chosen in (8, 7, 4) and all(m > 0 for m in ms)
         assert np.array_equal(s.get("x").view(np.uint32), x0.view(np.uint32))
         assert s.totals() == t0
         s.step(10)

@@ -314,7 +314,7 @@ __device__ __noinline__ bool analytic_contact(const DShape* S, f3 pcur, f3 pprev
 }
 
 // WIDE: descend the 4-wide form of the trees (cube layout), else the binary one.
-// MINB: CTAs per SM the registers are capped for (8: 64 registers, 6: 80,
+// MINB: CTAs per SM the registers are capped for (8: 64 registers, 7: 72,
 // 4: no cap); the results do not depend on it (ys_scene_autotune picks one).
 // ANA: the scene has analytic colliders (without them the kernel carries no
 // analytic branch).
@@ -595,16 +595,16 @@ __global__ void __launch_bounds__(128, MINB) k_fused(StepArgs A) {
     if (st) atomicOr(A.status, st);
 }
 
-static constexpr int FUSED_VARIANTS[3] = {8, 6, 4};  // register caps, as CTAs per SM
+static constexpr int FUSED_VARIANTS[3] = {8, 7, 4};  // register caps, as CTAs per SM
 
 template <bool ANA>
 void launch_fused_t(const StepArgs& A, dim3 g, dim3 b, cudaStream_t st, int minBlocks) {
     switch ((A.wide ? 0 : 10) + minBlocks) {
         case 8: k_fused<true, 8, ANA><<<g, b, 0, st>>>(A); break;
-        case 6: k_fused<true, 6, ANA><<<g, b, 0, st>>>(A); break;
+        case 7: k_fused<true, 7, ANA><<<g, b, 0, st>>>(A); break;
         case 4: k_fused<true, 4, ANA><<<g, b, 0, st>>>(A); break;
         case 18: k_fused<false, 8, ANA><<<g, b, 0, st>>>(A); break;
-        case 16: k_fused<false, 6, ANA><<<g, b, 0, st>>>(A); break;
+        case 17: k_fused<false, 7, ANA><<<g, b, 0, st>>>(A); break;
         default: k_fused<false, 4, ANA><<<g, b, 0, st>>>(A); break;
     }
 }
@@ -1872,8 +1872,8 @@ ys_status ys_scene_set_tree_builder(ys_scene* s, int builder) {
 
 ys_status ys_scene_set_fused_variant(ys_scene* s, int min_blocks) {
     if (!s) return fail(YS_ERR_BAD_ARG, "null scene");
-    if (min_blocks != 8 && min_blocks != 6 && min_blocks != 4)
-        return fail(YS_ERR_BAD_ARG, "fused variant: CTAs per SM must be 8, 6 or 4");
+    if (min_blocks != 8 && min_blocks != 7 && min_blocks != 4)
+        return fail(YS_ERR_BAD_ARG, "fused variant: CTAs per SM must be 8, 7 or 4");
     s->fused_min_blocks = min_blocks;
     drop_graphs(s);
     return YS_OK;
