@@ -184,8 +184,8 @@ ys_status ys_scene_set_record(ys_scene* s, int record);
 ys_status ys_scene_set_graphs(ys_scene* s, int on);
 /* Register cap of the fused substep kernel, as CTAs per SM (8: 64 registers,
  * 7: 72, 4: uncapped).  The results are the same for every value; the speed
- * depends on the scene (self-colliding scenes favour 8, spring-bound ones
- * fewer spills).  No counterpart in the reference (its Metal pipelines have
+ * depends on the scene (the self-colliding 262k-vertex cloth runs fastest at 7,
+ * the batched FastGrid instances at 8).  No counterpart in the reference (its Metal pipelines have
  * fixed threadgroup sizes). */
 ys_status ys_scene_set_fused_variant(ys_scene* s, int min_blocks);
 /* Autotuner: times each variant on the scene's current state (reps launches
