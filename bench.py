@@ -42,6 +42,12 @@ import numpy as np  # noqa: E402
 
 METRIC = "substeps/s at 262k-vert self-colliding cloth; batched vs plain; adjoint ms/step"
 UNIT = "substeps/s"
+# Untimed substeps before the warm-up of the headline workload.  The 512x512
+# cloth starts 0.046 above the obstacle's top and falls at 1 m/s^2: its first
+# contacts come near substep 370, and at substep 500 it has about 11k contacts
+# per substep (18k at 540, 54k at 800), so every timed substep is in the
+# contact regime whatever --steps is.
+PREROLL = 500
 
 
 def parse():
@@ -50,7 +56,11 @@ def parse():
     ap.add_argument("--steps", type=int, default=400)
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--preroll", type=int, default=240, help="untimed substeps before warm-up (reach contact)")
+    ap.add_argument("--preroll", type=int, default=PREROLL,
+                    help="untimed substeps before warm-up; the default puts the timed substeps in the contact "
+                         "regime of the drape (first contacts near substep 370, about 11k per substep at 500)")
+    ap.add_argument("--allow-free-fall", action="store_true",
+                    help="report a run whose timed substeps saw no contacts instead of failing it")
     ap.add_argument("--e2e-frames", type=int, default=None,
                     help="end-to-end frames (default: the frames the timed substeps make up)")
     ap.add_argument("--cpu-substeps", type=int, default=3, help="substeps of the CPU baseline sample")
@@ -257,32 +267,51 @@ def reference_scene(spec):
 
 def run_reference(args, rank, world):
     """Reference arm: the path's CPU implementation on the host cores, all
-    threads (OpenMP), on this arm's config.  Rank 0 alone works."""
+    threads (OpenMP), on this arm's config and the same stretch of the drape.
+    The pinned CPU restatement (bit-identical to the CUDA path's trajectory)
+    pre-rolls the scene to the substep the CUDA arm's timed substeps start
+    from (pre-roll + warm-up), untimed; the reference kernels then take that
+    state, rebuild their trees in an untimed frame-0 substep, and time
+    `steps` substeps (at most --cpu-substeps).  Rank 0 alone works."""
     if rank != 0:
         return
     from oracle import oracle as O
     spec = spec_for(args)
-    scene, kind = reference_scene(spec)
     cores = O.max_threads()
-    scene.step(1)  # frame-0 preamble (tree build), untimed
-    warm = min(max(args.warmup, 0), 1)
-    scene.step(warm)
+    start = args.preroll + max(args.warmup, 6)
+    t0 = time.perf_counter()
+    port = O.OracleScene(spec)
+    port.step(max(start - 1, 0))
+    preroll_s = time.perf_counter() - t0
+    state = {"x": port.get("x"), "v": port.get("v"), "xprev": port.get("xprev")}
+    scene, kind = reference_scene(spec)
+    if kind == "reference":
+        del port
+        scene.x, scene.v, scene.xp = state["x"].copy(), state["v"].copy(), state["xprev"].copy()
+    else:
+        scene = port
+    scene.step(1)  # frame-0 preamble of the reference kernels (tree build), untimed
     nsteps = max(1, min(args.steps, args.cpu_substeps))
     t0 = time.perf_counter()
     scene.step(nsteps)
     dt = time.perf_counter() - t0
+    contacts = getattr(scene, "ncontacts", None)
+    if contacts is None:
+        contacts = scene.stats()["contacts"]
     v = nsteps / dt
+    sample = (f"{nsteps} substeps of the full workload from substep {start} of the drape (the CUDA arm's first timed "
+              f"substep; pre-rolled by the pinned CPU restatement in {preroll_s:.0f} s, untimed), after an untimed "
+              "frame-0 tree build; ")
+    sample += ("the reference's Metal kernels compiled for the host (oracle/_ref) with the pinned CPU-hash "
+               "restatement for self rows" if kind == "reference" else "CPU restatement, OpenMP")
     line = {
         "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world, "steps": nsteps,
-        "warmup": warm, "ms_per_step": 1000.0 * dt / nsteps, "higher_is_better": True,
+        "warmup": start, "ms_per_step": 1000.0 * dt / nsteps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
-        "config": workload_config(args, spec, {"parallelism": "host cores, OpenMP over kernel thread ids"}),
-        "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": kind,
-                         "sample": f"{nsteps} substeps of the full workload after the frame-0 build and {warm} "
-                                   "warm-up substep(s); the reference's Metal kernels compiled for the host "
-                                   "(oracle/_ref) with the pinned CPU-hash restatement for self rows"
-                                   if kind == "reference" else
-                                   f"{nsteps} substeps of the full workload (CPU restatement, OpenMP)"},
+        "config": workload_config(args, spec, {"parallelism": "host cores, OpenMP over kernel thread ids",
+                                               "first_timed_substep": start,
+                                               "contacts_last_substep": int(contacts)}),
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample},
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -385,6 +414,14 @@ def run_ours(args, rank, world, local):
     cont_ps = (after[1] - before[1] - k_cont) / args.steps
     k_rows_ps = k_rows / ksteps
     k_cont_ps = k_cont / ksteps
+    if cont_ps == 0 and k_cont_ps == 0 and not args.allow_free_fall:
+        # a window with no contacts times the free fall, where the narrow
+        # phase's response and the contact lists never fire
+        if rank == 0:
+            print(json.dumps({"metric": METRIC, "error": "no contacts in the timed substeps (free fall); "
+                              "lengthen --preroll or pass --allow-free-fall",
+                              "preroll_substeps": args.preroll, "candidate_rows_per_substep": rows_ps}), flush=True)
+        sys.exit(4)
 
     # ---- e2e through the public API with host buffers
     nsub = spec.params.substeps
@@ -483,6 +520,7 @@ def run_ours(args, rank, world, local):
             "config": workload_config(args, spec, {"parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                                                    "candidate_rows_per_substep": rows_ps,
                                                    "contacts_per_substep": cont_ps, "preroll_substeps": args.preroll,
+                                                   "first_timed_substep": args.preroll + max(args.warmup, 6),
                                                    "fused_variant": {"ctas_per_sm": tuned,
                                                                      "autotune_ms": dict(zip(("8", "7", "4"), tune_ms))},
                                                    "flags": st["flags"]}),
