@@ -411,7 +411,9 @@ ys_status ys_radix_sort_pairs(uint32_t* d_keys, uint32_t* d_vals, uint32_t n, vo
  * __device__ array that every GPU loading this library holds until exit.
  * At most 1,048,576 pairs (larger n returns YS_ERR_CAPACITY).  The first call
  * on a device looks up that array's device address, so make it before any
- * stream capture.  All calls share the one array: calls that overlap on the
+ * stream capture; after a device reset (cudaDeviceReset) the device has a new
+ * context, and the first call in it looks the address up again, so make that
+ * one before any capture too.  All calls share the one array: calls that overlap on the
  * GPU (different streams or threads without ordering) race.  Asynchronous on
  * `stream`.  Has no counterpart in the reference. */
 ys_status ys_radix_sort_pairs_noalloc(uint32_t* d_keys, uint32_t* d_vals, uint32_t n, void* stream);

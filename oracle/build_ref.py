@@ -10,7 +10,11 @@ reference's scene-file, run-config and primitive-geometry headers
 the reference is copied into this repository.  Skipped (returns None) when the reference checkout is absent;
 the built library is git-ignored but travels with the working tree.
 
-    python -m oracle.build_ref
+The reference checkout is the directory given by --reference, else by the
+YSIM_REFERENCE environment variable, else a checkout named `reference` beside
+this repository's directory.
+
+    python -m oracle.build_ref [--reference DIR] [--force]
 """
 from __future__ import annotations
 
@@ -19,7 +23,7 @@ import subprocess
 import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF = os.environ.get("YSIM_REFERENCE", "/root/reference")
+REF = os.environ.get("YSIM_REFERENCE") or os.path.join(os.path.dirname(os.path.dirname(HERE)), "reference")
 OUT_DIR = os.path.join(HERE, "_ref")
 OUT = os.path.join(OUT_DIR, "libysref.so")
 SHADERS = {"BVH": "bvh.metal", "NARROW": "bruteforce.metal", "PHYSICS": "physics.metal",
@@ -69,4 +73,6 @@ def build(force: bool = False):
 
 
 if __name__ == "__main__":
+    if "--reference" in sys.argv:
+        REF = os.path.abspath(sys.argv[sys.argv.index("--reference") + 1])
     print(build(force="--force" in sys.argv))

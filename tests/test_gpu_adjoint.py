@@ -218,9 +218,11 @@ def test_fp64_adjoint_matches_fp64_reference_bit_for_bit(cuda_lib, height, T, la
 def test_fp64_adjoint_within_1e4_of_fp64_finite_differences(cuda_lib, height, contacts):
     """Central differences of the GPU's own FP64 rollout, per parameter group
     at the step that balances truncation against round-off (k: 1e-3
-    relative; L: 1e-6; v0: 1e-5), on the largest and on random components;
-    each must agree with the adjoint to 1e-4 of the larger of |fd| and 1% of
-    the group's largest gradient."""
+    relative; L: 1e-6; v0: 1e-5), on the largest and on random components.
+    A component whose |fd| is at least 1e-4 of the group's largest gradient
+    (and far above the difference's round-off) must agree with the adjoint to
+    1e-4 relative, |g - fd| / |fd|; a smaller one, whose difference is mostly
+    round-off and truncation, to 1e-8 of the group's largest gradient."""
     import torch
     spec = _f32_spec(_small(height=height))
     k, L, v0, w, _ = _problem(spec)
@@ -239,16 +241,24 @@ def test_fp64_adjoint_within_1e4_of_fp64_finite_differences(cuda_lib, height, co
                 return float((roll(p[0], p[1], p[2].reshape(-1, 3)) * w64).sum())
 
         rng = np.random.default_rng(7)
-        worst = 0.0
+        worst, n_rel = 0.0, 0
         for group, g in enumerate(grads):
+            gmax = float(np.abs(g).max())
             idx = list(np.argsort(-np.abs(g))[:3]) + list(rng.integers(len(g), size=3))
             for i in idx:
                 eps = 1e-3 * abs(float(base[0][i])) if group == 0 else (1e-6 if group == 1 else 1e-5)
-                fd = (loss(group, int(i), eps) - loss(group, int(i), -eps)) / (2 * eps)
-                err = abs(g[i] - fd) / max(abs(fd), 1e-2 * np.abs(g).max())
-                worst = max(worst, err)
-                assert err <= 1e-4, (group, int(i), g[i], fd, err)
-        print("fp64 adjoint vs fp64 fd, worst relative error", worst)
+                lp, lm = loss(group, int(i), eps), loss(group, int(i), -eps)
+                fd = (lp - lm) / (2 * eps)
+                noise = 64 * np.finfo(np.float64).eps * (abs(lp) + abs(lm)) / (2 * eps)
+                if abs(fd) >= max(1e-4 * gmax, 1e3 * noise):
+                    err = abs(g[i] - fd) / abs(fd)
+                    worst = max(worst, err)
+                    n_rel += 1
+                    assert err <= 1e-4, (group, int(i), g[i], fd, err)
+                else:
+                    assert abs(g[i] - fd) <= 1e-8 * gmax, (group, int(i), g[i], fd, gmax)
+        assert n_rel >= 9  # at least the three largest of each group
+        print("fp64 adjoint vs fp64 fd, worst relative error", worst, "over", n_rel, "components")
     finally:
         roll.close()
 

@@ -331,24 +331,6 @@ def test_scene_tree_matches_oracle(cuda_lib, oracle, builder):
         s.close()
 
 
-@pytest.mark.slow
-def test_full_size_c2_runs_clean(cuda_lib):
-    """Headline workload at full size: finite, in-box positions, no flags, and
-    the fused path equals the staged path (same kernels' arithmetic)."""
-    from ysim_b200 import generators as G
-    from ysim_b200.scene import Scene
-    spec = G.config_c2()
-    s = Scene(spec)
-    try:
-        s.step(2 * spec.params.substeps)
-        x = s.get("x")
-        assert np.isfinite(x).all()
-        st = s.stats()
-        assert st["flags"] & ~0 == 0, st
-    finally:
-        s.close()
-
-
 @pytest.mark.parametrize("case", ["soup", "sparse", "huge_tri"])
 def test_spatial_hash_equals_lbvh_query(cuda_lib, oracle, case):
     """Spatial-hash broad phase == LBVH point query (== brute force) as sets."""

@@ -14,7 +14,10 @@ namespace ys {
 ys_status fail(ys_status code, const std::string& msg);
 
 // queryPoints (bvh.metal:1394-1412): one thread per query point; pairs are
-// (point, triangle), appended with one atomic per lane-batch.
+// (point, triangle).  The lanes that reach a leaf together (the converged
+// lanes at the append) reserve their slots with one atomic, made by the
+// lowest of them; the reference appends with one atomic per pair
+// (bvh.metal:1372-1381).
 __global__ void __launch_bounds__(128) k_query_points(const Node* __restrict__ nodes, u32 numNodes,
                                                       const u32* __restrict__ F, const float* __restrict__ qx, u32 nQ,
                                                       const u32* __restrict__ order, float m, int self,
@@ -27,7 +30,12 @@ __global__ void __launch_bounds__(128) k_query_points(const Node* __restrict__ n
     const f3 qmn = q - mk(m, m, m), qmx = q + mk(m, m, m);
     u32 st = traverse(nodes, numNodes, qmn, qmx, [&](u32 f) {
         if (self && (F[3 * f] == p || F[3 * f + 1] == p || F[3 * f + 2] == p)) return;
-        unsigned long long i = atomicAdd(count, 1ull);
+        const unsigned act = __activemask();
+        const u32 lane = threadIdx.x & 31u, leader = (u32)__ffs(act) - 1u;
+        unsigned long long base = 0;
+        if (lane == leader) base = atomicAdd(count, (unsigned long long)__popc(act));
+        base = __shfl_sync(act, base, (int)leader);
+        const unsigned long long i = base + (u32)__popc(act & ((1u << lane) - 1u));
         if (i < cap) { pairs[2 * i] = p; pairs[2 * i + 1] = f; }
     });
     if (st) atomicOr(status, st);

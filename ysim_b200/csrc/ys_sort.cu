@@ -235,6 +235,32 @@ static __device__ __align__(256) unsigned char g_noalloc_sort_scratch[NOALLOC_SC
 
 static std::mutex g_noalloc_mutex;
 static void* g_noalloc_addr[64] = {};
+static unsigned long long g_noalloc_ctx[64] = {};  // context the address was looked up in
+
+// Unique id of the calling thread's current CUDA context (cuCtxGetId, through
+// the runtime's driver entry points, so the library needs no -lcuda).  A
+// device reset destroys the device's primary context and the next one gets a
+// new id, which is how a cached symbol address is known to be stale.
+static bool current_context_id(unsigned long long* id) {
+    typedef int (*GetCurrent)(void**);
+    typedef int (*GetId)(void*, unsigned long long*);
+    static GetCurrent get_current = nullptr;
+    static GetId get_id = nullptr;
+    static bool looked = false;
+    if (!looked) {
+        looked = true;
+        cudaDriverEntryPointQueryResult q1, q2;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", (void**)&get_current, cudaEnableDefault, &q1) != cudaSuccess ||
+            q1 != cudaDriverEntryPointSuccess)
+            get_current = nullptr;
+        if (cudaGetDriverEntryPoint("cuCtxGetId", (void**)&get_id, cudaEnableDefault, &q2) != cudaSuccess ||
+            q2 != cudaDriverEntryPointSuccess)
+            get_id = nullptr;
+    }
+    void* ctx = nullptr;
+    if (!get_current || !get_id || get_current(&ctx) != 0 || !ctx) return false;
+    return get_id(ctx, id) == 0;
+}
 }  // namespace ys
 
 extern "C" ys_status ys_radix_sort_pairs_noalloc(uint32_t* d_keys, uint32_t* d_vals, uint32_t n, void* stream) {
@@ -251,15 +277,19 @@ extern "C" ys_status ys_radix_sort_pairs_noalloc(uint32_t* d_keys, uint32_t* d_v
     if (dev < 0 || dev >= 64) return fail(YS_ERR_BAD_ARG, "device index out of range");
     void* scratch = nullptr;
     {
-        // first call on this device: look up the device address of the array
-        // (its host-side name is only a stand-in and must never reach a kernel)
+        // first call on this device (or in a new context of it, after a
+        // device reset): look up the device address of the array (its
+        // host-side name is only a stand-in and must never reach a kernel)
         std::lock_guard<std::mutex> lock(g_noalloc_mutex);
-        if (!g_noalloc_addr[dev]) {
+        unsigned long long ctx = 0;
+        const bool known = current_context_id(&ctx);
+        if (!g_noalloc_addr[dev] || (known && ctx != g_noalloc_ctx[dev])) {
             void* p = nullptr;
             e = cudaGetSymbolAddress(&p, g_noalloc_sort_scratch);
             if (e != cudaSuccess)
                 return fail(YS_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
             g_noalloc_addr[dev] = p;
+            g_noalloc_ctx[dev] = current_context_id(&ctx) ? ctx : 0;
         }
         scratch = g_noalloc_addr[dev];
     }
