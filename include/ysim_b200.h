@@ -188,6 +188,14 @@ ys_status ys_scene_set_graphs(ys_scene* s, int on);
  * the batched FastGrid instances at 8).  No counterpart in the reference (its Metal pipelines have
  * fixed threadgroup sizes). */
 ys_status ys_scene_set_fused_variant(ys_scene* s, int min_blocks);
+/* Thread order of the fused substep kernel: on (default), its threads take
+ * the working vertices (cloth, moving or querying; static obstacles are left
+ * out) in Morton order within each mesh, recomputed from the positions at
+ * every tree rebuild, so a warp's 32 vertices are a compact patch whose
+ * descents and candidate faces overlap; off, thread i takes vertex i.  The
+ * results are the same either way.  No counterpart in the reference (one
+ * Metal thread per vertex id). */
+ys_status ys_scene_set_thread_order(ys_scene* s, int on);
 /* Autotuner: times each variant on the scene's current state (reps launches
  * each; the kernel only writes the next-state buffers and the running totals
  * are restored, so the scene does not advance), keeps the fastest, and

@@ -229,17 +229,17 @@ __device__ __forceinline__ void h1_query_box(const H1Vertex& h, float m, f3& qmn
     qmn = mk(h.lo[0] - pad, h.lo[1] - pad, h.lo[2] - pad);
     qmx = mk(h.hi[0] + pad, h.hi[1] + pad, h.hi[2] + pad);
 }
-// Exact row test for face f of the vertex's own mesh: the face key box (tri
-// AABB +- m, collectFaceBoxes spatial_hash.hpp:1625-1643) overlaps the swept
-// vertex box, the face does not contain the vertex, and the point-triangle
-// distance^2 at x or xPrev is <= m^2 (spatial_hash.hpp:1804-1846).
+// Exact row test for face f of the vertex's own mesh (h1_face): the face does
+// not contain the vertex, the face key box (tri AABB +- m, collectFaceBoxes
+// spatial_hash.hpp:1625-1643) overlaps the swept vertex box, and the
+// point-triangle distance^2 at x or xPrev is <= m^2
+// (spatial_hash.hpp:1804-1846).  h1_face_at is the part after the own-face
+// check, on the face's three vertex positions.
 // span_check = false skips the face's 64-cell test, for callers whose cell
 // size is this mesh's largest key-box extent computed from the same positions
 // (the refit's H1 extent): every key box then spans at most two cells.
-__device__ __forceinline__ bool h1_face(const float4* __restrict__ X, u32 voff, uint4 tri, u32 v, float m, float inv,
-                                        const H1Vertex& h, bool span_check = true) {
-    if (tri.x == v || tri.y == v || tri.z == v) return false;
-    f3 P0 = ld(X, voff + tri.x), P1 = ld(X, voff + tri.y), P2 = ld(X, voff + tri.z);
+__device__ __forceinline__ bool h1_face_at(f3 P0, f3 P1, f3 P2, float m, float inv, const H1Vertex& h,
+                                           bool span_check) {
     const float A[3] = {P0.x, P0.y, P0.z}, B[3] = {P1.x, P1.y, P1.z}, C[3] = {P2.x, P2.y, P2.z};
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
@@ -269,6 +269,11 @@ __device__ __forceinline__ bool h1_face(const float4* __restrict__ X, u32 voff, 
     const float m2 = m * m;
     if (point_tri_sq(h.pc, A, B, C) > m2 && point_tri_sq(h.pp, A, B, C) > m2) return false;
     return true;
+}
+__device__ __forceinline__ bool h1_face(const float4* __restrict__ X, u32 voff, uint4 tri, u32 v, float m, float inv,
+                                        const H1Vertex& h, bool span_check = true) {
+    if (tri.x == v || tri.y == v || tri.z == v) return false;
+    return h1_face_at(ld(X, voff + tri.x), ld(X, voff + tri.y), ld(X, voff + tri.z), m, inv, h, span_check);
 }
 
 // ------------------------------------------------------------- N1 narrow

@@ -7,20 +7,6 @@
 namespace ys {
 
 // ------------------------------------------------------------------ scene box
-// Order-preserving float <-> uint map so atomicMin/atomicMax on uints give
-// float min/max (the min/max of a set does not depend on order).
-__device__ __forceinline__ u32 ford(float f) {
-    u32 u = __float_as_uint(f);
-    return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
-}
-__host__ __device__ __forceinline__ float funord(u32 u) {
-#ifdef __CUDA_ARCH__
-    return __uint_as_float((u & 0x80000000u) ? (u & 0x7FFFFFFFu) : ~u);
-#else
-    u32 r = (u & 0x80000000u) ? (u & 0x7FFFFFFFu) : ~u;
-    float f; memcpy(&f, &r, 4); return f;
-#endif
-}
 
 __global__ void k_box_init(u32* box) {
     int t = threadIdx.x;
@@ -77,13 +63,6 @@ void launch_box(const float4* x4, const float* x3, u32 voff, u32 nV, u32* box, c
 }
 
 // ------------------------------------------------------------------ Morton
-__device__ __forceinline__ u32 expand_bits(u32 v) {
-    v = (v * 0x00010001u) & 0xFF0000FFu;
-    v = (v * 0x00000101u) & 0x0F00F00Fu;
-    v = (v * 0x00000011u) & 0xC30C30C3u;
-    v = (v * 0x00000005u) & 0x49249249u;
-    return v;
-}
 __device__ __forceinline__ float clamp01023(float v) { return fminf(fmaxf(v, 0.f), 1023.f); }
 
 // fillMortons_Tri (bvh.metal:42-63): centroid ((x0+x1)+x2)/3, normalised by
@@ -509,10 +488,21 @@ __global__ void __launch_bounds__(256) k_refit(const RefitJob* __restrict__ jobs
     const u32 vid[3] = {J.facets[3 * f], J.facets[3 * f + 1], J.facets[3 * f + 2]};
     f3 lo, hi;
     float ext = 0.f;
+    f3 P[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const u32 gv = J.voff + vid[k];
+        P[k] = J.x4 ? ld(J.x4, gv) : ldp(J.x3, gv);
+    }
+    if (J.fpos && valid) {
+        float4* o = J.fpos + 3 * (size_t)f;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) o[k] = make_float4(P[k].x, P[k].y, P[k].z, __uint_as_float(vid[k]));
+    }
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
         u32 gv = J.voff + vid[k];
-        f3 p = J.x4 ? ld(J.x4, gv) : ldp(J.x3, gv);
+        f3 p = P[k];
         f3 a = p, b = p;
         if (J.swept) {
             f3 vv = J.v4 ? ld(J.v4, gv) : ldp(J.v3, gv);
@@ -528,13 +518,7 @@ __global__ void __launch_bounds__(256) k_refit(const RefitJob* __restrict__ jobs
         float m = J.selfMargin;
         bool ok = true;
         float e = 0.f;
-        f3 P0, P1, P2;
-        {
-            u32 g0 = J.voff + vid[0], g1 = J.voff + vid[1], g2 = J.voff + vid[2];
-            P0 = J.x4 ? ld(J.x4, g0) : ldp(J.x3, g0);
-            P1 = J.x4 ? ld(J.x4, g1) : ldp(J.x3, g1);
-            P2 = J.x4 ? ld(J.x4, g2) : ldp(J.x3, g2);
-        }
+        const f3 P0 = P[0], P1 = P[1], P2 = P[2];
         float pa[3][3] = {{P0.x, P1.x, P2.x}, {P0.y, P1.y, P2.y}, {P0.z, P1.z, P2.z}};
 #pragma unroll
         for (int a = 0; a < 3; ++a) {

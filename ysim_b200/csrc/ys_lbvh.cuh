@@ -3,10 +3,36 @@
 // (bvh.hpp:148-177, bvh.metal:260-393): internal nodes [0, N-2] with the root
 // at slot 0, leaves at [N-1, 2N-2].
 #pragma once
+#include <cstring>
+
 #include "ys_common.cuh"
 #include "ys_scan.cuh"
 
 namespace ys {
+
+// Order-preserving float <-> uint map so atomicMin/atomicMax on uints give
+// float min/max (the min/max of a set does not depend on order).
+__device__ __forceinline__ u32 ford(float f) {
+    u32 u = __float_as_uint(f);
+    return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+__host__ __device__ __forceinline__ float funord(u32 u) {
+#ifdef __CUDA_ARCH__
+    return __uint_as_float((u & 0x80000000u) ? (u & 0x7FFFFFFFu) : ~u);
+#else
+    u32 r = (u & 0x80000000u) ? (u & 0x7FFFFFFFu) : ~u;
+    float f; memcpy(&f, &r, 4); return f;
+#endif
+}
+
+// expandBits (bvh.metal:26-32): the 10 low bits of v spread to every third bit.
+__device__ __forceinline__ u32 expand_bits(u32 v) {
+    v = (v * 0x00010001u) & 0xFF0000FFu;
+    v = (v * 0x00000101u) & 0x0F00F00Fu;
+    v = (v * 0x00000011u) & 0xC30C30C3u;
+    v = (v * 0x00000005u) & 0x49249249u;
+    return v;
+}
 
 // One tree to refit: leaves are recomputed from positions (optionally swept by
 // v*dt) and combined bottom-up.  Positions/velocities are float4 (padded) or
@@ -49,6 +75,10 @@ struct RefitJob {
     const int2* leafWf;     // per face: (wide node, slot)
     const u32* wcount;      // number of wide nodes of this tree
     u32* hacc;              // per wide node: height (1 = leaf children only)
+    // face positions (or null): per face its three vertices' current
+    // positions, each float4 carrying the mesh-local vertex id in w, written
+    // by the leaf pass for the queries that test the face
+    float4* fpos;
 };
 
 // Scene box of a mesh (min/max over all its vertices) into box[6] (float

@@ -72,6 +72,10 @@ struct StepArgs {
     const MeshDev* meshes;
     const u32* targets;
     const uint4* F;
+    // per face (global face index): its three vertices' positions at the
+    // start of the substep, the mesh-local vertex id in w (written by the
+    // refit's leaf pass, or at the build of a tree that is never refit)
+    const float4* fpos;
     const Node* nodes;
     const Wide4* w4;  // 4-wide form of the trees (wide != 0)
     u32 wide;
@@ -97,6 +101,11 @@ struct StepArgs {
     u32 analytic;  // the scene has analytic colliders
     float subh, kair, kd, gx, gy, gz, margin, band, radius;
     u32 nV, self_mode, record, cap;
+    // fused kernel: thread t works on vertex vorder[t] (vertices in Morton
+    // order within their mesh, static non-query vertices left out), or on
+    // vertex t when vorder is null; nthreads threads carry a vertex
+    const u32* vorder;
+    u32 nthreads;
     u32* status;
     unsigned long long* counters;  // [0] broad rows, [1] contacts, [2] pool fill, [3] [4] running totals of 0, 1
     // fused record pool
@@ -323,8 +332,9 @@ __global__ void __launch_bounds__(128, MINB) k_fused(StepArgs A) {
     __shared__ WarpWork wq[FUSED_WARPS];
     const u32 lane = threadIdx.x & 31u;
     WarpWork& Q = wq[threadIdx.x >> 5];
-    const u32 g = blockIdx.x * blockDim.x + threadIdx.x;
-    const bool valid = g < A.nV;
+    const u32 t = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool valid = t < A.nthreads;
+    const u32 g = !valid ? 0u : (A.vorder ? A.vorder[t] : t);
     const u32 m = valid ? A.vobj[g] : 0u;
     const MeshDev* __restrict__ Mp = A.meshes + m;
     const u32 mflags = Mp->flags;
@@ -432,27 +442,27 @@ __global__ void __launch_bounds__(128, MINB) k_fused(StepArgs A) {
         VContact c;
         if (has) {
             const u32 t = k >> 6;
-            const u32 tvo = A.meshes[t].voff;
-            const uint4 tri = A.F[A.meshes[t].foff + f];
+            // the face's vertices in one 48-byte record (ids in w)
+            const float4* fp = A.fpos + 3 * (size_t)(A.meshes[t].foff + f);
+            const float4 q0 = __ldg(fp), q1 = __ldg(fp + 1), q2 = __ldg(fp + 2);
+            const f3 P0 = mk(q0.x, q0.y, q0.z), P1 = mk(q1.x, q1.y, q1.z), P2 = mk(q2.x, q2.y, q2.z);
             bool row = true;
             if (k & KEY_SELF) {
-                if (A.self_mode == YS_SELF_HASH) {
+                const u32 lid = og - A.meshes[t].voff;
+                row = !(__float_as_uint(q0.w) == lid || __float_as_uint(q1.w) == lid || __float_as_uint(q2.w) == lid);
+                if (row && A.self_mode == YS_SELF_HASH) {
                     // the owner passed its 64-cell check; the cell size is the
                     // extent the refit just took from these positions
                     H1Vertex h;
                     h1_vertex_box(oxc, oxp, h);
-                    row = h1_face(A.x, tvo, tri, og - tvo, mg, oinv, h, false);
-                } else {
-                    const u32 lid = og - tvo;
-                    row = !(tri.x == lid || tri.y == lid || tri.z == lid);
+                    row = h1_face_at(P0, P1, P2, mg, oinv, h, false);
                 }
             }
             if (row) {
                 ++rows;
                 f3 n;
                 float d;
-                if (narrow_one(oxc, oxp, ld(A.x, tvo + tri.x), ld(A.x, tvo + tri.y), ld(A.x, tvo + tri.z), A.band, n,
-                               d)) {
+                if (narrow_one(oxc, oxp, P0, P1, P2, A.band, n, d)) {
                     hit = true;
                     c = VContact{t, f, n.x, n.y, n.z, d};
                 }
@@ -609,8 +619,9 @@ void launch_fused_t(const StepArgs& A, dim3 g, dim3 b, cudaStream_t st, int minB
     }
 }
 
-void launch_fused(const StepArgs& A, u32 nV, cudaStream_t st, int minBlocks) {
-    const dim3 g(ceil_div(nV, 128)), b(128);
+void launch_fused(const StepArgs& A, cudaStream_t st, int minBlocks) {
+    if (A.nthreads == 0) return;
+    const dim3 g(ceil_div(A.nthreads, 128)), b(128);
     if (A.analytic) launch_fused_t<true>(A, g, b, st, minBlocks);
     else launch_fused_t<false>(A, g, b, st, minBlocks);
 }
@@ -756,6 +767,82 @@ __global__ void k_unpack4(const float4* __restrict__ in, float* __restrict__ out
     if (i < n) { float4 q = in[i]; out[3 * i] = q.x; out[3 * i + 1] = q.y; out[3 * i + 2] = q.z; }
 }
 
+// Face positions of one mesh (the layout of RefitJob::fpos) from x.
+__global__ void k_face_pos(const float4* __restrict__ x, u32 voff, const u32* __restrict__ F3, u32 n,
+                           float4* __restrict__ fpos) {
+    const u32 f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= n) return;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const u32 v = F3[3 * f + k];
+        const float4 p = x[voff + v];
+        fpos[3 * (size_t)f + k] = make_float4(p.x, p.y, p.z, __uint_as_float(v));
+    }
+}
+
+// ------------------------------------------------------------------ thread order
+// The fused kernel's threads take the scene's working vertices in Morton
+// order within each mesh, so the 32 vertices of a warp are a compact patch of
+// the mesh (an 8 x 4 tile of a grid cloth instead of 32 vertices of one row):
+// their tree descents share nodes and their candidate faces, which the L1
+// then serves.  Results do not depend on the order.  Mesh boxes first (one
+// atomic per warp and mesh), then keys (active-mesh rank in the high bits,
+// the Morton code of the vertex in its mesh box, all axes scaled by the
+// largest extent, below), then a radix sort of (key, vertex).
+__global__ void k_order_box(const float4* __restrict__ x, const u32* __restrict__ vobj,
+                            const u32* __restrict__ aoff, u32 nV, u32* __restrict__ mbox) {
+    const u32 g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= nV) return;
+    const u32 m = vobj[g];
+    if (aoff[m] == NO_PAIR) return;
+    const f3 p = ld(x, g);
+    const unsigned act = __activemask();
+    const unsigned peers = __match_any_sync(act, m);
+    const u32 v[6] = {ford(p.x), ford(p.y), ford(p.z), ford(p.x), ford(p.y), ford(p.z)};
+    u32 r[6];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        r[k] = __reduce_min_sync(peers, v[k]);
+        r[3 + k] = __reduce_max_sync(peers, v[3 + k]);
+    }
+    if ((threadIdx.x & 31) == (unsigned)(__ffs(peers) - 1)) {
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            atomicMin(&mbox[6 * m + k], r[k]);
+            atomicMax(&mbox[6 * m + 3 + k], r[3 + k]);
+        }
+    }
+}
+
+__global__ void k_order_keys(const float4* __restrict__ x, const u32* __restrict__ vobj,
+                             const u32* __restrict__ aoff, const u32* __restrict__ arank,
+                             const MeshDev* __restrict__ meshes, const u32* __restrict__ mbox, u32 nV, u32 kbits,
+                             u32* __restrict__ keys, u32* __restrict__ vals) {
+    const u32 g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= nV) return;
+    const u32 m = vobj[g];
+    if (aoff[m] == NO_PAIR) return;
+    const f3 p = ld(x, g);
+    const float lo[3] = {funord(mbox[6 * m]), funord(mbox[6 * m + 1]), funord(mbox[6 * m + 2])};
+    const float c[3] = {p.x, p.y, p.z};
+    float w = 0.f;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) w = fmaxf(w, funord(mbox[6 * m + 3 + a]) - lo[a]);
+    u32 q[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        const float t = w > 0.f ? (c[a] - lo[a]) / w : 0.f;
+        const int v = (int)(t * 1024.f);  // NaN converts to 0
+        q[a] = (u32)min(max(v, 0), 1023);
+    }
+    u32 code = (expand_bits(q[0]) << 2) | (expand_bits(q[1]) << 1) | expand_bits(q[2]);  // 30 bits
+    if (kbits < 30) code >>= (30 - kbits);
+    const u32 rank = arank[m];
+    const u32 i = aoff[m] + (g - meshes[m].voff);
+    keys[i] = (kbits >= 32 ? 0u : (rank << kbits)) | code;
+    vals[i] = g;
+}
+
 // ------------------------------------------------------------------ host
 struct HostMesh {
     ys_mesh_desc d;
@@ -878,6 +965,7 @@ struct ys_scene {
     DBuf<float> spr_rest, scratch3;
     DBuf<uint4> F4;
     DBuf<u32> F3;  // packed facets (3 per face) for the refit kernel
+    DBuf<float4> fpos;  // per face: its three vertex positions (id in w), for the fused kernel's tests
     DBuf<Node> nodes;
     DBuf<i32> parent, claims;        // largest claimant per node; claimant lists (offset node_off)
     DBuf<u32> claimOff;              // per mesh 2N entries at node_off + mesh index
@@ -929,6 +1017,12 @@ struct ys_scene {
     bool use_graphs = true;
     cudaGraphExec_t graphs[18] = {};
     int fused_min_blocks = 8;        // k_fused register cap (ys_scene_set_fused_variant / ys_scene_autotune)
+    // fused-kernel thread order (ys_scene_set_thread_order): working vertices
+    // in Morton order per mesh, recomputed at every tree rebuild
+    bool use_order = true;
+    u32 nact = 0, order_kbits = 0;   // working vertices; Morton bits below the mesh rank
+    DBuf<u32> vorder, okeys, oaoff, orank, obox;
+    DBuf<char> oscratch;
     int tree_layout = YS_TREE_CUBE;  // Morton normalisation of the scene trees
     int tree_builder = YS_BUILD_KARRAS;
     DBuf<char> aggScratch;           // Apetrei range ends and root slot
@@ -970,6 +1064,7 @@ StepArgs make_args(ys_scene* s) {
     A.meshes = s->dmeshes.p;
     A.targets = s->targets.p;
     A.F = s->F4.p;
+    A.fpos = s->fpos.p;
     A.nodes = s->nodes.p;
     A.w4 = s->w4.p;
     A.wide = s->tree_layout == YS_TREE_CUBE ? 1u : 0u;
@@ -997,6 +1092,8 @@ StepArgs make_args(ys_scene* s) {
     A.margin = s->P.margin;
     A.band = s->P.radius + s->P.margin;
     A.nV = s->nV;
+    A.vorder = s->use_order ? s->vorder.p : nullptr;
+    A.nthreads = s->use_order ? s->nact : s->nV;
     A.self_mode = s->P.self_mode;
     A.record = s->record ? 1u : 0u;
     A.cap = s->cap;
@@ -1053,6 +1150,8 @@ ys_status build_tree(ys_scene* s, HostMesh& H) {
         YS_CK(launch_wide_build(s->nodes.p + H.node_off, s->parent.p + H.node_off, n, s->w4.p + H.w4_off,
                                 s->leafW.p + H.foff, s->leafWf.p + H.foff, s->warrive.p + H.w4_off,
                                 s->wcount.p + (&H - s->meshes.data()), s->wideScratch.p, st));
+    k_face_pos<<<ceil_div(n, 256), 256, 0, st>>>(s->X[s->cur].p, H.voff, s->F3.p + 3 * (size_t)H.foff, n,
+                                                  s->fpos.p + 3 * (size_t)H.foff);
     RefitJob J;
     memset(&J, 0, sizeof(J));
     J.nodes = s->nodes.p + H.node_off;
@@ -1205,6 +1304,25 @@ ys_status refresh_shapes(ys_scene* s) {
     return YS_OK;
 }
 
+// Fused-kernel thread order from the current positions (see k_order_keys).
+ys_status compute_order(ys_scene* s) {
+    if (s->nact == 0) return YS_OK;
+    cudaStream_t st = s->stream;
+    const size_t nm = s->meshes.size();
+    std::vector<u32> init(6 * nm);
+    for (size_t m = 0; m < nm; ++m)
+        for (int k = 0; k < 6; ++k) init[6 * m + k] = k < 3 ? 0xFFFFFFFFu : 0u;
+    YS_CK(cudaMemcpyAsync(s->obox.p, init.data(), 4 * init.size(), cudaMemcpyHostToDevice, st));
+    k_order_box<<<ceil_div(s->nV, 256), 256, 0, st>>>(s->X[s->cur].p, s->vobj.p, s->oaoff.p, s->nV, s->obox.p);
+    k_order_keys<<<ceil_div(s->nV, 256), 256, 0, st>>>(s->X[s->cur].p, s->vobj.p, s->oaoff.p, s->orank.p,
+                                                       s->dmeshes.p, s->obox.p, s->nV, s->order_kbits, s->okeys.p,
+                                                       s->vorder.p);
+    YS_CK(cudaGetLastError());
+    YS_CK(radix_sort_pairs(s->okeys.p, s->vorder.p, s->nact, s->oscratch.p, 0, 32, st));
+    YS_CK(cudaStreamSynchronize(st));  // init lives on the host stack
+    return YS_OK;
+}
+
 ys_status preamble(ys_scene* s) {
     if (s->cursor != 0) return YS_OK;
     {
@@ -1223,6 +1341,7 @@ ys_status preamble(ys_scene* s) {
         if (rebuilt) {
             ys_status r = build_levels(s);
             if (r) return r;
+            if (s->use_order && (r = compute_order(s))) return r;
         }
     }
     // environment forces (ext = g * m) are evaluated inside the force kernels
@@ -1333,7 +1452,7 @@ ys_status enqueue_fused(ys_scene* s) {
     if (r) return r;
     YS_CK(cudaMemsetAsync(s->counters.p, 0, s->record ? 24 : 16, s->stream));
     StepArgs A = make_args(s);
-    launch_fused(A, s->nV, s->stream, s->fused_min_blocks);
+    launch_fused(A, s->stream, s->fused_min_blocks);
     YS_CK(cudaGetLastError());
     return YS_OK;
 }
@@ -1390,7 +1509,7 @@ ys_status fused_substep(ys_scene* s) {
         s->evFused.push_back(s->evUsed);
         YS_CK(cudaEventRecord(next_event(s), s->stream));
     }
-    launch_fused(A, s->nV, s->stream, s->fused_min_blocks);
+    launch_fused(A, s->stream, s->fused_min_blocks);
     YS_CK(cudaGetLastError());
     if (s->timing) YS_CK(cudaEventRecord(next_event(s), s->stream));
     s->snapshot_pending = true;
@@ -1439,6 +1558,7 @@ ys_status ys_scene_destroy(ys_scene* s) {
     s->scanScratch.free(); s->rows.free(); s->contacts.free(); s->csr.free(); s->pool.free(); s->bucket.free();
     drop_graphs(s);
     s->csr_off.free(); s->vstart.free(); s->vcount.free(); s->ext.free();
+    s->fpos.free(); s->vorder.free(); s->okeys.free(); s->oaoff.free(); s->orank.free(); s->obox.free(); s->oscratch.free();
     for (auto e : s->evPool) cudaEventDestroy(e);
     cudaStreamDestroy(s->stream);
     delete s;
@@ -1578,6 +1698,7 @@ ys_status ys_scene_pack(ys_scene* s) {
     YS_CK(s->maxext.alloc(s->meshes.size())); YS_CK(s->status.alloc(1)); YS_CK(s->box.alloc(8));
     YS_CK(s->codes.alloc(std::max(nF, 1u))); YS_CK(s->idx.alloc(std::max(nF, 1u))); YS_CK(s->visits.alloc(std::max(nF, 1u)));
     YS_CK(s->F4.alloc(std::max(nF, 1u))); YS_CK(s->F3.alloc(3 * (size_t)std::max(nF, 1u)));
+    YS_CK(s->fpos.alloc(3 * (size_t)std::max(nF, 1u)));
     YS_CK(s->nodes.alloc(std::max(nNodes, 1u))); YS_CK(s->parent.alloc(std::max(nNodes, 1u)));
     YS_CK(s->claims.alloc(std::max(nNodes, 1u)));
     YS_CK(s->claimOff.alloc((size_t)nNodes + s->meshes.size() + 1));
@@ -1739,6 +1860,7 @@ ys_status ys_scene_pack(ys_scene* s) {
             J.wcount = s->wcount.p + m;
             J.hacc = s->hacc.p + H.w4_off;
         }
+        if (!J.rootOnly) J.fpos = s->fpos.p + 3 * (size_t)H.foff;  // faces the fused kernel tests
         s->hjobs.push_back(J);
         leaves += J.n;
     }
@@ -1783,6 +1905,34 @@ ys_status ys_scene_pack(ys_scene* s) {
     }
     {
         ys_status r = build_levels(s);
+        if (r) return r;
+    }
+    {
+        // working vertices of the fused kernel: cloth, moving, or querying
+        std::vector<u32> aoff(s->meshes.size(), NO_PAIR), rank(s->meshes.size(), 0);
+        u32 na = 0, nmesh = 0;
+        for (size_t m = 0; m < s->meshes.size(); ++m) {
+            const u32 f = s->meshes[m].flags;
+            if (!(f & MF_CLOTH) && (f & MF_STATIC) && !(f & MF_QUERY)) continue;
+            if (s->meshes[m].d.num_vertices == 0) continue;
+            aoff[m] = na;
+            rank[m] = nmesh++;
+            na += s->meshes[m].d.num_vertices;
+        }
+        u32 mbits = 0;
+        while (mbits < 32 && (1ull << mbits) < nmesh) ++mbits;
+        s->nact = na;
+        s->order_kbits = 32 - mbits;
+        YS_CK(s->oaoff.alloc(aoff.size()));
+        YS_CK(s->orank.alloc(rank.size()));
+        YS_CK(s->obox.alloc(6 * aoff.size()));
+        YS_CK(s->vorder.alloc(std::max(na, 1u)));
+        YS_CK(s->okeys.alloc(std::max(na, 1u)));
+        YS_CK(s->oscratch.alloc(sort_scratch_bytes(std::max(na, 1u))));
+        YS_CK(cudaMemcpyAsync(s->oaoff.p, aoff.data(), 4 * aoff.size(), cudaMemcpyHostToDevice, st));
+        YS_CK(cudaMemcpyAsync(s->orank.p, rank.data(), 4 * rank.size(), cudaMemcpyHostToDevice, st));
+        YS_CK(cudaStreamSynchronize(st));
+        ys_status r = compute_order(s);
         if (r) return r;
     }
     YS_CK(cudaStreamSynchronize(st));
@@ -1879,6 +2029,16 @@ ys_status ys_scene_set_fused_variant(ys_scene* s, int min_blocks) {
     return YS_OK;
 }
 
+ys_status ys_scene_set_thread_order(ys_scene* s, int on) {
+    if (!s) return fail(YS_ERR_BAD_ARG, "null scene");
+    const bool want = on != 0;
+    if (want == s->use_order) return YS_OK;
+    s->use_order = want;
+    drop_graphs(s);
+    if (want && s->packed) return compute_order(s);
+    return YS_OK;
+}
+
 // Time every k_fused variant on the current state (the kernel only writes the
 // next-state buffers, which the next substep overwrites; the running totals
 // are restored) and keep the fastest.  The scene does not advance.
@@ -1902,11 +2062,11 @@ ys_status ys_scene_autotune(ys_scene* s, uint32_t reps, int* chosen, float* ms_o
     int bestV = s->fused_min_blocks;
     for (int i = 0; i < 3; ++i) {
         const int v = FUSED_VARIANTS[i];
-        launch_fused(A, s->nV, st, v);  // warm-up
+        launch_fused(A, st, v);  // warm-up
         float t = 0.f;
         for (u32 k = 0; k < reps; ++k) {
             cudaEventRecord(e0, st);
-            launch_fused(A, s->nV, st, v);
+            launch_fused(A, st, v);
             cudaEventRecord(e1, st);
             cudaEventSynchronize(e1);
             float ms = 0.f;

@@ -131,6 +131,11 @@ class Scene:
     def set_fused_variant(self, min_blocks: int):
         _lib.check(self.lib.ys_scene_set_fused_variant(self.h, min_blocks), "ys_scene_set_fused_variant")
 
+    def set_thread_order(self, on: bool):
+        """Fused-kernel threads over the working vertices in per-mesh Morton
+        order (True, default) or in vertex order (False); same results."""
+        _lib.check(self.lib.ys_scene_set_thread_order(self.h, 1 if on else 0), "ys_scene_set_thread_order")
+
     def pack(self):
         _lib.check(self.lib.ys_scene_pack(self.h), "ys_scene_pack")
 
