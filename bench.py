@@ -706,7 +706,8 @@ def measure_adjoint(args, local, steps=200, every=20, reps=4):
     Lt = torch.tensor(L, device=dev, requires_grad=True)
     vt = torch.zeros((c.nV, 3), device=dev, requires_grad=True)
     rng = np.random.default_rng(5)
-    kstar = torch.tensor((k * np.exp(rng.normal(0.0, 0.3, k.shape))).astype(np.float32), device=dev)
+    kstar_np = (k * np.exp(rng.normal(0.0, 0.3, k.shape))).astype(np.float32)
+    kstar = torch.tensor(kstar_np, device=dev)
     with torch.no_grad():
         target = roll(kstar, Lt, vt).clone()
     fw, bw = [], []
@@ -724,6 +725,7 @@ def measure_adjoint(args, local, steps=200, every=20, reps=4):
         if it:
             fw.append(a.elapsed_time(b))
             bw.append(b.elapsed_time(d))
+    g32 = [t.grad.double().cpu().numpy() for t in (kt, Lt, vt)]
     roll.close()
     s = Scene(spec, device=local)
     st = torch.cuda.ExternalStream(s.stream(), device=local)
@@ -740,12 +742,62 @@ def measure_adjoint(args, local, steps=200, every=20, reps=4):
     f = float(np.median(fw)) / steps
     g = float(np.median(bw)) / steps
     f64 = measure_adjoint_fp64(spec, k, L, target, local, steps, every, reps)
+    g64 = f64.pop("_grads")
+    full = {n_: float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+            for n_, a, b in zip(("k", "L", "v0"), g32, g64)}
+    prefix = fp32_vs_fp64_prefix(spec, k, L, kstar_np, local, every)
     return {"workload": "FastGridCloth 128x128 over a level-4 icosphere, 200 steps, checkpoint every 20",
             "forward_ms_per_step": f, "backward_ms_per_step": g, "backward_over_forward": g / f,
             "plain_forward_ms_per_step": plain, "unit": "ms/step",
             "gradients": "w.r.t. per-spring k, L and v0; checked against FP64 finite differences and an FP64 "
                          "reference adjoint in the GPU tests",
+            "fp32_vs_fp64": {"full_200_steps": full, "branch_stable_prefix": prefix,
+                             "measure": "norm-relative difference per parameter group between the FP32 adjoint "
+                                        "and the 64-bit mode on the same loss; over the full rollout the two "
+                                        "forwards take different branches at contact pushes (a pushed vertex is "
+                                        "re-tested exactly at the thickness), so only the prefix before the first "
+                                        "push compares derivatives of one function"},
             "fp64": f64}
+
+
+def fp32_vs_fp64_prefix(spec, k, L, kstar, local, every):
+    """FP32 adjoint against the 64-bit mode on the C5 problem's steps before
+    its first contact push (found from the recorded contacts of the FP32
+    forward: a contact with d below the thickness), MSE loss against the
+    perturbed-stiffness rollout at the same step."""
+    import torch
+    from ysim_b200.adjoint import ClothRollout
+    from ysim_b200.scene import Scene
+    c = spec.meshes[0]
+    s = Scene(spec, device=local)
+    s.set_record(True)
+    T = None
+    for t in range(1, 201):
+        s.step(1)
+        off, cc = s.contacts()
+        if (cc["d"][: int(off[c.nV])] < c.thickness).any():
+            T = t - 1
+            break
+    s.close()
+    if not T:
+        return None
+    dev = torch.device("cuda", local)
+    roll = ClothRollout(spec, steps=T, checkpoint_every=every, device=local)
+    with torch.no_grad():
+        target = roll(torch.tensor(kstar, device=dev), torch.tensor(L, device=dev),
+                      torch.zeros((c.nV, 3), device=dev)).double()
+    roll.close()
+    out = {}
+    for prec, dt in ((32, torch.float32), (64, torch.float64)):
+        roll = ClothRollout(spec, steps=T, checkpoint_every=every, device=local, precision=prec)
+        p = [torch.tensor(np.asarray(a), dtype=dt, device=dev, requires_grad=True)
+             for a in (k, L, np.zeros((c.nV, 3), np.float32))]
+        ((roll(*p) - target.to(dt)) ** 2).sum(1).mean().backward()
+        out[prec] = [t.grad.double().cpu().numpy() for t in p]
+        roll.close()
+    rel = {n_: float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+           for n_, a, b in zip(("k", "L", "v0"), out[32], out[64])}
+    return {"steps": T, **rel}
 
 
 def measure_adjoint_fp64(spec, k, L, target, local, steps, every, reps, window=40):
@@ -784,6 +836,7 @@ def measure_adjoint_fp64(spec, k, L, target, local, steps, every, reps, window=4
         if it:
             fw.append(a.elapsed_time(b) / steps)
             bw.append(b.elapsed_time(d) / steps)
+    g64 = [t.grad.double().cpu().numpy() for t in (kt, Lt, vt)]
     roll.close()
     # finite-difference check on the branch-stable window
     rng = np.random.default_rng(11)
@@ -814,7 +867,8 @@ def measure_adjoint_fp64(spec, k, L, target, local, steps, every, reps, window=4
     return {"forward_ms_per_step": f, "backward_ms_per_step": b, "backward_over_forward": b / f,
             "fd_check": {"window_steps": window, "components": n, "worst_rel_err": worst,
                          "loss": "sum(w x_T), random v0"},
-            "arithmetic": "binary64 throughout; bit-identical to the FP64 reference rollout in the GPU tests"}
+            "arithmetic": "binary64 throughout; bit-identical to the FP64 reference rollout in the GPU tests",
+            "_grads": g64}
 
 
 def run_batched(args, rank, world, local):

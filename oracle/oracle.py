@@ -70,6 +70,8 @@ def lib():
             "yso_scene_tree": (None, [vp, C.c_int, vp, vp, vp, vp]),
             "yso_scene_set_collider": (C.c_int, [vp, C.c_int, C.c_uint32, vp, vp, vp]),
             "yso_scene_shapes": (C.c_uint64, [vp, vp]),
+            "yso_scene_set_wind": (None, [vp, vp]),
+            "yso_scene_set_mesh_env": (C.c_int, [vp, C.c_int, C.c_int, C.c_int]),
             "yso_analytic_one": (C.c_int, [vp, vp, vp, C.c_float, C.c_float, C.c_float, vp, vp]),
             "yso_rot_margin": (C.c_float, [vp, C.c_float, C.c_float]),
             "yso_broad_box": (C.c_int, [vp, C.c_float, vp]),
@@ -300,6 +302,15 @@ class OracleScene:
         r = np.array(q, np.float32)
         if lib().yso_scene_set_collider(self.h, mesh, kind, P(c), P(h), P(r)) != 0:
             raise ValueError("yso_scene_set_collider rejected the collider")
+
+    def set_environment(self, wind, gates):
+        """applyEnvironmentForces inputs: the wind vector and, per mesh, its
+        (apply_gravity, apply_wind) gates; they act from the next frame
+        start."""
+        lib().yso_scene_set_wind(self.h, P(np.asarray(wind, np.float32)))
+        for m, (g, w) in enumerate(gates):
+            if lib().yso_scene_set_mesh_env(self.h, m, int(bool(g)), int(bool(w))) != 0:
+                raise ValueError("yso_scene_set_mesh_env rejected the mesh")
 
     def shapes(self):
         n = lib().yso_scene_shapes(self.h, None)

@@ -985,6 +985,8 @@ struct Mesh {
     // orientation w, x, y, z)
     u32 collider = CMesh;
     float pose[10] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 1.f, 0.f, 0.f, 0.f};
+    // GeneralMesh::applyGravity / applyWind (the per-object environment gates)
+    bool gravity_on = true, wind_on = false;
     bool cloth() const { return behavior == TriangularCloth || behavior == FastGridCloth; }
 };
 
@@ -1016,6 +1018,7 @@ struct Scene {
     bool primed = false;
     std::vector<std::pair<u32, u32>> mk_fresh, mk_held, mk_pairs;
     int builder = 0;  // 0 Karras (buildTree_Tri + bottomUpBoxes), 1 Apetrei (agglomerativeBuild_Tri)
+    float wind[3] = {0.f, 0.f, 0.f};  // Scene::environment.wind
 };
 
 // Scene::refreshAnalyticShapes (scene.hpp:659-745).
@@ -1355,14 +1358,24 @@ void system_update(Scene& S) {
     if (bad) { S.anomaly = 1; S.status |= ST_NONFINITE; }
 }
 
-// applyEnvironmentForces (simulator.hpp:3123-3166): ext = g * m for cloth.
+// applyEnvironmentForces (simulator.hpp:3123-3166): zero for Float, Rigid and
+// Kinematic meshes; otherwise g * m when the mesh's gravity gate is on (else
+// zero), plus the wind vector (a force per particle, no mass) when its wind
+// gate is on and it is cloth.
 void env_forces(Scene& S) {
-    for (auto& M : S.meshes)
+    for (auto& M : S.meshes) {
+        const bool moved = !(M.behavior == Float || M.behavior == Rigid || M.behavior == Kinematic);
+        const bool wind = M.wind_on && M.cloth();
         for (u32 i = 0; i < M.nV; ++i) {
             u32 g = M.voff + i;
-            V3 e = M.cloth() ? v3(S.P.gx * M.mass[i], S.P.gy * M.mass[i], S.P.gz * M.mass[i]) : v3(0.f, 0.f, 0.f);
+            V3 e = v3(0.f, 0.f, 0.f);
+            if (moved) {
+                if (M.gravity_on) e = v3(S.P.gx * M.mass[i], S.P.gy * M.mass[i], S.P.gz * M.mass[i]);
+                if (wind) e = v3(e.x + S.wind[0], e.y + S.wind[1], e.z + S.wind[2]);
+            }
             st3(S.ext.data(), g, e);
         }
+    }
 }
 
 // One substep of Simulator::update (simulator.hpp:3512-3815), frame preamble
@@ -1607,6 +1620,19 @@ int yso_scene_set_collider(void* h, int mesh, u32 kind, const float* c, const fl
     M.collider = kind;
     for (int i = 0; i < 3; ++i) { M.pose[i] = c[i]; M.pose[3 + i] = hx ? hx[i] : 0.f; }
     for (int i = 0; i < 4; ++i) M.pose[6 + i] = q[i];
+    return 0;
+}
+// Environment of the scene (wind) and the gravity / wind gates of a mesh;
+// they act from the next frame start.  Returns 0 on success.
+void yso_scene_set_wind(void* h, const float* wind) {
+    Scene* S = (Scene*)h;
+    for (int k = 0; k < 3; ++k) S->wind[k] = wind[k];
+}
+int yso_scene_set_mesh_env(void* h, int mesh, int gravity_on, int wind_on) {
+    Scene* S = (Scene*)h;
+    if (mesh < 0 || (size_t)mesh >= S->meshes.size()) return -1;
+    S->meshes[mesh].gravity_on = gravity_on != 0;
+    S->meshes[mesh].wind_on = wind_on != 0;
     return 0;
 }
 uint64_t yso_scene_shapes(void* h, void* out) {

@@ -188,3 +188,34 @@ def test_loader_forces_imports_and_errors(tmp_path):
     j["objects"][0]["behavior"]["params"]["particle_num_1d"] = 20
     with pytest.raises(SF.SceneFormatError, match="particle_num_1d"):
         L.load(SF.run_config_from_json(j))
+
+
+@pytest.mark.parametrize("gravity,wind", [(True, True), (False, True), (True, False), (False, False)])
+def test_loader_environment_forces_equal_the_oracle(oracle, gravity, wind):
+    """The loader's external-force buffer (applyEnvironmentForces,
+    simulator.hpp:3123-3166) equals the oracle's own restatement for every
+    combination of the cloth's gravity and wind gates, with wind on the Float
+    meshes' gates too (they get zero)."""
+    import numpy as np
+    from ysim_b200 import loader as L
+    from ysim_b200 import scene_format as SF
+    path = os.path.join(GOLD, "scenes", "drape.json")
+    cfg = SF.read_run_config(path)
+    snap = cfg.scene
+    snap.environment.wind = (0.4, 0.0, -0.25)
+    snap.objects[0].apply_gravity = gravity
+    snap.objects[0].apply_wind = wind
+    ls = L.load(cfg, path)
+    o = oracle.OracleScene(ls.spec)
+    o.set_environment(snap.environment.wind, [(ob.apply_gravity, ob.apply_wind) for ob in snap.objects])
+    o.step(1)
+    want = o.get("ext")
+    got = np.ascontiguousarray(ls.ext, np.float32) if ls.ext is not None else None
+    if gravity and not wind:
+        assert got is None  # the kernels' own g * m
+        g = np.asarray(ls.spec.params.gravity, np.float32)
+        c = ls.spec.meshes[0]
+        assert np.array_equal(want[: c.nV], (c.mass[:, None] * g[None, :]).astype(np.float32))
+        assert not want[c.nV:].any()
+    else:
+        assert np.array_equal(got, want)
