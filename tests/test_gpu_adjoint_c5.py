@@ -84,11 +84,14 @@ def test_c5_fp64_adjoint_bit_identical_to_fp64_reference(c5, oracle):
 
 def test_c5_fp64_adjoint_within_1e4_of_finite_differences(c5):
     """Central differences of the GPU's FP64 rollout on the branch-stable
-    prefix, at the step that balances truncation against round-off per
-    group (k: 1e-3 relative, L: 1e-6, v0: 1e-5).  |g - fd| / |fd| <= 1e-4,
-    where |fd| is at least 1e-4 of the group's largest gradient and a
-    thousand times the difference's own round-off; below either floor the
-    error is taken relative to that floor."""
+    prefix, Richardson-extrapolated from steps h and h/2 (truncation error of
+    order h^4), h per group balancing truncation against round-off (k: 1e-3
+    relative, L: 1e-6, v0: 1e-5).  |g - fd| / |fd| <= 1e-4, where |fd| is at
+    least 1e-4 of the group's largest gradient and ten times the difference's
+    round-off; below either floor the error is taken relative to that floor.
+    The round-off is that of the final positions (each rollout rounds x_T to
+    binary64, and the perturbations move it by only a few thousand ulps for
+    the smallest components): 64 eps sum_i |dL/dx_i| |x_i| per step h/2."""
     import torch
     from ysim_b200.adjoint import ClothRollout
     spec, k, L, v0, _, xs, T = c5
@@ -96,8 +99,11 @@ def test_c5_fp64_adjoint_within_1e4_of_finite_differences(c5):
     roll = ClothRollout(spec, steps=T, checkpoint_every=EVERY, precision=64)
     try:
         params = [torch.tensor(np.asarray(a, np.float64), device="cuda", requires_grad=True) for a in (k, L, v0)]
-        ((roll(*params) - xs_t) ** 2).sum(1).mean().backward()
+        xT = roll(*params)
+        ((xT - xs_t) ** 2).sum(1).mean().backward()
         grads = [p.grad.cpu().numpy().reshape(-1) for p in params]
+        xT = xT.detach().cpu().numpy()
+        sens = float((np.abs(_mse_seed(xT, xs)) * np.abs(xT)).sum())  # sum_i |dL/dx_i| |x_i|
         base = [p.detach().clone().reshape(-1) for p in params]
 
         def loss(group, i, delta):
@@ -115,9 +121,10 @@ def test_c5_fp64_adjoint_within_1e4_of_finite_differences(c5):
                 i = int(i)
                 eps = 1e-3 * abs(float(base[0][i])) if group == 0 else (1e-6 if group == 1 else 1e-5)
                 lp, lm = loss(group, i, eps), loss(group, i, -eps)
-                fd = (lp - lm) / (2 * eps)
-                noise = 64 * np.finfo(np.float64).eps * (abs(lp) + abs(lm)) / (2 * eps)
-                floor = max(1e-4 * gmax, 1e3 * noise)
+                hp, hm = loss(group, i, eps / 2), loss(group, i, -eps / 2)
+                fd = (4.0 * (hp - hm) / eps - (lp - lm) / (2 * eps)) / 3.0
+                noise = 64 * np.finfo(np.float64).eps * sens / (eps / 2)
+                floor = max(1e-4 * gmax, 10 * noise)
                 err = abs(g[i] - fd) / max(abs(fd), floor)
                 assert err <= 1e-4, (group, i, g[i], fd, floor, err)
                 n += 1
@@ -133,17 +140,22 @@ def test_c5_fp64_adjoint_within_1e4_of_finite_differences(c5):
 def test_c5_fp32_adjoint_tracks_fp64_on_the_prefix(c5):
     """The FP32 adjoint differentiates the FP32 rollout; on the branch-stable
     prefix its gradients are within 1e-3 (norm-relative, per group) of the
-    64-bit mode's."""
+    64-bit mode's.  Both reverse passes take the same seed, the loss gradient
+    of the binary64 rollout (rounded to binary32 for the FP32 pass): in the
+    first steps x_T - x* is a few ulps of x_T in binary32, so a seed formed
+    from the FP32 state would be mostly its rounding."""
     import torch
     from ysim_b200.adjoint import ClothRollout
     spec, k, L, v0, _, xs, T = c5
-    out = {}
-    for prec, dt in ((32, torch.float32), (64, torch.float64)):
+    out, seed = {}, None
+    for prec, dt in ((64, torch.float64), (32, torch.float32)):
         roll = ClothRollout(spec, steps=T, checkpoint_every=EVERY, precision=prec)
         try:
             params = [torch.tensor(np.asarray(a), dtype=dt, device="cuda", requires_grad=True) for a in (k, L, v0)]
             xT = roll(*params)
-            ((xT - torch.tensor(xs, dtype=dt, device="cuda")) ** 2).sum(1).mean().backward()
+            if seed is None:
+                seed = _mse_seed(xT.detach().cpu().numpy(), xs)
+            xT.backward(torch.tensor(seed, dtype=dt, device="cuda"))
             out[prec] = [p.grad.double().cpu().numpy() for p in params]
         finally:
             roll.close()

@@ -83,6 +83,32 @@ __device__ __forceinline__ u32 wide_step(const Wide4* __restrict__ w4, int w, f3
     return st;
 }
 
+// The same step with the pushes going through push(child), which returns
+// false when the stack is full.
+template <class Push, class Leaf>
+__device__ __forceinline__ u32 wide_step_p(const Wide4* __restrict__ w4, int w, f3 qmn, f3 qmx, Push&& push,
+                                           Leaf&& leaf) {
+    const float4* p = reinterpret_cast<const float4*>(w4 + w);
+    const float4 lx = __ldg(p), ly = __ldg(p + 1), lz = __ldg(p + 2);
+    const float4 hx = __ldg(p + 3), hy = __ldg(p + 4), hz = __ldg(p + 5);
+    const int4 ch = __ldg(reinterpret_cast<const int4*>(p + 6));
+    const float LX[4] = {lx.x, lx.y, lx.z, lx.w}, LY[4] = {ly.x, ly.y, ly.z, ly.w}, LZ[4] = {lz.x, lz.y, lz.z, lz.w};
+    const float HX[4] = {hx.x, hx.y, hx.z, hx.w}, HY[4] = {hy.x, hy.y, hy.z, hy.w}, HZ[4] = {hz.x, hz.y, hz.z, hz.w};
+    const int C[4] = {ch.x, ch.y, ch.z, ch.w};
+    u32 st = 0;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const int c = C[k];
+        if (c == W4_EMPTY || !overlap_xyz(qmn, qmx, LX[k], LY[k], LZ[k], HX[k], HY[k], HZ[k])) continue;
+        if (c < 0) {
+            leaf(k, (u32)~c);
+        } else if (!push(c)) {
+            st |= ST_STACK_OVF;
+        }
+    }
+    return st;
+}
+
 // Descent of the 4-wide form of a tree (same leaves as traverse on the binary
 // form): the root box first (binary root node), then wide nodes from 0.
 template <class Fn>
@@ -277,13 +303,20 @@ __device__ __forceinline__ bool h1_face(const float4* __restrict__ X, u32 voff, 
 }
 
 // ------------------------------------------------------------- N1 narrow
-// pointInTriangleBary (bruteforce.metal:9-28).
+// pointInTriangleBary (bruteforce.metal:9-28).  b and c are quotients of
+// the numerators below by den; an IEEE quotient is >= 0 exactly when its
+// numerator is a zero or has den's sign, so a point with b < 0 or c < 0 is
+// rejected from the signs alone, before the two divisions (the same result
+// as dividing first).
 __device__ __forceinline__ bool point_in_tri(f3 p, f3 e0, f3 e1) {
     float d00 = dot(e0, e0), d01 = dot(e0, e1), d11 = dot(e1, e1), d20 = dot(p, e0), d21 = dot(p, e1);
     float den = d00 * d11 - d01 * d01;
     if (fabsf(den) < 1e-12f) return false;
-    float b = (d11 * d20 - d01 * d21) / den;
-    float c = (d00 * d21 - d01 * d20) / den;
+    const float nb = d11 * d20 - d01 * d21, nc = d00 * d21 - d01 * d20;
+    const bool dneg = den < 0.0f;
+    if ((nb != 0.0f && (nb < 0.0f) != dneg) || (nc != 0.0f && (nc < 0.0f) != dneg)) return false;
+    float b = nb / den;
+    float c = nc / den;
     float a = 1.0f - b - c;
     return (a >= 0.0f && b >= 0.0f && c >= 0.0f);
 }

@@ -347,6 +347,12 @@ __global__ void __launch_bounds__(128, MINB) k_fused(StepArgs A) {
     // ---- descent state: the own tree first (set up here), then the targets
     int stack[STACK_DEPTH];
     int sp = 0;
+    auto push = [&](int v) -> bool {
+        if (sp >= STACK_DEPTH) return false;
+        stack[sp++] = v;
+        return true;
+    };
+    auto pop = [&]() -> int { return stack[--sp]; };
     u32 visited = 0, nn = 0, key = 0;
     const Node* nodes = A.nodes;  // binary form
     const Wide4* wn = A.w4;       // wide form
@@ -366,8 +372,8 @@ __global__ void __launch_bounds__(128, MINB) k_fused(StepArgs A) {
             nodes = A.nodes + T->node_off;
             nn = 2 * T->nF - 1;
         }
-        stack[0] = 0;
-        sp = 1;
+        sp = 0;
+        push(0);
     };
     if (query && Mp->nF) {
         bool selfOK = false;
@@ -504,9 +510,9 @@ __global__ void __launch_bounds__(128, MINB) k_fused(StepArgs A) {
                     st |= ST_STACK_OVF;
                     sp = 0;
                 } else {
-                    const int w = stack[--sp];
+                    const int w = pop();
                     if (w >= 0 && (u32)w < nn)
-                        st |= wide_step(wn, w, qmn, qmx, stack, sp, [&](int s, u32 f) { lf[s] = (int)f; });
+                        st |= wide_step_p(wn, w, qmn, qmx, push, [&](int s, u32 f) { lf[s] = (int)f; });
                 }
             }
 #pragma unroll
@@ -518,7 +524,7 @@ __global__ void __launch_bounds__(128, MINB) k_fused(StepArgs A) {
                     st |= ST_STACK_OVF;
                     sp = 0;
                 } else {
-                    const int id = stack[--sp];
+                    const int id = pop();
                     if (id >= 0 && (u32)id < nn) {
                         const float4* p = reinterpret_cast<const float4*>(nodes + id);
                         const float4 n0 = __ldg(p), n1 = __ldg(p + 1);
@@ -529,8 +535,8 @@ __global__ void __launch_bounds__(128, MINB) k_fused(StepArgs A) {
                             } else if (sp + 2 > STACK_DEPTH) {
                                 st |= ST_STACK_OVF;
                             } else {
-                                stack[sp++] = a;
-                                stack[sp++] = b;
+                                push(a);
+                                push(b);
                             }
                         }
                     }
