@@ -272,6 +272,14 @@ ys_status ys_scene_contacts(ys_scene* s, uint32_t* host_offsets, void* host_cont
  * primitive indices (any pointer may be NULL). */
 ys_status ys_scene_tree(ys_scene* s, int mesh, void* nodes, int32_t* parent, uint32_t* codes, uint32_t* idx,
                         uint32_t* num_prims_out);
+/* The 4-wide form of a mesh's tree (cube layout) as the last refit left it:
+ * *count wide nodes of 128 B (boxes of the four child slots as x, y, z
+ * minima then maxima, SoA; child words, >= 0 a wide node, < 0 the
+ * complement of a face, 0x7FFFFFFF empty; child count; parent; slot in the
+ * parent), the first min(*count, cap) into out.  *count = 0 for the
+ * reference layout or a tree never built.  An inspection entry point of this
+ * layout; no counterpart in the reference. */
+ys_status ys_scene_wide_tree(ys_scene* s, int mesh, void* out, uint32_t cap, uint32_t* count);
 
 /* ---- Differentiable rollouts (adjoint of the substep) --------------------
  * Per-spring parameters of a FastGridCloth (FastGridClothBehaviorParams has

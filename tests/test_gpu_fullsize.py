@@ -98,6 +98,22 @@ def test_c2_full_size_fused_matches_oracle(c2_draped, oracle):
         s.close()
 
 
+def test_c2_full_size_wide_refit_boxes_exact(c2_draped):
+    """The cloth's 4-wide tree after a refit of the draped state: leaf slots
+    are the swept leaf boxes, internal slots the unions of their children."""
+    from test_gpu_parity import check_wide_boxes
+    from ysim_b200.scene import Scene
+    spec, *state = c2_draped
+    s = Scene(spec)
+    try:
+        for k, a in zip(("x", "v", "xprev"), state):
+            s.set(k, a)
+        s.step(3)
+        assert check_wide_boxes(s, spec) > 100_000
+    finally:
+        s.close()
+
+
 def test_c2_full_size_staged_matches_oracle(c2_draped, oracle):
     """The staged path, stage by stage (broad rows, narrow contacts, forces,
     integration), for 3 substeps from the draped state."""

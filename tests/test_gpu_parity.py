@@ -543,3 +543,51 @@ def test_spatial_hash_bucket_collision_inside_one_triangle(cuda_lib):
         assert pairs[:2].cpu().tolist() == [0, 0]
     finally:
         _lib.check(cuda_lib.ys_shash_destroy(sh))
+
+
+def check_wide_boxes(s, spec, mesh=0):
+    """After a refit of the current state: every leaf slot of the mesh's
+    4-wide tree holds its face's swept box (x and x + v subh, float32 as the
+    reference computes buildSweptLeaf_Tri), and every internal slot the union
+    of its child's slots; returns the number of wide nodes checked."""
+    s.broad_phase.refit_swept()
+    W = s.wide_tree(mesh)
+    assert len(W) > 0
+    voff = sum(m.nV for m in spec.meshes[:mesh])
+    m = spec.meshes[mesh]
+    x = s.get("x")[voff:voff + m.nV]
+    v = s.get("v")[voff:voff + m.nV]
+    dt = np.float32(spec.params.subh)
+    p = x[m.facets]
+    sp = (p + (v[m.facets] * dt).astype(np.float32)).astype(np.float32)
+    leaf_lo = np.minimum(p, sp).min(1)
+    leaf_hi = np.maximum(p, sp).max(1)
+    child = W["child"]
+    lo = W["lo"].transpose(0, 2, 1)  # (node, slot, axis)
+    hi = W["hi"].transpose(0, 2, 1)
+    leaf = (child < 0)
+    f = ~child[leaf]
+    assert np.array_equal(lo[leaf], leaf_lo[f]) and np.array_equal(hi[leaf], leaf_hi[f])
+    inner = (child >= 0) & (child != 0x7FFFFFFF)
+    c = child[inner]
+    assert np.array_equal(lo[inner], lo[c].min(1)) and np.array_equal(hi[inner], hi[c].max(1))
+    # every face is a leaf exactly once
+    assert np.array_equal(np.sort(f), np.arange(m.nF))
+    return len(W)
+
+
+def test_wide_refit_boxes_are_exact(cuda_lib):
+    """The 4-wide refit (leaf slots from the swept leaf boxes, internal slots
+    as unions over sorted-leaf ranges) gives exactly the boxes a bottom-up
+    union gives, after steps and a rebuild."""
+    from ysim_b200.scene import Scene
+    spec = _small_specs()["c2hash"]
+    s = Scene(spec)
+    try:
+        s.step(2 * spec.params.substeps + 3)
+        assert check_wide_boxes(s, spec) > 100
+        s.step(10 * spec.params.substeps)  # through the rebuild at frame 10
+        check_wide_boxes(s, spec)
+        assert s.stats()["flags"] == 0
+    finally:
+        s.close()

@@ -94,6 +94,7 @@ _PROTOS = {
     "ys_scene_set_tree_layout": (C.c_int, [C.c_void_p, C.c_int]),
     "ys_scene_set_fused_variant": (C.c_int, [C.c_void_p, C.c_int]),
     "ys_scene_set_thread_order": (C.c_int, [C.c_void_p, C.c_int]),
+    "ys_scene_wide_tree": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_uint32, C.c_void_p]),
     "ys_scene_set_tree_builder": (C.c_int, [C.c_void_p, C.c_int]),
     "ys_lbvh_set_builder": (C.c_int, [C.c_void_p, C.c_int]),
     "ys_scene_set_collider": (C.c_int, [C.c_void_p, C.c_int, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p]),

@@ -466,6 +466,277 @@ __device__ __forceinline__ u32 job_of(const RefitJob* __restrict__ jobs, u32 num
     return lo;
 }
 
+// Range mode, leaf pass: the boxes of this block's 16-leaf groups and of the
+// whole block (256 consecutive sorted leaves i0 .. i0 + 255 of job J, i the
+// thread's leaf), and the slot boxes of the wide nodes whose range lies in
+// the block, from the leaf boxes in shared memory.  Every thread of the block
+// calls this.  Min and max of a set do not depend on the order they are taken
+// in, so the unions below equal the bottom-up ones.
+__device__ __forceinline__ void range_block_boxes(const RefitJob& J, u32 i, bool has, f3 lo, f3 hi) {
+    __shared__ float sh_box[8][6];
+    __shared__ float sh_leaf[6][256];
+    __shared__ float sh_g16[6][16];  // boxes of the block's 16-leaf groups
+    const float inf = __int_as_float(0x7F800000);
+    float v[6] = {has ? lo.x : inf, has ? lo.y : inf, has ? lo.z : inf,
+                  has ? hi.x : -inf, has ? hi.y : -inf, has ? hi.z : -inf};
+#pragma unroll
+    for (int k = 0; k < 6; ++k) sh_leaf[k][threadIdx.x] = v[k];
+    const u32 lane = threadIdx.x & 31u;
+#pragma unroll
+    for (int off = 8; off >= 1; off >>= 1) {
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            v[k] = fminf(v[k], __shfl_xor_sync(0xFFFFFFFFu, v[k], off));
+            v[3 + k] = fmaxf(v[3 + k], __shfl_xor_sync(0xFFFFFFFFu, v[3 + k], off));
+        }
+    }
+    if ((lane & 15u) == 0) {
+        store_box(J.bb16 + ((J.leafBase + i) >> 4), mk(v[0], v[1], v[2]), mk(v[3], v[4], v[5]));
+#pragma unroll
+        for (int k = 0; k < 6; ++k) sh_g16[k][threadIdx.x >> 4] = v[k];
+    }
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        v[k] = fminf(v[k], __shfl_xor_sync(0xFFFFFFFFu, v[k], 16));
+        v[3 + k] = fmaxf(v[3 + k], __shfl_xor_sync(0xFFFFFFFFu, v[3 + k], 16));
+    }
+    if (lane == 0)
+        for (int k = 0; k < 6; ++k) sh_box[threadIdx.x >> 5][k] = v[k];
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (u32 w = 1; w < (blockDim.x >> 5); ++w)
+            for (int k = 0; k < 3; ++k) {
+                v[k] = fminf(v[k], sh_box[w][k]);
+                v[3 + k] = fmaxf(v[3 + k], sh_box[w][3 + k]);
+            }
+        store_box(J.bb256 + ((J.leafBase + i) >> 8), mk(v[0], v[1], v[2]), mk(v[3], v[4], v[5]));
+    }
+    // the wide nodes inside this block: their parents' slots
+    const u32 gb = (J.leafBase + i) >> 8, i0 = i & ~255u;
+    const u32 eb = J.blkOff[gb], ee = J.blkOff[gb + 1];
+    for (u32 q = eb + threadIdx.x; q < ee; q += blockDim.x) {
+        const uint4 r = J.blkEnt[q];  // (parent, slot, first, last)
+        if (r.z < i0 || r.w > i0 + 255u || r.z > r.w || r.y > 3u) continue;
+        float b[6] = {inf, inf, inf, -inf, -inf, -inf};
+        // single leaves up to a 16-leaf boundary, whole groups, single leaves
+        const u32 L = r.z - i0, e = r.w - i0 + 1;
+        u32 s16 = (L + 15u) & ~15u, e16 = e & ~15u;
+        if (s16 >= e16) { s16 = e; e16 = e; }
+        auto take = [&](const float (*src)[256], u32 l) {
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                b[k] = fminf(b[k], src[k][l]);
+                b[3 + k] = fmaxf(b[3 + k], src[3 + k][l]);
+            }
+        };
+        for (u32 l = L; l < s16; ++l) take(sh_leaf, l);
+        for (u32 gq = s16 >> 4; gq < (e16 >> 4); ++gq) {
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                b[k] = fminf(b[k], sh_g16[k][gq]);
+                b[3 + k] = fmaxf(b[3 + k], sh_g16[3 + k][gq]);
+            }
+        }
+        for (u32 l = e16; l < e; ++l) take(sh_leaf, l);
+        Wide4* W = J.w4 + r.x;
+        W->lox[r.y] = b[0]; W->loy[r.y] = b[1]; W->loz[r.y] = b[2];
+        W->hix[r.y] = b[3]; W->hiy[r.y] = b[4]; W->hiz[r.y] = b[5];
+    }
+}
+
+__device__ __forceinline__ void box_union(f3& lo, f3& hi, const Node* nd) {
+    const float4* p = reinterpret_cast<const float4*>(nd);
+    const float4 a = __ldcg(p), b = __ldcg(p + 1);
+    lo = mk(fminf(lo.x, a.x), fminf(lo.y, a.y), fminf(lo.z, a.z));
+    hi = mk(fmaxf(hi.x, b.x), fmaxf(hi.y, b.y), fmaxf(hi.z, b.z));
+}
+
+// Union of the leaf boxes of sorted leaves [L, R] of job J by a group of G
+// threads (thread g of the group, g < G), reduced over groups of RED lanes
+// (RED divides 32, groups aligned; RED = G up to a warp): the range
+// splits into single leaves up to a 16-leaf boundary, 16-leaf blocks up to a
+// 256-leaf boundary, 256-leaf blocks, then 16-leaf blocks and single leaves
+// again; the lanes take those pieces in turn (four loads in flight per lane)
+// and the group reduces.  Every lane of the group gets the union.
+template <int G, int RED = G>
+__device__ __forceinline__ void range_union_group(const RefitJob& J, u32 L, u32 R, u32 g, f3& lo, f3& hi) {
+    const float inf = __int_as_float(0x7F800000);
+    const Node* leaves = J.nodes + (J.n - 1);
+    const u32 b = J.leafBase;  // a multiple of 256
+    const u32 e = R + 1;
+    u32 s16 = (L + 15u) & ~15u, e16 = e & ~15u;
+    if (s16 >= e16) { s16 = e; e16 = e; }
+    u32 s256 = (s16 + 255u) & ~255u, e256 = e16 & ~255u;
+    if (s256 >= e256) { s256 = e16; e256 = e16; }
+    const u32 n0 = s16 - L, n1 = (s256 - s16) >> 4, n2 = (e256 - s256) >> 8, n3 = (e16 - e256) >> 4;
+    const u32 total = n0 + n1 + n2 + n3 + (e - e16);
+    auto piece = [&](u32 r) -> const Node* {
+        if (r < n0) return leaves + L + r;
+        if ((r -= n0) < n1) return J.bb16 + ((b + s16) >> 4) + r;
+        if ((r -= n1) < n2) return J.bb256 + ((b + s256) >> 8) + r;
+        if ((r -= n2) < n3) return J.bb16 + ((b + e256) >> 4) + r;
+        return leaves + e16 + (r - n3);
+    };
+    float v[6] = {inf, inf, inf, -inf, -inf, -inf};
+    u32 q = g;
+    for (; q + 3 * G < total; q += 4 * G) {
+        float4 a[4], c[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const float4* p = reinterpret_cast<const float4*>(piece(q + u * G));
+            a[u] = __ldcg(p);
+            c[u] = __ldcg(p + 1);
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            v[0] = fminf(v[0], a[u].x); v[1] = fminf(v[1], a[u].y); v[2] = fminf(v[2], a[u].z);
+            v[3] = fmaxf(v[3], c[u].x); v[4] = fmaxf(v[4], c[u].y); v[5] = fmaxf(v[5], c[u].z);
+        }
+    }
+    for (; q < total; q += G) {
+        const float4* p = reinterpret_cast<const float4*>(piece(q));
+        const float4 a = __ldcg(p), c = __ldcg(p + 1);
+        v[0] = fminf(v[0], a.x); v[1] = fminf(v[1], a.y); v[2] = fminf(v[2], a.z);
+        v[3] = fmaxf(v[3], c.x); v[4] = fmaxf(v[4], c.y); v[5] = fmaxf(v[5], c.z);
+    }
+#pragma unroll
+    for (int off = RED / 2; off >= 1; off >>= 1) {
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            v[k] = fminf(v[k], __shfl_xor_sync(0xFFFFFFFFu, v[k], off));
+            v[3 + k] = fmaxf(v[3 + k], __shfl_xor_sync(0xFFFFFFFFu, v[3 + k], off));
+        }
+    }
+    lo = mk(v[0], v[1], v[2]);
+    hi = mk(v[3], v[4], v[5]);
+}
+
+// Union of the leaf boxes of sorted leaves [L, R] of job J by a whole block
+// (every thread calls this; each gets the union).
+__device__ __forceinline__ void range_union_block(const RefitJob& J, u32 L, u32 R, f3& lo, f3& hi) {
+    __shared__ float sh_red[8][6];
+    range_union_group<256, 32>(J, L, R, threadIdx.x, lo, hi);  // pieces over the block, reduced per warp
+    // then across the warps
+    if ((threadIdx.x & 31u) == 0) {
+        sh_red[threadIdx.x >> 5][0] = lo.x; sh_red[threadIdx.x >> 5][1] = lo.y; sh_red[threadIdx.x >> 5][2] = lo.z;
+        sh_red[threadIdx.x >> 5][3] = hi.x; sh_red[threadIdx.x >> 5][4] = hi.y; sh_red[threadIdx.x >> 5][5] = hi.z;
+    }
+    __syncthreads();
+    for (u32 w = 0; w < (blockDim.x >> 5); ++w) {
+        lo = mk(fminf(lo.x, sh_red[w][0]), fminf(lo.y, sh_red[w][1]), fminf(lo.z, sh_red[w][2]));
+        hi = mk(fmaxf(hi.x, sh_red[w][3]), fmaxf(hi.y, sh_red[w][4]), fmaxf(hi.z, sh_red[w][5]));
+    }
+    __syncthreads();
+}
+
+// Second pass of the range refit.  Blocks [0, nmed): 8 lanes per record of
+// the medium list (wide nodes whose range spans more than one 256-leaf
+// block); then one block per record of the huge list (ranges of more than
+// RANGE_HUGE leaves); then one block per job for the tree's root box (its
+// whole range).  A record sets its parent's slot from its sorted-leaf range.
+static constexpr u32 RANGE_HUGE = 16384;
+
+__device__ __forceinline__ void put_slot(const RefitJob& J, uint4 r, f3 lo, f3 hi) {
+    Wide4* W = J.w4 + r.x;
+    const u32 k = r.y & 3u;
+    W->lox[k] = lo.x; W->loy[k] = lo.y; W->loz[k] = lo.z;
+    W->hix[k] = hi.x; W->hiy[k] = hi.y; W->hiz[k] = hi.z;
+}
+
+__global__ void __launch_bounds__(256) k_refit_ranges(const RefitJob* __restrict__ jobs, u32 numJobs,
+                                                      const uint4* __restrict__ med, u32 nmed,
+                                                      const uint4* __restrict__ huge, u32 nhuge) {
+    const u32 medBlocks = (nmed + 31) / 32;  // 32 records of 8 lanes per block
+    const u32 lane = threadIdx.x & 31u;
+    if (blockIdx.x < medBlocks) {
+        const u32 grp = (blockIdx.x * blockDim.x + threadIdx.x) >> 3;
+        uint4 r = make_uint4(0u, 0u, 1u, 0u);  // empty: no pieces
+        const RefitJob* J = jobs;
+        if (grp < nmed) {
+            r = med[grp];
+            const u32 j = r.y >> 2;
+            if (j < numJobs && jobs[j].ranges && r.z <= r.w && r.w < jobs[j].n) J = jobs + j;
+            else r = make_uint4(0u, 0u, 1u, 0u);
+        }
+        f3 lo, hi;
+        range_union_group<8>(*J, r.z, r.w, lane & 7u, lo, hi);
+        if ((lane & 7u) == 0 && r.z <= r.w) put_slot(*J, r, lo, hi);
+        return;
+    }
+    u32 b = blockIdx.x - medBlocks;
+    if (b < nhuge) {
+        uint4 r = huge[b];
+        const u32 j = r.y >> 2;
+        const bool ok = j < numJobs && jobs[j].ranges && r.z <= r.w && r.w < jobs[j].n;  // uniform
+        if (!ok) return;
+        f3 lo, hi;
+        range_union_block(jobs[j], r.z, r.w, lo, hi);
+        if (threadIdx.x == 0) put_slot(jobs[j], r, lo, hi);
+        return;
+    }
+    b -= nhuge;
+    if (b >= numJobs || !jobs[b].ranges || jobs[b].n == 0) return;
+    f3 lo, hi;
+    range_union_block(jobs[b], 0u, jobs[b].n - 1, lo, hi);
+    if (threadIdx.x == 0) store_box(jobs[b].nodes, lo, hi);
+}
+
+// Range-refit records of the wide nodes (see launch_range_lists).
+__global__ void __launch_bounds__(256) k_range_records(const RefitJob* __restrict__ jobs, u32 numJobs,
+                                                       u32 totalLeaves, u32* __restrict__ blkCnt,
+                                                       const u32* __restrict__ blkOff, uint4* __restrict__ blkEnt,
+                                                       uint4* __restrict__ big, u32 bigCap, u32* __restrict__ bigCnt,
+                                                       int fill) {
+    const u32 g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= totalLeaves) return;
+    const u32 j = job_of(jobs, numJobs, g);
+    const RefitJob& J = jobs[j];
+    if (!J.ranges) return;
+    const u32 c = g - J.leafBase;
+    if (c >= *J.wcount) return;
+    const Wide4& W = J.w4[c];
+    if (W.parent < 0 || W.slot > 3u) return;  // the root: its box is the job's root pass
+    const uint2 r = J.wrange[c];
+    if (r.x > r.y || r.y >= J.n) return;
+    const uint4 rec = make_uint4((u32)W.parent, W.slot, r.x, r.y);
+    if ((r.x >> 8) == (r.y >> 8)) {
+        const u32 b = (J.leafBase + r.x) >> 8;
+        const u32 at = atomicAdd(&blkCnt[b], 1u);
+        if (fill) blkEnt[blkOff[b] + at] = rec;
+    } else {
+        // medium records from the front of `big`, huge ones from its back
+        const bool huge = r.y - r.x >= RANGE_HUGE;
+        const u32 at = atomicAdd(&bigCnt[huge ? 1 : 0], 1u);
+        if (fill) big[huge ? bigCap - 1 - at : at] = make_uint4(rec.x, rec.y | (j << 2), rec.z, rec.w);
+    }
+}
+
+cudaError_t launch_range_lists(const RefitJob* jobsDev, u32 numJobs, u32 totalLeaves, u32* blkCnt, u32* blkOff,
+                               uint4* blkEnt, uint4* big, u32 bigCap, u32* bigCnt, void* scanScratch,
+                               cudaStream_t s) {
+    const u32 nb = totalLeaves / 256 + 1;
+    cudaError_t e = cudaMemsetAsync(blkCnt, 0, 4 * (size_t)(nb + 1), s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(bigCnt, 0, 8, s);
+    if (e != cudaSuccess || totalLeaves == 0) return e;
+    const int grid = ceil_div(totalLeaves, 256);
+    k_range_records<<<grid, 256, 0, s>>>(jobsDev, numJobs, totalLeaves, blkCnt, blkOff, blkEnt, big, bigCap, bigCnt,
+                                         0);
+    e = cudaMemcpyAsync(blkOff, blkCnt, 4 * (size_t)(nb + 1), cudaMemcpyDeviceToDevice, s);
+    if (e == cudaSuccess) e = exclusive_scan(blkOff, nb + 1, scanScratch, s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(blkCnt, 0, 4 * (size_t)(nb + 1), s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(bigCnt, 0, 8, s);
+    if (e != cudaSuccess) return e;
+    k_range_records<<<grid, 256, 0, s>>>(jobsDev, numJobs, totalLeaves, blkCnt, blkOff, blkEnt, big, bigCap, bigCnt,
+                                         1);
+    return cudaGetLastError();
+}
+
+void launch_refit_ranges(const RefitJob* jobsDev, u32 numJobs, const uint4* big, u32 bigCap, u32 nmed, u32 nhuge,
+                         cudaStream_t s) {
+    const u32 blocks = (nmed + 31) / 32 + nhuge + numJobs;
+    if (blocks) k_refit_ranges<<<blocks, 256, 0, s>>>(jobsDev, numJobs, big, nmed, big + (bigCap - nhuge), nhuge);
+}
+
 __global__ void __launch_bounds__(256) k_refit(const RefitJob* __restrict__ jobs, u32 numJobs, u32 totalLeaves,
                                                u32* status) {
     __shared__ u32 sh_ext[8];
@@ -481,10 +752,14 @@ __global__ void __launch_bounds__(256) k_refit(const RefitJob* __restrict__ jobs
     const u32 n = J.n;
     const u32 i = g - J.leafBase;
     Node* nodes = J.nodes;
-    const u32 leaf = n - 1 + i;
+    // jobs' leaves may be padded to a multiple of 256 (range mode): the
+    // padding threads take the job's last leaf and drop it
+    const bool pad = i >= n;
+    const u32 li = pad ? n - 1 : i;
+    const u32 leaf = n - 1 + li;
     // root only: the tree is not built; levels: thread i is face i (its slot
-    // comes from leafWf)
-    const u32 f = (J.rootOnly || J.levels) ? i : (u32)__ldcg(&nodes[leaf].b);
+    // comes from leafWf); ranges: thread i is sorted leaf i
+    const u32 f = J.ranges ? J.idx[li] : ((J.rootOnly || J.levels) ? li : (u32)__ldcg(&nodes[leaf].b));
     const u32 vid[3] = {J.facets[3 * f], J.facets[3 * f + 1], J.facets[3 * f + 2]};
     f3 lo, hi;
     float ext = 0.f;
@@ -494,7 +769,7 @@ __global__ void __launch_bounds__(256) k_refit(const RefitJob* __restrict__ jobs
         const u32 gv = J.voff + vid[k];
         P[k] = J.x4 ? ld(J.x4, gv) : ldp(J.x3, gv);
     }
-    if (J.fpos && valid) {
+    if (J.fpos && valid && !pad) {
         float4* o = J.fpos + 3 * (size_t)f;
 #pragma unroll
         for (int k = 0; k < 3; ++k) o[k] = make_float4(P[k].x, P[k].y, P[k].z, __uint_as_float(vid[k]));
@@ -535,7 +810,7 @@ __global__ void __launch_bounds__(256) k_refit(const RefitJob* __restrict__ jobs
         // blocks hold one job), per warp and job for the others
         __syncthreads();
         const u32 j0 = sh_j0;
-        const u32 eb = valid ? __float_as_uint(ext) : 0u;  // positive floats order as ints
+        const u32 eb = (valid && !pad) ? __float_as_uint(ext) : 0u;  // positive floats order as ints
         const u32 e0 = __reduce_max_sync(0xFFFFFFFFu, j == j0 ? eb : 0u);
         if ((threadIdx.x & 31) == 0) sh_ext[threadIdx.x >> 5] = e0;
         if (valid && j != j0 && J.selfMargin > 0.f) {
@@ -550,7 +825,22 @@ __global__ void __launch_bounds__(256) k_refit(const RefitJob* __restrict__ jobs
             for (u32 w = 0; w < (blockDim.x >> 5); ++w) e = max(e, sh_ext[w]);
             atomicMax(jobs[j0].maxExt, e);
         }
-        if (!valid) return;
+        // range mode: a block holds 256 consecutive sorted leaves of one job
+        if (jobs[j0].ranges) range_block_boxes(J, i, valid && !pad, lo, hi);
+        if (!valid || pad) return;
+    }
+    if (J.ranges) {
+        store_box(&nodes[leaf], lo, hi);
+        const int2 ws = J.leafW[i];
+        if (ws.x < 0 || (u32)ws.x >= (n > 1 ? n - 1 : 1u) || ws.y < 0 || ws.y > 3) {
+            atomicOr(status, ST_ITER_CAP);
+            return;
+        }
+        Wide4* W = J.w4 + ws.x;
+        const int k = ws.y;
+        W->lox[k] = lo.x; W->loy[k] = lo.y; W->loz[k] = lo.z;
+        W->hix[k] = hi.x; W->hiy[k] = hi.y; W->hiz[k] = hi.z;
+        return;
     }
     if (J.rootOnly) {
         // union of the leaf boxes, one atomic per warp and job
@@ -723,16 +1013,25 @@ __global__ void __launch_bounds__(256) k_wide_heights(const RefitJob* __restrict
     const RefitJob& J = jobs[job_of(jobs, numJobs, g)];
     if (!J.w4 || !J.levels) return;
     const u32 i = g - J.leafBase;
+    if (i >= J.n) return;  // padding
     const u32 cap = J.n > 1 ? J.n - 1 : 1;
     i32 w = J.leafW[i].x;
-    u32 h = 0;
+    u32 h = 0, rlo = i, rhi = i;  // height and sorted-leaf range of the node carried up
     for (u32 step = 0; step < 128; ++step) {
         if (w < 0 || (u32)w >= cap) break;
         const u32 nc = __ldcg(&J.w4[w].nchild);
         if (nc == 0 || nc > 4) break;
         atomicMax(&J.hacc[w], h + 1);
+        if (J.wrange) {
+            atomicMin(&J.wrange[w].x, rlo);
+            atomicMax(&J.wrange[w].y, rhi);
+        }
         if (arrive_inc_acq_rel(&J.warrive[w], nc - 1) != nc - 1) return;
         h = __ldcg(&J.hacc[w]);
+        if (J.wrange) {
+            rlo = __ldcg(&J.wrange[w].x);
+            rhi = __ldcg(&J.wrange[w].y);
+        }
         w = __ldcg(&J.w4[w].parent);
         if (w < 0) return;
     }

@@ -79,6 +79,25 @@ struct RefitJob {
     // positions, each float4 carrying the mesh-local vertex id in w, written
     // by the leaf pass for the queries that test the face
     float4* fpos;
+    // range refit of the 4-wide form (with levels; leafBase a multiple of
+    // 256): the leaf pass runs in sorted-leaf order (idx: the face of each
+    // sorted leaf), writes each leaf box into its binary leaf node and its
+    // wide slot (leafW) and the boxes of every 16- and 256-leaf block (bb16 /
+    // bb256, indexed by (leafBase + leaf) / 16 and / 256);
+    // launch_refit_ranges then gives every internal wide child its slot box,
+    // and the tree its root box, as the union of the leaves of a sorted-leaf
+    // range (wrange), from the block boxes.
+    u32 ranges;
+    const u32* idx;
+    Node* bb16;
+    Node* bb256;
+    uint2* wrange;          // per wide node: (first, last) sorted leaf under it
+    // the wide nodes whose range lies in one 256-leaf block, per block (index
+    // (leafBase + leaf) / 256): (parent, slot, first, last) records
+    // blkEnt[blkOff[b] .. blkOff[b + 1]); the leaf pass's block fills their
+    // slots from its leaf boxes in shared memory
+    const uint4* blkEnt;
+    const u32* blkOff;
 };
 
 // Scene box of a mesh (min/max over all its vertices) into box[6] (float
@@ -153,6 +172,22 @@ static constexpr u32 QUERY_ORDER_MIN_HASH = 1u << 23;
 cudaError_t query_order(QueryOrder& o, const float* qx, u32 n, cudaStream_t s);
 void query_order_free(QueryOrder& o);
 
+// The range refit's second pass (after launch_refit) over the records
+// (parent, slot | job << 2, first, last) of the wide nodes whose range spans
+// more than one 256-leaf block: nmed at the front of big (8 lanes each), nhuge
+// at its back (ranges over 16384 leaves, a block each), then a block per job
+// for its root box.
+void launch_refit_ranges(const RefitJob* jobsDev, u32 numJobs, const uint4* big, u32 bigCap, u32 nmed, u32 nhuge,
+                         cudaStream_t s);
+// The range refit's node records after launch_wide_heights: each non-root
+// wide node of the range jobs goes to the list of the 256-leaf block holding
+// its range, or to big (bigCap records: medium ones from the front, huge
+// ones from the back).  blkCnt (numBlocks + 1 entries) is used as scratch;
+// blkOff gets the per-block offsets; bigCnt[0] / [1] the medium and huge
+// counts.  Scratch of scan_scratch_bytes(numBlocks + 1).
+cudaError_t launch_range_lists(const RefitJob* jobsDev, u32 numJobs, u32 totalLeaves, u32* blkCnt, u32* blkOff,
+                               uint4* blkEnt, uint4* big, u32 bigCap, u32* bigCnt, void* scanScratch,
+                               cudaStream_t s);
 // Allow the top-levels refit kernel its staging shared memory (once, before
 // the first launch_refit_levels; not during a stream capture).
 cudaError_t refit_levels_prepare();

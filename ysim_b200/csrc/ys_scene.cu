@@ -773,6 +773,12 @@ __global__ void k_unpack4(const float4* __restrict__ in, float* __restrict__ out
     if (i < n) { float4 q = in[i]; out[3 * i] = q.x; out[3 * i + 1] = q.y; out[3 * i + 2] = q.z; }
 }
 
+// Sorted-leaf ranges of the wide nodes before a height pass: empty.
+__global__ void k_range_init(uint2* __restrict__ r, u32 n) {
+    const u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) r[i] = make_uint2(0xFFFFFFFFu, 0u);
+}
+
 // Face positions of one mesh (the layout of RefitJob::fpos) from x.
 __global__ void k_face_pos(const float4* __restrict__ x, u32 voff, const u32* __restrict__ F3, u32 n,
                            float4* __restrict__ fpos) {
@@ -993,6 +999,15 @@ struct ys_scene {
     std::vector<u32> lvl_off;        // host copy of hoff (MAX_LEVELS + 2)
     u32 lvl_top = 0;
     bool use_levels = false;
+    // range refit (RefitJob::ranges): block boxes of 16 / 256 sorted leaves,
+    // per wide node its sorted-leaf range
+    bool use_ranges = true;
+    DBuf<Node> bb16, bb256;
+    DBuf<uint2> wrange;
+    DBuf<uint4> blkEnt, bigEnt;      // wide-node records: inside one 256-leaf block / spanning several
+    DBuf<u32> blkCnt, blkOff, bigCnt;
+    DBuf<char> rangeScratch;
+    u32 nbig = 0, nhuge = 0;
     DBuf<MeshDev> dmeshes;
     DBuf<RefitJob> jobs;            // 6 tables (cur x cv) of njobs, then one build slot
     std::vector<RefitJob> hjobs;
@@ -1202,6 +1217,7 @@ ys_status upload_jobs(ys_scene* s, bool levels) {
                 J.x4 = s->X[c].p;
                 J.v4 = s->V[w].p;
                 J.levels = (levels && J.w4) ? 1u : 0u;
+                J.ranges = (J.levels && s->use_ranges) ? 1u : 0u;
             }
             if (!t.empty())
                 YS_CK(cudaMemcpyAsync(s->jobs.p + (size_t)(c * 2 + w) * s->njobs, t.data(), t.size() * sizeof(RefitJob), cudaMemcpyHostToDevice, s->stream)); YS_CK(cudaStreamSynchronize(s->stream));
@@ -1224,7 +1240,21 @@ ys_status build_levels(ys_scene* s) {
     if (r) return r;
     const RefitJob* table = s->jobs.p;
     YS_CK(cudaMemsetAsync(s->hacc.p, 0, 4 * s->hacc.n, st));
+    if (s->wrange.p) k_range_init<<<ceil_div(s->wrange.n, 256), 256, 0, st>>>(s->wrange.p, (u32)s->wrange.n);
     launch_wide_heights(table, s->njobs, s->refitLeaves, s->status.p, st);
+    if (s->use_ranges) {
+        // range refit: the node records replace the level lists
+        YS_CK(launch_range_lists(table, s->njobs, s->refitLeaves, s->blkCnt.p, s->blkOff.p, s->blkEnt.p,
+                                 s->bigEnt.p, (u32)s->bigEnt.n, s->bigCnt.p, s->rangeScratch.p, st));
+        u32 nbig[2] = {0, 0};
+        YS_CK(cudaMemcpyAsync(nbig, s->bigCnt.p, 8, cudaMemcpyDeviceToHost, st));
+        YS_CK(cudaStreamSynchronize(st));
+        drop_graphs(s);
+        s->nbig = nbig[0];
+        s->nhuge = nbig[1];
+        s->use_levels = true;
+        return YS_OK;
+    }
     YS_CK(cudaMemsetAsync(s->hcount.p, 0, 4 * (MAX_LEVELS + 2), st));
     launch_level_count(table, s->njobs, s->refitLeaves, s->hcount.p, s->status.p, st);
     std::vector<u32> cnt(MAX_LEVELS + 2);
@@ -1365,8 +1395,11 @@ ys_status refit(ys_scene* s) {
         const RefitJob* table = s->jobs.p + (size_t)(s->cur * 2 + s->cv) * s->njobs;
         YS_CK(cudaMemsetAsync(s->maxext.p, 0, s->maxext.n * 4, s->stream));
         launch_refit(table, s->njobs, s->refitLeaves, s->status.p, s->stream);
-        if (s->use_levels)
+        if (s->use_levels && s->use_ranges) {
+            launch_refit_ranges(table, s->njobs, s->bigEnt.p, (u32)s->bigEnt.n, s->nbig, s->nhuge, s->stream);
+        } else if (s->use_levels) {
             launch_refit_levels(table, s->wlist.p, s->hoff.p, s->lvl_off.data(), s->lvl_top, s->stream);
+        }
         if (s->nRootOnly) launch_refit_roots(table, s->njobs, s->stream);
     }
     return YS_OK;
@@ -1564,7 +1597,8 @@ ys_status ys_scene_destroy(ys_scene* s) {
     s->scanScratch.free(); s->rows.free(); s->contacts.free(); s->csr.free(); s->pool.free(); s->bucket.free();
     drop_graphs(s);
     s->csr_off.free(); s->vstart.free(); s->vcount.free(); s->ext.free();
-    s->fpos.free(); s->vorder.free(); s->okeys.free(); s->oaoff.free(); s->orank.free(); s->obox.free(); s->oscratch.free();
+    s->fpos.free(); s->bb16.free(); s->bb256.free(); s->wrange.free(); s->blkEnt.free(); s->bigEnt.free();
+    s->blkCnt.free(); s->blkOff.free(); s->bigCnt.free(); s->rangeScratch.free(); s->vorder.free(); s->okeys.free(); s->oaoff.free(); s->orank.free(); s->obox.free(); s->oscratch.free();
     for (auto e : s->evPool) cudaEventDestroy(e);
     cudaStreamDestroy(s->stream);
     delete s;
@@ -1718,6 +1752,7 @@ ys_status ys_scene_pack(ys_scene* s) {
         YS_CK(cudaMemsetAsync(s->warrive.p, 0, 4 * s->warrive.n, s->stream));
         YS_CK(s->wcount.alloc(s->meshes.size())); YS_CK(cudaMemsetAsync(s->wcount.p, 0, 4 * s->meshes.size(), s->stream));
         YS_CK(s->hacc.alloc(std::max(nW4, 1u))); YS_CK(s->wlist.alloc(std::max(nW4, 1u)));
+        YS_CK(s->wrange.alloc(std::max(nW4, 1u)));
         YS_CK(s->hcount.alloc(MAX_LEVELS + 2)); YS_CK(s->hoff.alloc(MAX_LEVELS + 2));
         YS_CK(s->hcursor.alloc(MAX_LEVELS + 2));
     }
@@ -1867,10 +1902,26 @@ ys_status ys_scene_pack(ys_scene* s) {
             J.hacc = s->hacc.p + H.w4_off;
         }
         if (!J.rootOnly) J.fpos = s->fpos.p + 3 * (size_t)H.foff;  // faces the fused kernel tests
+        if (J.w4) { J.wrange = s->wrange.p + H.w4_off; J.idx = s->idx.p + H.foff; }
         s->hjobs.push_back(J);
-        leaves += J.n;
+        // every job's leaves start on a 256-leaf boundary (the range refit's
+        // blocks then never hold two jobs)
+        leaves = (leaves + J.n + 255u) & ~255u;
     }
     s->refitLeaves = leaves;
+    YS_CK(s->bb16.alloc(std::max<size_t>(leaves / 16, 1)));
+    YS_CK(s->bb256.alloc(std::max<size_t>(leaves / 256, 1)));
+    {
+        const u32 nb = leaves / 256 + 1;
+        YS_CK(s->blkCnt.alloc(nb + 1)); YS_CK(s->blkOff.alloc(nb + 1)); YS_CK(s->bigCnt.alloc(2));
+        YS_CK(s->blkEnt.alloc(std::max(nW4, 1u))); YS_CK(s->bigEnt.alloc(std::max(nW4, 1u)));
+        YS_CK(s->rangeScratch.alloc(scan_scratch_bytes(nb + 1)));
+        YS_CK(cudaMemsetAsync(s->blkOff.p, 0, 4 * (size_t)(nb + 1), s->stream));
+    }
+    for (auto& J : s->hjobs) {
+        J.bb16 = s->bb16.p; J.bb256 = s->bb256.p;
+        J.blkEnt = s->blkEnt.p; J.blkOff = s->blkOff.p;
+    }
     s->njobs = (u32)s->hjobs.size();
     s->nrjobs = (u32)hr.size();
     s->nrchunks = (u32)chunks.size();
@@ -1882,7 +1933,7 @@ ys_status ys_scene_pack(ys_scene* s) {
         YS_CK(s->rootAcc.alloc(acc.size()));
         YS_CK(cudaMemcpyAsync(s->rootAcc.p, acc.data(), 4 * acc.size(), cudaMemcpyHostToDevice, s->stream)); YS_CK(cudaStreamSynchronize(s->stream));
         for (size_t j = 0; j < s->hjobs.size(); ++j)
-            if (s->hjobs[j].rootOnly) s->hjobs[j].rootAcc = s->rootAcc.p + 32 * j;
+            s->hjobs[j].rootAcc = s->rootAcc.p + 32 * j;
         for (size_t j = 0; j < hr.size(); ++j) hr[j].rootAcc = s->rootAcc.p + 32 * (s->njobs + j);
     }
     if (s->nrjobs) {
@@ -2304,6 +2355,25 @@ ys_status ys_scene_contacts(ys_scene* s, uint32_t* off, void* out, uint64_t cap,
     }
     if (n_out) *n_out = 0;
     if (off) memset(off, 0, 4 * (size_t)(s->nV + 1));
+    return YS_OK;
+}
+
+ys_status ys_scene_wide_tree(ys_scene* s, int mesh, void* out, uint32_t cap, uint32_t* count) {
+    ys_status r = check_scene(s);
+    if (r) return r;
+    if (mesh < 0 || (size_t)mesh >= s->meshes.size()) return fail(YS_ERR_BAD_ARG, "bad mesh index");
+    if (!count) return fail(YS_ERR_BAD_ARG, "null count");
+    *count = 0;
+    HostMesh& H = s->meshes[mesh];
+    if (s->tree_layout != YS_TREE_CUBE || !H.built || H.d.num_facets == 0) return YS_OK;
+    u32 n = 0;
+    YS_CK(cudaMemcpyAsync(&n, s->wcount.p + mesh, 4, cudaMemcpyDeviceToHost, s->stream));
+    YS_CK(cudaStreamSynchronize(s->stream));
+    *count = n;
+    if (out && cap)
+        YS_CK(cudaMemcpyAsync(out, s->w4.p + H.w4_off, sizeof(Wide4) * std::min(n, cap), cudaMemcpyDeviceToHost,
+                              s->stream));
+    YS_CK(cudaStreamSynchronize(s->stream));
     return YS_OK;
 }
 

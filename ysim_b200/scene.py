@@ -25,6 +25,9 @@ ROW_DTYPE = np.dtype([("point", "<u4"), ("tri", "<u4"), ("qobj", "<u4"), ("tobj"
 VCONTACT_DTYPE = np.dtype([("tobj", "<u4"), ("tri", "<u4"), ("nx", "<f4"), ("ny", "<f4"), ("nz", "<f4"),
                            ("d", "<f4")])
 NODE_DTYPE = np.dtype([("mn", "<f4", 3), ("a", "<i4"), ("mx", "<f4", 3), ("b", "<i4")])
+WIDE_DTYPE = np.dtype([("lo", "<f4", (3, 4)), ("hi", "<f4", (3, 4)), ("child", "<i4", 4), ("nchild", "<u4"),
+                       ("parent", "<i4"), ("slot", "<u4"), ("pad", "<u4")])
+W4_EMPTY = 0x7FFFFFFF
 
 
 def _ptr(a: Optional[np.ndarray]):
@@ -214,6 +217,17 @@ class Scene:
         _lib.check(self.lib.ys_scene_contacts(self.h, _ptr(off), _ptr(out), n.value, C.byref(n)),
                    "ys_scene_contacts")
         return off, out
+
+    def wide_tree(self, mesh: int) -> np.ndarray:
+        """The 4-wide form of a mesh's tree as the last refit left it (cube
+        layout; empty otherwise): WIDE_DTYPE records, lo/hi[axis][slot]."""
+        n = C.c_uint32()
+        _lib.check(self.lib.ys_scene_wide_tree(self.h, mesh, None, 0, C.byref(n)), "ys_scene_wide_tree")
+        out = np.zeros(n.value, WIDE_DTYPE)
+        if n.value:
+            _lib.check(self.lib.ys_scene_wide_tree(self.h, mesh, _ptr(out), n.value, C.byref(n)),
+                       "ys_scene_wide_tree")
+        return out
 
     def tree(self, mesh: int):
         n = C.c_uint32()
