@@ -344,8 +344,12 @@ def run_ours(args, rank, world, local):
                                   "stats": st0}), flush=True)
             sys.exit(3)
     tuned, tune_ms = scene.autotune()
+    classes = scene.autotune_classes()
+    if classes:
+        tuned = classes[-1]["ctas_per_sm"]
     if args.fused_variant:  # a fixed variant (profiling: ncu perturbs the autotuner's timings)
         scene.set_fused_variant(args.fused_variant)
+        scene.set_thread_order(True)
         tuned = args.fused_variant
     scene.step(max(args.warmup, 6))  # also re-captures the graphs the autotuner dropped
     scene.sync()
@@ -522,7 +526,8 @@ def run_ours(args, rank, world, local):
                                                    "contacts_per_substep": cont_ps, "preroll_substeps": args.preroll,
                                                    "first_timed_substep": args.preroll + max(args.warmup, 6),
                                                    "fused_variant": {"ctas_per_sm": tuned,
-                                                                     "autotune_ms": dict(zip(("8", "7", "4"), tune_ms))},
+                                                                     "autotune_ms": dict(zip(("8", "7", "4"), tune_ms)),
+                                                                     "per_size_class": classes},
                                                    "flags": st["flags"]}),
             "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": nV * 12 / nsub,
                     "d2h_bytes_per_step": nV * 12 / nsub,
@@ -636,6 +641,7 @@ def measure_batched(args, rank, world, local, steps=100):
     stream = torch.cuda.ExternalStream(scene.stream(), device=local)
     scene.step(20)
     tuned, _ = scene.autotune()
+    classes = scene.autotune_classes()
     scene.step(6)  # re-capture the substep graphs of all six buffer-rotation states, untimed
     scene.sync()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -650,8 +656,14 @@ def measure_batched(args, rank, world, local, steps=100):
     flags = scene.stats()["flags"]
     scene.close()
     plain = [Scene(p, device=local) for p in parts]
-    for q in plain:
-        q.set_fused_variant(tuned)  # before the warm-up, which captures the graphs
+    for q, p in zip(plain, parts):
+        # each instance is one size class of its own: the batched scene's
+        # choice for that class, before the warm-up, which captures the graphs
+        nv = max(m.nV for m in p.meshes if m.grid_n)
+        ch = next((c for c in classes if nv <= c["max_mesh_vertices"]), None)
+        q.set_fused_variant(ch["ctas_per_sm"] if ch else tuned)
+        if ch:
+            q.set_thread_order(ch["thread_order"] == "morton")
         q.step(20)
     for q in plain:
         q.sync()
@@ -680,8 +692,10 @@ def measure_batched(args, rank, world, local, steps=100):
             "plain": {"value": 1000.0 / p_ms, "ms_per_substep": p_ms,
                       "timing": "host clock between synchronisations (one scene per instance, own stream)"},
             "batched_over_plain": p_ms / b_ms, "steps": steps, "flags": flags,
-            "fused_variant": {"ctas_per_sm": tuned, "note": "chosen by ys_scene_autotune on the batched scene, "
-                                                             "used for the plain scenes too"},
+            "fused_variant": {"per_size_class": classes,
+                              "note": "one fused launch per size class of the instances, each with the register-cap "
+                                      "variant and thread order ys_scene_autotune_classes chose on the batched "
+                                      "scene's live state; each plain instance uses its class's choice"},
             "note": "the ~4.3M vertices quoted for this config differ from the drawn total (vertices above)"}
 
 
@@ -763,8 +777,9 @@ def measure_adjoint(args, local, steps=200, every=20, reps=4):
 def fp32_vs_fp64_prefix(spec, k, L, kstar, local, every):
     """FP32 adjoint against the 64-bit mode on the C5 problem's steps before
     its first contact push (found from the recorded contacts of the FP32
-    forward: a contact with d below the thickness), MSE loss against the
-    perturbed-stiffness rollout at the same step."""
+    forward: a contact with d below the thickness), seeded with the gradient
+    of the MSE loss against the perturbed-stiffness rollout at the same step,
+    taken at the binary64 state."""
     import torch
     from ysim_b200.adjoint import ClothRollout
     from ysim_b200.scene import Scene
@@ -787,12 +802,18 @@ def fp32_vs_fp64_prefix(spec, k, L, kstar, local, every):
         target = roll(torch.tensor(kstar, device=dev), torch.tensor(L, device=dev),
                       torch.zeros((c.nV, 3), device=dev)).double()
     roll.close()
-    out = {}
-    for prec, dt in ((32, torch.float32), (64, torch.float64)):
+    # both reverse passes take the loss gradient of the binary64 rollout (a
+    # seed formed from the FP32 state would be mostly its rounding: x_T - x*
+    # is a few binary32 ulps of x_T in the first steps)
+    out, seed = {}, None
+    for prec, dt in ((64, torch.float64), (32, torch.float32)):
         roll = ClothRollout(spec, steps=T, checkpoint_every=every, device=local, precision=prec)
         p = [torch.tensor(np.asarray(a), dtype=dt, device=dev, requires_grad=True)
              for a in (k, L, np.zeros((c.nV, 3), np.float32))]
-        ((roll(*p) - target.to(dt)) ** 2).sum(1).mean().backward()
+        xT = roll(*p)
+        if seed is None:
+            seed = (2.0 * (xT.detach() - target) / c.nV).double()
+        xT.backward(seed.to(dt))
         out[prec] = [t.grad.double().cpu().numpy() for t in p]
         roll.close()
     rel = {n_: float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))

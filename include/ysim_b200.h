@@ -202,6 +202,24 @@ ys_status ys_scene_set_thread_order(ys_scene* s, int on);
  * reports it (*chosen) and the mean milliseconds per variant (ms_out[3], in
  * the order 8, 7, 4; may be null).  No counterpart in the reference. */
 ys_status ys_scene_autotune(ys_scene* s, uint32_t reps, int* chosen, float* ms_out);
+/* The fused substep runs one launch per size class of the working meshes
+ * (cloth, moving or querying meshes with at most 4096, 16384, 65536 vertices,
+ * and larger; a batch of instances of mixed sizes spans several).  Each
+ * class has its own register-cap variant and thread order. */
+typedef struct ys_fused_class {
+    uint32_t max_mesh_vertices;  /* the class's bound on a mesh's vertex count */
+    uint32_t meshes, vertices;   /* working meshes and vertices in the class */
+    int32_t ctas_per_sm;         /* chosen variant (8, 7 or 4) */
+    int32_t morton_order;        /* chosen thread order: 1 Morton, 0 vertex */
+    float ms[2][3];              /* mean ms per launch: [vertex, Morton order][8, 7, 4] */
+} ys_fused_class;
+/* Per-class autotuner: times every variant under both thread orders on each
+ * class's launch over the current state (the scene does not advance), keeps
+ * the fastest pair per class and reports the classes (out: up to cap
+ * records; *nclasses: the number of classes, 4).  No counterpart in the
+ * reference. */
+ys_status ys_scene_autotune_classes(ys_scene* s, uint32_t reps, ys_fused_class* out, uint32_t cap,
+                                    uint32_t* nclasses);
 /* Analytic collider (GeneralMesh::colliderKind and transform): kind
  * YS_COLLIDER_SPHERE / BOX / CYLINDER / PLANE (YS_COLLIDER_MESH: triangles,
  * the default), centre, local half extents (sphere: semi-axes; box: half

@@ -47,6 +47,11 @@ COLLIDER_CYLINDER = 3
 COLLIDER_PLANE = 4
 
 
+class FusedClass(C.Structure):
+    _fields_ = [("max_mesh_vertices", C.c_uint32), ("meshes", C.c_uint32), ("vertices", C.c_uint32),
+                ("ctas_per_sm", C.c_int32), ("morton_order", C.c_int32), ("ms", (C.c_float * 3) * 2)]
+
+
 class SimParams(C.Structure):
     _fields_ = [
         ("subh", C.c_float), ("kair", C.c_float), ("kd", C.c_float),
@@ -94,6 +99,7 @@ _PROTOS = {
     "ys_scene_set_tree_layout": (C.c_int, [C.c_void_p, C.c_int]),
     "ys_scene_set_fused_variant": (C.c_int, [C.c_void_p, C.c_int]),
     "ys_scene_set_thread_order": (C.c_int, [C.c_void_p, C.c_int]),
+    "ys_scene_autotune_classes": (C.c_int, [C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint32, C.c_void_p]),
     "ys_scene_wide_tree": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_uint32, C.c_void_p]),
     "ys_scene_set_tree_builder": (C.c_int, [C.c_void_p, C.c_int]),
     "ys_lbvh_set_builder": (C.c_int, [C.c_void_p, C.c_int]),

@@ -101,11 +101,13 @@ struct StepArgs {
     u32 analytic;  // the scene has analytic colliders
     float subh, kair, kd, gx, gy, gz, margin, band, radius;
     u32 nV, self_mode, record, cap;
-    // fused kernel: thread t works on vertex vorder[t] (vertices in Morton
-    // order within their mesh, static non-query vertices left out), or on
-    // vertex t when vorder is null; nthreads threads carry a vertex
+    // fused kernel: thread t of a launch works on vertex vorder[tbase + t]
+    // (the working vertices: static non-query vertices are left out) while
+    // tbase + t < tend.  vorder lists the meshes of one size class after
+    // another, each mesh's vertices in Morton or vertex order; a launch covers
+    // one class.
     const u32* vorder;
-    u32 nthreads;
+    u32 tbase, tend;
     u32* status;
     unsigned long long* counters;  // [0] broad rows, [1] contacts, [2] pool fill, [3] [4] running totals of 0, 1
     // fused record pool
@@ -332,9 +334,9 @@ __global__ void __launch_bounds__(128, MINB) k_fused(StepArgs A) {
     __shared__ WarpWork wq[FUSED_WARPS];
     const u32 lane = threadIdx.x & 31u;
     WarpWork& Q = wq[threadIdx.x >> 5];
-    const u32 t = blockIdx.x * blockDim.x + threadIdx.x;
-    const bool valid = t < A.nthreads;
-    const u32 g = !valid ? 0u : (A.vorder ? A.vorder[t] : t);
+    const u32 t = A.tbase + blockIdx.x * blockDim.x + threadIdx.x;
+    const bool valid = t < A.tend;
+    const u32 g = valid ? A.vorder[t] : 0u;
     const u32 m = valid ? A.vobj[g] : 0u;
     const MeshDev* __restrict__ Mp = A.meshes + m;
     const u32 mflags = Mp->flags;
@@ -612,6 +614,9 @@ __global__ void __launch_bounds__(128, MINB) k_fused(StepArgs A) {
 }
 
 static constexpr int FUSED_VARIANTS[3] = {8, 7, 4};  // register caps, as CTAs per SM
+// Size classes of the working meshes: at most 64^2, 128^2, 256^2 vertices, larger.
+static constexpr int NCLASS = 4;
+static constexpr u32 CLASS_MAX[NCLASS] = {4096u, 16384u, 65536u, 0xFFFFFFFFu};
 
 template <bool ANA>
 void launch_fused_t(const StepArgs& A, dim3 g, dim3 b, cudaStream_t st, int minBlocks) {
@@ -626,8 +631,8 @@ void launch_fused_t(const StepArgs& A, dim3 g, dim3 b, cudaStream_t st, int minB
 }
 
 void launch_fused(const StepArgs& A, cudaStream_t st, int minBlocks) {
-    if (A.nthreads == 0) return;
-    const dim3 g(ceil_div(A.nthreads, 128)), b(128);
+    if (A.tend <= A.tbase) return;
+    const dim3 g(ceil_div(A.tend - A.tbase, 128)), b(128);
     if (A.analytic) launch_fused_t<true>(A, g, b, st, minBlocks);
     else launch_fused_t<false>(A, g, b, st, minBlocks);
 }
@@ -828,12 +833,24 @@ __global__ void k_order_box(const float4* __restrict__ x, const u32* __restrict_
 
 __global__ void k_order_keys(const float4* __restrict__ x, const u32* __restrict__ vobj,
                              const u32* __restrict__ aoff, const u32* __restrict__ arank,
-                             const MeshDev* __restrict__ meshes, const u32* __restrict__ mbox, u32 nV, u32 kbits,
-                             u32* __restrict__ keys, u32* __restrict__ vals) {
+                             const u32* __restrict__ morton, const MeshDev* __restrict__ meshes,
+                             const u32* __restrict__ mbox, u32 nV, u32 kbits, u32* __restrict__ keys,
+                             u32* __restrict__ vals) {
     const u32 g = blockIdx.x * blockDim.x + threadIdx.x;
     if (g >= nV) return;
     const u32 m = vobj[g];
     if (aoff[m] == NO_PAIR) return;
+    const u32 rank = arank[m];
+    const u32 i = aoff[m] + (g - meshes[m].voff);
+    vals[i] = g;
+    if (!morton[m]) {
+        // vertex order: the vertex's index in its mesh (clamped: the sort is
+        // stable, so equal keys keep vertex order)
+        const u32 local = g - meshes[m].voff;
+        const u32 cap = kbits >= 32 ? 0xFFFFFFFFu : (1u << kbits) - 1u;
+        keys[i] = (kbits >= 32 ? 0u : (rank << kbits)) | min(local, cap);
+        return;
+    }
     const f3 p = ld(x, g);
     const float lo[3] = {funord(mbox[6 * m]), funord(mbox[6 * m + 1]), funord(mbox[6 * m + 2])};
     const float c[3] = {p.x, p.y, p.z};
@@ -849,10 +866,7 @@ __global__ void k_order_keys(const float4* __restrict__ x, const u32* __restrict
     }
     u32 code = (expand_bits(q[0]) << 2) | (expand_bits(q[1]) << 1) | expand_bits(q[2]);  // 30 bits
     if (kbits < 30) code >>= (30 - kbits);
-    const u32 rank = arank[m];
-    const u32 i = aoff[m] + (g - meshes[m].voff);
     keys[i] = (kbits >= 32 ? 0u : (rank << kbits)) | code;
-    vals[i] = g;
 }
 
 // ------------------------------------------------------------------ host
@@ -1040,9 +1054,16 @@ struct ys_scene {
     int fused_min_blocks = 8;        // k_fused register cap (ys_scene_set_fused_variant / ys_scene_autotune)
     // fused-kernel thread order (ys_scene_set_thread_order): working vertices
     // in Morton order per mesh, recomputed at every tree rebuild
-    bool use_order = true;
-    u32 nact = 0, order_kbits = 0;   // working vertices; Morton bits below the mesh rank
-    DBuf<u32> vorder, okeys, oaoff, orank, obox;
+    u32 nact = 0, order_kbits = 0;   // working vertices; key bits below the mesh rank
+    DBuf<u32> vorder, okeys, oaoff, orank, obox, omorton;
+    // size classes of the working meshes (by vertex count, bounds CLASS_MAX):
+    // each class is one k_fused launch over its contiguous part of vorder,
+    // with its own register-cap variant and thread order
+    std::vector<u32> cls_off;        // NCLASS + 1 offsets into vorder
+    std::vector<u32> cls_meshes;     // working meshes per class
+    std::vector<int> cls_variant;    // CTAs per SM of each class's launch
+    std::vector<int> cls_morton;     // 1: Morton thread order, 0: vertex order
+    std::vector<int> mesh_class;     // per mesh, or -1 (not working)
     DBuf<char> oscratch;
     int tree_layout = YS_TREE_CUBE;  // Morton normalisation of the scene trees
     int tree_builder = YS_BUILD_KARRAS;
@@ -1113,8 +1134,9 @@ StepArgs make_args(ys_scene* s) {
     A.margin = s->P.margin;
     A.band = s->P.radius + s->P.margin;
     A.nV = s->nV;
-    A.vorder = s->use_order ? s->vorder.p : nullptr;
-    A.nthreads = s->use_order ? s->nact : s->nV;
+    A.vorder = s->vorder.p;
+    A.tbase = 0;
+    A.tend = s->nact;
     A.self_mode = s->P.self_mode;
     A.record = s->record ? 1u : 0u;
     A.cap = s->cap;
@@ -1350,13 +1372,27 @@ ys_status compute_order(ys_scene* s) {
         for (int k = 0; k < 6; ++k) init[6 * m + k] = k < 3 ? 0xFFFFFFFFu : 0u;
     YS_CK(cudaMemcpyAsync(s->obox.p, init.data(), 4 * init.size(), cudaMemcpyHostToDevice, st));
     k_order_box<<<ceil_div(s->nV, 256), 256, 0, st>>>(s->X[s->cur].p, s->vobj.p, s->oaoff.p, s->nV, s->obox.p);
+    std::vector<u32> mort(nm, 0u);
+    for (size_t m = 0; m < nm; ++m)
+        if (s->mesh_class[m] >= 0) mort[m] = s->cls_morton[s->mesh_class[m]] ? 1u : 0u;
+    YS_CK(cudaMemcpyAsync(s->omorton.p, mort.data(), 4 * nm, cudaMemcpyHostToDevice, st));
     k_order_keys<<<ceil_div(s->nV, 256), 256, 0, st>>>(s->X[s->cur].p, s->vobj.p, s->oaoff.p, s->orank.p,
-                                                       s->dmeshes.p, s->obox.p, s->nV, s->order_kbits, s->okeys.p,
-                                                       s->vorder.p);
+                                                       s->omorton.p, s->dmeshes.p, s->obox.p, s->nV, s->order_kbits,
+                                                       s->okeys.p, s->vorder.p);
     YS_CK(cudaGetLastError());
     YS_CK(radix_sort_pairs(s->okeys.p, s->vorder.p, s->nact, s->oscratch.p, 0, 32, st));
-    YS_CK(cudaStreamSynchronize(st));  // init lives on the host stack
+    YS_CK(cudaStreamSynchronize(st));  // init and mort live on the host stack
     return YS_OK;
+}
+
+// One k_fused launch per non-empty size class (classes do not interact:
+// each launch writes only its own vertices' next state).
+void launch_fused_classes(ys_scene* s, StepArgs A) {
+    for (size_t c = 0; c + 1 < s->cls_off.size(); ++c) {
+        A.tbase = s->cls_off[c];
+        A.tend = s->cls_off[c + 1];
+        launch_fused(A, s->stream, s->cls_variant[c]);
+    }
 }
 
 ys_status preamble(ys_scene* s) {
@@ -1377,7 +1413,7 @@ ys_status preamble(ys_scene* s) {
         if (rebuilt) {
             ys_status r = build_levels(s);
             if (r) return r;
-            if (s->use_order && (r = compute_order(s))) return r;
+            if ((r = compute_order(s))) return r;
         }
     }
     // environment forces (ext = g * m) are evaluated inside the force kernels
@@ -1491,7 +1527,7 @@ ys_status enqueue_fused(ys_scene* s) {
     if (r) return r;
     YS_CK(cudaMemsetAsync(s->counters.p, 0, s->record ? 24 : 16, s->stream));
     StepArgs A = make_args(s);
-    launch_fused(A, s->stream, s->fused_min_blocks);
+    launch_fused_classes(s, A);
     YS_CK(cudaGetLastError());
     return YS_OK;
 }
@@ -1548,7 +1584,7 @@ ys_status fused_substep(ys_scene* s) {
         s->evFused.push_back(s->evUsed);
         YS_CK(cudaEventRecord(next_event(s), s->stream));
     }
-    launch_fused(A, s->stream, s->fused_min_blocks);
+    launch_fused_classes(s, A);
     YS_CK(cudaGetLastError());
     if (s->timing) YS_CK(cudaEventRecord(next_event(s), s->stream));
     s->snapshot_pending = true;
@@ -1598,7 +1634,7 @@ ys_status ys_scene_destroy(ys_scene* s) {
     drop_graphs(s);
     s->csr_off.free(); s->vstart.free(); s->vcount.free(); s->ext.free();
     s->fpos.free(); s->bb16.free(); s->bb256.free(); s->wrange.free(); s->blkEnt.free(); s->bigEnt.free();
-    s->blkCnt.free(); s->blkOff.free(); s->bigCnt.free(); s->rangeScratch.free(); s->vorder.free(); s->okeys.free(); s->oaoff.free(); s->orank.free(); s->obox.free(); s->oscratch.free();
+    s->blkCnt.free(); s->blkOff.free(); s->bigCnt.free(); s->rangeScratch.free(); s->vorder.free(); s->okeys.free(); s->oaoff.free(); s->orank.free(); s->obox.free(); s->oscratch.free(); s->omorton.free();
     for (auto e : s->evPool) cudaEventDestroy(e);
     cudaStreamDestroy(s->stream);
     delete s;
@@ -1965,17 +2001,36 @@ ys_status ys_scene_pack(ys_scene* s) {
         if (r) return r;
     }
     {
-        // working vertices of the fused kernel: cloth, moving, or querying
-        std::vector<u32> aoff(s->meshes.size(), NO_PAIR), rank(s->meshes.size(), 0);
-        u32 na = 0, nmesh = 0;
-        for (size_t m = 0; m < s->meshes.size(); ++m) {
+        // working vertices of the fused kernel (cloth, moving, or querying),
+        // mesh by mesh in size-class order
+        const size_t nm = s->meshes.size();
+        std::vector<u32> aoff(nm, NO_PAIR), rank(nm, 0);
+        s->mesh_class.assign(nm, -1);
+        s->cls_meshes.assign(NCLASS, 0);
+        for (size_t m = 0; m < nm; ++m) {
             const u32 f = s->meshes[m].flags;
             if (!(f & MF_CLOTH) && (f & MF_STATIC) && !(f & MF_QUERY)) continue;
-            if (s->meshes[m].d.num_vertices == 0) continue;
-            aoff[m] = na;
-            rank[m] = nmesh++;
-            na += s->meshes[m].d.num_vertices;
+            const u32 nv = s->meshes[m].d.num_vertices;
+            if (nv == 0) continue;
+            int c = 0;
+            while (c + 1 < NCLASS && nv > CLASS_MAX[c]) ++c;
+            s->mesh_class[m] = c;
+            s->cls_meshes[c]++;
         }
+        u32 na = 0, nmesh = 0;
+        s->cls_off.assign(NCLASS + 1, 0);
+        for (int c = 0; c < NCLASS; ++c) {
+            s->cls_off[c] = na;
+            for (size_t m = 0; m < nm; ++m) {
+                if (s->mesh_class[m] != c) continue;
+                aoff[m] = na;
+                rank[m] = nmesh++;
+                na += s->meshes[m].d.num_vertices;
+            }
+        }
+        s->cls_off[NCLASS] = na;
+        s->cls_variant.assign(NCLASS, s->fused_min_blocks);
+        s->cls_morton.assign(NCLASS, 1);
         u32 mbits = 0;
         while (mbits < 32 && (1ull << mbits) < nmesh) ++mbits;
         s->nact = na;
@@ -1983,6 +2038,7 @@ ys_status ys_scene_pack(ys_scene* s) {
         YS_CK(s->oaoff.alloc(aoff.size()));
         YS_CK(s->orank.alloc(rank.size()));
         YS_CK(s->obox.alloc(6 * aoff.size()));
+        YS_CK(s->omorton.alloc(aoff.size()));
         YS_CK(s->vorder.alloc(std::max(na, 1u)));
         YS_CK(s->okeys.alloc(std::max(na, 1u)));
         YS_CK(s->oscratch.alloc(sort_scratch_bytes(std::max(na, 1u))));
@@ -2082,18 +2138,17 @@ ys_status ys_scene_set_fused_variant(ys_scene* s, int min_blocks) {
     if (min_blocks != 8 && min_blocks != 7 && min_blocks != 4)
         return fail(YS_ERR_BAD_ARG, "fused variant: CTAs per SM must be 8, 7 or 4");
     s->fused_min_blocks = min_blocks;
+    for (auto& v : s->cls_variant) v = min_blocks;
     drop_graphs(s);
     return YS_OK;
 }
 
 ys_status ys_scene_set_thread_order(ys_scene* s, int on) {
-    if (!s) return fail(YS_ERR_BAD_ARG, "null scene");
-    const bool want = on != 0;
-    if (want == s->use_order) return YS_OK;
-    s->use_order = want;
+    ys_status r = check_scene(s);
+    if (r) return r;
+    for (auto& o : s->cls_morton) o = on ? 1 : 0;
     drop_graphs(s);
-    if (want && s->packed) return compute_order(s);
-    return YS_OK;
+    return compute_order(s);
 }
 
 // Time every k_fused variant on the current state (the kernel only writes the
@@ -2141,8 +2196,89 @@ ys_status ys_scene_autotune(ys_scene* s, uint32_t reps, int* chosen, float* ms_o
     YS_CK(cudaStreamSynchronize(st));
     s->record = rec;
     s->fused_min_blocks = bestV;
+    for (auto& v : s->cls_variant) v = bestV;
     drop_graphs(s);
     if (chosen) *chosen = bestV;
+    return YS_OK;
+}
+
+// Per size class: time each register-cap variant under each thread order on
+// the current state (the kernel writes only the next-state buffers; the
+// running totals are restored) and keep the fastest pair for the class.
+ys_status ys_scene_autotune_classes(ys_scene* s, uint32_t reps, ys_fused_class* out, uint32_t cap,
+                                    uint32_t* nclasses) {
+    ys_status r = check_scene(s);
+    if (r) return r;
+    if (reps == 0) reps = 5;
+    cudaStream_t st = s->stream;
+    const bool rec = s->record;
+    s->record = false;
+    r = refit(s);
+    if (r) { s->record = rec; return r; }
+    unsigned long long saved[8];
+    YS_CK(cudaMemcpyAsync(saved, s->counters.p, sizeof(saved), cudaMemcpyDeviceToHost, st));
+    YS_CK(cudaStreamSynchronize(st));
+    cudaEvent_t e0, e1;
+    YS_CK(cudaEventCreate(&e0));
+    YS_CK(cudaEventCreate(&e1));
+    float ms[NCLASS][2][3] = {};
+    for (int order = 0; order < 2 && !r; ++order) {
+        for (auto& o : s->cls_morton) o = order;
+        r = compute_order(s);
+        if (r) break;
+        StepArgs A = make_args(s);
+        for (int c = 0; c < NCLASS; ++c) {
+            A.tbase = s->cls_off[c];
+            A.tend = s->cls_off[c + 1];
+            if (A.tend <= A.tbase) continue;
+            for (int i = 0; i < 3; ++i) {
+                launch_fused(A, st, FUSED_VARIANTS[i]);  // warm-up
+                float t = 0.f;
+                for (u32 k = 0; k < reps; ++k) {
+                    cudaEventRecord(e0, st);
+                    launch_fused(A, st, FUSED_VARIANTS[i]);
+                    cudaEventRecord(e1, st);
+                    cudaEventSynchronize(e1);
+                    float m = 0.f;
+                    cudaEventElapsedTime(&m, e0, e1);
+                    t += m;
+                }
+                ms[c][order][i] = t / (float)reps;
+            }
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (!r) {
+        for (int c = 0; c < NCLASS; ++c) {
+            if (s->cls_off[c + 1] <= s->cls_off[c]) continue;
+            int bo = 1, bi = 0;
+            for (int o = 0; o < 2; ++o)
+                for (int i = 0; i < 3; ++i)
+                    if (ms[c][o][i] < ms[c][bo][bi]) { bo = o; bi = i; }
+            s->cls_morton[c] = bo;
+            s->cls_variant[c] = FUSED_VARIANTS[bi];
+        }
+        r = compute_order(s);
+    }
+    YS_CK(cudaGetLastError());
+    YS_CK(cudaMemcpyAsync(s->counters.p, saved, sizeof(saved), cudaMemcpyHostToDevice, st));
+    YS_CK(cudaStreamSynchronize(st));
+    s->record = rec;
+    drop_graphs(s);
+    if (r) return r;
+    if (nclasses) *nclasses = NCLASS;
+    for (int c = 0; c < NCLASS && out && (u32)c < cap; ++c) {
+        ys_fused_class& o = out[c];
+        memset(&o, 0, sizeof(o));
+        o.max_mesh_vertices = CLASS_MAX[c];
+        o.meshes = s->cls_meshes[c];
+        o.vertices = s->cls_off[c + 1] - s->cls_off[c];
+        o.ctas_per_sm = s->cls_variant[c];
+        o.morton_order = s->cls_morton[c];
+        for (int k = 0; k < 2; ++k)
+            for (int i = 0; i < 3; ++i) o.ms[k][i] = ms[c][k][i];
+    }
     return YS_OK;
 }
 

@@ -114,6 +114,23 @@ class Scene:
         _lib.check(self.lib.ys_scene_autotune(self.h, reps, C.byref(chosen), ms), "ys_scene_autotune")
         return chosen.value, list(ms)
 
+    def autotune_classes(self, reps: int = 5):
+        """Per size class of the working meshes, the fastest (register-cap
+        variant, thread order) on the current state (the scene does not
+        advance): a list of dicts for the non-empty classes."""
+        out = (_lib.FusedClass * 4)()
+        n = C.c_uint32()
+        _lib.check(self.lib.ys_scene_autotune_classes(self.h, reps, out, 4, C.byref(n)), "ys_scene_autotune_classes")
+        res = []
+        for c in out[: n.value]:
+            if c.vertices == 0:
+                continue
+            res.append({"max_mesh_vertices": int(c.max_mesh_vertices), "meshes": int(c.meshes),
+                        "vertices": int(c.vertices), "ctas_per_sm": int(c.ctas_per_sm),
+                        "thread_order": "morton" if c.morton_order else "vertex",
+                        "ms": {"vertex": [float(v) for v in c.ms[0]], "morton": [float(v) for v in c.ms[1]]}})
+        return res
+
     def set_collider(self, mesh: int, kind: int, center, half=(0.0, 0.0, 0.0), q=(1.0, 0.0, 0.0, 0.0)):
         """Analytic collider kind and pose of a mesh (before pack: declares
         it; after: moves it from the next frame on)."""
