@@ -23,6 +23,12 @@ the external-force buffer from pinned host memory (applyEnvironmentForces'
 output) and reads the positions back into pinned host memory.
 Multi-GPU: replicas only (one independent cloth per rank, no collective on the
 data path); value sums the ranks' substeps over the slowest rank's time.
+
+The line also carries, measured in the same run: batched vs plain (C4, 256
+instances), the adjoint (C5), the tree builders on the C2 cloth, C1 over
+analytic colliders, C2 with BVH self rows, and the collision microbenchmark
+(C3: LBVH and spatial hash at 1M / 4M / 16M triangles, face-face hash on the
+C2 geometry).  --no-batched / --no-adjoint / --no-collide leave those out.
 """
 from __future__ import annotations
 
@@ -69,6 +75,8 @@ def parse():
     ap.add_argument("--P", type=int, default=512)
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-vs-plain (C4) object")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint (C5) object")
+    ap.add_argument("--no-collide", action="store_true",
+                    help="skip the collision microbenchmark (C3: 1M / 4M / 16M triangles) object")
     ap.add_argument("--instances", type=int, default=256)
     ap.add_argument("--workload", choices=["cloth", "collide", "batched", "adjoint"], default="cloth",
                     help="cloth: the headline substep benchmark; collide: the LBVH / spatial-hash microbenchmark; "
@@ -151,6 +159,17 @@ class ClockSampler:
     def _read(self):
         for line in self.proc.stdout:
             self.lines.append(line.strip())
+
+    def count(self) -> int:
+        return len(self.lines)
+
+    def wait_samples(self, n: int, busy, timeout_s: float):
+        """Keep the GPU busy (busy()) until n samples have arrived or the
+        timeout passes: nvidia-smi takes a few hundred ms to start and then
+        samples every 200 ms, longer than a short timed region."""
+        t0 = time.time()
+        while self.proc and self.count() < n and time.time() - t0 < timeout_s:
+            busy()
 
     def stop(self):
         if not self.proc:
@@ -363,10 +382,17 @@ def run_ours(args, rank, world, local):
     starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
     ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
     sampler = ClockSampler(local)
+    def gpu_busy():  # L2-flush fills: load on the GPU without advancing the scene
+        with torch.cuda.stream(stream):
+            for _ in range(16):
+                flush.fill_(0.5)
+        torch.cuda.synchronize()
+
+    sampler.start()
+    sampler.wait_samples(1, gpu_busy, 10.0)
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
-    sampler.start()
     _lib_check = __import__("ysim_b200._lib", fromlist=["check"]).check
     # The substeps as the library runs them: one CUDA-graph launch each (the
     # flush before it keeps the GPU busy while the host enqueues, so no host
@@ -408,7 +434,10 @@ def run_ours(args, rank, world, local):
         ksteps += kper
     torch.cuda.synchronize()
     scene.sync()
+    sampler.wait_samples(sampler.count() + 2, gpu_busy, 3.0)
     clocks = sampler.stop()
+    clocks["window"] = ("nvidia-smi every 200 ms from its first sample before the timed substeps to two samples "
+                        "after them, the GPU kept busy by L2-flush fills outside the timed substeps")
     ms = sum(s_.elapsed_time(e_) for s_, e_ in zip(starts, ends))
     after = scene.totals()
     st = scene.stats()
@@ -502,13 +531,18 @@ def run_ours(args, rank, world, local):
                             if kind == "reference" else "CPU restatement)")
                          + "; single_thread_value: one more substep on one host thread"}
 
-    build = analytic = None
+    build = analytic = bvh_self = None
+    collide = []
     if rank == 0:
         m0 = spec.meshes[0]
         build = measure_build(scene.get("x")[: m0.nV], m0.facets, local)
         analytic = measure_analytic(local)
+        bvh_self = measure_bvh_self(args, spec, snap, local)
     batched = None if args.no_batched else measure_batched(args, rank, world, local)
     adjoint = None if (args.no_adjoint or rank != 0) else measure_adjoint(args, local)
+    if rank == 0 and not args.no_collide:
+        scene.close()  # room for the 16M-triangle microbenchmark
+        run_collide(args, collide.append)
 
     # launches in the timed loop: per substep the refit's leaf kernel, its
     # level kernels and its top-level kernel, and k_fused (one CUDA graph);
@@ -543,12 +577,52 @@ def run_ours(args, rank, world, local):
             "adjoint": adjoint,
             "tree_build": build,
             "analytic_colliders": analytic,
+            "c2_bvh_self": bvh_self,
+            "collide_c3": collide,
         }
         print(json.dumps(line), flush=True)
     scene.close()
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
+
+
+# ------------------------------------------------------------------ BVH self rows
+def measure_bvh_self(args, spec, snap, local, steps=20):
+    """C2 with BVH self rows (checkSelfCollisions, the reference's
+    YSIM_CPUSH_SELF=0 path) instead of the CPU-hash semantics, from the state
+    the headline's timed substeps started from: device-timed substeps/s of the
+    library's CUDA-graph substep (its own per-class autotune first)."""
+    import dataclasses
+    import torch
+    from ysim_b200 import _lib
+    from ysim_b200.scene import Scene
+    sp = dataclasses.replace(spec, params=dataclasses.replace(spec.params, self_mode=_lib.SELF_BVH))
+    s = Scene(sp, device=local)
+    try:
+        for k in ("x", "v", "xprev"):
+            s.set(k, snap[k])
+        s.step(1)  # frame-0 rebuild from the draped state
+        s.autotune_classes()
+        s.step(6)
+        stream = torch.cuda.ExternalStream(s.stream(), device=local)
+        s.sync()
+        before = s.totals()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        s.step(steps)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / steps
+        after = s.totals()
+        return {"workload": "C2 with BVH self rows, from the headline's first timed state", "steps": steps,
+                "substeps_per_s": 1000.0 / ms, "ms_per_substep": ms,
+                "candidate_rows_per_substep": (after[0] - before[0]) / steps,
+                "contacts_per_substep": (after[1] - before[1]) / steps, "flags": s.stats()["flags"],
+                "timing": "CUDA events around the substeps (graph replays, no L2 flush)"}
+    finally:
+        s.close()
 
 
 # ------------------------------------------------------------------ tree build
@@ -910,12 +984,16 @@ def run_batched(args, rank, world, local):
 
 
 # ------------------------------------------------------------------ collide
-def run_collide(args):
+def run_collide(args, emit=None):
     """Collision microbenchmark: N triangles (centroids U[0,1]^3, vertex
     offsets N(0, sigma^2), sigma log-normal around 1e-3) and N query points;
     LBVH build + refit + point query within h = 1e-3 against the spatial-hash
     broad phase (cell 2h).  Device-timed with CUDA events; the two candidate
-    sets are checked for equality on the device.  One JSON line per N."""
+    sets are checked for equality on the device.  One record per N (and one
+    for the face-face hash on the C2 geometry) to emit (printed as a JSON
+    line each by default)."""
+    if emit is None:
+        emit = lambda rec: print(json.dumps(rec), flush=True)  # noqa: E731
     import ctypes as C
     import torch
     from ysim_b200 import _lib, generators as G
@@ -993,21 +1071,29 @@ def run_collide(args):
                                             "leaves some leaves unreached and others reached twice"},
                 "timing": f"CUDA events, median of {reps}; calls include their host-side synchronisation; "
                           "LBVH times are for the reference split"}
-        print(json.dumps(line), flush=True)
+        emit(line)
         del dx, df, dq, v, pairs
-    run_face_face(args, lib, timed, dev, P)
+    torch.cuda.empty_cache()
+    run_face_face(args, lib, timed, dev, P, emit)
 
 
-def run_face_face(args, lib, timed, dev, P):
+def run_face_face(args, lib, timed, dev, P, emit):
     """The face-face spatial hash (the reference's SpatialHashing<METAL>
     broad phase) on the C2 geometry: the 512x512 cloth and the level-7
     icosphere as one packed scene, self rows on."""
     import ctypes as C
     import torch
-    from ysim_b200 import _lib, generators as G
-    from oracle import oracle as O
+    from ysim_b200 import _lib
     spec = spec_for(args)
-    x, so, fo, F, beh, shape = O.pack_meshes(spec.meshes)
+    # the packed scene arrays (Scene::pack): positions, per-mesh vertex and
+    # face offsets, facets with mesh-local ids, behaviours, shapes (meshes)
+    ms = spec.meshes
+    x = np.concatenate([np.asarray(m.x, np.float32) for m in ms])
+    so = np.concatenate([[0], np.cumsum([m.nV for m in ms])]).astype(np.uint32)
+    fo = np.concatenate([[0], np.cumsum([m.nF for m in ms])]).astype(np.uint32)
+    F = np.concatenate([np.asarray(m.facets, np.uint32) for m in ms])
+    beh = np.array([m.behavior for m in ms], np.uint32)
+    shape = np.zeros(len(ms), np.uint32)
     nF = len(F)
     cap = 64 * nF
     dx, dso, dF, dfo = dev(x.reshape(-1)), dev(so.view(np.int32)), dev(F.reshape(-1).view(np.int32)), dev(fo.view(np.int32))
@@ -1026,7 +1112,7 @@ def run_face_face(args, lib, timed, dev, P):
             "vertices": len(x), "margin": float(margin), "detect_ms": ms, "rows": int(cnt.item()),
             "entries": st[0], "cells": st[1], "candidate_pairs": st[2], "grid": [st[3], st[4], st[5]],
             "timing": "CUDA events around the whole detect (no host synchronisation inside), median of 10"}
-    print(json.dumps(line), flush=True)
+    emit(line)
 
 
 def main():
