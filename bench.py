@@ -78,9 +78,11 @@ def parse():
     ap.add_argument("--no-collide", action="store_true",
                     help="skip the collision microbenchmark (C3: 1M / 4M / 16M triangles) object")
     ap.add_argument("--instances", type=int, default=256)
-    ap.add_argument("--workload", choices=["cloth", "collide", "batched", "adjoint"], default="cloth",
+    ap.add_argument("--workload", choices=["cloth", "collide", "batched", "adjoint", "c2-kernels"], default="cloth",
                     help="cloth: the headline substep benchmark; collide: the LBVH / spatial-hash microbenchmark; "
-                         "batched / adjoint: that object of the headline line alone")
+                         "batched / adjoint: that object of the headline line alone; c2-kernels: the headline "
+                         "workload's kernels launched one by one for a profiler (pre-roll, --steps substeps "
+                         "without graphs, then one build of the cloth's tree with each builder)")
     ap.add_argument("--sizes", default="1000000,4000000,16000000")
     ap.add_argument("--fused-variant", type=int, choices=[8, 7, 4], default=None,
                     help="use this fused-kernel variant (CTAs per SM) instead of the autotuner's choice")
@@ -626,7 +628,7 @@ def measure_bvh_self(args, spec, snap, local, steps=20):
 
 
 # ------------------------------------------------------------------ tree build
-def measure_build(x, F, local, reps=10):
+def measure_build(x, F, local, reps=10, warm=3):
     """One full rebuild of a tree (scene box, Morton codes, radix sort, then
     Karras topology + bottom-up boxes, or the Apetrei one-pass build) through
     the standalone LBVH, on the cloth's positions at the end of the run;
@@ -644,7 +646,7 @@ def measure_build(x, F, local, reps=10):
         try:
             _lib.check(lib.ys_lbvh_set_builder(h, builder), "ys_lbvh_set_builder")
             times = []
-            for i in range(3 + reps):
+            for i in range(warm + reps):
                 e0 = torch.cuda.Event(enable_timing=True)
                 e1 = torch.cuda.Event(enable_timing=True)
                 torch.cuda.synchronize()
@@ -653,7 +655,7 @@ def measure_build(x, F, local, reps=10):
                                              len(F)), "ys_lbvh_build")
                 e1.record()
                 torch.cuda.synchronize()
-                if i >= 3:
+                if i >= warm:
                     times.append(e0.elapsed_time(e1))
             out[f"{name}_ms"] = float(np.median(times))
         finally:
@@ -1115,9 +1117,47 @@ def run_face_face(args, lib, timed, dev, P, emit):
     emit(line)
 
 
+def run_c2_kernels(args):
+    """The headline workload's kernels as separate launches, for a profiler's
+    launch list or a capture of one kernel: --preroll substeps (CUDA graphs),
+    then --steps substeps launched directly with CUDA events around the refit
+    and fused stages, then one standalone build of the cloth's tree with the
+    Karras and with the Apetrei builder.  Prints one JSON line."""
+    import ctypes as C
+    import torch
+    from ysim_b200 import _lib
+    from ysim_b200.scene import Scene
+    torch.cuda.set_device(0)
+    spec = spec_for(args)
+    scene = Scene(spec, device=0)
+    scene.step(args.preroll)
+    scene.autotune_classes()
+    if args.fused_variant:
+        scene.set_fused_variant(args.fused_variant)
+    scene.set_graphs(False)
+    _lib.check(scene.lib.ys_scene_set_timing(scene.h, 1), "set_timing")
+    t0 = scene.totals()
+    scene.step(args.steps)
+    scene.sync()
+    kt = (C.c_double * 4)()
+    _lib.check(scene.lib.ys_scene_kernel_times(scene.h, kt), "kernel_times")
+    t1 = scene.totals()
+    m0 = spec.meshes[0]
+    build = measure_build(scene.get("x")[: m0.nV], m0.facets, 0, reps=1, warm=0)
+    scene.close()
+    print(json.dumps({"workload": "C2 kernels, one by one", "preroll": args.preroll, "steps": args.steps,
+                      "refit_ms": kt[0] / max(kt[1], 1), "fused_ms": kt[2] / max(kt[3], 1),
+                      "rows_per_substep": (t1[0] - t0[0]) / max(args.steps, 1),
+                      "contacts_per_substep": (t1[1] - t0[1]) / max(args.steps, 1), "tree_build": build}), flush=True)
+
+
 def main():
     args = parse()
     rank, world, local = dist_env()
+    if args.workload == "c2-kernels":
+        if rank == 0:
+            run_c2_kernels(args)
+        return
     if args.workload == "collide":
         if rank == 0:
             run_collide(args)
