@@ -1143,8 +1143,9 @@ def run_c2_kernels(args):
     _lib.check(scene.lib.ys_scene_kernel_times(scene.h, kt), "kernel_times")
     t1 = scene.totals()
     m0 = spec.meshes[0]
-    build = measure_build(scene.get("x")[: m0.nV], m0.facets, 0, reps=1, warm=0)
-    scene.close()
+    x = scene.get("x")[: m0.nV]
+    scene.close()  # the builds run with the scene's memory released
+    build = measure_build(x, m0.facets, 0, reps=1, warm=0)
     print(json.dumps({"workload": "C2 kernels, one by one", "preroll": args.preroll, "steps": args.steps,
                       "refit_ms": kt[0] / max(kt[1], 1), "fused_ms": kt[2] / max(kt[3], 1),
                       "rows_per_substep": (t1[0] - t0[0]) / max(args.steps, 1),
