@@ -233,7 +233,8 @@ def measured_traffic(args):
     return {"k_fused": d.get("k_fused"), "refit": d.get("refit"),
             "k_fused_warp_instructions": d.get("k_fused_warp_instructions"),
             "k_fused_threads_per_instruction": d.get("k_fused_threads_per_instruction"),
-            "source": "ncu capture, profiles/traffic_c2_tricloth512.json (" + d.get("command", "") + ")"}
+            "source": "ncu captures of this workload in the contact phase: profiles/traffic_c2_tricloth512.json ("
+                      + d.get("source", "") + ")"}
 
 
 def measured_peak():
