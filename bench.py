@@ -1044,10 +1044,14 @@ def run_collide(args, emit=None):
         query_ms = timed(lambda: _lib.check(lib.ys_lbvh_query(t, P(dq), len(q), h, 0, P(pairs), cap, P(cnt))), reps)
         nb = int(cnt.item())
         key_ref = keys(nb)
-        # the same tree with the (code, index) split: one parent per node
+        # the same tree with the (code, index) split: one parent per node,
+        # every internal box the union of a sorted-leaf range (range refit)
         _lib.check(lib.ys_lbvh_set_split(t, 1))
+        cbuild_ms = timed(lambda: _lib.check(lib.ys_lbvh_build(t, P(dx), len(x), P(df), n)), reps)
+        crefit_ms = timed(lambda: _lib.check(lib.ys_lbvh_refit(t, P(dx), P(v), np.float32(1e-3), 1)), reps)
         _lib.check(lib.ys_lbvh_build(t, P(dx), len(x), P(df), n))
-        _lib.check(lib.ys_lbvh_query(t, P(dq), len(q), h, 0, P(pairs), cap, P(cnt)))
+        cquery_ms = timed(lambda: _lib.check(lib.ys_lbvh_query(t, P(dq), len(q), h, 0, P(pairs), cap, P(cnt))),
+                          reps)
         nc = int(cnt.item())
         key_b = keys(nc)
         _lib.check(lib.ys_lbvh_destroy(t), "lbvh_destroy")
@@ -1068,6 +1072,10 @@ def run_collide(args, emit=None):
                 "shash_build_ms": sh_build_ms, "shash_query_ms": sh_query_ms, "candidates": ns,
                 "shash_entries": ent.value, "shash_oversized": big.value, "candidate_sets_equal": same,
                 "equality": "spatial hash vs LBVH with the (code, index) split, as sets and counts",
+                "consistent_split": {"lbvh_build_ms": cbuild_ms, "lbvh_refit_swept_ms": crefit_ms,
+                                     "lbvh_query_ms": cquery_ms,
+                                     "refit": "sorted-leaf ranges: a leaf pass with block boxes, then the nodes "
+                                              "whose range crosses a 256-leaf block (no climb)"},
                 "reference_split": {"candidates": nb, "duplicates": nb - int(ref_unique.numel()),
                                     "missing": ref_missing,
                                     "note": "the reference's midpoint split of runs of >= 3 equal Morton codes "

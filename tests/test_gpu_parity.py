@@ -591,3 +591,51 @@ def test_wide_refit_boxes_are_exact(cuda_lib):
         assert s.stats()["flags"] == 0
     finally:
         s.close()
+
+
+@pytest.mark.parametrize("case", ["soup", "big_soup", "grid", "tiny1", "tiny2", "dups"])
+def test_consistent_lbvh_range_refit_is_the_bottom_up_refit(cuda_lib, case):
+    """With the (code, index) split the standalone LBVH refits by sorted-leaf
+    ranges (leaf pass with block boxes, then the nodes whose range crosses a
+    256-leaf block): after the build and after a swept refit, every leaf box is
+    its face's box (float32, as buildSweptLeaf_Tri computes it) and every
+    internal box the union of its two children's, bit for bit."""
+    from ysim_b200 import _lib, generators as G
+    if case in ("soup", "big_soup"):
+        x, f, _ = G.soup(50_000 if case == "soup" else 300_000, seed=5)
+    elif case == "grid":
+        x, f = G.grid_cloth(65, 1.0, (0.0, 0.5, 0.0))
+    elif case == "tiny1":
+        x, f, _ = G.soup(1, seed=6, nq=5)
+    elif case == "tiny2":
+        x, f, _ = G.soup(2, seed=7, nq=5)
+    else:
+        x, f, _ = G.soup(3000, seed=8)
+        x = np.tile(x[:3], (3000, 1)).astype(np.float32)
+    h, dx, df = _lbvh(cuda_lib, x, f, consistent=True)
+    try:
+        n = len(f)
+
+        def check(v, dt):
+            nodes, parent, _, idx = tree_arrays(cuda_lib, h)
+            p = x[f[idx]]
+            if v is None:
+                lo, hi = p.min(1), p.max(1)
+            else:
+                sp = (p + (v[f[idx]] * np.float32(dt)).astype(np.float32)).astype(np.float32)
+                lo, hi = np.minimum(p, sp).min(1), np.maximum(p, sp).max(1)
+            leaves = nodes[n - 1:]
+            assert np.array_equal(leaves["mn"], lo) and np.array_equal(leaves["mx"], hi)
+            inner = nodes[: n - 1]
+            a, b = inner["a"], inner["b"]
+            assert np.array_equal(inner["mn"], np.minimum(nodes["mn"][a], nodes["mn"][b]))
+            assert np.array_equal(inner["mx"], np.maximum(nodes["mx"][a], nodes["mx"][b]))
+            assert reachable(nodes).all()
+
+        check(None, 0.0)
+        v = np.random.default_rng(1).normal(0, 1.0, x.shape).astype(np.float32)
+        dv = _dev(v.reshape(-1))
+        _lib.check(cuda_lib.ys_lbvh_refit(h, _p(dx), _p(dv), np.float32(1.0 / 1200), 1))
+        check(v, 1.0 / 1200)
+    finally:
+        _lib.check(cuda_lib.ys_lbvh_destroy(h))

@@ -62,6 +62,13 @@ struct ys_lbvh {
     QueryOrder qorder;        // Morton order of large query sets
     int builder = YS_BUILD_KARRAS;  // ys_lbvh_set_builder
     void* aggScratch = nullptr;     // Apetrei range ends and root slot
+    // range refit of a consistent Karras tree: per internal node its
+    // sorted-leaf range, the nodes whose range leaves their block, block boxes
+    uint2* range = nullptr;
+    u32 *big = nullptr, *huge = nullptr, *bcount = nullptr;
+    Node *bb16 = nullptr, *bb256 = nullptr;
+    u32 nbig = 0, nhuge = 0;
+    bool ranged = false;            // the last build recorded ranges (consistent Karras split)
 };
 
 #define YS_CK2(call)                                                                                   \
@@ -94,6 +101,12 @@ ys_status ys_lbvh_create(ys_lbvh** out, uint32_t maxPrims, int device, void* str
     if (e == cudaSuccess) e = cudaMalloc((void**)&t->status, 4);
     if (e == cudaSuccess) e = cudaMalloc(&t->scratch, sort_scratch_bytes(maxPrims));
     if (e == cudaSuccess) e = cudaMalloc((void**)&t->job, sizeof(RefitJob));
+    if (e == cudaSuccess) e = cudaMalloc((void**)&t->range, (size_t)maxPrims * sizeof(uint2));
+    if (e == cudaSuccess) e = cudaMalloc((void**)&t->big, (size_t)maxPrims * 4);
+    if (e == cudaSuccess) e = cudaMalloc((void**)&t->huge, (size_t)maxPrims * 4);
+    if (e == cudaSuccess) e = cudaMalloc((void**)&t->bcount, 8);
+    if (e == cudaSuccess) e = cudaMalloc((void**)&t->bb16, ((size_t)maxPrims / 16 + 1) * sizeof(Node));
+    if (e == cudaSuccess) e = cudaMalloc((void**)&t->bb256, ((size_t)maxPrims / 256 + 1) * sizeof(Node));
     // completed before this returns: later launches may go to any stream,
     // including non-blocking ones that do not wait for the legacy stream
     if (e == cudaSuccess) e = cudaMemsetAsync(t->status, 0, 4, 0);
@@ -112,6 +125,7 @@ ys_status ys_lbvh_destroy(ys_lbvh* t) {
     cudaStreamSynchronize(t->stream);
     cudaFree(t->nodes); cudaFree(t->parent); cudaFree(t->claimOff); cudaFree(t->claims); cudaFree(t->karrasScratch); cudaFree(t->aggScratch); cudaFree(t->codes); cudaFree(t->idx); cudaFree(t->visits);
     cudaFree(t->box); cudaFree(t->status); cudaFree(t->scratch); cudaFree(t->job);
+    cudaFree(t->range); cudaFree(t->big); cudaFree(t->huge); cudaFree(t->bcount); cudaFree(t->bb16); cudaFree(t->bb256);
     query_order_free(t->qorder);
     delete t;
     return YS_OK;
@@ -123,6 +137,16 @@ static ys_status run_refit(ys_lbvh* t, const float* x, const float* v, float dt,
     J.nodes = t->nodes; J.parent = t->parent; J.claimOff = t->claimOff; J.claims = t->claims; J.visits = t->visits; J.facets = t->facets;
     J.x3 = x; J.v3 = v; J.voff = 0; J.n = t->n; J.leafBase = 0; J.dt = dt; J.swept = swept ? 1u : 0u;
     J.selfMargin = 0.f; J.maxExt = t->box;
+    if (t->ranged) {
+        // consistent tree: every internal box is the union of its sorted-leaf
+        // range, from the leaf pass's block boxes (no climb)
+        J.bb16 = t->bb16;
+        J.bb256 = t->bb256;
+        launch_refit_bin(J, t->range, t->big, t->nbig, t->huge, t->nhuge, t->stream);
+        YS_CK2(cudaGetLastError());
+        YS_CK2(cudaStreamSynchronize(t->stream));
+        return YS_OK;
+    }
     YS_CK2(cudaMemcpyAsync(t->job, &J, sizeof(J), cudaMemcpyHostToDevice, t->stream));
     launch_refit(t->job, 1, t->n, t->status, t->stream);
     YS_CK2(cudaGetLastError());
@@ -152,6 +176,7 @@ ys_status ys_lbvh_build(ys_lbvh* t, const float* x, uint32_t nV, const uint32_t*
     launch_box(nullptr, x, 0, nV, t->box, t->stream);
     launch_morton(nullptr, x, 0, F, nF, t->box, t->codes, t->idx, t->stream);
     YS_CK2(radix_sort_pairs(t->codes, t->idx, nF, t->scratch, 0, 32, t->stream));
+    t->ranged = false;
     if (t->builder == YS_BUILD_APETREI) {
         // topology and boxes in one pass: no refit afterwards
         YS_CK2(launch_apetrei(nullptr, x, 0, F, t->codes, t->idx, nF, t->nodes, t->parent, t->claimOff, t->claims,
@@ -159,9 +184,21 @@ ys_status ys_lbvh_build(ys_lbvh* t, const float* x, uint32_t nV, const uint32_t*
         YS_CK2(cudaStreamSynchronize(t->stream));
         return YS_OK;
     }
+    BinRanges R;
+    if (t->consistent) {  // one parent per node: boxes are unions of contiguous sorted-leaf ranges
+        R.range = t->range; R.big = t->big; R.huge = t->huge; R.count = t->bcount;
+    }
     YS_CK2(launch_karras(t->codes, t->idx, nF, t->nodes, t->parent, t->claimOff, t->claims, t->visits,
-                         t->karrasScratch, t->stream, t->consistent));
+                         t->karrasScratch, t->stream, t->consistent, R));
     YS_CK2(cudaGetLastError());
+    if (t->consistent) {
+        u32 cnt[2] = {0, 0};
+        YS_CK2(cudaMemcpyAsync(cnt, t->bcount, 8, cudaMemcpyDeviceToHost, t->stream));
+        YS_CK2(cudaStreamSynchronize(t->stream));
+        t->nbig = cnt[0];
+        t->nhuge = cnt[1];
+        t->ranged = true;
+    }
     return run_refit(t, x, nullptr, 0.f, 0);
 }
 

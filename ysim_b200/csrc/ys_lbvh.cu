@@ -178,7 +178,7 @@ __global__ void k_claim_fill(const Node* __restrict__ nodes, u32 nInner, u32* __
 __global__ void __launch_bounds__(256) k_karras(const u32* __restrict__ codes, const u32* __restrict__ idx, u32 n,
                                                 Node* __restrict__ nodes, i32* __restrict__ parent,
                                                 u32* __restrict__ claimCount, u32* __restrict__ visits,
-                                                int consistent) {
+                                                int consistent, BinRanges R) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= (int)n) return;
     KarrasView K{codes, idx, (int)n};
@@ -230,15 +230,39 @@ __global__ void __launch_bounds__(256) k_karras(const u32* __restrict__ codes, c
     atomicAdd(&claimCount[ca], 1u);
     atomicMax(&parent[cb], i);
     atomicAdd(&claimCount[cb], 1u);
+    if (R.range) {
+        // sorted-leaf range of node i (one end is leaf i); nodes whose range
+        // leaves i's 256-leaf block go to the big / huge lists
+        R.range[i] = make_uint2((u32)first, (u32)last);
+        const bool out = ((u32)first >> 8) != ((u32)last >> 8);
+        const bool huge = out && (u32)(last - first) >= BIN_RANGE_HUGE;
+        const unsigned act = __activemask();
+        const unsigned mb = __ballot_sync(act, out && !huge), mh = __ballot_sync(act, huge);
+        const u32 lane = threadIdx.x & 31u, lead = (u32)__ffs(act) - 1u;
+        u32 bb = 0, bh = 0;
+        if (lane == lead) {
+            if (mb) bb = atomicAdd(&R.count[0], (u32)__popc(mb));
+            if (mh) bh = atomicAdd(&R.count[1], (u32)__popc(mh));
+        }
+        bb = __shfl_sync(act, bb, (int)lead);
+        bh = __shfl_sync(act, bh, (int)lead);
+        const unsigned below = (1u << lane) - 1u;
+        if (out && !huge) R.big[bb + (u32)__popc(mb & below)] = (u32)i;
+        if (huge) R.huge[bh + (u32)__popc(mh & below)] = (u32)i;
+    }
 }
 
 size_t karras_scratch_bytes(u32 n) { return scan_scratch_bytes(n ? 2 * n : 1); }
 
 cudaError_t launch_karras(const u32* codes, const u32* idx, u32 n, Node* nodes, i32* parent, u32* claimOff,
-                          i32* claims, u32* visits, void* scratch, cudaStream_t s, bool consistent) {
+                          i32* claims, u32* visits, void* scratch, cudaStream_t s, bool consistent, BinRanges R) {
     if (n == 0) return cudaSuccess;
     k_parent_init<<<ceil_div(2 * n, 256), 256, 0, s>>>(parent, claimOff, 2 * n - 1);
-    k_karras<<<ceil_div(n, 256), 256, 0, s>>>(codes, idx, n, nodes, parent, claimOff, visits, consistent ? 1 : 0);
+    if (R.range) {
+        cudaError_t e0 = cudaMemsetAsync(R.count, 0, 8, s);
+        if (e0 != cudaSuccess) return e0;
+    }
+    k_karras<<<ceil_div(n, 256), 256, 0, s>>>(codes, idx, n, nodes, parent, claimOff, visits, consistent ? 1 : 0, R);
     cudaError_t e = exclusive_scan(claimOff, 2 * n, scratch, s);
     if (e != cudaSuccess) return e;
     if (n > 1) k_claim_fill<<<ceil_div(n - 1, 256), 256, 0, s>>>(nodes, n - 1, claimOff, claims);
@@ -729,6 +753,127 @@ cudaError_t launch_range_lists(const RefitJob* jobsDev, u32 numJobs, u32 totalLe
     k_range_records<<<grid, 256, 0, s>>>(jobsDev, numJobs, totalLeaves, blkCnt, blkOff, blkEnt, big, bigCap, bigCnt,
                                          1);
     return cudaGetLastError();
+}
+
+// ---- range refit of a consistent binary tree (the standalone LBVH)
+// Leaf pass: thread i is sorted leaf i (leaf node n - 1 + i, face in .b);
+// its swept or static box goes to the leaf node, the block's 16- and
+// 256-leaf boxes to bb16 / bb256, and internal node i (whose range has leaf
+// i at one end) gets its box here when its range stays in the block.
+__global__ void __launch_bounds__(256) k_refit_bin_leaves(RefitJob J, const uint2* __restrict__ range) {
+    __shared__ float sh_leaf[6][256];
+    __shared__ float sh_g16[6][16];
+    __shared__ float sh_box[8][6];
+    const u32 n = J.n;
+    const u32 i0 = blockIdx.x * 256u, i = i0 + threadIdx.x;
+    const bool has = i < n;
+    const u32 li = has ? i : n - 1;
+    Node* nodes = J.nodes;
+    const u32 f = (u32)__ldcg(&nodes[n - 1 + li].b);
+    f3 lo, hi;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const u32 gv = J.voff + J.facets[3 * f + k];
+        const f3 p = J.x4 ? ld(J.x4, gv) : ldp(J.x3, gv);
+        f3 a = p, b = p;
+        if (J.swept) {
+            const f3 vv = J.v4 ? ld(J.v4, gv) : ldp(J.v3, gv);
+            const f3 sp = p + vv * J.dt;
+            a = vmin(p, sp);
+            b = vmax(p, sp);
+        }
+        if (k == 0) { lo = a; hi = b; } else { lo = vmin(lo, a); hi = vmax(hi, b); }
+    }
+    if (has) store_box(&nodes[n - 1 + i], lo, hi);
+    const float inf = __int_as_float(0x7F800000);
+    float v[6] = {has ? lo.x : inf, has ? lo.y : inf, has ? lo.z : inf,
+                  has ? hi.x : -inf, has ? hi.y : -inf, has ? hi.z : -inf};
+#pragma unroll
+    for (int k = 0; k < 6; ++k) sh_leaf[k][threadIdx.x] = v[k];
+    const u32 lane = threadIdx.x & 31u;
+#pragma unroll
+    for (int off = 8; off >= 1; off >>= 1) {
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            v[k] = fminf(v[k], __shfl_xor_sync(0xFFFFFFFFu, v[k], off));
+            v[3 + k] = fmaxf(v[3 + k], __shfl_xor_sync(0xFFFFFFFFu, v[3 + k], off));
+        }
+    }
+    if ((lane & 15u) == 0) {
+        store_box(J.bb16 + (i >> 4), mk(v[0], v[1], v[2]), mk(v[3], v[4], v[5]));
+#pragma unroll
+        for (int k = 0; k < 6; ++k) sh_g16[k][threadIdx.x >> 4] = v[k];
+    }
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        v[k] = fminf(v[k], __shfl_xor_sync(0xFFFFFFFFu, v[k], 16));
+        v[3 + k] = fmaxf(v[3 + k], __shfl_xor_sync(0xFFFFFFFFu, v[3 + k], 16));
+    }
+    if (lane == 0)
+        for (int k = 0; k < 6; ++k) sh_box[threadIdx.x >> 5][k] = v[k];
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (u32 w = 1; w < 8; ++w)
+            for (int k = 0; k < 3; ++k) {
+                v[k] = fminf(v[k], sh_box[w][k]);
+                v[3 + k] = fmaxf(v[3 + k], sh_box[w][3 + k]);
+            }
+        store_box(J.bb256 + (i0 >> 8), mk(v[0], v[1], v[2]), mk(v[3], v[4], v[5]));
+    }
+    if (i + 1 >= n) return;  // no internal node i
+    const uint2 r = range[i];
+    if ((r.x >> 8) != (i0 >> 8) || (r.y >> 8) != (i0 >> 8) || r.x > r.y) return;  // a big node
+    float b[6] = {inf, inf, inf, -inf, -inf, -inf};
+    const u32 L = r.x - i0, e = r.y - i0 + 1;
+    u32 s16 = (L + 15u) & ~15u, e16 = e & ~15u;
+    if (s16 >= e16) { s16 = e; e16 = e; }
+    for (u32 l = L; l < s16; ++l)
+#pragma unroll
+        for (int k = 0; k < 3; ++k) { b[k] = fminf(b[k], sh_leaf[k][l]); b[3 + k] = fmaxf(b[3 + k], sh_leaf[3 + k][l]); }
+    for (u32 q = s16 >> 4; q < (e16 >> 4); ++q)
+#pragma unroll
+        for (int k = 0; k < 3; ++k) { b[k] = fminf(b[k], sh_g16[k][q]); b[3 + k] = fmaxf(b[3 + k], sh_g16[3 + k][q]); }
+    for (u32 l = e16; l < e; ++l)
+#pragma unroll
+        for (int k = 0; k < 3; ++k) { b[k] = fminf(b[k], sh_leaf[k][l]); b[3 + k] = fmaxf(b[3 + k], sh_leaf[3 + k][l]); }
+    store_box(&nodes[i], mk(b[0], b[1], b[2]), mk(b[3], b[4], b[5]));
+}
+
+// Big nodes (ranges across blocks): 8 lanes per node of big, then a block
+// per node of huge (ranges of BIN_RANGE_HUGE leaves or more).
+__global__ void __launch_bounds__(256) k_refit_bin_ranges(RefitJob J, const uint2* __restrict__ range,
+                                                          const u32* __restrict__ big, u32 nbig,
+                                                          const u32* __restrict__ huge, u32 nhuge) {
+    const u32 medBlocks = (nbig + 31) / 32;
+    if (blockIdx.x < medBlocks) {
+        const u32 grp = (blockIdx.x * blockDim.x + threadIdx.x) >> 3;
+        u32 node = 0;
+        uint2 r = make_uint2(1u, 0u);  // empty
+        if (grp < nbig) {
+            node = big[grp];
+            r = range[node];
+        }
+        f3 lo, hi;
+        range_union_group<8>(J, r.x, r.y, threadIdx.x & 7u, lo, hi);
+        if ((threadIdx.x & 7u) == 0 && r.x <= r.y) store_box(&J.nodes[node], lo, hi);
+        return;
+    }
+    const u32 b = blockIdx.x - medBlocks;
+    if (b >= nhuge) return;
+    const u32 node = huge[b];
+    const uint2 r = range[node];
+    if (r.x > r.y || r.y >= J.n) return;  // uniform over the block
+    f3 lo, hi;
+    range_union_block(J, r.x, r.y, lo, hi);
+    if (threadIdx.x == 0) store_box(&J.nodes[node], lo, hi);
+}
+
+void launch_refit_bin(const RefitJob& J, const uint2* range, const u32* big, u32 nbig, const u32* huge, u32 nhuge,
+                      cudaStream_t s) {
+    if (J.n == 0) return;
+    k_refit_bin_leaves<<<ceil_div(J.n, 256), 256, 0, s>>>(J, range);
+    const u32 blocks = (nbig + 31) / 32 + nhuge;
+    if (blocks) k_refit_bin_ranges<<<blocks, 256, 0, s>>>(J, range, big, nbig, huge, nhuge);
 }
 
 void launch_refit_ranges(const RefitJob* jobsDev, u32 numJobs, const uint4* big, u32 bigCap, u32 nmed, u32 nhuge,

@@ -120,8 +120,26 @@ void launch_morton(const float4* x4, const float* x3, u32 voff, const u32* facet
 // determineRange already orders them by, so every node has one parent (the
 // cube layout); false keeps the reference's midpoint split.
 size_t karras_scratch_bytes(u32 n);
+// Optional outputs of a Karras build for the range refit of a consistent
+// tree: per internal node its sorted-leaf range, and the nodes whose range
+// leaves the 256-leaf block of their own index, in big (ranges under
+// BIN_RANGE_HUGE leaves, count[0]) or huge (count[1]); both lists need n
+// entries.  range = null: none.
+static constexpr u32 BIN_RANGE_HUGE = 16384;
+struct BinRanges {
+    uint2* range = nullptr;
+    u32* big = nullptr;
+    u32* huge = nullptr;
+    u32* count = nullptr;
+};
 cudaError_t launch_karras(const u32* codes, const u32* idx, u32 n, Node* nodes, i32* parent, u32* claimOff,
-                          i32* claims, u32* visits, void* scratch, cudaStream_t s, bool consistent = false);
+                          i32* claims, u32* visits, void* scratch, cudaStream_t s, bool consistent = false,
+                          BinRanges R = BinRanges());
+// Range refit of a consistent binary tree built with BinRanges (J: nodes,
+// facets, positions (and velocities when swept), n; bb16 / bb256 with
+// n / 16 + 1 and n / 256 + 1 boxes): leaf pass, then the big and huge nodes.
+void launch_refit_bin(const RefitJob& J, const uint2* range, const u32* big, u32 nbig, const u32* huge, u32 nhuge,
+                      cudaStream_t s);
 // Apetrei build (agglomerativeBuild_Tri + agglomerativeSwapRoot,
 // bvh.metal:884-1199) of sorted (code, index) pairs: topology, leaf boxes
 // from the current positions and every internal box in one pass, the root
