@@ -76,6 +76,10 @@ struct StepArgs {
     // start of the substep, the mesh-local vertex id in w (written by the
     // refit's leaf pass, or at the build of a tree that is never refit)
     const float4* fpos;
+    // per vertex, its own faces (the faces holding it) as two windows of 8
+    // face ids: x = first id of window A, y = (B - A) << 16 | mask B << 8 |
+    // mask A; a vertex whose faces do not fit has both masks 0
+    const uint2* own;
     const Node* nodes;
     const Wide4* w4;  // 4-wide form of the trees (wide != 0)
     u32 wide;
@@ -345,6 +349,12 @@ __global__ void __launch_bounds__(128, MINB) k_fused(StepArgs A) {
     const f3 xpv = query ? ld(A.xp, g) : xc;
     const float mg = A.margin;
     u32 st = 0, rows = 0;
+    // own faces of this vertex: never a self row, dropped before the queue
+    const uint2 ownw = (query && A.own) ? A.own[g] : make_uint2(0u, 0u);
+    auto own_face = [&](u32 f) -> bool {
+        const u32 da = f - ownw.x, db = da - (ownw.y >> 16);
+        return (da < 8u && ((ownw.y >> da) & 1u)) || (db < 8u && ((ownw.y >> (8u + db)) & 1u));
+    };
 
     // ---- descent state: the own tree first (set up here), then the targets
     int stack[STACK_DEPTH];
@@ -513,8 +523,12 @@ __global__ void __launch_bounds__(128, MINB) k_fused(StepArgs A) {
                     sp = 0;
                 } else {
                     const int w = pop();
-                    if (w >= 0 && (u32)w < nn)
-                        st |= wide_step_p(wn, w, qmn, qmx, push, [&](int s, u32 f) { lf[s] = (int)f; });
+                    if (w >= 0 && (u32)w < nn) {
+                        const bool selfTree = (key & KEY_SELF) != 0;
+                        st |= wide_step_p(wn, w, qmn, qmx, push, [&](int s, u32 f) {
+                            if (!(selfTree && own_face(f))) lf[s] = (int)f;
+                        });
+                    }
                 }
             }
 #pragma unroll
@@ -533,7 +547,7 @@ __global__ void __launch_bounds__(128, MINB) k_fused(StepArgs A) {
                         if (overlap(qmn, qmx, n0, n1)) {
                             const int a = __float_as_int(n0.w), b = __float_as_int(n1.w);
                             if (a < 0) {
-                                leaf = b;
+                                if (!((key & KEY_SELF) && own_face((u32)b))) leaf = b;
                             } else if (sp + 2 > STACK_DEPTH) {
                                 st |= ST_STACK_OVF;
                             } else {
@@ -992,6 +1006,7 @@ struct ys_scene {
     DBuf<uint4> F4;
     DBuf<u32> F3;  // packed facets (3 per face) for the refit kernel
     DBuf<float4> fpos;  // per face: its three vertex positions (id in w), for the fused kernel's tests
+    DBuf<uint2> own;    // per vertex: its own faces as two 8-face windows (StepArgs::own)
     DBuf<Node> nodes;
     DBuf<i32> parent, claims;        // largest claimant per node; claimant lists (offset node_off)
     DBuf<u32> claimOff;              // per mesh 2N entries at node_off + mesh index
@@ -1107,6 +1122,7 @@ StepArgs make_args(ys_scene* s) {
     A.targets = s->targets.p;
     A.F = s->F4.p;
     A.fpos = s->fpos.p;
+    A.own = s->own.p;
     A.nodes = s->nodes.p;
     A.w4 = s->w4.p;
     A.wide = s->tree_layout == YS_TREE_CUBE ? 1u : 0u;
@@ -1633,7 +1649,7 @@ ys_status ys_scene_destroy(ys_scene* s) {
     s->scanScratch.free(); s->rows.free(); s->contacts.free(); s->csr.free(); s->pool.free(); s->bucket.free();
     drop_graphs(s);
     s->csr_off.free(); s->vstart.free(); s->vcount.free(); s->ext.free();
-    s->fpos.free(); s->bb16.free(); s->bb256.free(); s->wrange.free(); s->blkEnt.free(); s->bigEnt.free();
+    s->fpos.free(); s->own.free(); s->bb16.free(); s->bb256.free(); s->wrange.free(); s->blkEnt.free(); s->bigEnt.free();
     s->blkCnt.free(); s->blkOff.free(); s->bigCnt.free(); s->rangeScratch.free(); s->vorder.free(); s->okeys.free(); s->oaoff.free(); s->orank.free(); s->obox.free(); s->oscratch.free(); s->omorton.free();
     for (auto e : s->evPool) cudaEventDestroy(e);
     cudaStreamDestroy(s->stream);
@@ -1762,6 +1778,24 @@ ys_status ys_scene_pack(ys_scene* s) {
     }
     spr_off[nV] = (u32)spr_nbr.size();
     vaf_off[nV] = (u32)vaf.size();
+    // own-face windows: a vertex's faces, sorted, in at most two runs of 8
+    // ids each (a grid cloth's vertex: the two cell rows around it)
+    std::vector<uint2> ownw(nV, make_uint2(0u, 0u));
+    for (u32 gv = 0; gv < nV; ++gv) {
+        std::vector<u32> fs(vaf.begin() + vaf_off[gv], vaf.begin() + vaf_off[gv + 1]);
+        if (fs.empty()) continue;
+        std::sort(fs.begin(), fs.end());
+        const u32 a = fs[0];
+        size_t k = 0;
+        u32 ma = 0, mb = 0, b = a;
+        while (k < fs.size() && fs[k] - a < 8u) ma |= 1u << (fs[k++] - a);
+        if (k < fs.size()) {
+            b = fs[k];
+            while (k < fs.size() && fs[k] - b < 8u) mb |= 1u << (fs[k++] - b);
+        }
+        if (k < fs.size() || b - a >= 65536u) continue;  // does not fit: no filtering for this vertex
+        ownw[gv] = make_uint2(a, ((b - a) << 16) | (mb << 8) | ma);
+    }
     cudaStream_t st = s->stream;
     // device allocations
     for (auto& b : s->X) YS_CK(b.alloc(nV));
@@ -1775,6 +1809,7 @@ ys_status ys_scene_pack(ys_scene* s) {
     YS_CK(s->codes.alloc(std::max(nF, 1u))); YS_CK(s->idx.alloc(std::max(nF, 1u))); YS_CK(s->visits.alloc(std::max(nF, 1u)));
     YS_CK(s->F4.alloc(std::max(nF, 1u))); YS_CK(s->F3.alloc(3 * (size_t)std::max(nF, 1u)));
     YS_CK(s->fpos.alloc(3 * (size_t)std::max(nF, 1u)));
+    YS_CK(s->own.alloc(std::max(nV, 1u)));
     YS_CK(s->nodes.alloc(std::max(nNodes, 1u))); YS_CK(s->parent.alloc(std::max(nNodes, 1u)));
     YS_CK(s->claims.alloc(std::max(nNodes, 1u)));
     YS_CK(s->claimOff.alloc((size_t)nNodes + s->meshes.size() + 1));
@@ -1815,6 +1850,7 @@ ys_status ys_scene_pack(ys_scene* s) {
         YS_CK(cudaMemcpyAsync(s->spr_rest.p, spr_rest.data(), 4 * spr_rest.size(), cudaMemcpyHostToDevice, s->stream)); YS_CK(cudaStreamSynchronize(s->stream));
     }
     YS_CK(cudaMemcpyAsync(s->vaf_off.p, vaf_off.data(), 4 * (size_t)(nV + 1), cudaMemcpyHostToDevice, s->stream)); YS_CK(cudaStreamSynchronize(s->stream));
+    YS_CK(cudaMemcpyAsync(s->own.p, ownw.data(), sizeof(uint2) * (size_t)nV, cudaMemcpyHostToDevice, s->stream)); YS_CK(cudaStreamSynchronize(s->stream));
     if (!vaf.empty()) YS_CK(cudaMemcpyAsync(s->vaf.p, vaf.data(), 4 * vaf.size(), cudaMemcpyHostToDevice, s->stream)); YS_CK(cudaStreamSynchronize(s->stream));
     if (nF) {
         YS_CK(cudaMemcpyAsync(s->F4.p, F4.data(), 16 * (size_t)nF, cudaMemcpyHostToDevice, s->stream)); YS_CK(cudaStreamSynchronize(s->stream));
