@@ -702,11 +702,14 @@ def measure_batched(args, rank, world, local, steps=100):
     """Batched vs plain (C4): the instances of this rank's shard (balanced by
     vertex count, generators.shard_instances) as ONE scene -- one refit and one fused launch per
     substep for all of them, replayed as a CUDA graph -- against the same
-    instances as one scene each, stepped one after the other from the host.
-    Batched is device-timed (CUDA events on its stream); plain is timed by the
-    host clock between full synchronisations, since its scenes run on their
-    own streams.  Both are the max over ranks; the whole batch advancing one
-    substep is one batch substep."""
+    instances as one scene each, in two ways: (1) every instance stepped
+    before the next substep, each scene on its own stream, so that their
+    kernels overlap on the GPU (host clock between full synchronisations);
+    (2) as the workload states it, each instance run through the plain path
+    on its own, one after another (each run device-timed on its stream, the
+    times summed).  Batched is device-timed (CUDA events on its stream).  All
+    are the max over ranks; the whole batch advancing one substep is one
+    batch substep."""
     import time
     import torch
     from ysim_b200 import generators as G
@@ -740,7 +743,7 @@ def measure_batched(args, rank, world, local, steps=100):
         ch = next((c for c in classes if nv <= c["max_mesh_vertices"]), None)
         q.set_fused_variant(ch["ctas_per_sm"] if ch else tuned)
         if ch:
-            q.set_thread_order(ch["thread_order"] == "morton")
+            q.set_thread_order(ch["thread_order"])
         q.step(20)
     for q in plain:
         q.sync()
@@ -755,6 +758,20 @@ def measure_batched(args, rank, world, local, steps=100):
         q.sync()
     torch.cuda.synchronize()
     p_ms = max_over_ranks((time.perf_counter() - t) * 1e3 / steps, world, device=f"cuda:{local}")
+    # the comparison as the workload states it: each instance run through the
+    # plain path on its own, one after another; each run device-timed on its
+    # scene's stream, the times summed
+    seq = 0.0
+    for q in plain:
+        qs = torch.cuda.ExternalStream(q.stream(), device=local)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        a.record(qs)
+        q.step(steps)
+        b.record(qs)
+        b.synchronize()
+        seq += a.elapsed_time(b)
+    s_ms = max_over_ranks(seq / steps, world, device=f"cuda:{local}")
     for q in plain:
         flags |= q.stats()["flags"]
         q.close()
@@ -767,8 +784,13 @@ def measure_batched(args, rank, world, local, steps=100):
             "unit": "batch substeps/s", "ms_per_substep": b_ms,
             "vertex_substeps_per_s": nverts * 1000.0 / b_ms,
             "plain": {"value": 1000.0 / p_ms, "ms_per_substep": p_ms,
-                      "timing": "host clock between synchronisations (one scene per instance, own stream)"},
-            "batched_over_plain": p_ms / b_ms, "steps": steps, "flags": flags,
+                      "timing": "host clock between synchronisations (one scene per instance, own stream, "
+                                "all instances stepped before the next substep: their kernels overlap)"},
+            "batched_over_plain": p_ms / b_ms,
+            "plain_sequential": {"value": 1000.0 / s_ms, "ms_per_substep": s_ms,
+                                 "timing": "each instance alone through the plain path, one after another, "
+                                           "device-timed (CUDA events on its stream) and summed"},
+            "batched_over_plain_sequential": s_ms / b_ms, "steps": steps, "flags": flags,
             "fused_variant": {"per_size_class": classes,
                               "note": "one fused launch per size class of the instances, each with the register-cap "
                                       "variant and thread order ys_scene_autotune_classes chose on the batched "

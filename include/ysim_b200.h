@@ -188,14 +188,24 @@ ys_status ys_scene_set_graphs(ys_scene* s, int on);
  * the batched FastGrid instances at 8).  No counterpart in the reference (its Metal pipelines have
  * fixed threadgroup sizes). */
 ys_status ys_scene_set_fused_variant(ys_scene* s, int min_blocks);
-/* Thread order of the fused substep kernel: on (default), its threads take
- * the working vertices (cloth, moving or querying; static obstacles are left
- * out) in Morton order within each mesh, recomputed from the positions at
- * every tree rebuild, so a warp's 32 vertices are a compact patch whose
- * descents and candidate faces overlap; off, thread i takes vertex i.  The
- * results are the same either way.  No counterpart in the reference (one
- * Metal thread per vertex id). */
-ys_status ys_scene_set_thread_order(ys_scene* s, int on);
+/* Thread order of the fused substep kernel, for every size class.  Its
+ * threads take the working vertices (cloth, moving or querying; static
+ * obstacles are left out), mesh after mesh:
+ *   YS_ORDER_MORTON (default): in Morton order within each mesh, recomputed
+ *     from the positions at every tree rebuild, so a warp's 32 vertices are a
+ *     compact patch whose descents and candidate faces overlap;
+ *   YS_ORDER_VERTEX: thread i takes vertex i;
+ *   YS_ORDER_TILE: each CTA takes one 16 x 8 tile of a FastGridCloth (other
+ *     meshes in vertex order, each from a CTA boundary); the tile's positions
+ *     and velocities with a 2-vertex halo come into shared memory by TMA, and
+ *     each stencil spring with an end in the tile is evaluated once for both
+ *     of its ends (890 spring evaluations per tile instead of 1536).
+ * The results are the same, bit for bit, in every order.  No counterpart in
+ * the reference (one Metal thread per vertex id). */
+#define YS_ORDER_VERTEX 0
+#define YS_ORDER_MORTON 1
+#define YS_ORDER_TILE 2
+ys_status ys_scene_set_thread_order(ys_scene* s, int order);
 /* Autotuner: times each variant on the scene's current state (reps launches
  * each; the kernel only writes the next-state buffers and the running totals
  * are restored, so the scene does not advance), keeps the fastest, and
@@ -210,10 +220,10 @@ typedef struct ys_fused_class {
     uint32_t max_mesh_vertices;  /* the class's bound on a mesh's vertex count */
     uint32_t meshes, vertices;   /* working meshes and vertices in the class */
     int32_t ctas_per_sm;         /* chosen variant (8, 7 or 4) */
-    int32_t morton_order;        /* chosen thread order: 1 Morton, 0 vertex */
-    float ms[2][3];              /* mean ms per launch: [vertex, Morton order][8, 7, 4] */
+    int32_t thread_order;        /* chosen thread order: YS_ORDER_VERTEX, _MORTON or _TILE */
+    float ms[3][3];              /* mean ms per launch: [vertex, Morton, tile order][8, 7, 4] */
 } ys_fused_class;
-/* Per-class autotuner: times every variant under both thread orders on each
+/* Per-class autotuner: times every variant under each thread order on each
  * class's launch over the current state (the scene does not advance), keeps
  * the fastest pair per class and reports the classes (out: up to cap
  * records; *nclasses: the number of classes, 4).  No counterpart in the

@@ -76,7 +76,7 @@ def test_per_class_autotune_keeps_results(cuda_lib):
         classes = s.autotune_classes(reps=2)
         assert len(classes) >= 2 and sum(c["vertices"] for c in classes) == sum(m.nV for m in spec.meshes
                                                                                if m.grid_n)
-        assert all(c["ctas_per_sm"] in (8, 7, 4) and c["thread_order"] in ("morton", "vertex") for c in classes)
+        assert all(c["ctas_per_sm"] in (8, 7, 4) and c["thread_order"] in ("morton", "vertex", "tile") for c in classes)
         assert np.array_equal(s.get("x").view(np.uint32), x0.view(np.uint32)) and s.totals() == t0
         s.step(20)
         assert np.array_equal(s.get("x").view(np.uint32), runs[0][0].view(np.uint32))

@@ -47,9 +47,15 @@ COLLIDER_CYLINDER = 3
 COLLIDER_PLANE = 4
 
 
+ORDER_VERTEX = 0
+ORDER_MORTON = 1
+ORDER_TILE = 2
+ORDER_NAMES = ("vertex", "morton", "tile")
+
+
 class FusedClass(C.Structure):
     _fields_ = [("max_mesh_vertices", C.c_uint32), ("meshes", C.c_uint32), ("vertices", C.c_uint32),
-                ("ctas_per_sm", C.c_int32), ("morton_order", C.c_int32), ("ms", (C.c_float * 3) * 2)]
+                ("ctas_per_sm", C.c_int32), ("thread_order", C.c_int32), ("ms", (C.c_float * 3) * 3)]
 
 
 class SimParams(C.Structure):

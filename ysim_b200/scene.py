@@ -127,8 +127,8 @@ class Scene:
                 continue
             res.append({"max_mesh_vertices": int(c.max_mesh_vertices), "meshes": int(c.meshes),
                         "vertices": int(c.vertices), "ctas_per_sm": int(c.ctas_per_sm),
-                        "thread_order": "morton" if c.morton_order else "vertex",
-                        "ms": {"vertex": [float(v) for v in c.ms[0]], "morton": [float(v) for v in c.ms[1]]}})
+                        "thread_order": _lib.ORDER_NAMES[c.thread_order],
+                        "ms": {name: [float(v) for v in c.ms[k]] for k, name in enumerate(_lib.ORDER_NAMES)}})
         return res
 
     def set_collider(self, mesh: int, kind: int, center, half=(0.0, 0.0, 0.0), q=(1.0, 0.0, 0.0, 0.0)):
@@ -151,10 +151,16 @@ class Scene:
     def set_fused_variant(self, min_blocks: int):
         _lib.check(self.lib.ys_scene_set_fused_variant(self.h, min_blocks), "ys_scene_set_fused_variant")
 
-    def set_thread_order(self, on: bool):
+    def set_thread_order(self, order):
         """Fused-kernel threads over the working vertices in per-mesh Morton
-        order (True, default) or in vertex order (False); same results."""
-        _lib.check(self.lib.ys_scene_set_thread_order(self.h, 1 if on else 0), "ys_scene_set_thread_order")
+        order ("morton" or True, default), vertex order ("vertex" or False),
+        or 16 x 8 tiles of each grid cloth with TMA-staged spring tables
+        ("tile"); the results are the same in every order."""
+        if isinstance(order, str):
+            code = _lib.ORDER_NAMES.index(order)
+        else:
+            code = _lib.ORDER_MORTON if order is True else _lib.ORDER_VERTEX if order is False else int(order)
+        _lib.check(self.lib.ys_scene_set_thread_order(self.h, code), "ys_scene_set_thread_order")
 
     def pack(self):
         _lib.check(self.lib.ys_scene_pack(self.h), "ys_scene_pack")
