@@ -495,28 +495,38 @@ def test_equal_code_runs_reference_and_consistent_split(cuda_lib, oracle):
         _lib.check(cuda_lib.ys_shash_destroy(sh))
 
 
-def _teschner(x, y, z, mask):
-    return ((x * 73856093) ^ (y * 19349663) ^ (z * 83492791)) & 0xFFFFFFFF & mask
+def _expand10(v):
+    out = 0
+    for i in range(10):
+        out |= ((v >> i) & 1) << (3 * i)
+    return out
+
+
+def _cell_bucket(x, y, z, mask):
+    """The hash's bucket of cell (x, y, z): the cell's Morton code within its
+    1024^3 block, xor a Teschner hash of the block (ys_shash.cu)."""
+    m = (_expand10(x & 1023) << 2) | (_expand10(y & 1023) << 1) | _expand10(z & 1023)
+    blk = (((x >> 10) * 73856093) ^ ((y >> 10) * 19349663) ^ ((z >> 10) * 83492791)) & 0xFFFFFFFF
+    return (m ^ blk) & mask
 
 
 def test_spatial_hash_bucket_collision_inside_one_triangle(cuda_lib):
-    """Two cells of one triangle that share a hash bucket, both inside one
-    query's range: the pair is reported once (the entry is matched to the cell
-    it was binned for, not to any cell of the bucket)."""
+    """Two cells of one triangle that share a hash bucket, the query probing
+    one of them: the pair is reported once (the triangle's entries in one
+    bucket are seen once, whichever of its cells they were binned for).  The
+    triangle spans 3 x 2 x 2 cells, so the build's table has 32 buckets; cells
+    two apart in x can share one."""
     import torch
     from ysim_b200 import _lib
     max_entries = 1024
-    T = 1
-    while T < 2 * max_entries:
-        T <<= 1
-    mask = T - 1
+    mask = 31  # the build's table: 2 x 12 entries rounded up to a power of two
     found = None
     for x in range(100, 400):
         for y in range(100, 140):
             for z in range(100, 110):
-                h0 = _teschner(x, y, z, mask)
-                if any(_teschner(x + dx, y + dy, z + dz, mask) == h0
-                       for dx in (0, 1) for dy in (0, 1) for dz in (0, 1) if (dx, dy, dz) != (0, 0, 0)):
+                h0 = _cell_bucket(x, y, z, mask)
+                if any(_cell_bucket(x + dx, y + dy, z + dz, mask) == h0
+                       for dx in (0, 1, 2) for dy in (0, 1) for dz in (0, 1) if (dx, dy, dz) != (0, 0, 0)):
                     found = (x, y, z)
                     break
             if found:
@@ -527,7 +537,7 @@ def test_spatial_hash_bucket_collision_inside_one_triangle(cuda_lib):
     c = np.float32(2e-3)
     x0, y0, z0 = found
     lo = np.array([x0, y0, z0], np.float64) * float(c) + 1e-4
-    hi = (np.array([x0, y0, z0], np.float64) + 2) * float(c) - 1e-4
+    hi = (np.array([x0, y0, z0], np.float64) + np.array([3, 2, 2])) * float(c) - 1e-4
     tri = np.array([[lo[0], lo[1], lo[2]], [hi[0], lo[1], hi[2]], [lo[0], hi[1], hi[2]]], np.float32)
     f = np.arange(3, dtype=np.uint32).reshape(1, 3)
     q = ((np.array([[x0, y0, z0]], np.float64) + 1) * float(c)).astype(np.float32)

@@ -5,21 +5,29 @@
 // primitives into grid cells, probe the cells a query overlaps, and keep the
 // candidates that pass an AABB precull.  This is the B200 form for the
 // collision microbenchmark: triangles are binned by their AABB into every
-// cell it overlaps (cell edge = 2h by default), a counting sort groups the
-// entries by hash bucket, and each query point probes the <= 8 cells its box
-// [p - h, p + h] overlaps.  Every entry keeps the ordinal of the cell it was
-// binned for, so a bucket shared by two cells (a hash collision, possibly of
-// two cells of the same triangle) never passes an entry off as another
-// cell's.  A pair (p, t) is emitted only from the cell that is the
-// component-wise max of the two cell ranges' lower corners, so each
-// overlapping pair comes out exactly once, and the candidate set equals the
-// LBVH point query's (queryPoints, bvh.metal:1394-1412) under the same
-// inclusive AABB test.
+// cell it overlaps (cell edge = 2h by default), a radix sort of (bucket,
+// triangle) groups the entries by hash bucket, and each query point probes
+// the <= 8 cells its box [p - h, p + h] overlaps.  A bucket may hold entries
+// of other cells (hash collisions): an entry counts for a probed cell only
+// when the cell lies in its triangle's cell range, and the (stable) sort
+// keeps the entries of one triangle in one bucket side by side, so a
+// triangle with two cells in the bucket is seen once.  A pair (p, t) is
+// emitted only from the cell that is the component-wise max of the two cell
+// ranges' lower corners, so each overlapping pair comes out exactly once,
+// and the candidate set equals the LBVH point query's (queryPoints,
+// bvh.metal:1394-1412) under the same inclusive AABB test.
 //
-// Build: k_sh_bound (tri boxes + cell ranges + entry counts) -> exclusive
-// scan -> k_sh_emit (bucket ids) -> bucket histogram -> scan -> scatter.
-// Triangles spanning more than MAX_CELLS cells go to a short overflow list
-// that every query tests directly.
+// The bucket of a cell is its Morton code within its block of 1024^3 cells
+// (xor a hash of the block), so cells near each other have buckets near each
+// other: queries taken in Morton order of their points read the bucket
+// table, the sorted keys and the triangle list in nearly sequential runs
+// instead of one random sector per probed cell.
+//
+// Build: k_sh_bound (tri boxes, order keys) -> radix sort (the internal
+// order) -> k_sh_order (boxes in that order, entry counts) -> exclusive scan
+// -> k_sh_emit (bucket, internal triangle) -> radix sort -> k_sh_mark (first
+// slot of each bucket).  Triangles spanning more than MAX_CELLS cells go to a short
+// overflow list that every query tests directly.
 #include <algorithm>
 #include <string>
 
@@ -32,71 +40,79 @@
 namespace ys {
 ys_status fail(ys_status code, const std::string& msg);
 
-static constexpr u32 MAX_CELLS = 512;
+static constexpr u32 MAX_CELLS = 4096;  // larger boxes go to the overflow list, tested by every query
 
-__device__ __forceinline__ u32 cell_hash(int x, int y, int z, u32 mask) {
-    // Teschner et al. 2003 spatial-hash primes
-    return (((u32)x * 73856093u) ^ ((u32)y * 19349663u) ^ ((u32)z * 83492791u)) & mask;
+__device__ __forceinline__ u32 cell_bucket(int x, int y, int z, u32 mask) {
+    const u32 m = (expand_bits((u32)x & 1023u) << 2) | (expand_bits((u32)y & 1023u) << 1) | expand_bits((u32)z & 1023u);
+    // the block (floor division by 1024), hashed with Teschner et al. 2003's
+    // spatial-hash primes
+    const u32 blk = ((u32)(x >> 10) * 73856093u) ^ ((u32)(y >> 10) * 19349663u) ^ ((u32)(z >> 10) * 83492791u);
+    return (m ^ blk) & mask;
 }
 
-struct ShTri { float mn[3]; int lo[3]; float mx[3]; int hi[3]; };  // 48 B
+struct ShBox { float4 mn, mx; };  // a triangle's box (w unused): 32 B, one sector
 
+__device__ __forceinline__ void cell_range(const ShBox& r, float inv, int lo[3], int hi[3]) {
+    lo[0] = (int)floorf(r.mn.x * inv); lo[1] = (int)floorf(r.mn.y * inv); lo[2] = (int)floorf(r.mn.z * inv);
+    hi[0] = (int)floorf(r.mx.x * inv); hi[1] = (int)floorf(r.mx.y * inv); hi[2] = (int)floorf(r.mx.z * inv);
+}
+
+// Triangle boxes, and the key that orders the triangles internally: the
+// bucket code of the first cell of each box (unmasked), so that the
+// triangles of one cell and of neighbouring cells sit side by side.
 __global__ void k_sh_bound(const float* __restrict__ x, const u32* __restrict__ F, u32 nF, float inv,
-                           ShTri* __restrict__ tris, u32* __restrict__ counts) {
+                           ShBox* __restrict__ tris, u32* __restrict__ key, u32* __restrict__ idx) {
     u32 t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= nF) return;
     f3 a = ldp(x, F[3 * t]), b = ldp(x, F[3 * t + 1]), c = ldp(x, F[3 * t + 2]);
     f3 lo = vmin(vmin(a, b), c), hi = vmax(vmax(a, b), c);  // leaf box (buildLeaf_Tri)
-    ShTri r;
-    const float l3[3] = {lo.x, lo.y, lo.z}, h3[3] = {hi.x, hi.y, hi.z};
-    unsigned long long cells = 1;
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-        r.mn[k] = l3[k];
-        r.mx[k] = h3[k];
-        r.lo[k] = (int)floorf(l3[k] * inv);
-        r.hi[k] = (int)floorf(h3[k] * inv);
-        cells *= (unsigned long long)(r.hi[k] - r.lo[k] + 1);
-    }
+    ShBox r;
+    r.mn = make_float4(lo.x, lo.y, lo.z, 0.f);
+    r.mx = make_float4(hi.x, hi.y, hi.z, 0.f);
+    int l[3], h[3];
+    cell_range(r, inv, l, h);
     tris[t] = r;
-    counts[t] = cells <= MAX_CELLS ? (u32)cells : 0u;
+    key[t] = cell_bucket(l[0], l[1], l[2], 0xFFFFFFFFu);
+    idx[t] = t;
 }
 
-__global__ void k_sh_emit(const ShTri* __restrict__ tris, const u32* __restrict__ off, u32 nF, u32 mask,
-                          u32* __restrict__ ebucket, u32* __restrict__ etri, unsigned short* __restrict__ eord,
-                          u32* __restrict__ eidx, u32* __restrict__ big, u32* __restrict__ nbig) {
+// Internal triangle i is triangle idx[i] (after the sort by key): its box in
+// internal order and its entry count (0: spans more than MAX_CELLS cells).
+__global__ void k_sh_order(const ShBox* __restrict__ tris, const u32* __restrict__ idx, u32 nF, float inv,
+                           ShBox* __restrict__ sbox, u32* __restrict__ counts) {
+    const u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nF) return;
+    const ShBox r = tris[idx[i]];
+    int l[3], h[3];
+    cell_range(r, inv, l, h);
+    unsigned long long cells = 1;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) cells *= (unsigned long long)(h[k] - l[k] + 1);
+    sbox[i] = r;
+    counts[i] = cells <= MAX_CELLS ? (u32)cells : 0u;
+}
+
+__global__ void k_sh_emit(const ShBox* __restrict__ tris, const u32* __restrict__ off, u32 nF, float inv, u32 mask,
+                          u32* __restrict__ ebucket, u32* __restrict__ etri, u32* __restrict__ big,
+                          u32* __restrict__ nbig) {
     u32 t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= nF) return;
-    const ShTri r = tris[t];
     const u32 base = off[t], end = off[t + 1];
     if (base == end) {  // oversized: tested by every query
         u32 i = atomicAdd(nbig, 1u);
         big[i] = t;
         return;
     }
+    int lo[3], hi[3];
+    cell_range(tris[t], inv, lo, hi);
     u32 k = base;
-    for (int z = r.lo[2]; z <= r.hi[2]; ++z)
-        for (int y = r.lo[1]; y <= r.hi[1]; ++y)
-            for (int xx = r.lo[0]; xx <= r.hi[0]; ++xx) {
-                u32 b = cell_hash(xx, y, z, mask);
-                ebucket[k] = b;
+    for (int z = lo[2]; z <= hi[2]; ++z)
+        for (int y = lo[1]; y <= hi[1]; ++y)
+            for (int xx = lo[0]; xx <= hi[0]; ++xx) {
+                ebucket[k] = cell_bucket(xx, y, z, mask);
                 etri[k] = t;
-                eord[k] = (unsigned short)(k - base);  // < MAX_CELLS
-                eidx[k] = k;
                 ++k;
             }
-}
-
-// After the entries are sorted by bucket (radix sort of (bucket, entry)):
-// the triangle and cell ordinal of each sorted slot.
-__global__ void k_sh_gather(const u32* __restrict__ eidx, const u32* __restrict__ etri,
-                            const unsigned short* __restrict__ eord, u32 nE, u32* __restrict__ sorted,
-                            unsigned short* __restrict__ sord) {
-    const u32 k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= nE) return;
-    const u32 e = eidx[k];
-    sorted[k] = etri[e];
-    sord[k] = eord[e];
 }
 
 // First slot of each bucket's run in the sorted keys (buckets with no entry
@@ -108,18 +124,17 @@ __global__ void k_sh_mark(const u32* __restrict__ skey, u32 nE, u32* __restrict_
     if (k == 0 || skey[k - 1] != b) bstart[b] = k;
 }
 
-__device__ __forceinline__ bool box_hit(f3 qmn, f3 qmx, const ShTri& r) {
-    if (qmx.x < r.mn[0] || qmn.x > r.mx[0]) return false;
-    if (qmx.y < r.mn[1] || qmn.y > r.mx[1]) return false;
-    if (qmx.z < r.mn[2] || qmn.z > r.mx[2]) return false;
+__device__ __forceinline__ bool box_hit(f3 qmn, f3 qmx, const ShBox& r) {
+    if (qmx.x < r.mn.x || qmn.x > r.mx.x) return false;
+    if (qmx.y < r.mn.y || qmn.y > r.mx.y) return false;
+    if (qmx.z < r.mn.z || qmn.z > r.mx.z) return false;
     return true;
 }
 
 __global__ void __launch_bounds__(128) k_sh_query(const float* __restrict__ qx, u32 nQ, float m, float inv, u32 mask,
-                                                  const ShTri* __restrict__ tris, const u32* __restrict__ bstart,
-                                                  const u32* __restrict__ skey, u32 nE,
-                                                  const u32* __restrict__ sorted,
-                                                  const unsigned short* __restrict__ sord, const u32* __restrict__ big,
+                                                  const ShBox* __restrict__ tris, const u32* __restrict__ tid,
+                                                  const u32* __restrict__ bstart, const u32* __restrict__ skey, u32 nE,
+                                                  const u32* __restrict__ sorted, const u32* __restrict__ big,
                                                   const u32* __restrict__ nbig, const u32* __restrict__ order,
                                                   u32* __restrict__ pairs, u64 cap, unsigned long long* count) {
     const u32 k0 = blockIdx.x * blockDim.x + threadIdx.x;
@@ -134,25 +149,33 @@ __global__ void __launch_bounds__(128) k_sh_query(const float* __restrict__ qx, 
         lo[k] = (int)floorf(a3[k] * inv);
         hi[k] = (int)floorf(b3[k] * inv);
     }
+    // the lanes appending together reserve their slots with one atomic
     auto emit = [&](u32 t) {
-        unsigned long long i = atomicAdd(count, 1ull);
-        if (i < cap) { pairs[2 * i] = p; pairs[2 * i + 1] = t; }
+        const unsigned act = __activemask();
+        const u32 lane = threadIdx.x & 31u, leader = (u32)__ffs(act) - 1u;
+        unsigned long long base = 0;
+        if (lane == leader) base = atomicAdd(count, (unsigned long long)__popc(act));
+        base = __shfl_sync(act, base, (int)leader);
+        const unsigned long long i = base + (u32)__popc(act & ((1u << lane) - 1u));
+        if (i < cap) { pairs[2 * i] = p; pairs[2 * i + 1] = tid[t]; }
     };
     for (int z = lo[2]; z <= hi[2]; ++z)
         for (int y = lo[1]; y <= hi[1]; ++y)
             for (int xx = lo[0]; xx <= hi[0]; ++xx) {
-                const u32 b = cell_hash(xx, y, z, mask);
+                const u32 b = cell_bucket(xx, y, z, mask);
+                u32 prev = 0xFFFFFFFFu;
                 for (u32 k = bstart[b]; k < nE && skey[k] == b; ++k) {
                     const u32 t = sorted[k];
-                    const ShTri r = tris[t];
-                    // the entry was binned for this very cell (not for another
-                    // cell hashing to the same bucket)
-                    if (xx < r.lo[0] || xx > r.hi[0] || y < r.lo[1] || y > r.hi[1] || z < r.lo[2] || z > r.hi[2])
-                        continue;
-                    const int nx = r.hi[0] - r.lo[0] + 1, ny = r.hi[1] - r.lo[1] + 1;
-                    if ((int)sord[k] != ((z - r.lo[2]) * ny + (y - r.lo[1])) * nx + (xx - r.lo[0])) continue;
+                    if (t == prev) continue;  // the same triangle, for another of its cells
+                    prev = t;
+                    const ShBox r = tris[t];
+                    int rl[3], rh[3];
+                    cell_range(r, inv, rl, rh);
+                    // this cell is one of the triangle's (not another cell
+                    // hashing to the same bucket)
+                    if (xx < rl[0] || xx > rh[0] || y < rl[1] || y > rh[1] || z < rl[2] || z > rh[2]) continue;
                     // emit from the first common cell only
-                    if (xx != max(lo[0], r.lo[0]) || y != max(lo[1], r.lo[1]) || z != max(lo[2], r.lo[2])) continue;
+                    if (xx != max(lo[0], rl[0]) || y != max(lo[1], rl[1]) || z != max(lo[2], rl[2])) continue;
                     if (box_hit(qmn, qmx, r)) emit(t);
                 }
             }
@@ -173,13 +196,15 @@ struct ys_shash {
     u32 maxTris = 0, maxEntries = 0, nF = 0, mask = 0, nE = 0;
     u32 tableCap = 0;  // buckets allocated (power of two); each build uses 2 nE rounded up, at most this
     float cell = 0.f, inv = 0.f;
-    ShTri* tris = nullptr;
-    // entries: bucket (sorted in place by the build: the key of each sorted
-    // slot), triangle, cell ordinal and entry index (the sort's values)
-    u32 *counts = nullptr, *ebucket = nullptr, *etri = nullptr, *eidx = nullptr, *bstart = nullptr, *sorted = nullptr,
-        *big = nullptr, *nbig = nullptr;
+    // triangle boxes in the caller's order and in the internal order (by the
+    // bucket code of each box's first cell), the key of that order and the
+    // caller's id of each internal triangle
+    ShBox *tris = nullptr, *sbox = nullptr;
+    u32 *tkey = nullptr, *tid = nullptr;
+    // entries: bucket and internal triangle, sorted in place by the build
+    // into the key and the triangle of each sorted slot
+    u32 *counts = nullptr, *ebucket = nullptr, *etri = nullptr, *bstart = nullptr, *big = nullptr, *nbig = nullptr;
     void* sortScratch = nullptr;
-    unsigned short *eord = nullptr, *sord = nullptr;  // cell ordinal of each entry within its triangle's range
     void* scan = nullptr;
     QueryOrder qorder;  // Morton order of large query sets
 };
@@ -205,16 +230,15 @@ ys_status ys_shash_create(ys_shash** out, uint32_t max_tris, uint32_t max_entrie
     h->mask = T - 1;
     h->tableCap = T;
     cudaError_t e = cudaSuccess;
-    if (e == cudaSuccess) e = cudaMalloc((void**)&h->tris, sizeof(ShTri) * (size_t)max_tris);
+    if (e == cudaSuccess) e = cudaMalloc((void**)&h->tris, sizeof(ShBox) * (size_t)max_tris);
+    if (e == cudaSuccess) e = cudaMalloc((void**)&h->sbox, sizeof(ShBox) * (size_t)max_tris);
+    if (e == cudaSuccess) e = cudaMalloc((void**)&h->tkey, 4 * (size_t)max_tris);
+    if (e == cudaSuccess) e = cudaMalloc((void**)&h->tid, 4 * (size_t)max_tris);
     if (e == cudaSuccess) e = cudaMalloc((void**)&h->counts, 4 * ((size_t)max_tris + 1));
     if (e == cudaSuccess) e = cudaMalloc((void**)&h->ebucket, 4 * (size_t)max_entries);
     if (e == cudaSuccess) e = cudaMalloc((void**)&h->etri, 4 * (size_t)max_entries);
-    if (e == cudaSuccess) e = cudaMalloc((void**)&h->sorted, 4 * (size_t)max_entries);
-    if (e == cudaSuccess) e = cudaMalloc((void**)&h->eord, 2 * (size_t)max_entries);
-    if (e == cudaSuccess) e = cudaMalloc((void**)&h->sord, 2 * (size_t)max_entries);
     if (e == cudaSuccess) e = cudaMalloc((void**)&h->bstart, 4 * ((size_t)T + 1));
-    if (e == cudaSuccess) e = cudaMalloc((void**)&h->eidx, 4 * (size_t)max_entries);
-    if (e == cudaSuccess) e = cudaMalloc(&h->sortScratch, sort_scratch_bytes(max_entries));
+    if (e == cudaSuccess) e = cudaMalloc(&h->sortScratch, sort_scratch_bytes(std::max(max_entries, max_tris)));
     if (e == cudaSuccess) e = cudaMalloc((void**)&h->big, 4 * (size_t)max_tris);
     if (e == cudaSuccess) e = cudaMalloc((void**)&h->nbig, 4);
     size_t sb = scan_scratch_bytes(max_tris + 1);
@@ -231,8 +255,9 @@ ys_status ys_shash_destroy(ys_shash* h) {
     if (!h) return YS_OK;
     cudaSetDevice(h->device);
     cudaStreamSynchronize(h->stream);
-    cudaFree(h->tris); cudaFree(h->counts); cudaFree(h->ebucket); cudaFree(h->etri); cudaFree(h->sorted); cudaFree(h->eord); cudaFree(h->sord);
-    cudaFree(h->bstart); cudaFree(h->eidx); cudaFree(h->sortScratch); cudaFree(h->big); cudaFree(h->nbig);
+    cudaFree(h->tris); cudaFree(h->sbox); cudaFree(h->tkey); cudaFree(h->tid);
+    cudaFree(h->counts); cudaFree(h->ebucket); cudaFree(h->etri);
+    cudaFree(h->bstart); cudaFree(h->sortScratch); cudaFree(h->big); cudaFree(h->nbig);
     cudaFree(h->scan);
     query_order_free(h->qorder);
     delete h;
@@ -246,7 +271,11 @@ ys_status ys_shash_build(ys_shash* h, const float* d_x, const uint32_t* d_facets
     h->nF = nF;
     h->cell = cell;
     h->inv = 1.0f / cell;
-    k_sh_bound<<<ceil_div(nF, 256), 256, 0, s>>>(d_x, d_facets, nF, h->inv, h->tris, h->counts);
+    k_sh_bound<<<ceil_div(nF, 256), 256, 0, s>>>(d_x, d_facets, nF, h->inv, h->tris, h->tkey, h->tid);
+    // internal order: neighbouring cells' triangles side by side, so a query's
+    // box reads are local
+    YS_CK3(radix_sort_pairs(h->tkey, h->tid, nF, h->sortScratch, 0, 32, s));
+    k_sh_order<<<ceil_div(nF, 256), 256, 0, s>>>(h->tris, h->tid, nF, h->inv, h->sbox, h->counts);
     YS_CK3(cudaMemsetAsync(h->counts + nF, 0, 4, s));
     YS_CK3(exclusive_scan(h->counts, nF + 1, h->scan, s));
     u32 nE = 0;
@@ -263,15 +292,14 @@ ys_status ys_shash_build(ys_shash* h, const float* d_x, const uint32_t* d_facets
     while ((1u << bits) < T) ++bits;
     YS_CK3(cudaMemsetAsync(h->bstart, 0xFF, 4 * ((size_t)T + 1), s));
     YS_CK3(cudaMemsetAsync(h->nbig, 0, 4, s));
-    k_sh_emit<<<ceil_div(nF, 256), 256, 0, s>>>(h->tris, h->counts, nF, h->mask, h->ebucket, h->etri, h->eord,
-                                                 h->eidx, h->big, h->nbig);
-    // entries grouped by bucket with a radix sort of (bucket, entry) in place
-    // of per-entry atomics on bucket counters: those are random atomics into
-    // a table of up to 2^31 buckets, and two passes of them were most of the
-    // build
+    k_sh_emit<<<ceil_div(nF, 256), 256, 0, s>>>(h->sbox, h->counts, nF, h->inv, h->mask, h->ebucket, h->etri,
+                                                 h->big, h->nbig);
+    // entries grouped by bucket with a stable radix sort of (bucket,
+    // triangle) in place of per-entry atomics on bucket counters (random
+    // atomics into a table of up to 2^31 buckets); the triangle rides along
+    // as the value, so no gather follows
     if (nE) {
-        YS_CK3(radix_sort_pairs(h->ebucket, h->eidx, nE, h->sortScratch, 0, bits, s));
-        k_sh_gather<<<ceil_div(nE, 256), 256, 0, s>>>(h->eidx, h->etri, h->eord, nE, h->sorted, h->sord);
+        YS_CK3(radix_sort_pairs(h->ebucket, h->etri, nE, h->sortScratch, 0, bits, s));
         k_sh_mark<<<ceil_div(nE, 256), 256, 0, s>>>(h->ebucket, nE, h->bstart);
     }
     YS_CK3(cudaGetLastError());
@@ -290,8 +318,8 @@ ys_status ys_shash_query(ys_shash* h, const float* d_qx, uint32_t nQ, float marg
         YS_CK3(query_order(h->qorder, d_qx, nQ, s));
         order = h->qorder.idx;
     }
-    if (nQ) k_sh_query<<<ceil_div(nQ, 128), 128, 0, s>>>(d_qx, nQ, margin, h->inv, h->mask, h->tris, h->bstart,
-                                                          h->ebucket, h->nE, h->sorted, h->sord, h->big, h->nbig,
+    if (nQ) k_sh_query<<<ceil_div(nQ, 128), 128, 0, s>>>(d_qx, nQ, margin, h->inv, h->mask, h->sbox, h->tid, h->bstart,
+                                                          h->ebucket, h->nE, h->etri, h->big, h->nbig,
                                                           order, d_pairs, cap, d_count);
     YS_CK3(cudaGetLastError());
     YS_CK3(cudaStreamSynchronize(s));
