@@ -391,8 +391,9 @@ ys_status ys_lbvh_arrays(ys_lbvh* t, void** nodes, int32_t** parent, uint32_t** 
 typedef struct ys_shff ys_shff;
 ys_status ys_shff_create(ys_shff** out, uint32_t max_faces, int device, void* stream);
 ys_status ys_shff_destroy(ys_shff* h);
-/* Rows (BroadCollision layout, 32 B) into d_rows[0, cap); *d_count receives
- * the number of rows (rows beyond cap are counted, not written). */
+/* Rows (BroadCollision layout, 32 B) into d_rows[0, cap), which must be
+ * 16-byte aligned; *d_count receives the number of rows (rows beyond cap are
+ * counted, not written). */
 ys_status ys_shff_detect(ys_shff* h, const float* d_x, uint32_t num_vertices, const uint32_t* d_state_off,
                          const uint32_t* d_facets, const uint32_t* d_facet_off, uint32_t num_faces,
                          const uint32_t* d_behaviors, const uint32_t* d_shapes, uint32_t num_meshes, float margin,

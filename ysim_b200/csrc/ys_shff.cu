@@ -150,7 +150,7 @@ __global__ void __launch_bounds__(256) k_ff_flags(const u32* __restrict__ keys, 
 // Per entry: its cell (scan + flag - 1), home / phantom counts, the cell's
 // start and parity type; the last valid entry records the counts.
 __global__ void __launch_bounds__(256) k_ff_cells(const u32* __restrict__ keys, const u32* __restrict__ vals,
-                                                  const u32* __restrict__ flag, const u32* __restrict__ scan, u32 n,
+                                                  u32* __restrict__ flag, const u32* __restrict__ scan, u32 n,
                                                   ShffParams* __restrict__ P, u32* __restrict__ cstart,
                                                   u32* __restrict__ nh, u32* __restrict__ np, u32* __restrict__ ctype) {
     const u32 i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -169,6 +169,7 @@ __global__ void __launch_bounds__(256) k_ff_cells(const u32* __restrict__ keys, 
         P->numValid = i + 1;
         P->numCells = c + 1;
     }
+    flag[i] = c;  // from here on: the entry's cell
 }
 
 // Candidate pairs per cell (zero past the last cell, for the scan).
@@ -186,63 +187,81 @@ __global__ void k_ff_total(const u32* __restrict__ pc, const u32* __restrict__ p
     P->numPairs = c ? prefix[c - 1] + pc[c - 1] : 0u;
 }
 
-// Offset (from the cell start) of the k-th entry of kind `ph` in the cell.
-__device__ __forceinline__ u32 kth_in_cell(const u32* __restrict__ vals, u32 start, u32 n, u32 k, u32 ph) {
-    u32 seen = 0;
-    for (u32 i = 0; i < n; ++i) {
-        if ((vals[start + i] & 1u) == ph) {
-            if (seen == k) return i;
-            ++seen;
-        }
-    }
-    return 0;
-}
-
-__global__ void __launch_bounds__(256) k_ff_broad(const u32* __restrict__ vals, const u32* __restrict__ cstart,
-                                                  const u32* __restrict__ nh, const u32* __restrict__ np,
-                                                  const u32* __restrict__ ctype, const u32* __restrict__ prefix,
+// Candidate pairs, one warp per home entry (grid-stride over the cell-sorted
+// entries, so that a crowded cell spreads over many warps): the entry against
+// every later entry of its cell and every earlier phantom entry, the lanes
+// taking the partners in step.  Per cell these are the h (h - 1) / 2 + h p
+// pairs of the reference's unranking (spatialhashing.metal), each once.  The
+// lanes that accept a pair together reserve their 6 rows with one atomic,
+// stage them in shared memory, and the warp writes the run out in 16-byte
+// lane stores (a scattered 32-byte row store per lane kept the load-store
+// queue full).
+static constexpr int FF_WARPS = 4;  // 128-thread blocks
+__global__ void __launch_bounds__(128) k_ff_broad(const u32* __restrict__ vals, const u32* __restrict__ ecell,
+                                                  const u32* __restrict__ cstart, const u32* __restrict__ nh,
+                                                  const u32* __restrict__ np, const u32* __restrict__ ctype,
                                                   const ShffParams* __restrict__ P, const u32* __restrict__ mask,
                                                   const float4* __restrict__ sph, const u32* __restrict__ F,
                                                   const u32* __restrict__ facetOff, const u32* __restrict__ beh,
-                                                  const u32* __restrict__ shape, u32 nM, int self, Row* __restrict__ out,
-                                                  u64 cap, unsigned long long* __restrict__ count) {
-    const u32 numPairs = P->numPairs, numCells = P->numCells;
+                                                  const u32* __restrict__ shape, u32 nM, int self,
+                                                  Row* __restrict__ out, u64 cap,
+                                                  unsigned long long* __restrict__ count) {
+    __shared__ uint4 stage[FF_WARPS][32 * 6 * 2];  // 32 pairs x 6 rows x 32 bytes per warp
+    uint4* st = stage[threadIdx.x >> 5];
+    const u32 numValid = P->numValid;
     const float margin = P->margin;
-    for (u32 p = blockIdx.x * blockDim.x + threadIdx.x; p < numPairs; p += gridDim.x * blockDim.x) {
-        u32 lo = 0, hi = numCells;  // the cell with prefix[c] <= p < prefix[c] + pc[c]
-        while (hi - lo > 1) {
-            const u32 mid = (lo + hi) >> 1;
-            if (prefix[mid] <= p) lo = mid; else hi = mid;
-        }
-        const u32 c = lo, start = cstart[c], h = nh[c], ph = np[c], n = h + ph;
-        const u32 k = p - prefix[c], nhh = (h * (h - 1u)) / 2u;
-        u32 oa, ob;
-        if (k < nhh) {
-            u32 a = 0, cum = 0;
-            while (cum + (h - 1u - a) <= k) { cum += h - 1u - a; ++a; }
-            oa = kth_in_cell(vals, start, n, a, 0u);
-            ob = kth_in_cell(vals, start, n, a + 1u + (k - cum), 0u);
-        } else {
-            const u32 k2 = k - nhh;
-            oa = kth_in_cell(vals, start, n, k2 / ph, 0u);
-            ob = kth_in_cell(vals, start, n, k2 % ph, 1u);
-        }
-        const u32 A = vals[start + oa] >> 1, B = vals[start + ob] >> 1;
-        const u32 oA = face_obj(facetOff, nM, A), oB = face_obj(facetOff, nM, B);
-        if (!self && oA == oB) continue;
-        if (beh[oA] == YS_FLOAT && beh[oB] == YS_FLOAT) continue;
-        if (mask[A] & mask[B] & ((1u << ctype[c]) - 1u)) continue;
-        const float4 sA = sph[A], sB = sph[B];
-        const f3 d = mk(sA.x, sA.y, sA.z) - mk(sB.x, sB.y, sB.z);
-        if (sqrtf(dot(d, d)) > sA.w + sB.w + margin) continue;
-        const unsigned long long base = atomicAdd(count, 6ull);
-        const u32 fA = A - facetOff[oA], fB = B - facetOff[oB];
+    const u32 lane = threadIdx.x & 31u;
+    const u32 warps = (gridDim.x * blockDim.x) >> 5;
+    for (u32 e = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; e < numValid; e += warps) {
+        const u32 va = vals[e];
+        if (va & 1u) continue;  // a phantom entry pairs only with homes, from their side
+        const u32 c = ecell[e];
+        const u32 start = cstart[c], end = start + nh[c] + np[c], cbit = (1u << ctype[c]) - 1u;
+        const u32 A = va >> 1;
+        const u32 oA = face_obj(facetOff, nM, A);
+        const u32 mA = mask[A];
+        const float4 sA = sph[A];
+        for (u32 j0 = start; j0 < end; j0 += 32u) {
+            const u32 j = j0 + lane;
+            bool ok = false;
+            u32 B = 0, oB = 0;
+            if (j < end) {
+                const u32 vb = vals[j];
+                if ((vb & 1u) || j > e) {  // later entries, and earlier phantoms
+                    B = vb >> 1;
+                    oB = face_obj(facetOff, nM, B);
+                    ok = (self || oA != oB) && !(beh[oA] == YS_FLOAT && beh[oB] == YS_FLOAT) && !(mA & mask[B] & cbit);
+                    if (ok) {
+                        const float4 sB = sph[B];
+                        const f3 d = mk(sA.x, sA.y, sA.z) - mk(sB.x, sB.y, sB.z);
+                        ok = !(sqrtf(dot(d, d)) > sA.w + sB.w + margin);
+                    }
+                }
+            }
+            const unsigned acc = __ballot_sync(0xFFFFFFFFu, ok);
+            if (!acc) continue;
+            const u32 cnt = (u32)__popc(acc);
+            unsigned long long wbase = 0;
+            if (lane == 0) wbase = atomicAdd(count, 6ull * cnt);
+            wbase = __shfl_sync(0xFFFFFFFFu, wbase, 0);
+            if (ok) {
+                const u32 r = 6u * (u32)__popc(acc & ((1u << lane) - 1u));  // this pair's first staged row
+                const u32 fA = A - facetOff[oA], fB = B - facetOff[oB];
 #pragma unroll
-        for (int q = 0; q < 6; ++q) {
-            if (base + q >= cap) break;
-            const bool second = q >= 3;
-            const u32 Pf = second ? B : A, oP = second ? oB : oA, oT = second ? oA : oB;
-            out[base + q] = Row{F[3 * Pf + (q % 3)], second ? fA : fB, oP, oT, beh[oP], beh[oT], shape[oP], shape[oT]};
+                for (int q = 0; q < 6; ++q) {
+                    const bool second = q >= 3;
+                    const u32 Pf = second ? B : A, oP = second ? oB : oA, oT = second ? oA : oB;
+                    st[2 * (r + q)] = make_uint4(F[3 * Pf + (q % 3)], second ? fA : fB, oP, oT);
+                    st[2 * (r + q) + 1] = make_uint4(beh[oP], beh[oT], shape[oP], shape[oT]);
+                }
+            }
+            __syncwarp();
+            // the warp's rows [wbase, wbase + 6 cnt), as far as the capacity goes
+            const unsigned long long room = wbase < cap ? cap - wbase : 0ull;
+            const u32 rows = (u32)min((unsigned long long)(6u * cnt), room);
+            uint4* dst = reinterpret_cast<uint4*>(out + wbase);
+            for (u32 i = lane; i < 2u * rows; i += 32u) dst[i] = st[i];
+            __syncwarp();
         }
     }
 }
@@ -318,6 +337,7 @@ ys_status ys_shff_detect(ys_shff* h, const float* d_x, uint32_t num_vertices, co
         num_meshes == 0 || num_vertices == 0 || (cap && !d_rows))
         return fail(YS_ERR_BAD_ARG, "bad argument");
     if (num_faces > h->maxFaces) return fail(YS_ERR_CAPACITY, "more faces than the hash was created for");
+    if (reinterpret_cast<uintptr_t>(d_rows) & 15u) return fail(YS_ERR_BAD_ARG, "rows must be 16-byte aligned");
     cudaStream_t s = h->stream;
     YS_CK4(cudaMemsetAsync(d_count, 0, 8, s));
     if (num_faces == 0) return YS_OK;
@@ -346,8 +366,8 @@ ys_status ys_shff_detect(ys_shff* h, const float* d_x, uint32_t num_vertices, co
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    k_ff_broad<<<sms * 8, 256, 0, s>>>(h->vals, h->cstart, h->nh, h->np, h->ctype, h->scan, h->params, h->mask,
-                                       h->sph, d_facets, d_facet_off, d_behaviors, d_shapes, num_meshes,
+    k_ff_broad<<<sms * 16, 128, 0, s>>>(h->vals, h->flag, h->cstart, h->nh, h->np, h->ctype, h->params, h->mask, h->sph,
+                                       d_facets, d_facet_off, d_behaviors, d_shapes, num_meshes,
                                        enable_self ? 1 : 0, (Row*)d_rows, cap, d_count);
     YS_CK4(cudaGetLastError());
     return YS_OK;
