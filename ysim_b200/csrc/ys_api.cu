@@ -67,6 +67,8 @@ struct ys_lbvh {
     uint2* range = nullptr;
     u32 *big = nullptr, *huge = nullptr, *bcount = nullptr;
     Node *bb16 = nullptr, *bb256 = nullptr;
+    u32* rank = nullptr;      // sorted-leaf position of each face
+    float4* lbox = nullptr;   // leaf boxes in sorted order (face-order pass of the refit)
     u32 nbig = 0, nhuge = 0;
     bool ranged = false;            // the last build recorded ranges (consistent Karras split)
 };
@@ -107,6 +109,8 @@ ys_status ys_lbvh_create(ys_lbvh** out, uint32_t maxPrims, int device, void* str
     if (e == cudaSuccess) e = cudaMalloc((void**)&t->bcount, 8);
     if (e == cudaSuccess) e = cudaMalloc((void**)&t->bb16, ((size_t)maxPrims / 16 + 1) * sizeof(Node));
     if (e == cudaSuccess) e = cudaMalloc((void**)&t->bb256, ((size_t)maxPrims / 256 + 1) * sizeof(Node));
+    if (e == cudaSuccess) e = cudaMalloc((void**)&t->rank, (size_t)maxPrims * 4);
+    if (e == cudaSuccess) e = cudaMalloc((void**)&t->lbox, (size_t)maxPrims * 2 * sizeof(float4));
     // completed before this returns: later launches may go to any stream,
     // including non-blocking ones that do not wait for the legacy stream
     if (e == cudaSuccess) e = cudaMemsetAsync(t->status, 0, 4, 0);
@@ -126,6 +130,7 @@ ys_status ys_lbvh_destroy(ys_lbvh* t) {
     cudaFree(t->nodes); cudaFree(t->parent); cudaFree(t->claimOff); cudaFree(t->claims); cudaFree(t->karrasScratch); cudaFree(t->aggScratch); cudaFree(t->codes); cudaFree(t->idx); cudaFree(t->visits);
     cudaFree(t->box); cudaFree(t->status); cudaFree(t->scratch); cudaFree(t->job);
     cudaFree(t->range); cudaFree(t->big); cudaFree(t->huge); cudaFree(t->bcount); cudaFree(t->bb16); cudaFree(t->bb256);
+    cudaFree(t->rank); cudaFree(t->lbox);
     query_order_free(t->qorder);
     delete t;
     return YS_OK;
@@ -142,7 +147,7 @@ static ys_status run_refit(ys_lbvh* t, const float* x, const float* v, float dt,
         // range, from the leaf pass's block boxes (no climb)
         J.bb16 = t->bb16;
         J.bb256 = t->bb256;
-        launch_refit_bin(J, t->range, t->big, t->nbig, t->huge, t->nhuge, t->stream);
+        launch_refit_bin(J, t->range, t->big, t->nbig, t->huge, t->nhuge, t->rank, t->lbox, t->stream);
         YS_CK2(cudaGetLastError());
         YS_CK2(cudaStreamSynchronize(t->stream));
         return YS_OK;
@@ -198,6 +203,7 @@ ys_status ys_lbvh_build(ys_lbvh* t, const float* x, uint32_t nV, const uint32_t*
         t->nbig = cnt[0];
         t->nhuge = cnt[1];
         t->ranged = true;
+        launch_leaf_rank(t->idx, nF, t->rank, t->stream);
     }
     return run_refit(t, x, nullptr, 0.f, 0);
 }

@@ -756,21 +756,8 @@ cudaError_t launch_range_lists(const RefitJob* jobsDev, u32 numJobs, u32 totalLe
 }
 
 // ---- range refit of a consistent binary tree (the standalone LBVH)
-// Leaf pass: thread i is sorted leaf i (leaf node n - 1 + i, face in .b);
-// its swept or static box goes to the leaf node, the block's 16- and
-// 256-leaf boxes to bb16 / bb256, and internal node i (whose range has leaf
-// i at one end) gets its box here when its range stays in the block.
-__global__ void __launch_bounds__(256) k_refit_bin_leaves(RefitJob J, const uint2* __restrict__ range) {
-    __shared__ float sh_leaf[6][256];
-    __shared__ float sh_g16[6][16];
-    __shared__ float sh_box[8][6];
-    const u32 n = J.n;
-    const u32 i0 = blockIdx.x * 256u, i = i0 + threadIdx.x;
-    const bool has = i < n;
-    const u32 li = has ? i : n - 1;
-    Node* nodes = J.nodes;
-    const u32 f = (u32)__ldcg(&nodes[n - 1 + li].b);
-    f3 lo, hi;
+// The swept or static box of face f (buildLeaf_Tri / buildSweptLeaf_Tri).
+__device__ __forceinline__ void face_box(const RefitJob& J, u32 f, f3& lo, f3& hi) {
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
         const u32 gv = J.voff + J.facets[3 * f + k];
@@ -784,7 +771,54 @@ __global__ void __launch_bounds__(256) k_refit_bin_leaves(RefitJob J, const uint
         }
         if (k == 0) { lo = a; hi = b; } else { lo = vmin(lo, a); hi = vmax(hi, b); }
     }
-    if (has) store_box(&nodes[n - 1 + i], lo, hi);
+}
+
+// Face pass: thread f is face f, so the facet and vertex reads stream in the
+// caller's order; its box goes to its sorted slot rank[f] of lbox (one full
+// 32-byte sector).  In sorted-leaf order these reads were random gathers,
+// several sectors per leaf.
+__global__ void __launch_bounds__(256) k_refit_bin_faces(RefitJob J, const u32* __restrict__ rank,
+                                                         float4* __restrict__ lbox) {
+    const u32 f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= J.n) return;
+    f3 lo, hi;
+    face_box(J, f, lo, hi);
+    const u32 r = rank[f];
+    __stcg(lbox + 2 * (size_t)r, make_float4(lo.x, lo.y, lo.z, __int_as_float(-1)));  // the leaf node's a
+    __stcg(lbox + 2 * (size_t)r + 1, make_float4(hi.x, hi.y, hi.z, __uint_as_float(f)));  // and b (its face)
+}
+
+// Leaf pass: thread i is sorted leaf i (leaf node n - 1 + i, face in .b);
+// its box (from lbox when the face pass ran, else gathered here) goes to the
+// leaf node, the block's 16- and 256-leaf boxes to bb16 / bb256, and
+// internal node i (whose range has leaf i at one end) gets its box here when
+// its range stays in the block.
+__global__ void __launch_bounds__(256) k_refit_bin_leaves(RefitJob J, const uint2* __restrict__ range,
+                                                          const float4* __restrict__ lbox) {
+    __shared__ float sh_leaf[6][256];
+    __shared__ float sh_g16[6][16];
+    __shared__ float sh_box[8][6];
+    const u32 n = J.n;
+    const u32 i0 = blockIdx.x * 256u, i = i0 + threadIdx.x;
+    const bool has = i < n;
+    const u32 li = has ? i : n - 1;
+    Node* nodes = J.nodes;
+    f3 lo, hi;
+    if (lbox) {
+        // the whole leaf node (box, a = -1, b = face) in two 16-byte stores:
+        // no read of the node to merge a partial write
+        const float4 a = __ldcs(lbox + 2 * (size_t)li), b = __ldcs(lbox + 2 * (size_t)li + 1);
+        lo = mk(a.x, a.y, a.z);
+        hi = mk(b.x, b.y, b.z);
+        if (has) {
+            float4* nd = reinterpret_cast<float4*>(&nodes[n - 1 + i]);
+            __stcg(nd, a);
+            __stcg(nd + 1, b);
+        }
+    } else {
+        face_box(J, (u32)__ldcg(&nodes[n - 1 + li].b), lo, hi);
+        if (has) store_box(&nodes[n - 1 + i], lo, hi);
+    }
     const float inf = __int_as_float(0x7F800000);
     float v[6] = {has ? lo.x : inf, has ? lo.y : inf, has ? lo.z : inf,
                   has ? hi.x : -inf, has ? hi.y : -inf, has ? hi.z : -inf};
@@ -868,10 +902,21 @@ __global__ void __launch_bounds__(256) k_refit_bin_ranges(RefitJob J, const uint
     if (threadIdx.x == 0) store_box(&J.nodes[node], lo, hi);
 }
 
+// Sorted-leaf rank of each face: rank[idx[i]] = i.
+__global__ void k_leaf_rank(const u32* __restrict__ idx, u32 n, u32* __restrict__ rank) {
+    const u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) rank[idx[i]] = i;
+}
+
+void launch_leaf_rank(const u32* idx, u32 n, u32* rank, cudaStream_t s) {
+    if (n) k_leaf_rank<<<ceil_div(n, 256), 256, 0, s>>>(idx, n, rank);
+}
+
 void launch_refit_bin(const RefitJob& J, const uint2* range, const u32* big, u32 nbig, const u32* huge, u32 nhuge,
-                      cudaStream_t s) {
+                      const u32* rank, float4* lbox, cudaStream_t s) {
     if (J.n == 0) return;
-    k_refit_bin_leaves<<<ceil_div(J.n, 256), 256, 0, s>>>(J, range);
+    if (rank && lbox) k_refit_bin_faces<<<ceil_div(J.n, 256), 256, 0, s>>>(J, rank, lbox);
+    k_refit_bin_leaves<<<ceil_div(J.n, 256), 256, 0, s>>>(J, range, rank && lbox ? lbox : nullptr);
     const u32 blocks = (nbig + 31) / 32 + nhuge;
     if (blocks) k_refit_bin_ranges<<<blocks, 256, 0, s>>>(J, range, big, nbig, huge, nhuge);
 }

@@ -138,8 +138,13 @@ cudaError_t launch_karras(const u32* codes, const u32* idx, u32 n, Node* nodes, 
 // Range refit of a consistent binary tree built with BinRanges (J: nodes,
 // facets, positions (and velocities when swept), n; bb16 / bb256 with
 // n / 16 + 1 and n / 256 + 1 boxes): leaf pass, then the big and huge nodes.
+// With rank (each face's sorted-leaf position) and lbox (2 float4 per leaf) a
+// face-order pass computes the leaf boxes first, so the leaf pass reads them
+// in order instead of gathering facets and vertices.
 void launch_refit_bin(const RefitJob& J, const uint2* range, const u32* big, u32 nbig, const u32* huge, u32 nhuge,
-                      cudaStream_t s);
+                      const u32* rank, float4* lbox, cudaStream_t s);
+// rank[idx[i]] = i for the sorted face indices of a build.
+void launch_leaf_rank(const u32* idx, u32 n, u32* rank, cudaStream_t s);
 // Apetrei build (agglomerativeBuild_Tri + agglomerativeSwapRoot,
 // bvh.metal:884-1199) of sorted (code, index) pairs: topology, leaf boxes
 // from the current positions and every internal box in one pass, the root

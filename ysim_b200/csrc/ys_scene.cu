@@ -270,11 +270,15 @@ __device__ __forceinline__ f3 vertex_force(const StepArgs& A, const MeshDev& M, 
 // In tile thread order a CTA's 128 threads are one 16 x 8 tile of a
 // FastGridCloth (tile-row-major, 16 vertices per tile row).  Each spring with
 // an end in the tile is evaluated once, as the force on its first end a from
-// its second end b; the force on b is its negation, bit for bit (dx, dv and
-// the unit vector change sign exactly, the length and the scalar factor do
-// not change), so each vertex sums its 12 stencil springs in the reference's
-// order from the tile's table and gets the per-vertex loop's result exactly.
-// 890 evaluations per full tile instead of 1536.
+// its second end b.  Seen from b the force is its negation, bit for bit (dx,
+// dv and the unit vector change sign exactly, the length and the scalar
+// factor do not change), except where both ends compute the same value: a
+// component whose dx is exactly zero (+0 in the unit vector from either end)
+// and a degenerate spring (+0 from both ends).  The table keeps those cases
+// in a flag byte per spring, so each vertex sums its 12 stencil springs in
+// the reference's order from the table and gets the per-vertex loop's result
+// exactly, signed zeros included.  890 evaluations per full tile instead of
+// 1536.
 //
 // Springs of the tile, by family (first end a, second end b = a + (dr, dc)),
 // a's rows and columns relative to the tile origin:
@@ -287,7 +291,9 @@ __device__ __forceinline__ f3 vertex_force(const StepArgs& A, const MeshDev& M, 
 static constexpr int TILE_W = 16, TILE_H = 8;
 static constexpr int HALO_W = TILE_W + 4, HALO_H = TILE_H + 4;  // the stencil reaches 2 vertices out
 static constexpr u32 TILE_BOX_BYTES = HALO_W * HALO_H * 16;      // one float4 buffer's tile
-static constexpr size_t TILE_SMEM = 2 * TILE_BOX_BYTES + 128;    // x and v tiles, 128-byte aligned
+static constexpr u32 TILE_FLAG_BYTES = 896;                      // one flag byte per tile spring
+// x and v tiles, then the spring flags; 128-byte aligned
+static constexpr size_t TILE_SMEM = 2 * TILE_BOX_BYTES + TILE_FLAG_BYTES + 128;
 // first spring of each family in the tile's table
 static constexpr u32 TS_SX = 0, TS_SY = 136, TS_HA = 280, TS_HB = 433, TS_BX = 586, TS_BY = 730;
 static constexpr u32 TILE_SPRINGS = 890;
@@ -335,7 +341,7 @@ __device__ __forceinline__ bool tile_wait(unsigned long long* bar) {
 // the family's values, or per spring from gk / gL at gspr (not NO_SPRINGS).
 template <int FAM>
 __device__ __forceinline__ void tile_family(const StepArgs& A, u32 gspr, u32 n, int r0, int c0, float kf, float restf,
-                                            const float4* xs, const float4* vs, float* sf) {
+                                            const float4* xs, const float4* vs, float* sf, unsigned char* flags) {
     constexpr u32 W = FAM == 4 ? 18u : ((FAM == 1 || FAM == 5) ? 16u : 17u);
     constexpr u32 H = FAM == 5 ? 10u : ((FAM >= 1 && FAM <= 3) ? 9u : 8u);
     constexpr u32 BASE = FAM == 0 ? TS_SX : FAM == 1 ? TS_SY : FAM == 2 ? TS_HA : FAM == 3 ? TS_HB : FAM == 4 ? TS_BX : TS_BY;
@@ -348,6 +354,7 @@ __device__ __forceinline__ void tile_family(const StepArgs& A, u32 gspr, u32 n, 
         const int rr = (int)(i / W), cc = (int)(i % W);
         const int ar = r0 + AR + rr, ac = c0 + AC + cc, br = ar + DR, bc = ac + DC;
         f3 F = mk(0.f, 0.f, 0.f);
+        u32 fl = 0;
         if ((u32)ar < n && (u32)ac < n && (u32)br < n && (u32)bc < n) {
             const int ia = (AR + 2 + rr) * HALO_W + (AC + 2 + cc), ib = ia + DR * HALO_W + DC;
             float k = kf, rest = restf;
@@ -365,9 +372,14 @@ __device__ __forceinline__ void tile_family(const StepArgs& A, u32 gspr, u32 n, 
                 rest = A.gL[gspr + sid];
             }
             const float4 pa = xs[ia], va = vs[ia], pb = xs[ib], vb = vs[ib];
-            F = spring(mk(pa.x, pa.y, pa.z), mk(va.x, va.y, va.z), mk(pb.x, pb.y, pb.z), mk(vb.x, vb.y, vb.z), rest, k,
-                       A.kd);
+            const f3 P0 = mk(pa.x, pa.y, pa.z), P1 = mk(pb.x, pb.y, pb.z);
+            F = spring(P0, mk(va.x, va.y, va.z), P1, mk(vb.x, vb.y, vb.z), rest, k, A.kd);
+            // the cases where b computes the same value as a (see above)
+            const f3 dx = P1 - P0;
+            fl = (dx.x == 0.f ? 1u : 0u) | (dx.y == 0.f ? 2u : 0u) | (dx.z == 0.f ? 4u : 0u) |
+                 (sqrtf(dot(dx, dx)) < 1e-7f ? 7u : 0u);
         }
+        flags[BASE + i] = (unsigned char)fl;
         sf[BASE + i] = F.x;
         sf[TILE_SPRINGS + BASE + i] = F.y;
         sf[2 * TILE_SPRINGS + BASE + i] = F.z;
@@ -376,25 +388,31 @@ __device__ __forceinline__ void tile_family(const StepArgs& A, u32 gspr, u32 n, 
 
 // Every spring of the tile at origin (r0, c0) of grid mesh M.
 __device__ __forceinline__ void tile_springs(const StepArgs& A, const MeshDev& M, int r0, int c0, const float4* xs,
-                                             const float4* vs, float* sf) {
+                                             const float4* vs, float* sf, unsigned char* flags) {
     const u32 n = M.grid_n, gspr = M.gspr;
     const float ks = M.kstretch, kh = M.kshear, kb = M.kbend;
     const float r[6] = {M.rest[0], M.rest[1], M.rest[2], M.rest[3], M.rest[4], M.rest[5]};
-    tile_family<0>(A, gspr, n, r0, c0, ks, r[0], xs, vs, sf);
-    tile_family<1>(A, gspr, n, r0, c0, ks, r[1], xs, vs, sf);
-    tile_family<2>(A, gspr, n, r0, c0, kh, r[2], xs, vs, sf);
-    tile_family<3>(A, gspr, n, r0, c0, kh, r[3], xs, vs, sf);
-    tile_family<4>(A, gspr, n, r0, c0, kb, r[4], xs, vs, sf);
-    tile_family<5>(A, gspr, n, r0, c0, kb, r[5], xs, vs, sf);
+    tile_family<0>(A, gspr, n, r0, c0, ks, r[0], xs, vs, sf, flags);
+    tile_family<1>(A, gspr, n, r0, c0, ks, r[1], xs, vs, sf, flags);
+    tile_family<2>(A, gspr, n, r0, c0, kh, r[2], xs, vs, sf, flags);
+    tile_family<3>(A, gspr, n, r0, c0, kh, r[3], xs, vs, sf, flags);
+    tile_family<4>(A, gspr, n, r0, c0, kb, r[4], xs, vs, sf, flags);
+    tile_family<5>(A, gspr, n, r0, c0, kb, r[5], xs, vs, sf, flags);
 }
 
 // The 12 stencil springs of vertex (row, col) at (ty, tx) in its tile, in
-// grid_stencil's order, from the tile's table: + for the springs whose first
-// end is the vertex, - for the others.
-__device__ __forceinline__ f3 tile_force(f3 force, int N, int row, int col, int ty, int tx, const float* sf) {
+// grid_stencil's order, from the tile's table: the table's force for the
+// springs whose first end is the vertex, its negation for the others (but
+// for the components the flags keep).
+__device__ __forceinline__ f3 tile_force(f3 force, int N, int row, int col, int ty, int tx, const float* sf,
+                                         const unsigned char* flags) {
     auto add = [&](u32 i, bool neg) {
-        const f3 F = mk(sf[i], sf[TILE_SPRINGS + i], sf[2 * TILE_SPRINGS + i]);
-        force = neg ? force - F : force + F;
+        f3 F = mk(sf[i], sf[TILE_SPRINGS + i], sf[2 * TILE_SPRINGS + i]);
+        if (neg) {
+            const u32 fl = flags[i];
+            F = mk((fl & 1u) ? F.x : -F.x, (fl & 2u) ? F.y : -F.y, (fl & 4u) ? F.z : -F.z);
+        }
+        force = force + F;
     };
     const u32 y = (u32)ty, x = (u32)tx;
     if (col > 0) add(TS_SX + y * 17 + x, true);
@@ -763,7 +781,8 @@ __global__ void __launch_bounds__(128, MINB) k_fused(StepArgs A) {
     if (tile) {
         __syncthreads();  // also orders the barrier's initialisation before the waits
         if (!tile_wait(&tile_bar)) st |= ST_ITER_CAP;
-        tile_springs(A, *TM, tr0, tc0, xs, xs + HALO_W * HALO_H, sf);
+        tile_springs(A, *TM, tr0, tc0, xs, xs + HALO_W * HALO_H, sf,
+                     reinterpret_cast<unsigned char*>(xs + 2 * HALO_W * HALO_H));
         __syncthreads();
     }
     if (valid && (mflags & MF_CLOTH)) {
@@ -776,7 +795,8 @@ __global__ void __launch_bounds__(128, MINB) k_fused(StepArgs A) {
         const bool in = tile && Mp == TM;
         const int row = in ? (int)(lid / N) : 0, col = in ? (int)(lid % N) : 0;
         if (in && row >= tr0 && row < tr0 + TILE_H && col >= tc0 && col < tc0 + TILE_W)
-            force = tile_force(base_force(A, g, vel, mass), (int)N, row, col, row - tr0, col - tc0, sf);
+            force = tile_force(base_force(A, g, vel, mass), (int)N, row, col, row - tr0, col - tc0, sf,
+                               reinterpret_cast<const unsigned char*>(xs + 2 * HALO_W * HALO_H));
         else
             force = vertex_force(A, *Mp, g, xc, vel, mass);
         f3 pos = xc;
