@@ -508,7 +508,7 @@ def run_ours(args, rank, world, local):
             "traffic": traffic.get("k_fused"), "algorithmic_bytes": ab["fused"], "avg_launch_ms": fused_ms,
             "refit_kernel": {"achieved": ab["refit"] / (refit_ms / 1000.0) / 1e9, "algorithmic_bytes": ab["refit"],
                              "avg_launch_ms": refit_ms, "traffic": traffic.get("refit"),
-                             "launches_per_substep": "leaf kernel + one per low level + one top-level block"},
+                             "launches_per_substep": "range refit: leaf pass (sorted-leaf order, block boxes) + one pass for the nodes whose range crosses a 256-leaf block and the root"},
             "traffic_source": traffic.get("source")}
     # The kernel is issue- and latency-bound, not bandwidth-bound: the same
     # launch against the SMs' instruction-issue peak (148 SMs x 4 schedulers x
