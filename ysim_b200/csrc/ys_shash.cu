@@ -92,27 +92,52 @@ __global__ void k_sh_order(const ShBox* __restrict__ tris, const u32* __restrict
     counts[i] = cells <= MAX_CELLS ? (u32)cells : 0u;
 }
 
+// Entries of 32 triangles per warp: the warp walks their concatenated
+// entries (contiguous in the output, the counts being scanned), lane by
+// entry, each lane finding its triangle by a search over the lanes' first
+// entries; cell ordinal o of a triangle is cell (x, y, z) with x fastest.
+// A triangle's loop of 1 to MAX_CELLS cells no longer holds its warp.
 __global__ void k_sh_emit(const ShBox* __restrict__ tris, const u32* __restrict__ off, u32 nF, float inv, u32 mask,
                           u32* __restrict__ ebucket, u32* __restrict__ etri, u32* __restrict__ big,
                           u32* __restrict__ nbig) {
-    u32 t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= nF) return;
-    const u32 base = off[t], end = off[t + 1];
-    if (base == end) {  // oversized: tested by every query
-        u32 i = atomicAdd(nbig, 1u);
-        big[i] = t;
-        return;
+    const u32 lane = threadIdx.x & 31u;
+    const u32 t0 = (blockIdx.x * blockDim.x + threadIdx.x) & ~31u;
+    if (t0 >= nF) return;  // whole warps
+    const u32 t = t0 + lane;
+    const u32 tEnd = min(t0 + 32u, nF);
+    const u32 start = off[t0], total = off[tEnd] - start;
+    int lo[3] = {0, 0, 0}, hi[3] = {-1, -1, -1};
+    u32 rel = total;  // this lane's first entry, relative to the warp's
+    if (t < nF) {
+        const u32 base = off[t], end = off[t + 1];
+        rel = base - start;
+        if (base == end) {  // oversized: tested by every query
+            const u32 i = atomicAdd(nbig, 1u);
+            big[i] = t;
+        } else {
+            cell_range(tris[t], inv, lo, hi);
+        }
     }
-    int lo[3], hi[3];
-    cell_range(tris[t], inv, lo, hi);
-    u32 k = base;
-    for (int z = lo[2]; z <= hi[2]; ++z)
-        for (int y = lo[1]; y <= hi[1]; ++y)
-            for (int xx = lo[0]; xx <= hi[0]; ++xx) {
-                ebucket[k] = cell_bucket(xx, y, z, mask);
-                etri[k] = t;
-                ++k;
-            }
+    for (u32 e0 = 0; e0 < total; e0 += 32u) {
+        const u32 e = e0 + lane;
+        // the last lane whose first entry is <= e (first entries are non-decreasing)
+        u32 j = 0;
+#pragma unroll
+        for (u32 step = 16; step >= 1; step >>= 1) {
+            const u32 r = __shfl_sync(0xFFFFFFFFu, rel, (int)(j + step));
+            if (r <= e) j += step;
+        }
+        const u32 rj = __shfl_sync(0xFFFFFFFFu, rel, (int)j);
+        const int lx = __shfl_sync(0xFFFFFFFFu, lo[0], (int)j), ly = __shfl_sync(0xFFFFFFFFu, lo[1], (int)j),
+                  lz = __shfl_sync(0xFFFFFFFFu, lo[2], (int)j);
+        const int hx = __shfl_sync(0xFFFFFFFFu, hi[0], (int)j), hy = __shfl_sync(0xFFFFFFFFu, hi[1], (int)j);
+        if (e < total) {
+            const u32 o = e - rj, nx = (u32)(hx - lx + 1), ny = (u32)(hy - ly + 1);
+            const u32 q = o / nx;
+            ebucket[start + e] = cell_bucket(lx + (int)(o - q * nx), ly + (int)(q % ny), lz + (int)(q / ny), mask);
+            etri[start + e] = t0 + j;
+        }
+    }
 }
 
 // First slot of each bucket's run in the sorted keys (buckets with no entry
