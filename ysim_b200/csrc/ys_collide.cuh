@@ -23,25 +23,53 @@ __device__ __forceinline__ bool overlap(f3 qmn, f3 qmx, float4 n0, float4 n1) {
 
 // Depth-first descent from slot 0 (queryAABB, bvh.metal:1322-1392), calling
 // fn(face) for every leaf whose box overlaps [qmn, qmx].  Returns status bits.
+// Both children of a node are loaded and tested together (two independent
+// loads per step); the walk goes on into an overlapping internal child and
+// pushes the other only when both overlap.  The reference pops every child
+// and tests it after the pop: the same nodes pass the test and the same
+// leaves are reported (once per path, as there), with one dependent load per
+// level instead of one per child and no stack traffic for rejected children.
 template <class Fn>
 __device__ __forceinline__ u32 traverse(const Node* __restrict__ nodes, u32 numNodes, f3 qmn, f3 qmx, Fn&& fn) {
     if (numNodes == 0) return 0;
-    int stack[STACK_DEPTH];
+    const float4* r = reinterpret_cast<const float4*>(nodes);
+    const float4 r0 = __ldg(r), r1 = __ldg(r + 1);
+    if (!overlap(qmn, qmx, r0, r1)) return 0;
+    int a = __float_as_int(r0.w), b = __float_as_int(r1.w);
+    if (a < 0) { fn((u32)b); return 0; }  // a tree of one leaf
+    int stack[2 * STACK_DEPTH];  // pending (a, b) child pairs: STACK_DEPTH subtrees, as the reference's stack
     int sp = 0;
-    stack[sp++] = 0;
     u32 visited = 0, st = 0;
-    while (sp > 0) {
+    while (true) {
         if (++visited > VISIT_CAP) { st |= ST_STACK_OVF; break; }
-        int id = stack[--sp];
-        if (id < 0 || (u32)id >= numNodes) continue;
-        const float4* p = reinterpret_cast<const float4*>(nodes + id);
-        float4 n0 = __ldg(p), n1 = __ldg(p + 1);
-        if (!overlap(qmn, qmx, n0, n1)) continue;
-        int a = __float_as_int(n0.w), b = __float_as_int(n1.w);
-        if (a < 0) { fn((u32)b); continue; }
-        if (sp + 2 > STACK_DEPTH) { st |= ST_STACK_OVF; continue; }
-        stack[sp++] = a;
-        stack[sp++] = b;
+        // children a and b of the current node
+        bool ga = false, gb = false;
+        int aa = -1, ab = -1, ba = -1, bb = -1;
+        if (a >= 0 && (u32)a < numNodes && b >= 0 && (u32)b < numNodes) {
+            const float4* pa = reinterpret_cast<const float4*>(nodes + a);
+            const float4* pb = reinterpret_cast<const float4*>(nodes + b);
+            const float4 a0 = __ldg(pa), a1 = __ldg(pa + 1), b0 = __ldg(pb), b1 = __ldg(pb + 1);
+            if (overlap(qmn, qmx, a0, a1)) {
+                aa = __float_as_int(a0.w); ab = __float_as_int(a1.w);
+                if (aa < 0) fn((u32)ab); else ga = true;
+            }
+            if (overlap(qmn, qmx, b0, b1)) {
+                ba = __float_as_int(b0.w); bb = __float_as_int(b1.w);
+                if (ba < 0) fn((u32)bb); else gb = true;
+            }
+        }
+        if (ga) {
+            if (gb) {
+                if (sp + 2 > 2 * STACK_DEPTH) { st |= ST_STACK_OVF; } else { stack[sp++] = ba; stack[sp++] = bb; }
+            }
+            a = aa; b = ab;
+        } else if (gb) {
+            a = ba; b = bb;
+        } else {
+            if (sp == 0) break;
+            b = stack[--sp];
+            a = stack[--sp];
+        }
     }
     return st;
 }
