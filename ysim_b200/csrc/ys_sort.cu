@@ -141,14 +141,24 @@ __global__ void __launch_bounds__(SORT_THREADS) k_sort_scatter(const u32* __rest
     lofs[tid] = scanTmp[tid] - mine;
     __syncthreads();
 
+    // the thread's keys and values of all rounds, loaded at once (one memory
+    // latency for the tile instead of one per round)
+    u32 kr[SORT_ITEMS], vr[SORT_ITEMS];
+#pragma unroll
+    for (int r = 0; r < SORT_ITEMS; ++r) {
+        const u32 i = tileBase + (u32)r * SORT_THREADS + tid;
+        kr[r] = i < n ? __ldcs(kin + i) : 0u;
+        vr[r] = i < n ? __ldcs(vin + i) : 0u;
+    }
     // stable rank of every key within the tile, into shared memory
+#pragma unroll
     for (int r = 0; r < SORT_ITEMS; ++r) {
         for (int k = tid; k < W * 256; k += SORT_THREADS) (&wcnt[0][0])[k] = 0;
         __syncthreads();
         const u32 i = tileBase + (u32)r * SORT_THREADS + tid;
         const bool valid = i < n;
         u32 key = 0, val = 0, d = 256u + lane;
-        if (valid) { key = kin[i]; val = vin[i]; d = (key >> shift) & 255u; }
+        if (valid) { key = kr[r]; val = vr[r]; d = (key >> shift) & 255u; }
         const u32 peers = __match_any_sync(0xffffffffu, d);
         const u32 lower = __popc(peers & ((1u << lane) - 1u));
         const int leader = __ffs(peers) - 1;
