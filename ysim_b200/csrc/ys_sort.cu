@@ -105,8 +105,8 @@ __global__ void __launch_bounds__(SORT_THREADS) k_sort_scatter(const u32* __rest
     constexpr int W = SORT_THREADS / 32;
     __shared__ u32 base[256];         // global start of each digit for this tile
     __shared__ u32 lofs[256];         // start of each digit within the tile
-    __shared__ u32 running[256];      // keys of each digit already placed by this tile
-    __shared__ u32 wcnt[W][256];      // per-warp digit counts of the current round
+    __shared__ u32 running[2][256];   // keys of each digit already placed by this tile (by round parity)
+    __shared__ unsigned short wcnt[2][W][256];  // per-warp digit counts of a round (<= 32; by round parity)
     __shared__ u32 scanTmp[256];
     __shared__ u32 sk[TILE], sv[TILE];  // the tile, stably ordered by digit
     const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
@@ -128,7 +128,8 @@ __global__ void __launch_bounds__(SORT_THREADS) k_sort_scatter(const u32* __rest
     const u32 before_tiles = hist[(u32)tid * numTiles + blockIdx.x];
     const u32 mine = (blockIdx.x + 1 < numTiles ? hist[(u32)tid * numTiles + blockIdx.x + 1] : t) - before_tiles;
     base[tid] = scanTmp[tid] - t + before_tiles;
-    running[tid] = 0;
+    running[0][tid] = 0;
+    for (int k = tid; k < W * 256; k += SORT_THREADS) (&wcnt[0][0][0])[k] = 0;
     __syncthreads();
     scanTmp[tid] = mine;
     __syncthreads();
@@ -150,11 +151,14 @@ __global__ void __launch_bounds__(SORT_THREADS) k_sort_scatter(const u32* __rest
         kr[r] = i < n ? __ldcs(kin + i) : 0u;
         vr[r] = i < n ? __ldcs(vin + i) : 0u;
     }
-    // stable rank of every key within the tile, into shared memory
+    // stable rank of every key within the tile, into shared memory.  Round r
+    // counts into wcnt[r & 1] and reads running[r & 1]; it clears the other
+    // counts (last read in round r - 1, before its second barrier) and
+    // writes the next running counts, so a round takes two barriers.
 #pragma unroll
     for (int r = 0; r < SORT_ITEMS; ++r) {
-        for (int k = tid; k < W * 256; k += SORT_THREADS) (&wcnt[0][0])[k] = 0;
-        __syncthreads();
+        const int b = r & 1;
+        for (int k = tid; k < W * 256; k += SORT_THREADS) (&wcnt[b ^ 1][0][0])[k] = 0;
         const u32 i = tileBase + (u32)r * SORT_THREADS + tid;
         const bool valid = i < n;
         u32 key = 0, val = 0, d = 256u + lane;
@@ -162,22 +166,21 @@ __global__ void __launch_bounds__(SORT_THREADS) k_sort_scatter(const u32* __rest
         const u32 peers = __match_any_sync(0xffffffffu, d);
         const u32 lower = __popc(peers & ((1u << lane) - 1u));
         const int leader = __ffs(peers) - 1;
-        if (valid && lane == leader) wcnt[w][d] = (u32)__popc(peers);
+        if (valid && lane == leader) wcnt[b][w][d] = (unsigned short)__popc(peers);
         __syncthreads();
         if (valid) {
             u32 before = 0;
-            for (int ww = 0; ww < w; ++ww) before += wcnt[ww][d];
-            const u32 p = lofs[d] + running[d] + before + lower;
+            for (int ww = 0; ww < w; ++ww) before += wcnt[b][ww][d];
+            const u32 p = lofs[d] + running[b][d] + before + lower;
             sk[p] = key;
             sv[p] = val;
         }
-        __syncthreads();
-        // advance running counts by this round's totals
+        // the next round's running counts: this round's totals added
         {
             u32 s = 0;
 #pragma unroll
-            for (int ww = 0; ww < W; ++ww) s += wcnt[ww][tid];
-            running[tid] += s;
+            for (int ww = 0; ww < W; ++ww) s += wcnt[b][ww][tid];
+            running[b ^ 1][tid] = running[b][tid] + s;
         }
         __syncthreads();
     }
