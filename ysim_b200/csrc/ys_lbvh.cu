@@ -902,6 +902,18 @@ __global__ void __launch_bounds__(256) k_refit_bin_ranges(RefitJob J, const uint
     if (threadIdx.x == 0) store_box(&J.nodes[node], lo, hi);
 }
 
+__global__ void k_leaf_vids(const u32* __restrict__ idx, const u32* __restrict__ facets, u32 n,
+                            uint4* __restrict__ lvid) {
+    const u32 i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const u32 f = idx[i];
+    lvid[i] = make_uint4(facets[3 * f], facets[3 * f + 1], facets[3 * f + 2], f);
+}
+
+void launch_leaf_vids(const u32* idx, const u32* facets, u32 n, uint4* lvid, cudaStream_t s) {
+    if (n) k_leaf_vids<<<ceil_div(n, 256), 256, 0, s>>>(idx, facets, n, lvid);
+}
+
 // Sorted-leaf rank of each face: rank[idx[i]] = i.
 __global__ void k_leaf_rank(const u32* __restrict__ idx, u32 n, u32* __restrict__ rank) {
     const u32 i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -949,8 +961,14 @@ __global__ void __launch_bounds__(256) k_refit(const RefitJob* __restrict__ jobs
     const u32 leaf = n - 1 + li;
     // root only: the tree is not built; levels: thread i is face i (its slot
     // comes from leafWf); ranges: thread i is sorted leaf i
-    const u32 f = J.ranges ? J.idx[li] : ((J.rootOnly || J.levels) ? li : (u32)__ldcg(&nodes[leaf].b));
-    const u32 vid[3] = {J.facets[3 * f], J.facets[3 * f + 1], J.facets[3 * f + 2]};
+    u32 f, vid[3];
+    if (J.ranges && J.lvid) {
+        const uint4 q = J.lvid[li];
+        f = q.w; vid[0] = q.x; vid[1] = q.y; vid[2] = q.z;
+    } else {
+        f = J.ranges ? J.idx[li] : ((J.rootOnly || J.levels) ? li : (u32)__ldcg(&nodes[leaf].b));
+        vid[0] = J.facets[3 * f]; vid[1] = J.facets[3 * f + 1]; vid[2] = J.facets[3 * f + 2];
+    }
     f3 lo, hi;
     float ext = 0.f;
     f3 P[3];

@@ -89,6 +89,10 @@ struct RefitJob {
     // range (wrange), from the block boxes.
     u32 ranges;
     const u32* idx;
+    // range mode, optional: per sorted leaf its face's three vertex ids and
+    // the face id (w), written at the build (one coalesced load in place of
+    // the face index and the facet)
+    const uint4* lvid;
     Node* bb16;
     Node* bb256;
     uint2* wrange;          // per wide node: (first, last) sorted leaf under it
@@ -143,6 +147,8 @@ cudaError_t launch_karras(const u32* codes, const u32* idx, u32 n, Node* nodes, 
 // in order instead of gathering facets and vertices.
 void launch_refit_bin(const RefitJob& J, const uint2* range, const u32* big, u32 nbig, const u32* huge, u32 nhuge,
                       const u32* rank, float4* lbox, cudaStream_t s);
+// lvid[i] = (facet of idx[i], idx[i]) for the sorted faces of a build.
+void launch_leaf_vids(const u32* idx, const u32* facets, u32 n, uint4* lvid, cudaStream_t s);
 // rank[idx[i]] = i for the sorted face indices of a build.
 void launch_leaf_rank(const u32* idx, u32 n, u32* rank, cudaStream_t s);
 // Apetrei build (agglomerativeBuild_Tri + agglomerativeSwapRoot,

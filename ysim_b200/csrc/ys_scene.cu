@@ -1248,6 +1248,7 @@ struct ys_scene {
     DBuf<uint4> F4;
     DBuf<u32> F3;  // packed facets (3 per face) for the refit kernel
     DBuf<float4> fpos;  // per face: its three vertex positions (id in w), for the fused kernel's tests
+    DBuf<uint4> lvid;   // per sorted leaf: its face's vertex ids and the face id (range refit)
     DBuf<uint2> own;    // per vertex: its own faces as two 8-face windows (StepArgs::own)
     DBuf<Node> nodes;
     DBuf<i32> parent, claims;        // largest claimant per node; claimant lists (offset node_off)
@@ -1442,6 +1443,7 @@ ys_status build_tree(ys_scene* s, HostMesh& H) {
     launch_morton(s->X[s->cur].p, nullptr, H.voff, s->F3.p + 3 * (size_t)H.foff, n, s->box.p, codes, idx, st,
                   s->tree_layout == YS_TREE_CUBE);
     YS_CK(radix_sort_pairs(codes, idx, n, s->sortScratch.p, 0, 32, st));
+    launch_leaf_vids(idx, s->F3.p + 3 * (size_t)H.foff, n, s->lvid.p + H.foff, st);  // for the range refit
     const bool cube = s->tree_layout == YS_TREE_CUBE;
     const bool agg = s->tree_builder == YS_BUILD_APETREI;
     if (agg)
@@ -1986,7 +1988,7 @@ ys_status ys_scene_destroy(ys_scene* s) {
     for (auto& b : s->V) b.free();
     s->Fbuf.free(); s->mass.free(); s->mask.free(); s->vobj.free(); s->targets.free(); s->spr_off.free();
     s->spr_split.free(); s->spr_nbr.free(); s->vaf_off.free(); s->vaf.free(); s->maxext.free(); s->status.free();
-    s->codes.free(); s->idx.free(); s->visits.free(); s->box.free(); s->spr_rest.free(); s->scratch3.free(); s->gk.free(); s->gL.free(); s->F4.free(); s->F3.free();
+    s->codes.free(); s->idx.free(); s->lvid.free(); s->visits.free(); s->box.free(); s->spr_rest.free(); s->scratch3.free(); s->gk.free(); s->gL.free(); s->F4.free(); s->F3.free();
     s->nodes.free(); s->parent.free(); s->claims.free(); s->claimOff.free(); s->karrasScratch.free(); s->aggScratch.free(); s->rootAcc.free();
     s->rjobs.free(); s->rchunks.free(); s->dmeshes.free(); s->jobs.free(); s->counters.free(); s->sortScratch.free();
     s->w4.free(); s->leafW.free(); s->warrive.free(); s->wideScratch.free();
@@ -2153,7 +2155,7 @@ ys_status ys_scene_pack(ys_scene* s) {
     YS_CK(s->spr_nbr.alloc(std::max<size_t>(spr_nbr.size(), 1))); YS_CK(s->spr_rest.alloc(std::max<size_t>(spr_rest.size(), 1)));
     YS_CK(s->vaf_off.alloc(nV + 1)); YS_CK(s->vaf.alloc(std::max<size_t>(vaf.size(), 1)));
     YS_CK(s->maxext.alloc(s->meshes.size())); YS_CK(s->status.alloc(1)); YS_CK(s->box.alloc(8));
-    YS_CK(s->codes.alloc(std::max(nF, 1u))); YS_CK(s->idx.alloc(std::max(nF, 1u))); YS_CK(s->visits.alloc(std::max(nF, 1u)));
+    YS_CK(s->codes.alloc(std::max(nF, 1u))); YS_CK(s->idx.alloc(std::max(nF, 1u))); YS_CK(s->lvid.alloc(std::max(nF, 1u))); YS_CK(s->visits.alloc(std::max(nF, 1u)));
     YS_CK(s->F4.alloc(std::max(nF, 1u))); YS_CK(s->F3.alloc(3 * (size_t)std::max(nF, 1u)));
     YS_CK(s->fpos.alloc(3 * (size_t)std::max(nF, 1u)));
     YS_CK(s->own.alloc(std::max(nV, 1u)));
@@ -2321,7 +2323,7 @@ ys_status ys_scene_pack(ys_scene* s) {
             J.hacc = s->hacc.p + H.w4_off;
         }
         if (!J.rootOnly) J.fpos = s->fpos.p + 3 * (size_t)H.foff;  // faces the fused kernel tests
-        if (J.w4) { J.wrange = s->wrange.p + H.w4_off; J.idx = s->idx.p + H.foff; }
+        if (J.w4) { J.wrange = s->wrange.p + H.w4_off; J.idx = s->idx.p + H.foff; J.lvid = s->lvid.p + H.foff; }
         s->hjobs.push_back(J);
         // every job's leaves start on a 256-leaf boundary (the range refit's
         // blocks then never hold two jobs)
