@@ -91,3 +91,29 @@ def test_face_face_hash_soup_of_meshes(cuda_lib, oracle):
     assert n_s == n and len(got_s) == n // 3
     full = {tuple(r) for r in canon_rows_full(want).tolist()}
     assert all(tuple(r) in full for r in canon_rows_full(got_s).tolist())
+
+
+def test_face_face_hash_rejects_unaligned_rows(cuda_lib):
+    """The broad kernel writes rows as 16-byte stores, so a row buffer that
+    is not 16-byte aligned is refused before any launch (YS_ERR_BAD_ARG)."""
+    import torch
+    from ysim_b200 import _lib
+    spec = _scenes()["c1"][0]
+    x = np.concatenate([m.x for m in spec.meshes]).astype(np.float32)
+    F = np.concatenate([m.facets for m in spec.meshes]).astype(np.uint32)
+    so = np.concatenate([[0], np.cumsum([m.nV for m in spec.meshes])]).astype(np.uint32)
+    fo = np.concatenate([[0], np.cumsum([m.nF for m in spec.meshes])]).astype(np.uint32)
+    beh = np.array([m.behavior for m in spec.meshes], np.uint32)
+    shape = np.zeros(len(spec.meshes), np.uint32)
+    h = C.c_void_p()
+    _lib.check(cuda_lib.ys_shff_create(C.byref(h), len(F), 0, None))
+    try:
+        dx, dso, dF, dfo = _dev(x, np.float32), _dev(so, np.uint32), _dev(F, np.uint32), _dev(fo, np.uint32)
+        db, ds = _dev(beh, np.uint32), _dev(shape, np.uint32)
+        rows = torch.empty(64 * 8 + 4, dtype=torch.int32, device="cuda")
+        cnt = torch.zeros(1, dtype=torch.int64, device="cuda")
+        r = cuda_lib.ys_shff_detect(h, _p(dx), len(x), _p(dso), _p(dF), _p(dfo), len(F), _p(db), _p(ds), len(beh),
+                                    np.float32(0.015), 1, C.c_void_p(rows.data_ptr() + 4), 64, _p(cnt))
+        assert r == _lib.YS_ERR_BAD_ARG
+    finally:
+        _lib.check(cuda_lib.ys_shff_destroy(h))

@@ -133,3 +133,19 @@ def test_tile_order_signed_zeros(cuda_lib):
         ref = _run(spec, "vertex", steps)
         out = _run(spec, "tile", steps)
         _same(out, ref)
+
+
+def test_thread_order_rejects_unknown_order(cuda_lib):
+    """Only vertex (0), Morton (1) and tile (2) order exist."""
+    from ysim_b200 import _lib
+    from ysim_b200 import generators as G
+    from ysim_b200.scene import Scene
+    s = Scene(G.config_c1(P=16, level=1, height=0.2999))
+    try:
+        assert s.lib.ys_scene_set_thread_order(s.h, 3) == _lib.YS_ERR_BAD_ARG
+        assert s.lib.ys_scene_set_thread_order(s.h, -1) == _lib.YS_ERR_BAD_ARG
+        s.set_thread_order("tile")
+        s.step(2)
+        assert s.stats()["flags"] == 0
+    finally:
+        s.close()

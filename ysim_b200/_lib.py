@@ -14,6 +14,7 @@ LIB_PATH = os.path.join(_HERE, "lib", "libysim_b200.so")
 
 # status codes / flags (ysim_b200.h)
 YS_OK = 0
+YS_ERR_BAD_ARG = -1  # include/ysim_b200.h
 FLAG_NONFINITE = 1
 FLAG_STACK_OVF = 2
 FLAG_PAIR_OVF = 4
