@@ -407,6 +407,8 @@ ys_status ys_shff_stats(ys_shff* h, uint32_t out6[6]);
  * spatial_hash.hpp:880-960, and CpuSpatialHash, spatial_hash.hpp:1547-2016).
  * Its candidate set equals ys_lbvh_query's under the same inclusive AABB test.
  * Device pointers; x packed xyz floats. ------------------------------------ */
+/* max_entries (cell entries of a build) is capped at 2^28 - 2; a build that
+ * needs more fails with YS_ERR_CAPACITY. */
 ys_status ys_shash_create(ys_shash** out, uint32_t max_tris, uint32_t max_entries, int device, void* stream);
 ys_status ys_shash_destroy(ys_shash* h);
 /* Bin every triangle's AABB into the grid cells (edge `cell`) it overlaps. */

@@ -140,13 +140,20 @@ __global__ void k_sh_emit(const ShBox* __restrict__ tris, const u32* __restrict_
     }
 }
 
-// First slot of each bucket's run in the sorted keys (buckets with no entry
-// keep 0xFFFFFFFF); a bucket's run ends where the key changes.
+// Each bucket's run in the sorted keys as one word: first slot << 4 | run
+// length, the length saturating at RUN_LONG (a query then finds the end
+// where the key changes).  Buckets with no entry keep 0xFFFFFFFF; first
+// slots stay below 2^28 - 1 (MAX_ENTRIES).
+static constexpr u32 RUN_LONG = 15;
+static constexpr u32 MAX_ENTRIES = (1u << 28) - 2;
 __global__ void k_sh_mark(const u32* __restrict__ skey, u32 nE, u32* __restrict__ bstart) {
     const u32 k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= nE) return;
     const u32 b = skey[k];
-    if (k == 0 || skey[k - 1] != b) bstart[b] = k;
+    if (k != 0 && skey[k - 1] == b) return;
+    u32 c = 1;
+    while (c < RUN_LONG && k + c < nE && skey[k + c] == b) ++c;
+    bstart[b] = (k << 4) | c;
 }
 
 __device__ __forceinline__ bool box_hit(f3 qmn, f3 qmx, const ShBox& r) {
@@ -188,8 +195,12 @@ __global__ void __launch_bounds__(128) k_sh_query(const float* __restrict__ qx, 
         for (int y = lo[1]; y <= hi[1]; ++y)
             for (int xx = lo[0]; xx <= hi[0]; ++xx) {
                 const u32 b = cell_bucket(xx, y, z, mask);
+                const u32 e = bstart[b];
+                if (e == 0xFFFFFFFFu) continue;  // empty bucket
+                // a short run is read by its length, a long one up to where the key changes
+                const u32 k0 = e >> 4, len = e & 15u;
                 u32 prev = 0xFFFFFFFFu;
-                for (u32 k = bstart[b]; k < nE && skey[k] == b; ++k) {
+                for (u32 k = k0; k < nE && (len < RUN_LONG ? k < k0 + len : skey[k] == b); ++k) {
                     const u32 t = sorted[k];
                     if (t == prev) continue;  // the same triangle, for another of its cells
                     prev = t;
@@ -244,6 +255,7 @@ extern "C" {
 
 ys_status ys_shash_create(ys_shash** out, uint32_t max_tris, uint32_t max_entries, int device, void* stream) {
     if (!out || max_tris == 0 || max_entries == 0) return fail(YS_ERR_BAD_ARG, "bad argument");
+    max_entries = std::min(max_entries, MAX_ENTRIES);  // the bucket words hold first slots below 2^28 - 1
     YS_CK3(cudaSetDevice(device));
     ys_shash* h = new ys_shash();
     h->device = device;
